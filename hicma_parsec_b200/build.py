@@ -1,0 +1,84 @@
+"""Build the in-tree CUDA library ``lib/libhicma_tlr.so`` (sm_100a) and the
+``testing_dpotrf_tlr`` command-line driver.
+
+Usage: ``python -m hicma_parsec_b200.build [--force]`` (also called by
+``__graft_entry__.build()``).  nvcc cross-compiles for sm_100a without a GPU.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIBDIR = os.path.join(HERE, "lib")
+LIB = os.path.join(LIBDIR, "libhicma_tlr.so")
+CLI_SRC = os.path.join(HERE, "cli", "testing_dpotrf_tlr.c")
+CLI = os.path.join(LIBDIR, "testing_dpotrf_tlr")
+SOURCES = ["k_gemm.cu", "k_tile.cu", "k_potrf.cu", "k_qr.cu", "k_svd.cu", "tlr_engine.cu"]
+HEADERS = ["tlr_internal.h"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
+              "-Xptxas", "-v"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _newer(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(d) <= t for d in deps)
+
+
+def _compile(nvcc: str, src: str, force: bool) -> tuple[str, str]:
+    out = os.path.join(OBJ, os.path.basename(src).replace(".cu", ".o"))
+    deps = [src] + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "hicma_tlr.h")]
+    if not force and _newer(out, deps):
+        return out, ""
+    cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-c", src, "-o", out]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+    return out, r.stderr
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(OBJ, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    nvcc = _nvcc()
+    srcs = [os.path.join(CSRC, s) for s in SOURCES]
+    with cf.ThreadPoolExecutor(max_workers=len(srcs)) as ex:
+        results = list(ex.map(lambda s: _compile(nvcc, s, force), srcs))
+    objs = [o for o, _ in results]
+    if verbose:
+        for _, log in results:
+            if log:
+                sys.stderr.write(log)
+    if force or not _newer(LIB, objs):
+        cmd = [nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", LIB, *objs, "-lpthread"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    if os.path.exists(CLI_SRC) and (force or not _newer(CLI, [CLI_SRC, LIB])):
+        cmd = ["gcc", "-O2", "-std=c11", "-ffp-contract=off", "-I", os.path.join(ROOT, "include"),
+               CLI_SRC, "-o", CLI, "-L", LIBDIR, "-lhicma_tlr", f"-Wl,-rpath,$ORIGIN", "-lm"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"CLI build failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

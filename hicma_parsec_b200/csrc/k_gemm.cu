@@ -1,0 +1,235 @@
+// Batched variable-size FP64 GEMM on the FP64 tensor cores (DMMA,
+// mma.sync m8n8k4 f64) for sm_100a.  tcgen05 has no f64 kind, so FP64
+// tensor-core work on Blackwell goes through DMMA.
+//
+// Replaces the CORE_dgemm / cblas_dgemm bodies of the reference task classes
+// (hicma_parsec/HiCMA_dpotrf_L_2flow.jdf:704-708,717-728,745-778) and the
+// products inside HCORE (low-rank SYRK/GEMM, QR/SVD recompression).
+//
+// CTA tile 64 x 64 x 16, 4 warps (2 x 2, 32 x 32 each = 4 x 4 DMMA tiles),
+// operands staged in shared memory by cp.async (2 stages, zero-filled at the
+// edges).  op(A)/op(B) transposes are handled by the load mapping so every
+// global load walks the contiguous dimension.  A batch is a list of tasks
+// whose output tiles are flattened into one grid (prefix sums in tile_off).
+#include "tlr_internal.h"
+
+namespace tlr {
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 16, PAD = 8, NT = 128;
+
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async8(void *smem, const double *gmem, bool pred) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int sz = pred ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+struct Smem {
+    double A[2][BK][BM + PAD];
+    double B[2][BK][BN + PAD];
+};
+
+__device__ __forceinline__ void load_stage(Smem &sm, int s, const GemmTask &t, int i0, int j0,
+                                           int k0) {
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < (BM * BK) / NT; ++q) {
+        const int e = tid + q * NT;
+        int i, kk;
+        if (t.opA == 0) { i = e & (BM - 1); kk = e / BM; }
+        else            { kk = e & (BK - 1); i = e / BK; }
+        const int gi = i0 + i, gk = k0 + kk;
+        const bool p = gi < t.m && gk < t.k;
+        const double *src = t.A;
+        if (p) src += (t.opA == 0) ? ((size_t)gi + (size_t)gk * t.lda) : ((size_t)gk + (size_t)gi * t.lda);
+        cp_async8(&sm.A[s][kk][i], src, p);
+    }
+#pragma unroll
+    for (int q = 0; q < (BN * BK) / NT; ++q) {
+        const int e = tid + q * NT;
+        int j, kk;
+        if (t.opB == 0) { kk = e & (BK - 1); j = e / BK; }
+        else            { j = e & (BN - 1); kk = e / BN; }
+        const int gj = j0 + j, gk = k0 + kk;
+        const bool p = gj < t.n && gk < t.k;
+        const double *src = t.B;
+        if (p) src += (t.opB == 0) ? ((size_t)gk + (size_t)gj * t.ldb) : ((size_t)gj + (size_t)gk * t.ldb);
+        cp_async8(&sm.B[s][kk][j], src, p);
+    }
+    cp_async_commit();
+}
+
+__device__ __forceinline__ void gemm_tile(Smem &sm, const GemmTask &t, int tm, int tn) {
+    const int i0 = tm * BM, j0 = tn * BN;
+    if (t.lower && j0 >= i0 + BM) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, tig = lane & 3;
+    const int wm = warp & 1, wn = warp >> 1;
+
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+
+    const int ktiles = (t.k + BK - 1) / BK;
+    if (ktiles > 0) load_stage(sm, 0, t, i0, j0, 0);
+    for (int kt = 0; kt < ktiles; ++kt) {
+        const int s = kt & 1;
+        if (kt + 1 < ktiles) {
+            load_stage(sm, s ^ 1, t, i0, j0, (kt + 1) * BK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k4 = 0; k4 < BK; k4 += 4) {
+            double a[4], b[4];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi) a[mi] = sm.A[s][k4 + tig][wm * 32 + mi * 8 + g];
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) b[ni] = sm.B[s][k4 + tig][wn * 32 + ni * 8 + g];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni], a[mi], b[ni]);
+        }
+        __syncthreads();
+    }
+
+    const double alpha = t.alpha, beta = t.beta;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+        const int row = i0 + wm * 32 + mi * 8 + g;
+        if (row >= t.m) continue;
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int col = j0 + wn * 32 + ni * 8 + tig * 2 + e;
+                if (col >= t.n) continue;
+                double *c = t.C + (size_t)row + (size_t)col * t.ldc;
+                double v = alpha * acc[mi][ni][e];
+                if (beta != 0.0) v += beta * (*c);
+                *c = v;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(NT) k_gemm_batched(const GemmTask *__restrict__ tasks,
+                                                     const int *__restrict__ tile_off, int ntasks) {
+    __shared__ __align__(16) Smem sm;
+    const int bid = blockIdx.x;
+    int lo = 0, hi = ntasks - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile_off[mid] <= bid) lo = mid; else hi = mid - 1;
+    }
+    const GemmTask t = tasks[lo];
+    const int local = bid - tile_off[lo];
+    gemm_tile(sm, t, local % t.tiles_m, local / t.tiles_m);
+}
+
+__global__ void __launch_bounds__(NT) k_gemm_single(GemmTask t) {
+    __shared__ __align__(16) Smem sm;
+    gemm_tile(sm, t, blockIdx.x, blockIdx.y);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 product path of the mixed-precision policy: operands are read in FP64,
+// rounded to FP32 in shared memory and multiplied with FP32 FMAs (FP32
+// accumulation); the result is scaled and written back in FP64.
+constexpr int FB = 64, FK = 16;
+__global__ void __launch_bounds__(256) k_sgemm_batched(const GemmTask *__restrict__ tasks,
+                                                       const int *__restrict__ tile_off, int ntasks) {
+    __shared__ float As[FK][FB + 4];
+    __shared__ float Bs[FK][FB + 4];
+    const int bid = blockIdx.x;
+    int lo = 0, hi = ntasks - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile_off[mid] <= bid) lo = mid; else hi = mid - 1;
+    }
+    const GemmTask t = tasks[lo];
+    const int local = bid - tile_off[lo];
+    const int i0 = (local % t.tiles_m) * FB, j0 = (local / t.tiles_m) * FB;
+    if (t.lower && j0 >= i0 + FB) return;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    float acc[4][4] = {};
+    for (int k0 = 0; k0 < t.k; k0 += FK) {
+        for (int e = tid; e < FB * FK; e += 256) {
+            int i, kk;
+            if (t.opA == 0) { i = e & (FB - 1); kk = e / FB; } else { kk = e & (FK - 1); i = e / FK; }
+            const int gi = i0 + i, gk = k0 + kk;
+            float v = 0.f;
+            if (gi < t.m && gk < t.k)
+                v = (float)((t.opA == 0) ? t.A[(size_t)gi + (size_t)gk * t.lda] : t.A[(size_t)gk + (size_t)gi * t.lda]);
+            As[kk][i] = v;
+            int j;
+            if (t.opB == 0) { kk = e & (FK - 1); j = e / FK; } else { j = e & (FB - 1); kk = e / FB; }
+            const int gj = j0 + j, gk2 = k0 + kk;
+            float w = 0.f;
+            if (gj < t.n && gk2 < t.k)
+                w = (float)((t.opB == 0) ? t.B[(size_t)gk2 + (size_t)gj * t.ldb] : t.B[(size_t)gj + (size_t)gk2 * t.ldb]);
+            Bs[kk][j] = w;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < FK; ++kk) {
+            float a[4], b[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) { a[q] = As[kk][tx + 16 * q]; b[q] = Bs[kk][ty + 16 * q]; }
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[p][q] = fmaf(a[p], b[q], acc[p][q]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int row = i0 + tx + 16 * p;
+        if (row >= t.m) continue;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int col = j0 + ty + 16 * q;
+            if (col >= t.n) continue;
+            double *c = t.C + (size_t)row + (size_t)col * t.ldc;
+            double v = t.alpha * (double)acc[p][q];
+            if (t.beta != 0.0) v += t.beta * (*c);
+            *c = v;
+        }
+    }
+}
+
+}  // namespace
+
+void launch_gemm_batched(const GemmTask *d_tasks, const int *d_tile_off, int ntasks, int total_tiles,
+                         cudaStream_t st, bool fp32) {
+    if (ntasks <= 0 || total_tiles <= 0) return;
+    if (fp32)
+        k_sgemm_batched<<<total_tiles, 256, 0, st>>>(d_tasks, d_tile_off, ntasks);
+    else
+        k_gemm_batched<<<total_tiles, NT, 0, st>>>(d_tasks, d_tile_off, ntasks);
+}
+
+void launch_gemm_single(const GemmTask &t, cudaStream_t st) {
+    if (t.m <= 0 || t.n <= 0) return;
+    dim3 grid((t.m + BM - 1) / BM, (t.n + BN - 1) / BN);
+    k_gemm_single<<<grid, NT, 0, st>>>(t);
+}
+
+}  // namespace tlr

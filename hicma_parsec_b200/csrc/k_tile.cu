@@ -1,0 +1,156 @@
+// Tile generation (STARS-H covariance kernels), Gaussian sketch matrices,
+// batched copies and small reductions.
+//
+// The covariance kernel restates starsh_ssdata_block_{sqrexp_kernel_2d,
+// sqrexp_kernel_3d,exp_kernel_3d} (kernel pointers chosen at
+// hicma_parsec/testing_dpotrf.c:338,346,354; call shape of
+// hicma_parsec/STARSH_gen.jdf:70-72): A_ij = sigma * k(|x_i - x_j|) with the
+// nugget added where the global row and column indices coincide.  Distances
+// are accumulated with explicitly rounded operations (no FMA contraction) so
+// that they match the CPU restatement bit for bit; exp/sqrt are CUDA's.
+#include "tlr_internal.h"
+
+namespace tlr {
+namespace {
+
+constexpr int COV_ROWS = 256;   // threads per block = rows per block
+constexpr int COV_COLS = 8;     // columns per block
+
+__global__ void __launch_bounds__(COV_ROWS) k_cov_batched(CovParams p, const CovTask *__restrict__ tasks) {
+    const CovTask t = tasks[blockIdx.z];
+    const int r = blockIdx.x * COV_ROWS + threadIdx.x;
+    const int c0 = blockIdx.y * COV_COLS;
+    if (r >= t.nr || c0 >= t.nc) return;
+    const int gr = t.r0 + r;
+    double xr[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) xr[a] = a < p.ndim ? p.pts[(size_t)a * p.N + gr] : 0.0;
+    const double den = __dmul_rn(__dmul_rn(2.0, p.beta), p.beta);
+    const int cend = min(c0 + COV_COLS, t.nc);
+    for (int c = c0; c < cend; ++c) {
+        const int gc = t.c0 + c;
+        double r2 = 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (a < p.ndim) {
+                const double d = __dsub_rn(xr[a], p.pts[(size_t)a * p.N + gc]);
+                r2 = __dadd_rn(r2, __dmul_rn(d, d));
+            }
+        }
+        double v;
+        if (p.kind == HICMA_TLR_KIND_EXP_3D)
+            v = __dmul_rn(p.sigma, exp(-__ddiv_rn(__dsqrt_rn(r2), p.beta)));
+        else
+            v = __dmul_rn(p.sigma, exp(-__ddiv_rn(r2, den)));
+        if (gr == gc) v = __dadd_rn(v, p.noise);
+        t.out[(size_t)r + (size_t)c * t.ld] = v;
+    }
+}
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
+    unsigned long long z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Box-Muller on two counter-based uniforms (u1 in (0,1], u2 in [0,1)).
+__global__ void k_gaussian(double *out, int rows, int cols, int ld, unsigned long long seed) {
+    const long long n = (long long)rows * cols;
+    const unsigned long long base = mix64(seed);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long z1 = mix64(base + 2ull * (unsigned long long)i);
+        const unsigned long long z2 = mix64(base + 2ull * (unsigned long long)i + 1ull);
+        const double u1 = ((double)(z1 >> 11) + 1.0) * 0x1.0p-53;
+        const double u2 = (double)(z2 >> 11) * 0x1.0p-53;
+        const double g = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+        const int r = (int)(i % rows), c = (int)(i / rows);
+        out[(size_t)r + (size_t)c * ld] = g;
+    }
+}
+
+constexpr int CP_COLS = 4;
+__global__ void __launch_bounds__(256) k_copy_batched(const CopyTask *__restrict__ tasks) {
+    const CopyTask t = tasks[blockIdx.y];
+    const int c0 = blockIdx.x * CP_COLS;
+    if (c0 >= t.cols) return;
+    const int cend = min(c0 + CP_COLS, t.cols);
+    for (int c = c0; c < cend; ++c) {
+        const double *s = t.src + (size_t)c * t.lds;
+        double *d = t.dst + (size_t)c * t.ldd;
+        if (t.alpha == 1.0)
+            for (int r = threadIdx.x; r < t.rows; r += blockDim.x) d[r] = s[r];
+        else
+            for (int r = threadIdx.x; r < t.rows; r += blockDim.x) d[r] = t.alpha * s[r];
+    }
+}
+
+__global__ void k_zero_upper(double *A, int n, int lda) {
+    const int c = blockIdx.x;
+    for (int r = threadIdx.x; r < c && r < n; r += blockDim.x) A[(size_t)r + (size_t)c * lda] = 0.0;
+}
+
+__global__ void k_set_identity(double *A, int n, int lda) {
+    const int c = blockIdx.x;
+    for (int r = threadIdx.x; r < n; r += blockDim.x) A[(size_t)r + (size_t)c * lda] = (r == c) ? 1.0 : 0.0;
+}
+
+// Deterministic single-block reduction of 2*log(diag).
+__global__ void __launch_bounds__(1024) k_logdiag_sum(const double *const *tiles, int ntiles, int n,
+                                                      int ld, double *out) {
+    __shared__ double red[1024];
+    double s = 0.0;
+    const long long total = (long long)ntiles * n;
+    for (long long i = threadIdx.x; i < total; i += blockDim.x) {
+        const int t = (int)(i / n), j = (int)(i % n);
+        s += 2.0 * log(tiles[t][(size_t)j + (size_t)j * ld]);
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
+}  // namespace
+
+void launch_cov_batched(const CovParams &p, const CovTask *d_tasks, int ntasks, int max_nr, int max_nc,
+                        cudaStream_t st) {
+    if (ntasks <= 0) return;
+    dim3 grid((max_nr + COV_ROWS - 1) / COV_ROWS, (max_nc + COV_COLS - 1) / COV_COLS, ntasks);
+    k_cov_batched<<<grid, COV_ROWS, 0, st>>>(p, d_tasks);
+}
+
+void launch_gaussian(double *out, int rows, int cols, int ld, unsigned long long seed, cudaStream_t st) {
+    const long long n = (long long)rows * cols;
+    if (n <= 0) return;
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    k_gaussian<<<blocks, 256, 0, st>>>(out, rows, cols, ld, seed);
+}
+
+void launch_copy_batched(const CopyTask *d_tasks, int ntasks, int max_cols, cudaStream_t st) {
+    if (ntasks <= 0 || max_cols <= 0) return;
+    dim3 grid((max_cols + CP_COLS - 1) / CP_COLS, ntasks);
+    k_copy_batched<<<grid, 256, 0, st>>>(d_tasks);
+}
+
+void launch_zero_upper(double *A, int n, int lda, cudaStream_t st) {
+    if (n <= 1) return;
+    k_zero_upper<<<n, 256, 0, st>>>(A, n, lda);
+}
+
+void launch_set_identity(double *A, int n, int lda, cudaStream_t st) {
+    if (n <= 0) return;
+    k_set_identity<<<n, 256, 0, st>>>(A, n, lda);
+}
+
+void launch_logdiag_sum(const double *const *d_tiles, int ntiles, int n, int ld, double *out,
+                        cudaStream_t st) {
+    k_logdiag_sum<<<1, 1024, 0, st>>>(d_tiles, ntiles, n, ld, out);
+}
+
+}  // namespace tlr

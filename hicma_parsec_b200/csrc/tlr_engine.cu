@@ -1,0 +1,1513 @@
+// Host engine of the B200 TLR Cholesky: contexts, descriptors, the
+// device-resident tile store, the per-panel scheduler that replaces PaRSEC's
+// task graph, generation, band auto-tuning, solve and the C ABI.
+//
+// Scheduler.  The reference runs HiCMA_dpotrf_L_2flow.jdf as a distributed
+// DAG.  On one GPU every panel k is executed as a short sequence of batched
+// launches on one stream: POTRF(k) (blocked, DMMA updates) and L_kk^-1, then
+// one batched launch group each for all TRSM(m,k), all SYRK(k,m) and all
+// GEMM(m,n,k) of the panel.  Tasks of one class inside a panel are
+// independent (JDF flows: TRSM(m,k) <- POTRF(k); SYRK/GEMM read column k and
+// write disjoint tiles), so batching them preserves the reference's data
+// flow.  The host reads the rank map once per panel (the sizes of the next
+// panel's tasks depend on the ranks the recompressions produced).
+#include "tlr_internal.h"
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace tlr;
+
+// --------------------------------------------------------------- errors ----
+static thread_local std::string g_err;
+static void set_err(const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+extern "C" const char *hicma_tlr_last_error(void) { return g_err.c_str(); }
+
+#define CUDA_TRY(x)                                                                         \
+    do {                                                                                    \
+        cudaError_t e__ = (x);                                                              \
+        if (e__ != cudaSuccess) {                                                           \
+            set_err("%s:%d %s: %s", __FILE__, __LINE__, #x, cudaGetErrorString(e__));       \
+            return e__ == cudaErrorMemoryAllocation ? HICMA_TLR_ERR_OOM : HICMA_TLR_ERR_CUDA; \
+        }                                                                                   \
+    } while (0)
+#define TRY(x)                         \
+    do {                               \
+        int r__ = (x);                 \
+        if (r__ != 0) return r__;      \
+    } while (0)
+#define ARG_CHECK(cond, msg)                      \
+    do {                                          \
+        if (!(cond)) {                            \
+            set_err("invalid argument: %s", msg); \
+            return HICMA_TLR_ERR_ARG;             \
+        }                                         \
+    } while (0)
+
+// --------------------------------------------------------------- context ---
+struct hicma_tlr_ctx_s {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    char *d_ws = nullptr;
+    size_t ws_bytes = 0, ws_off = 0;
+    char *h_stage = nullptr, *d_stage = nullptr;
+    size_t stage_bytes = 0, stage_off = 0;
+    int *d_flags = nullptr;     // [0] info, [1] overflow count
+    double *d_scal = nullptr;   // device scalars
+    int precision = HICMA_TLR_PREC_FP64;
+    long long launches = 0;
+    std::recursive_mutex mu;
+    std::thread async_thread;
+    int async_ret = 0;
+};
+
+struct hicma_tlr_desc_s {
+    hicma_tlr_ctx *ctx = nullptr;
+    int N = 0, NB = 0, NT = 0, maxrank = 0, band = 1, slot_band = 1, band_alloc = 1;
+    int ndim = 0;
+    double *d_pts = nullptr;
+    double *d_band = nullptr;
+    double *d_lr = nullptr;
+    long long nslots = 0;
+    int *d_rank = nullptr;
+    std::vector<int> h_rank;
+    double *d_linv = nullptr;
+    bool factored = false;
+    double stats[8] = {0};
+    double async_acc = 0;
+    int async_fixed = 0, async_maxrank = 0;
+
+    double *dense(int m, int n) const {
+        return d_band + ((size_t)m * band_alloc + (size_t)(m - n)) * (size_t)NB * NB;
+    }
+    long long slot(int m, int n) const {
+        const long long mm = m - slot_band;
+        return mm * (mm + 1) / 2 + n;
+    }
+    double *U(int m, int n) const { return d_lr + (size_t)slot(m, n) * 2 * (size_t)NB * maxrank; }
+    double *V(int m, int n) const { return U(m, n) + (size_t)NB * maxrank; }
+    double *linv(int k) const { return d_linv + (size_t)k * NB * NB; }
+    bool is_dense(int m, int n) const { return m - n < band; }
+    int rank(int m, int n) const { return h_rank[(size_t)n * NT + m]; }
+};
+
+namespace {
+
+size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+int ctx_sync(hicma_tlr_ctx *c) {
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->stage_off = 0;
+    return 0;
+}
+
+void ws_reset(hicma_tlr_ctx *c) { c->ws_off = 0; }
+template <class T>
+T *ws_alloc(hicma_tlr_ctx *c, size_t n) {
+    const size_t bytes = align_up(n * sizeof(T) + 1);
+    if (c->ws_off + bytes > c->ws_bytes) return nullptr;
+    T *p = (T *)(c->d_ws + c->ws_off);
+    c->ws_off += bytes;
+    return p;
+}
+size_t ws_free(hicma_tlr_ctx *c) { return c->ws_bytes - c->ws_off; }
+
+template <class T>
+T *stage(hicma_tlr_ctx *c, const T *src, size_t n) {
+    const size_t raw = n * sizeof(T);
+    const size_t bytes = align_up(raw + 1);
+    if (bytes > c->stage_bytes) return nullptr;
+    if (c->stage_off + bytes > c->stage_bytes) {
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) return nullptr;
+        c->stage_off = 0;
+    }
+    std::memcpy(c->h_stage + c->stage_off, src, raw);
+    if (cudaMemcpyAsync(c->d_stage + c->stage_off, c->h_stage + c->stage_off, raw,
+                        cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+        return nullptr;
+    T *d = (T *)(c->d_stage + c->stage_off);
+    c->stage_off += bytes;
+    return d;
+}
+
+int check_launch(hicma_tlr_ctx *c) {
+    c->launches++;
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false) {
+    if (v.empty()) return 0;
+    std::vector<int> off(v.size() + 1);
+    off[0] = 0;
+    for (size_t i = 0; i < v.size(); ++i) off[i + 1] = off[i] + gemm_tiles(v[i]);
+    if (off.back() == 0) { v.clear(); return 0; }
+    GemmTask *dt = stage(c, v.data(), v.size());
+    int *doff = stage(c, off.data(), off.size());
+    if (!dt || !doff) { set_err("task staging failed"); return HICMA_TLR_ERR_CUDA; }
+    launch_gemm_batched(dt, doff, (int)v.size(), off.back(), c->stream, fp32);
+    v.clear();
+    return check_launch(c);
+}
+
+int run_copies(hicma_tlr_ctx *c, std::vector<CopyTask> &v) {
+    if (v.empty()) return 0;
+    int maxc = 0;
+    for (auto &t : v) maxc = std::max(maxc, t.cols);
+    CopyTask *dt = stage(c, v.data(), v.size());
+    if (!dt) { set_err("task staging failed"); return HICMA_TLR_ERR_CUDA; }
+    launch_copy_batched(dt, (int)v.size(), maxc, c->stream);
+    v.clear();
+    return check_launch(c);
+}
+
+CopyTask make_copy(const double *src, int lds, double *dst, int ldd, int rows, int cols, double alpha = 1.0) {
+    CopyTask t;
+    t.src = src; t.dst = dst; t.lds = lds; t.ldd = ldd; t.rows = rows; t.cols = cols; t.alpha = alpha;
+    return t;
+}
+
+// ----------------------------------------------------------- tile POTRF ----
+// Blocked right-looking Cholesky of an n x n tile (64-column panels): the
+// diagonal block is factored and inverted in one CTA, the panel below is
+// multiplied by the block inverse, the trailing matrix gets a lower DMMA
+// SYRK.  With Linv, L^-1 is then assembled block row by block row.
+int potrf_tile(hicma_tlr_ctx *c, double *A, int n, int lda, double *Linv, int ldl, int *d_info,
+               int info_base) {
+    const int DBK = 64;
+    cudaStream_t st = c->stream;
+    const size_t mark = c->ws_off;
+    double *dscr = nullptr;
+    if (!Linv) {
+        dscr = ws_alloc<double>(c, DBK * DBK);
+        if (!dscr) { set_err("workspace exhausted (potrf)"); return HICMA_TLR_ERR_OOM; }
+    } else {
+        CUDA_TRY(cudaMemset2DAsync(Linv, (size_t)ldl * sizeof(double), 0, sizeof(double) * n, n, st));
+    }
+    for (int j = 0; j < n; j += DBK) {
+        const int jb = std::min(DBK, n - j);
+        double *Dinv = Linv ? Linv + j + (size_t)j * ldl : dscr;
+        const int ldd = Linv ? ldl : DBK;
+        launch_potrf_diag(A + j + (size_t)j * lda, lda, jb, Dinv, ldd, d_info, info_base + j, st);
+        TRY(check_launch(c));
+        if (j + jb < n) {
+            const int rows = n - j - jb;
+            double *Pn = A + (j + jb) + (size_t)j * lda;
+            launch_gemm_single(make_gemm(0, 1, rows, jb, jb, 1.0, Pn, lda, Dinv, ldd, 0.0, Pn, lda), st);
+            TRY(check_launch(c));
+            launch_gemm_single(make_gemm(0, 1, rows, rows, jb, -1.0, Pn, lda, Pn, lda, 1.0,
+                                         A + (j + jb) + (size_t)(j + jb) * lda, lda, 1),
+                               st);
+            TRY(check_launch(c));
+        }
+    }
+    launch_zero_upper(A, n, lda, st);
+    TRY(check_launch(c));
+    if (Linv && n > DBK) {
+        double *tmp = ws_alloc<double>(c, (size_t)DBK * n);
+        if (!tmp) { set_err("workspace exhausted (trtri)"); return HICMA_TLR_ERR_OOM; }
+        for (int i0 = DBK; i0 < n; i0 += DBK) {
+            const int ib = std::min(DBK, n - i0);
+            launch_gemm_single(make_gemm(0, 0, ib, i0, i0, 1.0, A + i0, lda, Linv, ldl, 0.0, tmp, ib), st);
+            TRY(check_launch(c));
+            launch_gemm_single(make_gemm(0, 0, ib, i0, ib, -1.0, Linv + i0 + (size_t)i0 * ldl, ldl, tmp, ib,
+                                         0.0, Linv + i0, ldl),
+                               st);
+            TRY(check_launch(c));
+        }
+    }
+    c->ws_off = mark;
+    return 0;
+}
+
+// ----------------------------------------------------- recompression -------
+// One low-rank-C GEMM update (HCORE_dgemm_qr_svd{,_b_dense} + ormqr):
+// C = [Cu Au] [Cv -Y]^T, Y = Bu (Bv^T Av) (B low rank) or Y = B Av (B dense).
+struct RecompTask {
+    const double *Cu, *Cv;
+    int rc;
+    const double *Au, *Av;
+    int ra;
+    const double *Bu, *Bv;   // Bv == nullptr: B dense in Bu (NB x NB)
+    int rb;
+    double *outU, *outV;
+    int *rank_dst;
+};
+
+size_t recomp_ws_bytes(int nb, const RecompTask &t) {
+    const int K = t.rc + t.ra;
+    const int pb = qr_panel_width(nb);
+    const size_t npan = (size_t)(K + pb - 1) / pb + 1;
+    size_t b = 0;
+    b += align_up(sizeof(double) * (size_t)nb * K + 1) * 2;        // Us, Vs
+    b += align_up(sizeof(double) * (size_t)K + 1) * 2;             // tau
+    b += align_up(sizeof(double) * npan * pb * pb + 1) * 2;        // T factors
+    b += align_up(sizeof(double) * (size_t)K * K + 1) * 2;         // SU, SV
+    if (K > core_smem_kmax()) b += align_up(sizeof(double) * 2 * (size_t)K * K + 1);
+    if (t.Bv) b += align_up(sizeof(double) * (size_t)t.rb * t.ra + 1);
+    return b + 1024;
+}
+
+int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, double acc, int maxrank,
+                   int fixed_rank, int *d_rank_task_base, bool fp32) {
+    if (tasks.empty()) return 0;
+    cudaStream_t st = c->stream;
+    const size_t mark = c->ws_off;
+    size_t i0 = 0;
+    while (i0 < tasks.size()) {
+        c->ws_off = mark;
+        std::vector<CopyTask> copies;
+        std::vector<GemmTask> g1, g2;
+        std::vector<QRTask> qrs;
+        std::vector<CoreTask> cores;
+        std::vector<QApplyTask> apps;
+        int kmax = 0;
+        size_t i = i0;
+        int *rank_task = d_rank_task_base;
+        for (; i < tasks.size(); ++i) {
+            const RecompTask &t = tasks[i];
+            const size_t need = recomp_ws_bytes(nb, t);
+            if (need > ws_free(c)) {
+                if (i == i0) { set_err("workspace too small for one recompression (K=%d)", t.rc + t.ra); return HICMA_TLR_ERR_OOM; }
+                break;
+            }
+            const int K = t.rc + t.ra;
+            CoreTask ct{};
+            ct.rank_out = t.rank_dst;
+            ct.rank_task = rank_task + (i - i0);
+            ct.K = K;
+            if (K == 0) { cores.push_back(ct); continue; }
+            const int pb = qr_panel_width(nb);
+            const size_t npan = (size_t)(K + pb - 1) / pb + 1;
+            double *Us = ws_alloc<double>(c, (size_t)nb * K);
+            double *Vs = ws_alloc<double>(c, (size_t)nb * K);
+            double *tauU = ws_alloc<double>(c, K), *tauV = ws_alloc<double>(c, K);
+            double *TU = ws_alloc<double>(c, npan * pb * pb), *TV = ws_alloc<double>(c, npan * pb * pb);
+            double *SU = ws_alloc<double>(c, (size_t)K * K), *SV = ws_alloc<double>(c, (size_t)K * K);
+            double *work = K > core_smem_kmax() ? ws_alloc<double>(c, 2 * (size_t)K * K) : nullptr;
+            if (t.rc > 0) {
+                copies.push_back(make_copy(t.Cu, nb, Us, nb, nb, t.rc));
+                copies.push_back(make_copy(t.Cv, nb, Vs, nb, nb, t.rc));
+            }
+            if (t.ra > 0) {
+                copies.push_back(make_copy(t.Au, nb, Us + (size_t)nb * t.rc, nb, nb, t.ra));
+                double *Y = Vs + (size_t)nb * t.rc;
+                if (t.Bv) {
+                    double *P = ws_alloc<double>(c, (size_t)t.rb * t.ra);
+                    g1.push_back(make_gemm(1, 0, t.rb, t.ra, nb, 1.0, t.Bv, nb, t.Av, nb, 0.0, P, t.rb));
+                    g2.push_back(make_gemm(0, 0, nb, t.ra, t.rb, -1.0, t.Bu, nb, P, t.rb, 0.0, Y, nb));
+                } else {
+                    g1.push_back(make_gemm(0, 0, nb, t.ra, nb, -1.0, t.Bu, nb, t.Av, nb, 0.0, Y, nb));
+                }
+            }
+            qrs.push_back(QRTask{Us, tauU, TU, nb, K, nb});
+            qrs.push_back(QRTask{Vs, tauV, TV, nb, K, nb});
+            ct.RU = Us; ct.RV = Vs; ct.ldru = nb; ct.ldrv = nb;
+            ct.SU = SU; ct.SV = SV; ct.work = work;
+            cores.push_back(ct);
+            QApplyTask au{Us, TU, SU, t.outU, ct.rank_task, nb, K, nb, K, nb, maxrank};
+            QApplyTask av{Vs, TV, SV, t.outV, ct.rank_task, nb, K, nb, K, nb, maxrank};
+            apps.push_back(au);
+            apps.push_back(av);
+            kmax = std::max(kmax, K);
+        }
+        TRY(run_copies(c, copies));
+        TRY(run_gemms(c, g1, fp32));
+        TRY(run_gemms(c, g2, fp32));
+        if (!qrs.empty()) {
+            QRTask *dq = stage(c, qrs.data(), qrs.size());
+            if (!dq) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+            launch_qr_batched(dq, (int)qrs.size(), nb, st);
+            TRY(check_launch(c));
+        }
+        CoreParams cp{0, acc, maxrank, fixed_rank, nb, c->d_flags + 1};
+        CoreTask *dc = stage(c, cores.data(), cores.size());
+        if (!dc) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+        launch_core_svd_batched(dc, (int)cores.size(), std::max(kmax, 1), cp, st);
+        TRY(check_launch(c));
+        if (!apps.empty()) {
+            QApplyTask *da = stage(c, apps.data(), apps.size());
+            if (!da) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+            launch_qapply_batched(da, (int)apps.size(), nb, st);
+            TRY(check_launch(c));
+        }
+        i0 = i;
+    }
+    c->ws_off = mark;
+    return 0;
+}
+
+// --------------------------------------------------------- op_counts -------
+// hicma_parsec/op_counts.h:10-72 restated with its unsigned arithmetic and
+// float32 casts.
+unsigned long op_counts(char op, unsigned long a, unsigned long b, unsigned long cc, unsigned long d) {
+    unsigned long res = 0;
+    if (op == 'q') {
+        const unsigned long m = a, n = b;
+        res = 2 * m * n * n - (unsigned long)((float)(2 * n * n * n) / 3.0f) + 2 * m * n +
+              (unsigned long)((float)(17 * n) / 3.0f);
+    } else if (op == 'c') {
+        const unsigned long n = a;
+        res = (unsigned long)((double)(n * n * n / 3) - (double)(n * n) / 2.0 + (double)(n / 6));
+    } else if (op == 't') {
+        const unsigned long m = a, n = b;
+        res = (cc == 1) ? n * m * m : m * n * n;
+    } else if (op == 'm') {
+        res = a * b * cc * 2;
+    } else if (op == 's') {
+        res = 22 * a * a * a;
+    } else if (op == 'o') {
+        const unsigned long m = a, n = b, k = cc;
+        if (d == 1) res = 4 * n * m * k - 2 * n * k * k + 3 * n * k;
+        else res = 4 * n * m * k - 2 * m * k * k + 2 * m * k + n * k - k * k / 2 + k / 2;
+    } else if (op == 'r') {
+        const unsigned long m = a, n = b;
+        res = (cc == 1) ? m * m * n : m * n * n;
+    }
+    return res;
+}
+
+unsigned long gemm_lr_ops(unsigned long nb, unsigned long ra, unsigned long rb, unsigned long rc_old,
+                          unsigned long rc_new, bool b_dense) {
+    const unsigned long ka = rc_old + ra;
+    const unsigned long qra = op_counts('q', nb, ka, 0, 0);
+    unsigned long qrb;
+    if (b_dense) qrb = op_counts('q', nb, ka, 0, 0) + op_counts('m', ra, nb, nb, 0);
+    else qrb = op_counts('m', ra, rb, nb, 0) + op_counts('m', ra, nb, rb, 0) + op_counts('q', nb, ka, 0, 0);
+    unsigned long svd = op_counts('r', ka, ka, 2, 0) + op_counts('s', ka, 0, 0, 0) + ka * rc_new;
+    const unsigned long newu = op_counts('o', nb, rc_new, ka, 1);
+    const unsigned long newv = op_counts('o', rc_new, nb, ka, 2);
+    return qra + qrb + svd + newu + newv;
+}
+
+// ---------------------------------------------------------------- points ---
+uint64_t mix64h(uint64_t x) {
+    uint64_t z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+int kind_ndim(int kind) {
+    switch (kind) {
+        case HICMA_TLR_KIND_SQEXP_2D: return 2;
+        case HICMA_TLR_KIND_SQEXP_3D: return 3;
+        case HICMA_TLR_KIND_EXP_3D: return 3;
+        default: return 0;
+    }
+}
+
+int grid_side(long long n, int ndim) {
+    long long s = std::max(1LL, (long long)llround(std::pow((double)n, 1.0 / ndim)));
+    auto pw = [&](long long x) { long long r = 1; for (int i = 0; i < ndim; ++i) r *= x; return r; };
+    while (pw(s) < n) ++s;
+    while (s > 1 && pw(s - 1) >= n) --s;
+    return (int)s;
+}
+
+}  // namespace
+
+// ======================================================================
+//                                C ABI
+// ======================================================================
+extern "C" {
+
+int hicma_tlr_points(const hicma_tlr_problem *prob, int N, double *points) {
+    ARG_CHECK(prob && points && N > 0, "hicma_tlr_points");
+    const int ndim = kind_ndim(prob->kind);
+    ARG_CHECK(ndim > 0, "unsupported problem kind");
+    const int side = grid_side(N, ndim);
+    long long total = 1;
+    for (int a = 0; a < ndim; ++a) total *= side;
+    std::vector<double> c((size_t)total * ndim);
+    std::vector<uint64_t> code((size_t)total, 0);
+    const uint64_t base = mix64h((uint64_t)prob->seed);
+    for (long long idx = 0; idx < total; ++idx) {
+        long long div = 1;
+        for (int a = 0; a < ndim; ++a) {
+            const long long cc = (idx / div) % side;
+            div *= side;
+            const uint64_t z = mix64h(base + (uint64_t)(idx * ndim + a));
+            const double u = (double)(z >> 11) * 0x1.0p-53;
+            const double x = (((double)cc + 0.1) + 0.8 * u) / (double)side;
+            c[(size_t)idx * ndim + a] = x;
+            long long q = (long long)std::floor(x * 2097152.0);
+            if (q < 0) q = 0;
+            if (q > 2097151) q = 2097151;
+            for (int b = 0; b < 21; ++b)
+                code[(size_t)idx] |= (((uint64_t)q >> b) & 1ull) << (b * ndim + a);
+        }
+    }
+    std::vector<long long> order((size_t)total);
+    for (long long i = 0; i < total; ++i) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](long long x, long long y) { return code[(size_t)x] < code[(size_t)y]; });
+    for (int i = 0; i < N; ++i)
+        for (int a = 0; a < ndim; ++a) points[(size_t)a * N + i] = c[(size_t)order[i] * ndim + a];
+    return 0;
+}
+
+int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
+    ARG_CHECK(out, "ctx pointer");
+    *out = nullptr;
+    CUDA_TRY(cudaSetDevice(device));
+    auto *c = new hicma_tlr_ctx_s();
+    c->device = device;
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    size_t free_b = 0, total_b = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    if (workspace_bytes == 0) {
+        workspace_bytes = std::min<size_t>(free_b / 8, (size_t)8 << 30);
+        workspace_bytes = std::max<size_t>(workspace_bytes, (size_t)256 << 20);
+    }
+    c->ws_bytes = workspace_bytes;
+    if (cudaMalloc(&c->d_ws, c->ws_bytes) != cudaSuccess) {
+        set_err("cudaMalloc workspace of %zu bytes failed", c->ws_bytes);
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return HICMA_TLR_ERR_OOM;
+    }
+    c->stage_bytes = (size_t)64 << 20;
+    CUDA_TRY(cudaMallocHost(&c->h_stage, c->stage_bytes));
+    CUDA_TRY(cudaMalloc(&c->d_stage, c->stage_bytes));
+    CUDA_TRY(cudaMalloc(&c->d_flags, 64 * sizeof(int)));
+    CUDA_TRY(cudaMalloc(&c->d_scal, 64 * sizeof(double)));
+    CUDA_TRY(cudaMemset(c->d_flags, 0, 64 * sizeof(int)));
+    *out = c;
+    return 0;
+}
+
+int hicma_tlr_fini(hicma_tlr_ctx *c) {
+    if (!c) return 0;
+    if (c->async_thread.joinable()) c->async_thread.join();
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_ws);
+    cudaFree(c->d_stage);
+    cudaFreeHost(c->h_stage);
+    cudaFree(c->d_flags);
+    cudaFree(c->d_scal);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return 0;
+}
+
+void *hicma_tlr_stream(hicma_tlr_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+int hicma_tlr_set_precision(hicma_tlr_ctx *c, int precision) {
+    ARG_CHECK(c && (precision == HICMA_TLR_PREC_FP64 || precision == HICMA_TLR_PREC_MIXED), "precision");
+    c->precision = precision;
+    return 0;
+}
+
+int hicma_tlr_desc_create(hicma_tlr_ctx *c, int N, int NB, int maxrank, int band_size, hicma_tlr_desc **out) {
+    ARG_CHECK(c && out, "null");
+    ARG_CHECK(N > 0 && NB > 0, "N, NB must be positive");
+    if (N % NB != 0) {
+        set_err("N (%d) must be a multiple of NB (%d): ragged last tiles are not supported", N, NB);
+        return HICMA_TLR_ERR_NOT_SUPPORTED;
+    }
+    ARG_CHECK(maxrank >= 1 && maxrank <= NB, "maxrank in [1, NB]");
+    ARG_CHECK(band_size >= 1, "band_size >= 1");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    CUDA_TRY(cudaSetDevice(c->device));
+    auto *A = new hicma_tlr_desc_s();
+    A->ctx = c;
+    A->N = N; A->NB = NB; A->NT = N / NB; A->maxrank = maxrank;
+    A->band = std::min(band_size, A->NT);
+    A->slot_band = A->band;
+    A->band_alloc = A->band;
+    const int NT = A->NT;
+    const long long mm = NT - A->slot_band;
+    A->nslots = mm > 0 ? mm * (mm + 1) / 2 : 0;
+    const size_t band_bytes = (size_t)NT * A->band_alloc * NB * (size_t)NB * sizeof(double);
+    const size_t lr_bytes = (size_t)A->nslots * 2 * (size_t)NB * maxrank * sizeof(double);
+    if (cudaMalloc(&A->d_band, band_bytes) != cudaSuccess ||
+        (lr_bytes && cudaMalloc(&A->d_lr, lr_bytes) != cudaSuccess) ||
+        cudaMalloc(&A->d_rank, (size_t)NT * NT * sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        set_err("descriptor allocation failed (band %zu B, low-rank slots %zu B)", band_bytes, lr_bytes);
+        cudaFree(A->d_band); cudaFree(A->d_lr); cudaFree(A->d_rank);
+        delete A;
+        return HICMA_TLR_ERR_OOM;
+    }
+    A->h_rank.assign((size_t)NT * NT, -1);
+    for (int m = 0; m < NT; ++m)
+        for (int n = 0; n <= m - A->band; ++n) A->h_rank[(size_t)n * NT + m] = 0;
+    CUDA_TRY(cudaMemcpy(A->d_rank, A->h_rank.data(), (size_t)NT * NT * sizeof(int), cudaMemcpyHostToDevice));
+    *out = A;
+    return 0;
+}
+
+int hicma_tlr_desc_destroy(hicma_tlr_desc *A) {
+    if (!A) return 0;
+    cudaSetDevice(A->ctx->device);
+    cudaStreamSynchronize(A->ctx->stream);
+    cudaFree(A->d_pts);
+    cudaFree(A->d_band);
+    cudaFree(A->d_lr);
+    cudaFree(A->d_rank);
+    cudaFree(A->d_linv);
+    delete A;
+    return 0;
+}
+
+int hicma_tlr_desc_info(const hicma_tlr_desc *A, int *N, int *NB, int *NT, int *maxrank, int *band_size) {
+    ARG_CHECK(A, "null desc");
+    if (N) *N = A->N;
+    if (NB) *NB = A->NB;
+    if (NT) *NT = A->NT;
+    if (maxrank) *maxrank = A->maxrank;
+    if (band_size) *band_size = A->band;
+    return 0;
+}
+
+int hicma_tlr_desc_copy(hicma_tlr_ctx *c, const hicma_tlr_desc *src, hicma_tlr_desc *dst) {
+    ARG_CHECK(c && src && dst, "null");
+    ARG_CHECK(src->N == dst->N && src->NB == dst->NB && src->maxrank == dst->maxrank &&
+                  src->band_alloc == dst->band_alloc && src->slot_band == dst->slot_band,
+              "descriptor shapes differ");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    const size_t NB = src->NB, NT = src->NT;
+    CUDA_TRY(cudaMemcpyAsync(dst->d_band, src->d_band, NT * src->band_alloc * NB * NB * sizeof(double),
+                             cudaMemcpyDeviceToDevice, c->stream));
+    if (src->nslots)
+        CUDA_TRY(cudaMemcpyAsync(dst->d_lr, src->d_lr, (size_t)src->nslots * 2 * NB * src->maxrank * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(dst->d_rank, src->d_rank, NT * NT * sizeof(int), cudaMemcpyDeviceToDevice, c->stream));
+    dst->h_rank = src->h_rank;
+    dst->band = src->band;
+    dst->factored = src->factored;
+    if (src->d_pts) {
+        if (!dst->d_pts || dst->ndim != src->ndim) {
+            cudaFree(dst->d_pts);
+            CUDA_TRY(cudaMalloc(&dst->d_pts, (size_t)src->ndim * src->N * sizeof(double)));
+        }
+        dst->ndim = src->ndim;
+        CUDA_TRY(cudaMemcpyAsync(dst->d_pts, src->d_pts, (size_t)src->ndim * src->N * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, c->stream));
+    }
+    if (src->factored && src->d_linv) {
+        if (!dst->d_linv) CUDA_TRY(cudaMalloc(&dst->d_linv, NT * NB * NB * sizeof(double)));
+        CUDA_TRY(cudaMemcpyAsync(dst->d_linv, src->d_linv, NT * NB * NB * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, c->stream));
+    }
+    return ctx_sync(c);
+}
+
+static int set_points(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_problem *prob, const double *points) {
+    const int ndim = kind_ndim(prob->kind);
+    ARG_CHECK(ndim > 0, "unsupported problem kind (-D 2, 3 or 4)");
+    std::vector<double> h;
+    if (!points) {
+        h.resize((size_t)ndim * A->N);
+        TRY(hicma_tlr_points(prob, A->N, h.data()));
+        points = h.data();
+    }
+    if (!A->d_pts || A->ndim != ndim) {
+        cudaFree(A->d_pts);
+        A->d_pts = nullptr;
+        CUDA_TRY(cudaMalloc(&A->d_pts, (size_t)ndim * A->N * sizeof(double)));
+    }
+    A->ndim = ndim;
+    CUDA_TRY(cudaMemcpyAsync(A->d_pts, points, (size_t)ndim * A->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    return ctx_sync(c);
+}
+
+static CovParams cov_params(const hicma_tlr_desc *A, const hicma_tlr_problem *prob) {
+    CovParams p;
+    p.pts = A->d_pts; p.N = A->N; p.ndim = A->ndim; p.kind = prob->kind;
+    p.beta = prob->beta; p.sigma = prob->sigma; p.noise = prob->noise;
+    return p;
+}
+
+static int gen_band_tiles(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_problem *prob) {
+    std::vector<CovTask> tasks;
+    for (int m = 0; m < A->NT; ++m)
+        for (int n = std::max(m - A->band + 1, 0); n <= m; ++n)
+            tasks.push_back(CovTask{A->dense(m, n), A->NB, m * A->NB, n * A->NB, A->NB, A->NB});
+    CovTask *dt = stage(c, tasks.data(), tasks.size());
+    if (!dt) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+    launch_cov_batched(cov_params(A, prob), dt, (int)tasks.size(), A->NB, A->NB, c->stream);
+    return check_launch(c);
+}
+
+// Randomized range finder + truncated SVD of a batch of dense tiles
+// (restated starsh_dense_dlrrsdd): Y = A Omega, Q = qr(Y), W = A^T Q,
+// W = Q_W R_W, svd(R_W^T) = U S V^T, rank by relative Frobenius tol;
+// U_tile = Q U_r, V_tile = Q_W V_r S_r.
+struct CompressTask {
+    const double *A;     // nb x nb dense (ld nb)
+    double *outU, *outV;
+    int *rank_dst;
+};
+
+static size_t compress_ws_bytes(int nb, int s) {
+    const int pb = qr_panel_width(nb);
+    const size_t npan = (size_t)(s + pb - 1) / pb + 1;
+    size_t b = 0;
+    b += align_up(sizeof(double) * (size_t)nb * s + 1) * 3;   // Y, Q, W
+    b += align_up(sizeof(double) * (size_t)s + 1) * 2;
+    b += align_up(sizeof(double) * npan * pb * pb + 1) * 2;
+    b += align_up(sizeof(double) * (size_t)s * s + 1) * 2;
+    if (s > core_smem_kmax()) b += align_up(sizeof(double) * 2 * (size_t)s * s + 1);
+    return b + 1024;
+}
+
+static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const double *Omega, int s,
+                        std::vector<CompressTask> &tasks, const double *d_identity, int *d_rank_task_base) {
+    cudaStream_t st = c->stream;
+    const int pb = qr_panel_width(nb);
+    const size_t npan = (size_t)(s + pb - 1) / pb + 1;
+    const size_t mark = c->ws_off;
+    size_t i0 = 0;
+    while (i0 < tasks.size()) {
+        c->ws_off = mark;
+        std::vector<GemmTask> gy, gw;
+        std::vector<QRTask> qy, qw;
+        std::vector<QApplyTask> aq, au;
+        std::vector<CoreTask> cores;
+        size_t i = i0;
+        for (; i < tasks.size(); ++i) {
+            if (compress_ws_bytes(nb, s) > ws_free(c)) {
+                if (i == i0) { set_err("workspace too small for one tile compression"); return HICMA_TLR_ERR_OOM; }
+                break;
+            }
+            const CompressTask &t = tasks[i];
+            double *Y = ws_alloc<double>(c, (size_t)nb * s);
+            double *Q = ws_alloc<double>(c, (size_t)nb * s);
+            double *W = ws_alloc<double>(c, (size_t)nb * s);
+            double *tauY = ws_alloc<double>(c, s), *tauW = ws_alloc<double>(c, s);
+            double *TY = ws_alloc<double>(c, npan * pb * pb), *TW = ws_alloc<double>(c, npan * pb * pb);
+            double *SU = ws_alloc<double>(c, (size_t)s * s), *SV = ws_alloc<double>(c, (size_t)s * s);
+            double *work = s > core_smem_kmax() ? ws_alloc<double>(c, 2 * (size_t)s * s) : nullptr;
+            int *rt = d_rank_task_base + (i - i0);
+            gy.push_back(make_gemm(0, 0, nb, s, nb, 1.0, t.A, nb, Omega, nb, 0.0, Y, nb));
+            qy.push_back(QRTask{Y, tauY, TY, nb, s, nb});
+            aq.push_back(QApplyTask{Y, TY, d_identity, Q, nullptr, nb, s, nb, s, nb, s});
+            gw.push_back(make_gemm(1, 0, nb, s, nb, 1.0, t.A, nb, Q, nb, 0.0, W, nb));
+            qw.push_back(QRTask{W, tauW, TW, nb, s, nb});
+            CoreTask ct{};
+            ct.RU = nullptr; ct.RV = W; ct.ldru = nb; ct.ldrv = nb;
+            ct.SU = SU; ct.SV = SV; ct.work = work;
+            ct.rank_out = t.rank_dst; ct.rank_task = rt; ct.K = s;
+            cores.push_back(ct);
+            au.push_back(QApplyTask{Y, TY, SU, t.outU, rt, nb, s, nb, s, nb, maxrank});
+            au.push_back(QApplyTask{W, TW, SV, t.outV, rt, nb, s, nb, s, nb, maxrank});
+        }
+        TRY(run_gemms(c, gy));
+        QRTask *d1 = stage(c, qy.data(), qy.size());
+        launch_qr_batched(d1, (int)qy.size(), nb, st);
+        TRY(check_launch(c));
+        QApplyTask *d2 = stage(c, aq.data(), aq.size());
+        launch_qapply_batched(d2, (int)aq.size(), nb, st);
+        TRY(check_launch(c));
+        TRY(run_gemms(c, gw));
+        QRTask *d3 = stage(c, qw.data(), qw.size());
+        launch_qr_batched(d3, (int)qw.size(), nb, st);
+        TRY(check_launch(c));
+        CoreParams cp{1, tol, maxrank, 0, nb, nullptr};
+        CoreTask *d4 = stage(c, cores.data(), cores.size());
+        launch_core_svd_batched(d4, (int)cores.size(), s, cp, st);
+        TRY(check_launch(c));
+        QApplyTask *d5 = stage(c, au.data(), au.size());
+        launch_qapply_batched(d5, (int)au.size(), nb, st);
+        TRY(check_launch(c));
+        if (!d1 || !d2 || !d3 || !d4 || !d5) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+        i0 = i;
+    }
+    c->ws_off = mark;
+    return 0;
+}
+
+int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, const hicma_tlr_problem *prob,
+                       const double *points, double tol, int maxrank, int band_size, int send_full_tile,
+                       int *info) {
+    (void)send_full_tile;
+    ARG_CHECK(c && A && prob, "null");
+    if (uplo != HICMA_TLR_LOWER) { set_err("only uplo = Lower is supported"); return HICMA_TLR_ERR_NOT_SUPPORTED; }
+    ARG_CHECK(band_size >= 1, "band_size should be not less than 1");
+    ARG_CHECK(band_size == A->band, "band_size must equal the descriptor's band size");
+    ARG_CHECK(maxrank >= 1 && maxrank <= A->maxrank, "maxrank must be in [1, descriptor maxrank]");
+    ARG_CHECK(tol > 0.0, "tol > 0");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (info) *info = 0;
+    TRY(set_points(c, A, prob, points));
+    ws_reset(c);
+    const int NT = A->NT, NB = A->NB;
+    TRY(gen_band_tiles(c, A, prob));
+    // off-band tiles: generate dense into the workspace, compress into slots
+    const int s = std::min(maxrank + 10, NB);    // STARSH_gen.jdf:262-266
+    double *Omega = ws_alloc<double>(c, (size_t)NB * s);
+    double *Ident = ws_alloc<double>(c, (size_t)s * s);
+    int *rtask = ws_alloc<int>(c, (size_t)NT * NT + 1);
+    if (!Omega || !Ident || !rtask) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
+    launch_gaussian(Omega, NB, s, NB, prob->seed ^ 0x5DEECE66Dull, c->stream);
+    TRY(check_launch(c));
+    launch_set_identity(Ident, s, s, c->stream);
+    TRY(check_launch(c));
+    std::vector<std::pair<int, int>> tiles;
+    for (int m = A->band; m < NT; ++m)
+        for (int n = 0; n <= m - A->band; ++n) tiles.push_back({m, n});
+    const size_t per_tile = align_up(sizeof(double) * (size_t)NB * NB + 1) + compress_ws_bytes(NB, s);
+    size_t chunk = std::max<size_t>(1, ws_free(c) / (per_tile + 4096));
+    const CovParams cp = cov_params(A, prob);
+    for (size_t t0 = 0; t0 < tiles.size(); t0 += chunk) {
+        const size_t t1 = std::min(tiles.size(), t0 + chunk);
+        const size_t mark = c->ws_off;
+        std::vector<CovTask> cov;
+        std::vector<CompressTask> comp;
+        for (size_t i = t0; i < t1; ++i) {
+            const int m = tiles[i].first, n = tiles[i].second;
+            double *D = ws_alloc<double>(c, (size_t)NB * NB);
+            cov.push_back(CovTask{D, NB, m * NB, n * NB, NB, NB});
+            comp.push_back(CompressTask{D, A->U(m, n), A->V(m, n), A->d_rank + (size_t)n * NT + m});
+        }
+        CovTask *dcov = stage(c, cov.data(), cov.size());
+        if (!dcov) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+        launch_cov_batched(cp, dcov, (int)cov.size(), NB, NB, c->stream);
+        TRY(check_launch(c));
+        TRY(run_compress(c, NB, maxrank, tol, Omega, s, comp, Ident, rtask));
+        c->ws_off = mark;
+    }
+    TRY(ctx_sync(c));
+    CUDA_TRY(cudaMemcpy(A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
+    int bad = 0;
+    for (int m = A->band; m < NT; ++m)
+        for (int n = 0; n <= m - A->band; ++n)
+            if (A->rank(m, n) < 0) {
+                if (bad < 4) fprintf(stderr, "Tile(%d, %d) is dense, try increasing NB or maxrank \n", m, n);
+                ++bad;
+            }
+    if (bad) {
+        for (int m = A->band; m < NT; ++m)
+            for (int n = 0; n <= m - A->band; ++n)
+                if (A->h_rank[(size_t)n * NT + m] < 0) A->h_rank[(size_t)n * NT + m] = 0;
+        CUDA_TRY(cudaMemcpy(A->d_rank, A->h_rank.data(), (size_t)NT * NT * sizeof(int), cudaMemcpyHostToDevice));
+        if (info) *info = -1;
+    }
+    A->factored = false;
+    if (Ar) std::memcpy(Ar, A->h_rank.data(), (size_t)NT * NT * sizeof(int));
+    return 0;
+}
+
+int hicma_tlr_rank_gather(hicma_tlr_ctx *c, hicma_tlr_desc *A, int *rank_array, int band_size) {
+    ARG_CHECK(c && A && rank_array, "null");
+    (void)band_size;
+    const int NT = A->NT;
+    for (int n = 0; n < NT; ++n)
+        for (int m = 0; m < NT; ++m) rank_array[(size_t)n * NT + m] = A->is_dense(m, n) || m < n ? -1 : A->rank(m, n);
+    return 0;
+}
+
+int hicma_tlr_rank_stat(const int *G, int NT, int band_size, int *minrk, int *maxrk, double *avgrk) {
+    ARG_CHECK(G && NT > 0 && band_size >= 1, "rank_stat");
+    int mn = 2147483647, mx = 0;
+    long long sum = 0, num = 0;
+    for (int i = band_size; i < NT; ++i)
+        for (int j = 0; j < i - band_size + 1; ++j) {
+            const int v = G[(size_t)j * NT + i];
+            sum += v; ++num;
+            mn = std::min(mn, v); mx = std::max(mx, v);
+        }
+    if (minrk) *minrk = mn;
+    if (maxrk) *maxrk = mx;
+    if (avgrk) *avgrk = num ? (double)sum / (double)num : NAN;
+    return 0;
+}
+
+int hicma_tlr_band_autotune(const int *G, int NT, int NB, int verbose) {
+    ARG_CHECK(G && NT > 0 && NB > 0, "band_autotune");
+    const double FLUCTUATION = 0.66666667;   // hicma_parsec_internal.h:107
+    int indicator_min = 0, opt_min = 0;
+    for (int band = 2; band < NT; ++band) {
+        long long t_tlr = 0, t_dense = 0, g_tlr = 0, g_dense = 0;
+        for (int m = band - 1; m < NT; ++m) {
+            const int k = m + 1 - band;
+            const int ar = G[(size_t)k * NT + m];
+            t_tlr += (long long)NB * NB * ar;
+            t_dense += (long long)NB * NB * NB;
+        }
+        for (int k = 0; k <= NT - 3; ++k)
+            for (int m = k + band; m < NT; ++m) {
+                const int n = m + 1 - band;
+                const int ar = G[(size_t)k * NT + m], br = G[(size_t)k * NT + n], cr = G[(size_t)n * NT + m];
+                const unsigned long ca = (unsigned long)(cr + ar);
+                const unsigned long qra = op_counts('q', NB, ca, 0, 0);
+                unsigned long qrb = op_counts('m', ar, br, NB, 0);
+                qrb += op_counts('m', ar, NB, br, 0);
+                qrb += op_counts('q', NB, ca, 0, 0);
+                unsigned long svd = op_counts('r', ca, ca, 2, 0);
+                svd += op_counts('s', ca, 0, 0, 0);
+                svd += ca * (unsigned long)cr;
+                const unsigned long nu = op_counts('o', NB, cr, ca, 1);
+                const unsigned long nv = op_counts('o', cr, NB, ca, 2);
+                g_tlr += (long long)qra + qrb + svd + nu + nv;
+                if (m - k < band) g_dense += (long long)2 * NB * NB * NB;
+                else if (n - k < band && m - n < band) g_dense += (long long)4 * NB * NB * ar;
+                else if (m - n < band) g_dense += (long long)2 * NB * NB * std::min(ar, br) + (long long)4 * NB * ar * br;
+            }
+        const long long s_tlr = t_tlr + g_tlr, s_dense = t_dense + g_dense;
+        if (verbose)
+            fprintf(stderr, "band_size: %d, ops_sum_tlr: %e, ops_sum_dense: %e\n", band, (double)s_tlr, (double)s_dense);
+        if ((double)s_tlr * FLUCTUATION <= (double)s_dense && indicator_min == 0) {
+            indicator_min = 1;
+            opt_min = band - 1;
+        }
+        if (s_tlr <= s_dense) return opt_min;
+    }
+    return NT;
+}
+
+int hicma_tlr_band_regenerate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, const hicma_tlr_problem *prob,
+                              int band_size) {
+    ARG_CHECK(c && A && prob, "null");
+    if (uplo != HICMA_TLR_LOWER) { set_err("only uplo = Lower is supported"); return HICMA_TLR_ERR_NOT_SUPPORTED; }
+    ARG_CHECK(band_size >= A->slot_band, "band_size cannot shrink below the slot band");
+    ARG_CHECK(A->d_pts, "no points: generate first");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    const int NT = A->NT, NB = A->NB;
+    band_size = std::min(band_size, NT);
+    TRY(ctx_sync(c));
+    if (band_size > A->band_alloc) {
+        cudaFree(A->d_band);
+        A->d_band = nullptr;
+        const size_t bytes = (size_t)NT * band_size * NB * (size_t)NB * sizeof(double);
+        if (cudaMalloc(&A->d_band, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            set_err("band allocation of %zu bytes failed", bytes);
+            return HICMA_TLR_ERR_OOM;
+        }
+        A->band_alloc = band_size;
+    }
+    A->band = band_size;
+    TRY(gen_band_tiles(c, A, prob));
+    for (int m = 0; m < NT; ++m)
+        for (int n = 0; n < NT; ++n)
+            if (m < n || m - n < band_size) A->h_rank[(size_t)n * NT + m] = -1;
+    CUDA_TRY(cudaMemcpyAsync(A->d_rank, A->h_rank.data(), (size_t)NT * NT * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    A->factored = false;
+    return ctx_sync(c);
+}
+
+// ------------------------------------------------------- factorization -----
+static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_rank, int maxrank,
+                     unsigned long *tileops, unsigned long *opcounters, double *cpt, int verbose) {
+    const int NT = A->NT, NB = A->NB, band = A->band;
+    cudaStream_t st = c->stream;
+    const bool mixed = c->precision == HICMA_TLR_PREC_MIXED;
+    if (!A->d_linv) {
+        if (cudaMalloc(&A->d_linv, (size_t)NT * NB * NB * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            set_err("allocation of the diagonal inverses failed");
+            return HICMA_TLR_ERR_OOM;
+        }
+    }
+    ws_reset(c);
+    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 2 * sizeof(int), st));
+    int *d_info = c->d_flags;
+    int *rtask = ws_alloc<int>(c, (size_t)NT * NT + 16);
+    if (!rtask) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
+    const size_t base_mark = c->ws_off;
+    std::vector<unsigned long> tops((size_t)NT * NT, 0);
+    unsigned long op_total = 0;
+    cudaEvent_t ev[5];
+    for (auto &e : ev) CUDA_TRY(cudaEventCreate(&e));
+    double t_phase[4] = {0, 0, 0, 0};
+    const auto t_start = std::chrono::steady_clock::now();
+    const long long launches0 = c->launches;
+    int info = 0;
+    auto log_op = [&](unsigned long cnt, int i, int j) {
+        tops[(size_t)i * NT + j] += cnt;
+        op_total += cnt;
+    };
+    for (int k = 0; k < NT; ++k) {
+        CUDA_TRY(cudaEventRecord(ev[0], st));
+        // ---- POTRF(k)
+        log_op(op_counts('c', NB, 0, 0, 0), k, k);
+        TRY(potrf_tile(c, A->dense(k, k), NB, NB, A->linv(k), NB, d_info, k * NB));
+        CUDA_TRY(cudaEventRecord(ev[1], st));
+        const double *Li = A->linv(k);
+        // ---- TRSM(m, k): dense C <- C L^-T ; low rank V <- L^-1 V
+        {
+            c->ws_off = base_mark;
+            std::vector<GemmTask> g;
+            std::vector<CopyTask> cp;
+            for (int m = k + 1; m < NT; ++m) {
+                if (A->is_dense(m, k)) {
+                    log_op(op_counts('t', NB, NB, 1, 0), m, k);
+                    double *tmp = ws_alloc<double>(c, (size_t)NB * NB);
+                    if (!tmp) {
+                        TRY(run_gemms(c, g)); TRY(run_copies(c, cp));
+                        c->ws_off = base_mark;
+                        tmp = ws_alloc<double>(c, (size_t)NB * NB);
+                        if (!tmp) { set_err("workspace too small (trsm)"); return HICMA_TLR_ERR_OOM; }
+                    }
+                    g.push_back(make_gemm(0, 1, NB, NB, NB, 1.0, A->dense(m, k), NB, Li, NB, 0.0, tmp, NB));
+                    cp.push_back(make_copy(tmp, NB, A->dense(m, k), NB, NB, NB));
+                } else {
+                    const int r = A->rank(m, k);
+                    log_op(op_counts('t', NB, r, 1, 0), m, k);
+                    if (r == 0) continue;
+                    double *tmp = ws_alloc<double>(c, (size_t)NB * r);
+                    if (!tmp) {
+                        TRY(run_gemms(c, g)); TRY(run_copies(c, cp));
+                        c->ws_off = base_mark;
+                        tmp = ws_alloc<double>(c, (size_t)NB * r);
+                        if (!tmp) { set_err("workspace too small (trsm)"); return HICMA_TLR_ERR_OOM; }
+                    }
+                    g.push_back(make_gemm(0, 0, NB, r, NB, 1.0, Li, NB, A->V(m, k), NB, 0.0, tmp, NB));
+                    cp.push_back(make_copy(tmp, NB, A->V(m, k), NB, NB, r));
+                }
+            }
+            TRY(run_gemms(c, g));
+            TRY(run_copies(c, cp));
+        }
+        CUDA_TRY(cudaEventRecord(ev[2], st));
+        // ---- SYRK(k, m)
+        {
+            c->ws_off = base_mark;
+            std::vector<GemmTask> g1, g2, g3;
+            for (int m = k + 1; m < NT; ++m) {
+                if (A->is_dense(m, k)) {
+                    log_op(op_counts('m', NB, NB, NB, 0), m, m);
+                    g1.push_back(make_gemm(0, 1, NB, NB, NB, -1.0, A->dense(m, k), NB, A->dense(m, k), NB, 1.0,
+                                           A->dense(m, m), NB));
+                } else {
+                    const int r = A->rank(m, k);
+                    log_op(op_counts('m', r, r, NB, 0) + op_counts('m', NB, r, r, 0) + op_counts('m', NB, NB, r, 0), m, m);
+                    if (r == 0) continue;
+                    double *W = ws_alloc<double>(c, (size_t)r * r);
+                    double *X = ws_alloc<double>(c, (size_t)NB * r);
+                    if (!W || !X) {
+                        TRY(run_gemms(c, g1)); TRY(run_gemms(c, g2)); TRY(run_gemms(c, g3));
+                        c->ws_off = base_mark;
+                        W = ws_alloc<double>(c, (size_t)r * r);
+                        X = ws_alloc<double>(c, (size_t)NB * r);
+                        if (!W || !X) { set_err("workspace too small (syrk)"); return HICMA_TLR_ERR_OOM; }
+                    }
+                    g1.push_back(make_gemm(1, 0, r, r, NB, 1.0, A->V(m, k), NB, A->V(m, k), NB, 0.0, W, r));
+                    g2.push_back(make_gemm(0, 0, NB, r, r, 1.0, A->U(m, k), NB, W, r, 0.0, X, NB));
+                    g3.push_back(make_gemm(0, 1, NB, NB, r, -1.0, X, NB, A->U(m, k), NB, 1.0, A->dense(m, m), NB));
+                }
+            }
+            TRY(run_gemms(c, g1));
+            TRY(run_gemms(c, g2));
+            TRY(run_gemms(c, g3));
+        }
+        CUDA_TRY(cudaEventRecord(ev[3], st));
+        // ---- GEMM(m, n, k)
+        std::vector<RecompTask> rec;
+        std::vector<int> rec_case;   // 0: B low rank, 1: B dense
+        std::vector<std::array<int, 5>> rec_meta;
+        {
+            c->ws_off = base_mark;
+            std::vector<GemmTask> g1, g2, g3;
+            for (int m = k + 2; m < NT; ++m) {
+                for (int n = k + 1; n < m; ++n) {
+                    if (m - k < band) {                                    // (i)
+                        log_op(op_counts('m', NB, NB, NB, 0), m, n);
+                        g1.push_back(make_gemm(0, 1, NB, NB, NB, -1.0, A->dense(m, k), NB, A->dense(n, k), NB, 1.0,
+                                               A->dense(m, n), NB));
+                    } else if (n - k < band && m - n < band) {             // (ii)
+                        const int ra = A->rank(m, k);
+                        log_op(op_counts('m', NB, NB, ra, 0) * 2, m, n);
+                        if (ra == 0) continue;
+                        double *tmp = ws_alloc<double>(c, (size_t)ra * NB);
+                        if (!tmp) {
+                            TRY(run_gemms(c, g1)); TRY(run_gemms(c, g2)); TRY(run_gemms(c, g3));
+                            c->ws_off = base_mark;
+                            tmp = ws_alloc<double>(c, (size_t)ra * NB);
+                            if (!tmp) { set_err("workspace too small (gemm)"); return HICMA_TLR_ERR_OOM; }
+                        }
+                        g1.push_back(make_gemm(1, 1, ra, NB, NB, 1.0, A->V(m, k), NB, A->dense(n, k), NB, 0.0, tmp, ra));
+                        g2.push_back(make_gemm(0, 0, NB, NB, ra, -1.0, A->U(m, k), NB, tmp, ra, 1.0, A->dense(m, n), NB));
+                    } else if (m - n < band) {                             // (iii)
+                        const int ra = A->rank(m, k), rb = A->rank(n, k);
+                        log_op(op_counts('m', NB, NB, std::min(ra, rb), 0) + op_counts('m', NB, ra, rb, 0) * 2, m, n);
+                        if (ra == 0 || rb == 0) continue;
+                        double *rr = ws_alloc<double>(c, (size_t)ra * rb);
+                        double *tmp = ws_alloc<double>(c, (size_t)NB * std::max(ra, rb));
+                        if (!rr || !tmp) {
+                            TRY(run_gemms(c, g1)); TRY(run_gemms(c, g2)); TRY(run_gemms(c, g3));
+                            c->ws_off = base_mark;
+                            rr = ws_alloc<double>(c, (size_t)ra * rb);
+                            tmp = ws_alloc<double>(c, (size_t)NB * std::max(ra, rb));
+                            if (!rr || !tmp) { set_err("workspace too small (gemm)"); return HICMA_TLR_ERR_OOM; }
+                        }
+                        g1.push_back(make_gemm(1, 0, ra, rb, NB, 1.0, A->V(m, k), NB, A->V(n, k), NB, 0.0, rr, ra));
+                        if (ra > rb) {
+                            g2.push_back(make_gemm(0, 0, NB, rb, ra, 1.0, A->U(m, k), NB, rr, ra, 0.0, tmp, NB));
+                            g3.push_back(make_gemm(0, 1, NB, NB, rb, -1.0, tmp, NB, A->U(n, k), NB, 1.0, A->dense(m, n), NB));
+                        } else {
+                            g2.push_back(make_gemm(0, 1, ra, NB, rb, 1.0, rr, ra, A->U(n, k), NB, 0.0, tmp, ra));
+                            g3.push_back(make_gemm(0, 0, NB, NB, ra, -1.0, A->U(m, k), NB, tmp, ra, 1.0, A->dense(m, n), NB));
+                        }
+                    } else if (n - k < band) {                             // (iv)
+                        const int ra = A->rank(m, k), rc = A->rank(m, n);
+                        rec.push_back(RecompTask{A->U(m, n), A->V(m, n), rc, A->U(m, k), A->V(m, k), ra,
+                                                 A->dense(n, k), nullptr, NB, A->U(m, n), A->V(m, n),
+                                                 A->d_rank + (size_t)n * NT + m});
+                        rec_meta.push_back({m, n, ra, 0, rc});
+                        rec_case.push_back(1);
+                    } else {                                               // (v)
+                        const int ra = A->rank(m, k), rb = A->rank(n, k), rc = A->rank(m, n);
+                        if (ra == 0 || rb == 0) continue;
+                        rec.push_back(RecompTask{A->U(m, n), A->V(m, n), rc, A->U(m, k), A->V(m, k), ra,
+                                                 A->U(n, k), A->V(n, k), rb, A->U(m, n), A->V(m, n),
+                                                 A->d_rank + (size_t)n * NT + m});
+                        rec_meta.push_back({m, n, ra, rb, rc});
+                        rec_case.push_back(0);
+                    }
+                }
+            }
+            TRY(run_gemms(c, g1));
+            TRY(run_gemms(c, g2));
+            TRY(run_gemms(c, g3));
+            c->ws_off = base_mark;
+            TRY(run_recompress(c, NB, rec, acc, maxrank, fixed_rank, rtask, mixed));
+        }
+        CUDA_TRY(cudaEventRecord(ev[4], st));
+        // ---- panel end: info, ranks, timings
+        TRY(ctx_sync(c));
+        int hinfo = 0;
+        CUDA_TRY(cudaMemcpy(&hinfo, d_info, sizeof(int), cudaMemcpyDeviceToHost));
+        if (!rec.empty())
+            CUDA_TRY(cudaMemcpy(A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < rec.size(); ++i) {
+            const auto &mt = rec_meta[i];
+            const int rnew = A->rank(mt[0], mt[1]);
+            log_op(gemm_lr_ops(NB, mt[2], mt[3], mt[4], rnew, rec_case[i] == 1), mt[0], mt[1]);
+        }
+        float ms;
+        for (int p = 0; p < 4; ++p) {
+            CUDA_TRY(cudaEventElapsedTime(&ms, ev[p], ev[p + 1]));
+            t_phase[p] += ms * 1e-3;
+        }
+        if (hinfo != 0) {
+            info = hinfo;
+            if (verbose) fprintf(stderr, "dpotrf failed: info = %d (panel %d)\n", info, k);
+            break;
+        }
+        if (verbose > 1) fprintf(stderr, "panel %d done\n", k);
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    int overflow = 0;
+    CUDA_TRY(cudaMemcpy(&overflow, c->d_flags + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    if (tileops)
+        for (size_t i = 0; i < tops.size(); ++i) tileops[i] += tops[i];
+    if (opcounters) opcounters[0] += op_total;
+    if (cpt) {
+        cpt[0] = t_phase[0]; cpt[1] = t_phase[1]; cpt[2] = t_phase[2];
+        cpt[3] = secs; cpt[4] = t_phase[1] + t_phase[2] + t_phase[3]; cpt[5] = t_phase[3];
+    }
+    A->stats[0] = secs;
+    A->stats[1] = (double)op_total;
+    A->stats[2] = overflow;
+    A->stats[3] = (double)(c->launches - launches0);
+    A->stats[4] = t_phase[0]; A->stats[5] = t_phase[1]; A->stats[6] = t_phase[2]; A->stats[7] = t_phase[3];
+    A->factored = (info == 0);
+    ws_reset(c);
+    return info;
+}
+
+int hicma_tlr_dpotrf_L(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, double acc, int fixed_rank,
+                       int maxrank, int *lookahead, int band_size, int hmb, int compmaxrank, int send_full_tile,
+                       int *two_flow, unsigned long *tileopcounters, unsigned long *opcounters,
+                       double *critical_path_time, int verbose) {
+    (void)hmb; (void)send_full_tile;
+    ARG_CHECK(c && A, "null");
+    // HiCMA_dpotrf_L_2flow_wrapper.c:219-237
+    if (uplo != HICMA_TLR_LOWER) { set_err("HiCMA_dpotrf_L_2flow does not support dplasmaUpper"); return HICMA_TLR_ERR_NOT_SUPPORTED; }
+    if (compmaxrank <= 0) compmaxrank = maxrank;
+    ARG_CHECK(maxrank <= compmaxrank, "maxrank for storage larger than maxrank for buffers is not meaningful");
+    ARG_CHECK(maxrank <= A->NB / 2, "maxrank should not be larger than half of block size");
+    ARG_CHECK(maxrank <= A->maxrank, "maxrank larger than the descriptor's slot capacity");
+    ARG_CHECK(band_size == A->band, "band_size must equal the descriptor's band size");
+    ARG_CHECK(acc > 0.0 || fixed_rank > 0, "acc > 0 or fixed_rank > 0");
+    if (lookahead) {
+        ARG_CHECK(*lookahead >= -1, "lookahead >= -1");
+        if (*lookahead == -1) *lookahead = band_size;   // hicma_parsec.c:489-495
+    }
+    if (two_flow) *two_flow = 1;
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    CUDA_TRY(cudaSetDevice(c->device));
+    const int info = factorize(c, A, acc, fixed_rank, maxrank, tileopcounters, opcounters, critical_path_time, verbose);
+    if (Ar) std::memcpy(Ar, A->h_rank.data(), (size_t)A->NT * A->NT * sizeof(int));
+    return info;
+}
+
+int hicma_tlr_dpotrf_L_start(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_rank, int maxrank) {
+    ARG_CHECK(c && A, "null");
+    if (c->async_thread.joinable()) { set_err("a factorization is already in flight on this context"); return HICMA_TLR_ERR_STATE; }
+    c->async_thread = std::thread([=]() {
+        int la = -1, tf = 0;
+        c->async_ret = hicma_tlr_dpotrf_L(c, HICMA_TLR_LOWER, A, nullptr, acc, fixed_rank, maxrank, &la, A->band, A->NB,
+                                          maxrank, 0, &tf, nullptr, nullptr, nullptr, 0);
+    });
+    return 0;
+}
+
+int hicma_tlr_dpotrf_L_wait(hicma_tlr_ctx *c, hicma_tlr_desc *A, int *Ar) {
+    ARG_CHECK(c && A, "null");
+    if (!c->async_thread.joinable()) { set_err("no factorization in flight"); return HICMA_TLR_ERR_STATE; }
+    c->async_thread.join();
+    if (Ar) std::memcpy(Ar, A->h_rank.data(), (size_t)A->NT * A->NT * sizeof(int));
+    return c->async_ret;
+}
+
+int hicma_tlr_last_stats(hicma_tlr_desc *A, double *stats, int nstats) {
+    ARG_CHECK(A && stats, "null");
+    for (int i = 0; i < nstats && i < 8; ++i) stats[i] = A->stats[i];
+    return 0;
+}
+
+// ------------------------------------------------------------ transfers ----
+int hicma_tlr_tile_get(hicma_tlr_ctx *c, hicma_tlr_desc *A, int m, int n, double *buf, int *rank) {
+    ARG_CHECK(c && A, "null");
+    ARG_CHECK(m >= 0 && n >= 0 && m < A->NT && n <= m, "tile index (lower triangle only)");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    const size_t NB = A->NB;
+    TRY(ctx_sync(c));
+    if (A->is_dense(m, n)) {
+        if (rank) *rank = -1;
+        if (buf) CUDA_TRY(cudaMemcpy(buf, A->dense(m, n), NB * NB * sizeof(double), cudaMemcpyDeviceToHost));
+        return 0;
+    }
+    const int r = A->rank(m, n);
+    if (rank) *rank = r;
+    if (buf && r > 0) {
+        CUDA_TRY(cudaMemcpy(buf, A->U(m, n), NB * r * sizeof(double), cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(buf + NB * r, A->V(m, n), NB * r * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    return 0;
+}
+
+int hicma_tlr_tile_set(hicma_tlr_ctx *c, hicma_tlr_desc *A, int m, int n, const double *buf, int rank) {
+    ARG_CHECK(c && A && buf, "null");
+    ARG_CHECK(m >= 0 && n >= 0 && m < A->NT && n <= m, "tile index (lower triangle only)");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    const size_t NB = A->NB, NT = A->NT;
+    TRY(ctx_sync(c));
+    if (A->is_dense(m, n)) {
+        CUDA_TRY(cudaMemcpy(A->dense(m, n), buf, NB * NB * sizeof(double), cudaMemcpyHostToDevice));
+        return 0;
+    }
+    ARG_CHECK(rank >= 0 && rank <= A->maxrank, "rank in [0, maxrank]");
+    if (rank > 0) {
+        CUDA_TRY(cudaMemcpy(A->U(m, n), buf, NB * rank * sizeof(double), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(A->V(m, n), buf + NB * rank, NB * rank * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    A->h_rank[(size_t)n * NT + m] = rank;
+    CUDA_TRY(cudaMemcpy(A->d_rank + (size_t)n * NT + m, &rank, sizeof(int), cudaMemcpyHostToDevice));
+    A->factored = false;
+    return 0;
+}
+
+int hicma_tlr_store_bytes(hicma_tlr_ctx *c, hicma_tlr_desc *A, size_t *bytes) {
+    ARG_CHECK(c && A && bytes, "null");
+    const size_t NB = A->NB;
+    size_t b = 0;
+    for (int m = 0; m < A->NT; ++m)
+        for (int n = 0; n <= m; ++n)
+            b += A->is_dense(m, n) ? NB * NB : 2 * NB * (size_t)A->rank(m, n);
+    *bytes = b * sizeof(double);
+    return 0;
+}
+
+int hicma_tlr_store_get(hicma_tlr_ctx *c, hicma_tlr_desc *A, double *buf, int *Ar) {
+    ARG_CHECK(c && A && buf, "null");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    const size_t NB = A->NB;
+    TRY(ctx_sync(c));
+    double *p = buf;
+    for (int m = 0; m < A->NT; ++m)
+        for (int n = std::max(0, m - A->band + 1); n <= m; ++n) {
+            CUDA_TRY(cudaMemcpyAsync(p, A->dense(m, n), NB * NB * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            p += NB * NB;
+        }
+    for (int m = A->band; m < A->NT; ++m)
+        for (int n = 0; n <= m - A->band; ++n) {
+            const int r = A->rank(m, n);
+            if (r > 0) {
+                CUDA_TRY(cudaMemcpyAsync(p, A->U(m, n), NB * r * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+                CUDA_TRY(cudaMemcpyAsync(p + NB * r, A->V(m, n), NB * r * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            }
+            p += 2 * NB * (size_t)r;
+        }
+    if (Ar) std::memcpy(Ar, A->h_rank.data(), (size_t)A->NT * A->NT * sizeof(int));
+    return ctx_sync(c);
+}
+
+int hicma_tlr_store_set(hicma_tlr_ctx *c, hicma_tlr_desc *A, const double *buf, const int *Ar) {
+    ARG_CHECK(c && A && buf && Ar, "null");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    const size_t NB = A->NB, NT = A->NT;
+    TRY(ctx_sync(c));
+    for (int m = A->band; m < A->NT; ++m)
+        for (int n = 0; n <= m - A->band; ++n)
+            ARG_CHECK(Ar[(size_t)n * NT + m] >= 0 && Ar[(size_t)n * NT + m] <= A->maxrank, "rank out of range");
+    const double *p = buf;
+    for (int m = 0; m < A->NT; ++m)
+        for (int n = std::max(0, m - A->band + 1); n <= m; ++n) {
+            CUDA_TRY(cudaMemcpyAsync(A->dense(m, n), p, NB * NB * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+            p += NB * NB;
+        }
+    for (int m = A->band; m < A->NT; ++m)
+        for (int n = 0; n <= m - A->band; ++n) {
+            const int r = Ar[(size_t)n * NT + m];
+            if (r > 0) {
+                CUDA_TRY(cudaMemcpyAsync(A->U(m, n), p, NB * r * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+                CUDA_TRY(cudaMemcpyAsync(A->V(m, n), p + NB * r, NB * r * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+            }
+            p += 2 * NB * (size_t)r;
+        }
+    for (int m = 0; m < A->NT; ++m)
+        for (int n = 0; n < A->NT; ++n)
+            A->h_rank[(size_t)n * NT + m] = (m < n || A->is_dense(m, n)) ? -1 : Ar[(size_t)n * NT + m];
+    CUDA_TRY(cudaMemcpyAsync(A->d_rank, A->h_rank.data(), NT * NT * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    A->factored = false;
+    return ctx_sync(c);
+}
+
+int hicma_tlr_uncompress(hicma_tlr_ctx *c, hicma_tlr_desc *A, double *dense, long ld) {
+    ARG_CHECK(c && A && dense && ld >= A->N, "null or ld < N");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    const int NT = A->NT, NB = A->NB;
+    TRY(ctx_sync(c));
+    ws_reset(c);
+    double *tmp = ws_alloc<double>(c, (size_t)NB * NB);
+    if (!tmp) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
+    std::vector<double> h((size_t)NB * NB);
+    for (int n = 0; n < NT; ++n)
+        for (int m = 0; m < NT; ++m) {
+            if (m < n) {
+                for (int j = 0; j < NB; ++j)
+                    std::memset(dense + (size_t)(n * NB + j) * ld + (size_t)m * NB, 0, sizeof(double) * NB);
+                continue;
+            }
+            const double *src;
+            if (A->is_dense(m, n)) {
+                src = A->dense(m, n);
+            } else {
+                const int r = A->rank(m, n);
+                launch_gemm_single(make_gemm(0, 1, NB, NB, r, 1.0, A->U(m, n), NB, A->V(m, n), NB, 0.0, tmp, NB), c->stream);
+                TRY(check_launch(c));
+                src = tmp;
+            }
+            CUDA_TRY(cudaMemcpy2DAsync(dense + (size_t)(n * NB) * ld + (size_t)m * NB, ld * sizeof(double), src,
+                                       NB * sizeof(double), NB * sizeof(double), NB, cudaMemcpyDeviceToHost, c->stream));
+            TRY(ctx_sync(c));
+            if (m == n)
+                for (int j = 0; j < NB; ++j)
+                    for (int i = 0; i < j; ++i) dense[(size_t)(n * NB + j) * ld + (size_t)m * NB + i] = 0.0;
+        }
+    ws_reset(c);
+    return 0;
+}
+
+// --------------------------------------------------- log-det and solves ----
+int hicma_tlr_logdet(hicma_tlr_ctx *c, hicma_tlr_desc *A, double *logdet) {
+    ARG_CHECK(c && A && logdet, "null");
+    if (!A->factored) { set_err("descriptor is not factored"); return HICMA_TLR_ERR_STATE; }
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    std::vector<const double *> ptrs(A->NT);
+    for (int k = 0; k < A->NT; ++k) ptrs[k] = A->dense(k, k);
+    const double **dp = stage(c, ptrs.data(), ptrs.size());
+    if (!dp) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+    launch_logdiag_sum(dp, A->NT, A->NB, A->NB, c->d_scal, c->stream);
+    TRY(check_launch(c));
+    CUDA_TRY(cudaMemcpyAsync(logdet, c->d_scal, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return ctx_sync(c);
+}
+
+// Forward (L z = b) then backward (L^T x = z) substitution over tiles with
+// the stored L_kk^-1; off-diagonal updates of one step are batched.
+static int solve_dev(hicma_tlr_ctx *c, hicma_tlr_desc *A, double *X, int nrhs) {
+    const int NT = A->NT, NB = A->NB;
+    const size_t N = A->N;
+    double *tmp = ws_alloc<double>(c, (size_t)NB * nrhs);
+    double *T2 = ws_alloc<double>(c, (size_t)NT * A->maxrank * nrhs + 1);
+    if (!tmp || !T2) { set_err("workspace too small (solve)"); return HICMA_TLR_ERR_OOM; }
+    std::vector<GemmTask> g1, g2;
+    std::vector<CopyTask> cp;
+    for (int k = 0; k < NT; ++k) {
+        double *xk = X + (size_t)k * NB;
+        g1.push_back(make_gemm(0, 0, NB, nrhs, NB, 1.0, A->linv(k), NB, xk, (int)N, 0.0, tmp, NB));
+        TRY(run_gemms(c, g1));
+        cp.push_back(make_copy(tmp, NB, xk, (int)N, NB, nrhs));
+        TRY(run_copies(c, cp));
+        for (int m = k + 1; m < NT; ++m) {
+            double *xm = X + (size_t)m * NB;
+            if (A->is_dense(m, k)) {
+                g2.push_back(make_gemm(0, 0, NB, nrhs, NB, -1.0, A->dense(m, k), NB, xk, (int)N, 1.0, xm, (int)N));
+            } else {
+                const int r = A->rank(m, k);
+                if (r == 0) continue;
+                double *t = T2 + (size_t)m * A->maxrank * nrhs;
+                g1.push_back(make_gemm(1, 0, r, nrhs, NB, 1.0, A->V(m, k), NB, xk, (int)N, 0.0, t, r));
+                g2.push_back(make_gemm(0, 0, NB, nrhs, r, -1.0, A->U(m, k), NB, t, r, 1.0, xm, (int)N));
+            }
+        }
+        TRY(run_gemms(c, g1));
+        TRY(run_gemms(c, g2));
+    }
+    for (int k = NT - 1; k >= 0; --k) {
+        double *xk = X + (size_t)k * NB;
+        g1.push_back(make_gemm(1, 0, NB, nrhs, NB, 1.0, A->linv(k), NB, xk, (int)N, 0.0, tmp, NB));
+        TRY(run_gemms(c, g1));
+        cp.push_back(make_copy(tmp, NB, xk, (int)N, NB, nrhs));
+        TRY(run_copies(c, cp));
+        for (int j = 0; j < k; ++j) {
+            double *xj = X + (size_t)j * NB;
+            if (A->is_dense(k, j)) {
+                g2.push_back(make_gemm(1, 0, NB, nrhs, NB, -1.0, A->dense(k, j), NB, xk, (int)N, 1.0, xj, (int)N));
+            } else {
+                const int r = A->rank(k, j);
+                if (r == 0) continue;
+                double *t = T2 + (size_t)j * A->maxrank * nrhs;
+                g1.push_back(make_gemm(1, 0, r, nrhs, NB, 1.0, A->U(k, j), NB, xk, (int)N, 0.0, t, r));
+                g2.push_back(make_gemm(0, 0, NB, nrhs, r, -1.0, A->V(k, j), NB, t, r, 1.0, xj, (int)N));
+            }
+        }
+        TRY(run_gemms(c, g1));
+        TRY(run_gemms(c, g2));
+    }
+    return 0;
+}
+
+int hicma_tlr_solve(hicma_tlr_ctx *c, hicma_tlr_desc *A, int nrhs, double *B, long ldb) {
+    ARG_CHECK(c && A && B && nrhs > 0 && ldb >= A->N, "solve arguments");
+    if (!A->factored) { set_err("descriptor is not factored"); return HICMA_TLR_ERR_STATE; }
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    CUDA_TRY(cudaSetDevice(c->device));
+    ws_reset(c);
+    const size_t N = A->N;
+    double *X = ws_alloc<double>(c, N * nrhs);
+    if (!X) { set_err("workspace too small (solve)"); return HICMA_TLR_ERR_OOM; }
+    CUDA_TRY(cudaMemcpy2DAsync(X, N * sizeof(double), B, ldb * sizeof(double), N * sizeof(double), nrhs,
+                               cudaMemcpyHostToDevice, c->stream));
+    TRY(solve_dev(c, A, X, nrhs));
+    CUDA_TRY(cudaMemcpy2DAsync(B, ldb * sizeof(double), X, N * sizeof(double), N * sizeof(double), nrhs,
+                               cudaMemcpyDeviceToHost, c->stream));
+    TRY(ctx_sync(c));
+    ws_reset(c);
+    return 0;
+}
+
+int hicma_tlr_loglik(hicma_tlr_ctx *c, hicma_tlr_desc *A, const double *y, double *loglik, double *logdet, double *x) {
+    ARG_CHECK(c && A && y, "null");
+    if (!A->factored) { set_err("descriptor is not factored"); return HICMA_TLR_ERR_STATE; }
+    std::vector<double> xs(y, y + A->N);
+    TRY(hicma_tlr_solve(c, A, 1, xs.data(), A->N));
+    double ld = 0.0;
+    TRY(hicma_tlr_logdet(c, A, &ld));
+    double q = 0.0;
+    for (int i = 0; i < A->N; ++i) q += y[i] * xs[i];
+    if (loglik) *loglik = -0.5 * (q + ld + A->N * std::log(2.0 * M_PI));
+    if (logdet) *logdet = ld;
+    if (x) std::memcpy(x, xs.data(), sizeof(double) * A->N);
+    return 0;
+}
+
+// ------------------------------------------------- kernel-level entries ----
+int hicma_tlr_k_cov(const hicma_tlr_problem *prob, const double *d_points, int N, int r0, int nr, int c0, int nc,
+                    double *d_out, int ld, void *stream) {
+    ARG_CHECK(prob && d_points && d_out && N > 0 && nr >= 0 && nc >= 0 && ld >= nr, "k_cov arguments");
+    ARG_CHECK(r0 >= 0 && c0 >= 0 && r0 + nr <= N && c0 + nc <= N, "k_cov range");
+    const int ndim = kind_ndim(prob->kind);
+    ARG_CHECK(ndim > 0, "kind");
+    CovParams p;
+    p.pts = d_points; p.N = N; p.ndim = ndim; p.kind = prob->kind;
+    p.beta = prob->beta; p.sigma = prob->sigma; p.noise = prob->noise;
+    CovTask t{d_out, ld, r0, c0, nr, nc};
+    CovTask *dt = nullptr;
+    cudaStream_t st = (cudaStream_t)stream;
+    CUDA_TRY(cudaMallocAsync(&dt, sizeof(CovTask), st));
+    CUDA_TRY(cudaMemcpyAsync(dt, &t, sizeof t, cudaMemcpyHostToDevice, st));
+    launch_cov_batched(p, dt, 1, nr, nc, st);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaFreeAsync(dt, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return 0;
+}
+
+int hicma_tlr_k_dgemm(int transA, int transB, int m, int n, int k, double alpha, const double *A, int lda,
+                      const double *B, int ldb, double beta, double *C, int ldc, void *stream) {
+    ARG_CHECK(m >= 0 && n >= 0 && k >= 0 && A && B && C, "k_dgemm arguments");
+    launch_gemm_single(make_gemm(transA ? 1 : 0, transB ? 1 : 0, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc),
+                       (cudaStream_t)stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return 0;
+}
+
+int hicma_tlr_k_potrf(hicma_tlr_ctx *c, int n, double *d_A, int lda, double *d_linv, int *d_info, int info_offset) {
+    ARG_CHECK(c && d_A && n > 0 && lda >= n && d_info, "k_potrf arguments");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    ws_reset(c);
+    TRY(potrf_tile(c, d_A, n, lda, d_linv, n, d_info, info_offset));
+    return ctx_sync(c);
+}
+
+int hicma_tlr_k_lr_update(hicma_tlr_ctx *c, int nb, const double *d_Au, const double *d_Av, int ra,
+                          const double *d_Bu, const double *d_Bv, int rb, double *d_Cu, double *d_Cv, int *rc,
+                          double acc, int maxrank, int fixed_rank) {
+    ARG_CHECK(c && rc && d_Cu && d_Cv && nb > 0, "k_lr_update arguments");
+    ARG_CHECK(ra >= 0 && rb >= 0 && *rc >= 0 && maxrank >= 1, "ranks");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    ws_reset(c);
+    int *d_r = ws_alloc<int>(c, 2);
+    if (!d_r) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
+    std::vector<RecompTask> v{RecompTask{d_Cu, d_Cv, *rc, d_Au, d_Av, ra, d_Bu, d_Bv, rb, d_Cu, d_Cv, d_r}};
+    CUDA_TRY(cudaMemsetAsync(c->d_flags + 1, 0, sizeof(int), c->stream));
+    TRY(run_recompress(c, nb, v, acc, maxrank, fixed_rank, d_r + 1, c->precision == HICMA_TLR_PREC_MIXED));
+    int r = 0;
+    CUDA_TRY(cudaMemcpyAsync(&r, d_r, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    TRY(ctx_sync(c));
+    *rc = r;
+    ws_reset(c);
+    return 0;
+}
+
+int hicma_tlr_k_compress(hicma_tlr_ctx *c, int nb, const double *d_A, double *d_U, double *d_V, int maxrank,
+                         double tol, int *rank) {
+    ARG_CHECK(c && d_A && d_U && d_V && rank && nb > 0 && maxrank >= 1 && tol > 0, "k_compress arguments");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    ws_reset(c);
+    const int s = std::min(maxrank + 10, nb);
+    double *Omega = ws_alloc<double>(c, (size_t)nb * s);
+    double *Ident = ws_alloc<double>(c, (size_t)s * s);
+    int *d_r = ws_alloc<int>(c, 2);
+    if (!Omega || !Ident || !d_r) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
+    launch_gaussian(Omega, nb, s, nb, 0x5DEECE66Dull, c->stream);
+    launch_set_identity(Ident, s, s, c->stream);
+    std::vector<CompressTask> v{CompressTask{d_A, d_U, d_V, d_r}};
+    TRY(run_compress(c, nb, maxrank, tol, Omega, s, v, Ident, d_r + 1));
+    int r = 0;
+    CUDA_TRY(cudaMemcpyAsync(&r, d_r, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    TRY(ctx_sync(c));
+    *rank = r;
+    ws_reset(c);
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,146 @@
+// Internal declarations of the B200 TLR engine: batched task descriptors and
+// the host-side launchers of every kernel.  Column-major FP64 throughout.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "../../include/hicma_tlr.h"
+
+namespace tlr {
+
+// ----------------------------------------------------------- batched DGEMM --
+// One problem of a batched C = alpha op(A) op(B) + beta C.  Tiles of 64x64
+// outputs are flattened over the batch with tile_off (prefix sums).
+struct GemmTask {
+    const double *A;
+    const double *B;
+    double *C;
+    int m, n, k;
+    int lda, ldb, ldc;
+    int opA, opB;       // 0 = N, 1 = T
+    int lower;          // skip output tiles strictly above the diagonal
+    int tiles_m;        // ceil(m / 64)
+    double alpha, beta;
+};
+
+// Single-precision variant used by the mixed-precision policy: operands are
+// FP64 in memory, products are formed in FP32 with FP32 accumulation and the
+// result is written back in FP64.
+void launch_gemm_batched(const GemmTask *d_tasks, const int *d_tile_off, int ntasks,
+                         int total_tiles, cudaStream_t st, bool fp32 = false);
+void launch_gemm_single(const GemmTask &t, cudaStream_t st);
+
+inline int gemm_tiles_m(int m) { return (m + 63) / 64; }
+inline int gemm_tiles(const GemmTask &t) { return gemm_tiles_m(t.m) * gemm_tiles_m(t.n); }
+inline GemmTask make_gemm(int opA, int opB, int m, int n, int k, double alpha, const double *A,
+                          int lda, const double *B, int ldb, double beta, double *C, int ldc,
+                          int lower = 0) {
+    GemmTask t;
+    t.A = A; t.B = B; t.C = C;
+    t.m = m; t.n = n; t.k = k;
+    t.lda = lda; t.ldb = ldb; t.ldc = ldc;
+    t.opA = opA; t.opB = opB; t.lower = lower;
+    t.tiles_m = gemm_tiles_m(m);
+    t.alpha = alpha; t.beta = beta;
+    return t;
+}
+
+// ------------------------------------------------------------ generation ----
+struct CovTask {
+    double *out;
+    int ld;
+    int r0, c0;     // global row / column offsets
+    int nr, nc;
+};
+struct CovParams {
+    const double *pts;  // [ndim][N]
+    int N, ndim, kind;
+    double beta, sigma, noise;
+};
+void launch_cov_batched(const CovParams &p, const CovTask *d_tasks, int ntasks, int max_nr,
+                        int max_nc, cudaStream_t st);
+// Gaussian N(0,1) matrix (counter based, seeded), column-major rows x cols.
+void launch_gaussian(double *out, int rows, int cols, int ld, unsigned long long seed,
+                     cudaStream_t st);
+
+// --------------------------------------------------------------- copies -----
+struct CopyTask {
+    const double *src;
+    double *dst;
+    int lds, ldd;
+    int rows, cols;
+    double alpha;
+};
+void launch_copy_batched(const CopyTask *d_tasks, int ntasks, int max_cols, cudaStream_t st);
+void launch_zero_upper(double *A, int n, int lda, cudaStream_t st);
+void launch_set_identity(double *A, int n, int lda, cudaStream_t st);
+
+// ---------------------------------------------------------------- POTRF -----
+// Factor the jb x jb diagonal block at A (lda) in place (lower), write its
+// inverse into Dinv (ldd); on failure set *info = info_base + j + 1 once.
+void launch_potrf_diag(double *A, int lda, int jb, double *Dinv, int ldd, int *info,
+                       int info_base, cudaStream_t st);
+
+// --------------------------------------------------------- tall-skinny QR ---
+// Blocked Householder QR of an m x K matrix X (ld), one CTA per task.  X is
+// overwritten by R (upper) and the reflectors (below the diagonal); tau[K]
+// and the block-reflector T factors (ceil(K/PB) blocks of PB x PB) are
+// written.  PB is chosen from m by qr_panel_width().
+struct QRTask {
+    double *X;
+    double *tau;
+    double *T;
+    int m, K, ld;
+};
+int qr_panel_width(int m);
+size_t qr_smem_bytes(int m);
+void launch_qr_batched(const QRTask *d_tasks, int ntasks, int m_max, cudaStream_t st);
+
+// out (m x r, ldo) = Q [S; 0] with Q from a QRTask factorisation and S K x r
+// (lds).  r is read from *r_dev (device) at run time, capped by r_cap.
+struct QApplyTask {
+    const double *X;
+    const double *T;
+    const double *S;
+    double *out;
+    const int *r_dev;
+    int m, K, ld, lds, ldo;
+    int r_cap;
+};
+void launch_qapply_batched(const QApplyTask *d_tasks, int ntasks, int m_max, cudaStream_t st);
+
+// ------------------------------------------------------------- core SVD -----
+// M = RU RV^T (RU, RV: K x K upper from the QRs; RU == nullptr means I),
+// one-sided Jacobi SVD, truncation and outputs SU = U_r, SV = V_r Sigma_r
+// (K x r each, ld K).  mode 0: absolute sigma >= tol (recompression);
+// mode 1: relative Frobenius tol (generation, with reject rules).
+struct CoreTask {
+    const double *RU;
+    const double *RV;
+    double *SU;
+    double *SV;
+    double *work;        // 2*K*K doubles when K > core_smem_kmax()
+    int *rank_out;       // rank map entry (may be null)
+    int *rank_task;      // per-task rank for the Q-apply step
+    int K, ldru, ldrv;
+};
+struct CoreParams {
+    int mode;
+    double tol;
+    int maxrank;
+    int fixed_rank;
+    int nb;              // tile size (generation reject rule r >= nb/2)
+    int *overflow;       // device counter of capped recompressions
+};
+int core_smem_kmax();
+void launch_core_svd_batched(const CoreTask *d_tasks, int ntasks, int kmax, const CoreParams &p,
+                             cudaStream_t st);
+
+// ---------------------------------------------------------------- misc ------
+// sum of 2*log(diag) over n diagonal entries of ntiles tiles, into *out
+void launch_logdiag_sum(const double *const *d_tiles, int ntiles, int n, int ld, double *out,
+                        cudaStream_t st);
+
+// Device-side helpers for pointer arrays are built by the host engine.
+}  // namespace tlr

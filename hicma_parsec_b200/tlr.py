@@ -1,0 +1,346 @@
+"""Python binding of the C ABI (``include/hicma_tlr.h``) through ctypes.
+
+The classes mirror the reference's operator surface for the factorization
+path: ``STARSH_gen`` (hicma_parsec/hicma_parsec.h:187-198), ``HiCMA_dpotrf_L``
+(hicma_parsec.h:38-56), ``parsec_band_size_auto_tuning`` (hicma_parsec.h:111-115),
+``parsec_band_regenerate`` (hicma_parsec.h:94-100), ``parsec_rank_gather``
+(hicma_parsec.h:124-127), ``HICMA_get_stat2`` (hicma_internal.c:52-71) and
+``STARSH_check`` (hicma_parsec.h:162-169), plus the log-determinant / solve /
+log-likelihood additions.  Every call goes to the CUDA library; there is no
+CPU fallback: if the library is missing this module raises on import of the
+library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libhicma_tlr.so")
+
+LOWER = 122
+UPPER = 121
+KIND_SQEXP_2D, KIND_SQEXP_3D, KIND_EXP_3D = 2, 3, 4
+KIND_NDIM = {2: 2, 3: 3, 4: 3}
+PREC_FP64, PREC_MIXED = 0, 1
+ERR_ARG, ERR_CUDA, ERR_OOM, ERR_RANK_OVERFLOW, ERR_TIMEOUT, ERR_STATE, ERR_NOT_SUPPORTED = -1, -2, -3, -4, -5, -6, -7
+
+_lib = None
+
+
+class TLRError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where} failed with code {code}: {msg}")
+        self.code = code
+
+
+class CProblem(C.Structure):
+    _fields_ = [("kind", C.c_int), ("beta", C.c_double), ("nu", C.c_double), ("noise", C.c_double),
+                ("sigma", C.c_double), ("seed", C.c_ulonglong)]
+
+
+@dataclass
+class Problem:
+    """STARS-H spatial-statistics problem (``starsh_ssdata_generate`` arguments,
+    hicma_parsec/testing_dpotrf.c:300-358; defaults of the reference)."""
+    kind: int = KIND_SQEXP_2D
+    beta: float = 0.1
+    nu: float = 0.5
+    noise: float = 0.1
+    sigma: float = 1.0
+    seed: int = 0
+
+    @property
+    def ndim(self) -> int:
+        return KIND_NDIM[self.kind]
+
+    def c(self) -> CProblem:
+        return CProblem(self.kind, self.beta, self.nu, self.noise, self.sigma, self.seed)
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def load_library(path: str | None = None):
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise RuntimeError(f"CUDA library not built: {path} (run python -m hicma_parsec_b200.build)")
+    lib = C.CDLL(path)
+    vp, i, d, ip, dp, ul = C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_int), C.POINTER(C.c_double), C.POINTER(C.c_ulong)
+    sig = {
+        "hicma_tlr_init": (i, [i, C.c_size_t, C.POINTER(vp)]),
+        "hicma_tlr_fini": (i, [vp]),
+        "hicma_tlr_stream": (vp, [vp]),
+        "hicma_tlr_last_error": (C.c_char_p, []),
+        "hicma_tlr_desc_create": (i, [vp, i, i, i, i, C.POINTER(vp)]),
+        "hicma_tlr_desc_destroy": (i, [vp]),
+        "hicma_tlr_desc_info": (i, [vp, ip, ip, ip, ip, ip]),
+        "hicma_tlr_desc_copy": (i, [vp, vp, vp]),
+        "hicma_tlr_points": (i, [C.POINTER(CProblem), i, vp]),
+        "hicma_tlr_generate": (i, [vp, i, vp, vp, C.POINTER(CProblem), vp, d, i, i, i, ip]),
+        "hicma_tlr_rank_gather": (i, [vp, vp, vp, i]),
+        "hicma_tlr_rank_stat": (i, [vp, i, i, ip, ip, dp]),
+        "hicma_tlr_band_autotune": (i, [vp, i, i, i]),
+        "hicma_tlr_band_regenerate": (i, [vp, i, vp, C.POINTER(CProblem), i]),
+        "hicma_tlr_dpotrf_L": (i, [vp, i, vp, vp, d, i, i, ip, i, i, i, i, ip, vp, vp, vp, i]),
+        "hicma_tlr_set_precision": (i, [vp, i]),
+        "hicma_tlr_dpotrf_L_start": (i, [vp, vp, d, i, i]),
+        "hicma_tlr_dpotrf_L_wait": (i, [vp, vp, vp]),
+        "hicma_tlr_uncompress": (i, [vp, vp, vp, C.c_long]),
+        "hicma_tlr_tile_get": (i, [vp, vp, i, i, vp, ip]),
+        "hicma_tlr_tile_set": (i, [vp, vp, i, i, vp, i]),
+        "hicma_tlr_store_bytes": (i, [vp, vp, C.POINTER(C.c_size_t)]),
+        "hicma_tlr_store_get": (i, [vp, vp, vp, vp]),
+        "hicma_tlr_store_set": (i, [vp, vp, vp, vp]),
+        "hicma_tlr_logdet": (i, [vp, vp, dp]),
+        "hicma_tlr_solve": (i, [vp, vp, i, vp, C.c_long]),
+        "hicma_tlr_loglik": (i, [vp, vp, vp, dp, dp, vp]),
+        "hicma_tlr_last_stats": (i, [vp, vp, i]),
+        "hicma_tlr_k_cov": (i, [C.POINTER(CProblem), vp, i, i, i, i, i, vp, i, vp]),
+        "hicma_tlr_k_dgemm": (i, [i, i, i, i, i, d, vp, i, vp, i, d, vp, i, vp]),
+        "hicma_tlr_k_potrf": (i, [vp, i, vp, i, vp, vp, i]),
+        "hicma_tlr_k_lr_update": (i, [vp, i, vp, vp, i, vp, vp, i, vp, vp, ip, d, i, i]),
+        "hicma_tlr_k_compress": (i, [vp, i, vp, vp, vp, i, d, ip]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load_library().hicma_tlr_last_error().decode()
+
+
+def _check(code: int, where: str) -> int:
+    if code < 0:
+        raise TLRError(code, where, last_error())
+    return code
+
+
+def points(prob: Problem, n: int) -> np.ndarray:
+    """Points [ndim][n] of the problem (host generator of the library)."""
+    lib = load_library()
+    out = np.empty((prob.ndim, n), dtype=np.float64)
+    cp = prob.c()
+    _check(lib.hicma_tlr_points(C.byref(cp), n, _p(out)), "hicma_tlr_points")
+    return out
+
+
+class Context:
+    """One GPU, one stream, one workspace (setup_parsec / cleanup_parsec)."""
+
+    def __init__(self, device: int = 0, workspace_bytes: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        _check(self.lib.hicma_tlr_init(device, workspace_bytes, C.byref(h)), "hicma_tlr_init")
+        self.h = h
+
+    @property
+    def stream(self) -> int:
+        return self.lib.hicma_tlr_stream(self.h) or 0
+
+    def set_precision(self, prec: int) -> None:
+        _check(self.lib.hicma_tlr_set_precision(self.h, prec), "hicma_tlr_set_precision")
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.hicma_tlr_fini(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class TLRMatrix:
+    """Device tile store: dense band + packed [U, V] off-band tiles + rank map
+    (dcA / dcAr of hicma_parsec/testing_dpotrf.c:418-453)."""
+
+    def __init__(self, ctx: Context, n: int, nb: int, maxrank: int, band_size: int = 1):
+        self.ctx, self.lib = ctx, ctx.lib
+        h = C.c_void_p()
+        _check(self.lib.hicma_tlr_desc_create(ctx.h, n, nb, maxrank, band_size, C.byref(h)), "hicma_tlr_desc_create")
+        self.h = h
+        self.n, self.nb, self.maxrank = n, nb, maxrank
+        self.nt = n // nb
+
+    @property
+    def band_size(self) -> int:
+        b = C.c_int()
+        _check(self.lib.hicma_tlr_desc_info(self.h, None, None, None, None, C.byref(b)), "hicma_tlr_desc_info")
+        return b.value
+
+    def close(self):
+        if self.h:
+            self.lib.hicma_tlr_desc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- generation -----------------------------------------------------
+    def generate(self, prob: Problem, tol: float, maxrank: int | None = None, pts: np.ndarray | None = None) -> int:
+        """STARSH_gen; returns info (0, or -1 when a tile is rejected)."""
+        info = C.c_int(0)
+        cp = prob.c()
+        if pts is not None:
+            pts = np.ascontiguousarray(pts, dtype=np.float64)
+        _check(self.lib.hicma_tlr_generate(self.ctx.h, LOWER, self.h, None, C.byref(cp), _p(pts), tol,
+                                           maxrank or self.maxrank, self.band_size, 0, C.byref(info)),
+               "hicma_tlr_generate")
+        return info.value
+
+    def rank_map(self) -> np.ndarray:
+        G = np.empty(self.nt * self.nt, dtype=np.int32)
+        _check(self.lib.hicma_tlr_rank_gather(self.ctx.h, self.h, _p(G), self.band_size), "hicma_tlr_rank_gather")
+        return G
+
+    def band_regenerate(self, prob: Problem, band_size: int) -> None:
+        cp = prob.c()
+        _check(self.lib.hicma_tlr_band_regenerate(self.ctx.h, LOWER, self.h, C.byref(cp), band_size),
+               "hicma_tlr_band_regenerate")
+
+    # --- factorization --------------------------------------------------
+    def potrf(self, acc: float, maxrank: int | None = None, fixed_rank: int = 0, lookahead: int = -1,
+              want_counters: bool = False, verbose: int = 0):
+        """HiCMA_dpotrf_L; returns info (and op counters when asked)."""
+        la = C.c_int(lookahead)
+        two = C.c_int(0)
+        tiles = np.zeros(self.nt * self.nt, dtype=np.uint64) if want_counters else None
+        ops = np.zeros(1, dtype=np.uint64) if want_counters else None
+        cpt = np.zeros(6, dtype=np.float64)
+        mr = maxrank or self.maxrank
+        info = _check(self.lib.hicma_tlr_dpotrf_L(self.ctx.h, LOWER, self.h, None, acc, fixed_rank, mr,
+                                                  C.byref(la), self.band_size, self.nb, mr, 0, C.byref(two),
+                                                  _p(tiles), _p(ops), _p(cpt), verbose), "hicma_tlr_dpotrf_L")
+        if want_counters:
+            return info, tiles.reshape(self.nt, self.nt), int(ops[0]), cpt
+        return info
+
+    def stats(self) -> np.ndarray:
+        s = np.zeros(8)
+        _check(self.lib.hicma_tlr_last_stats(self.h, _p(s), 8), "hicma_tlr_last_stats")
+        return s
+
+    def copy_from(self, other: "TLRMatrix") -> None:
+        _check(self.lib.hicma_tlr_desc_copy(self.ctx.h, other.h, self.h), "hicma_tlr_desc_copy")
+
+    # --- results --------------------------------------------------------
+    def uncompress(self) -> np.ndarray:
+        D = np.empty((self.n, self.n), dtype=np.float64, order="F")
+        _check(self.lib.hicma_tlr_uncompress(self.ctx.h, self.h, _p(D), self.n), "hicma_tlr_uncompress")
+        return D
+
+    def tile(self, m: int, n: int):
+        r = C.c_int()
+        _check(self.lib.hicma_tlr_tile_get(self.ctx.h, self.h, m, n, None, C.byref(r)), "hicma_tlr_tile_get")
+        if r.value < 0:
+            buf = np.empty((self.nb, self.nb), dtype=np.float64, order="F")
+            _check(self.lib.hicma_tlr_tile_get(self.ctx.h, self.h, m, n, _p(buf), C.byref(r)), "hicma_tlr_tile_get")
+            return buf
+        buf = np.empty((self.nb, 2 * r.value), dtype=np.float64, order="F")
+        _check(self.lib.hicma_tlr_tile_get(self.ctx.h, self.h, m, n, _p(buf), C.byref(r)), "hicma_tlr_tile_get")
+        return buf[:, :r.value], buf[:, r.value:]
+
+    def set_tile(self, m: int, n: int, data) -> None:
+        if isinstance(data, tuple):
+            U, V = data
+            buf = np.asfortranarray(np.hstack([U, V]), dtype=np.float64)
+            r = U.shape[1]
+        else:
+            buf = np.asfortranarray(data, dtype=np.float64)
+            r = -1
+        _check(self.lib.hicma_tlr_tile_set(self.ctx.h, self.h, m, n, _p(buf), r), "hicma_tlr_tile_set")
+
+    def store_bytes(self) -> int:
+        b = C.c_size_t()
+        _check(self.lib.hicma_tlr_store_bytes(self.ctx.h, self.h, C.byref(b)), "hicma_tlr_store_bytes")
+        return b.value
+
+    def store_get(self, buf_ptr: int, ranks: np.ndarray | None = None) -> None:
+        _check(self.lib.hicma_tlr_store_get(self.ctx.h, self.h, C.c_void_p(buf_ptr), _p(ranks)), "hicma_tlr_store_get")
+
+    def store_set(self, buf_ptr: int, ranks: np.ndarray) -> None:
+        _check(self.lib.hicma_tlr_store_set(self.ctx.h, self.h, C.c_void_p(buf_ptr), _p(ranks)), "hicma_tlr_store_set")
+
+    def logdet(self) -> float:
+        v = C.c_double()
+        _check(self.lib.hicma_tlr_logdet(self.ctx.h, self.h, C.byref(v)), "hicma_tlr_logdet")
+        return v.value
+
+    def solve(self, b: np.ndarray) -> np.ndarray:
+        X = np.asfortranarray(np.array(b, dtype=np.float64, copy=True).reshape(self.n, -1))
+        _check(self.lib.hicma_tlr_solve(self.ctx.h, self.h, X.shape[1], _p(X), self.n), "hicma_tlr_solve")
+        return X[:, 0] if np.ndim(b) == 1 else X
+
+    def loglik(self, y: np.ndarray):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        ll, ld = C.c_double(), C.c_double()
+        x = np.empty(self.n)
+        _check(self.lib.hicma_tlr_loglik(self.ctx.h, self.h, _p(y), C.byref(ll), C.byref(ld), _p(x)), "hicma_tlr_loglik")
+        return ll.value, ld.value, x
+
+
+# ---------------------------------------------------------------------------
+# Reference-named entry points (same argument meaning and error behaviour,
+# except that argument errors raise instead of returning 0 silently).
+# ---------------------------------------------------------------------------
+def STARSH_gen(ctx: Context, uplo: int, A: TLRMatrix, prob: Problem, tol: float, maxrank: int,
+               band_size: int, send_full_tile: int = 0) -> int:
+    if uplo != LOWER:
+        raise TLRError(ERR_NOT_SUPPORTED, "STARSH_gen", "only dplasmaLower")
+    if band_size != A.band_size:
+        raise TLRError(ERR_ARG, "STARSH_gen", "band_size differs from the descriptor")
+    return A.generate(prob, tol, maxrank)
+
+
+def HiCMA_dpotrf_L(ctx: Context, uplo: int, A: TLRMatrix, acc: float, fixed_rank: int, maxrank: int,
+                   lookahead: int = -1, band_size: int | None = None, hmb: int = 300, compmaxrank: int = 0,
+                   send_full_tile: int = 0, verbose: int = 0):
+    """Returns (info, tileopcounters NT x NT, total opcount, critical_path_time[6])."""
+    lib = ctx.lib
+    la = C.c_int(lookahead)
+    two = C.c_int(0)
+    tiles = np.zeros(A.nt * A.nt, dtype=np.uint64)
+    ops = np.zeros(1, dtype=np.uint64)
+    cpt = np.zeros(6)
+    info = _check(lib.hicma_tlr_dpotrf_L(ctx.h, uplo, A.h, None, acc, fixed_rank, maxrank, C.byref(la),
+                                         A.band_size if band_size is None else band_size, hmb,
+                                         compmaxrank or maxrank, send_full_tile, C.byref(two), _p(tiles), _p(ops),
+                                         _p(cpt), verbose), "HiCMA_dpotrf_L")
+    return info, tiles.reshape(A.nt, A.nt), int(ops[0]), cpt
+
+
+def parsec_band_size_auto_tuning(rank_array: np.ndarray, nt: int, nb: int, verbose: int = 0) -> int:
+    G = np.ascontiguousarray(rank_array, dtype=np.int32)
+    return _check(load_library().hicma_tlr_band_autotune(_p(G), nt, nb, verbose), "band_autotune")
+
+
+def HICMA_get_stat2(rank_array: np.ndarray, nt: int, band_size: int):
+    G = np.ascontiguousarray(rank_array, dtype=np.int32)
+    mn, mx, av = C.c_int(), C.c_int(), C.c_double()
+    _check(load_library().hicma_tlr_rank_stat(_p(G), nt, band_size, C.byref(mn), C.byref(mx), C.byref(av)),
+           "HICMA_get_stat2")
+    return mn.value, mx.value, av.value

@@ -1,0 +1,231 @@
+/*
+ * hicma_tlr.h -- C ABI of the B200 tile-low-rank (TLR) Cholesky engine.
+ *
+ * This is the drop-in boundary for HiCMA-PaRSEC's factorization path.  Every
+ * entry point below names the reference interface it replaces (paths are
+ * relative to the reference project root).  Plain C types only: opaque
+ * handles, pointers and sizes.  All device work runs on the CUDA stream owned
+ * by the context; calls return after the work is complete unless stated.
+ *
+ * Storage conventions (shared with the reference):
+ *   - tiles are NB x NB, column-major, ld = NB (BLKLDD);
+ *   - a tile (m, n) with m - n < band_size is dense; an off-band tile is the
+ *     packed pair [U, V] (U: NB x r at offset 0, V: NB x r at offset NB*r) with
+ *     A(m, n) ~= U V^T (hicma_parsec/HiCMA_dpotrf_L_2flow.jdf:386,518-519);
+ *   - the rank map is an NT x NT column-major int array, entry n*NT + m for
+ *     tile (m, n), -1 on the band (hicma_parsec/testing_dpotrf.c:441-453).
+ *   - U has orthonormal columns; V carries the singular values.
+ *
+ * Return codes: 0 on success; > 0 is the reference's Cholesky INFO
+ * (k*NB + i, the order of the first leading minor that is not positive
+ * definite, hicma_parsec/HiCMA_dpotrf_L_2flow.jdf:241-242); < 0 is one of
+ * the HICMA_TLR_ERR_* codes below.  Unlike the reference (which returns a NULL
+ * taskpool and then 0, hicma_parsec/hicma_parsec.c:595), argument errors are
+ * reported as HICMA_TLR_ERR_ARG.
+ */
+#ifndef HICMA_TLR_H
+#define HICMA_TLR_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HICMA_TLR_SUCCESS              0
+#define HICMA_TLR_ERR_ARG             -1  /* invalid argument                        */
+#define HICMA_TLR_ERR_CUDA            -2  /* CUDA runtime error                      */
+#define HICMA_TLR_ERR_OOM             -3  /* device memory exhausted                 */
+#define HICMA_TLR_ERR_RANK_OVERFLOW   -4  /* a tile needs a rank above maxrank
+                                             (STARS-H INFO=-1, STARSH_gen.jdf:169-171) */
+#define HICMA_TLR_ERR_TIMEOUT         -5  /* a bounded device wait gave up           */
+#define HICMA_TLR_ERR_STATE           -6  /* call out of order (e.g. solve before factor) */
+#define HICMA_TLR_ERR_NOT_SUPPORTED   -7  /* e.g. uplo = Upper, N % NB != 0          */
+
+/* uplo values of DPLASMA (dplasmaUpper / dplasmaLower). */
+#define HICMA_TLR_UPPER 121
+#define HICMA_TLR_LOWER 122
+
+/* -D problem kinds (hicma_parsec/testing_dpotrf.c:12, :336-358). */
+#define HICMA_TLR_KIND_SQEXP_2D 2
+#define HICMA_TLR_KIND_SQEXP_3D 3
+#define HICMA_TLR_KIND_EXP_3D   4
+
+/* Precision policy of the factorization (north-star addition). */
+#define HICMA_TLR_PREC_FP64   0   /* everything in FP64                              */
+#define HICMA_TLR_PREC_MIXED  1   /* off-band low-rank products of small-norm tiles in
+                                     FP32; band, diagonal and truncation stay FP64     */
+
+typedef struct hicma_tlr_ctx_s  hicma_tlr_ctx;   /* device, stream, workspace      */
+typedef struct hicma_tlr_desc_s hicma_tlr_desc;  /* device tile store of a matrix */
+
+/* STARS-H spatial-statistics problem (starsh_ssdata_generate arguments,
+ * hicma_parsec/testing_dpotrf.c:300-358). */
+typedef struct {
+    int    kind;      /* HICMA_TLR_KIND_*                                   */
+    double beta;      /* length scale (reference default 0.1)               */
+    double nu;        /* smoothness, unused by sqexp/exp (default 0.5)      */
+    double noise;     /* nugget added on the diagonal (reference 0.1)       */
+    double sigma;     /* variance (default 1.0)                             */
+    unsigned long long seed;  /* point placement seed (reference srand(0)) */
+} hicma_tlr_problem;
+
+/* ---------------------------------------------------------------- setup -- */
+
+/* setup_parsec / cleanup_parsec (hicma_parsec/hicma_parsec.h:201-204).
+ * workspace_bytes = 0 picks a default sized from free device memory. */
+int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **ctx);
+int hicma_tlr_fini(hicma_tlr_ctx *ctx);
+/* The CUDA stream (cudaStream_t) the context launches on. */
+void *hicma_tlr_stream(hicma_tlr_ctx *ctx);
+/* Last error message of this thread ("" if none). */
+const char *hicma_tlr_last_error(void);
+
+/* Descriptor = dcA (band + off-band) + dcAr of hicma_parsec/testing_dpotrf.c:418-453.
+ * Off-band tiles get fixed slots of capacity maxrank columns for U and V. */
+int hicma_tlr_desc_create(hicma_tlr_ctx *ctx, int N, int NB, int maxrank, int band_size,
+                          hicma_tlr_desc **A);
+int hicma_tlr_desc_destroy(hicma_tlr_desc *A);
+int hicma_tlr_desc_info(const hicma_tlr_desc *A, int *N, int *NB, int *NT, int *maxrank,
+                        int *band_size);
+/* Device-to-device copy of all tiles and ranks (same shape required). */
+int hicma_tlr_desc_copy(hicma_tlr_ctx *ctx, const hicma_tlr_desc *src, hicma_tlr_desc *dst);
+
+/* ----------------------------------------------------------- generation -- */
+
+/* Points of the problem (starsh_ssdata_generate, testing_dpotrf.c:305-312,
+ * 336-358): jittered grid, Morton order.  points is [ndim][N] (SoA). */
+int hicma_tlr_points(const hicma_tlr_problem *prob, int N, double *points);
+
+/* STARSH_gen (hicma_parsec/hicma_parsec.h:187-198; STARSH_gen.jdf:342-369):
+ * band tiles dense, off-band tiles compressed to tolerance tol and at most
+ * maxrank columns.  points may be NULL (then hicma_tlr_points is used).
+ * Ar (host, NT*NT, may be NULL) receives the rank map.  *info = -1 when a
+ * tile is rejected (STARSH_gen.jdf:169-171). */
+int hicma_tlr_generate(hicma_tlr_ctx *ctx, int uplo, hicma_tlr_desc *A, int *Ar,
+                       const hicma_tlr_problem *prob, const double *points,
+                       double tol, int maxrank, int band_size, int send_full_tile,
+                       int *info);
+
+/* parsec_rank_gather (hicma_parsec.h:124-127): device rank map -> host. */
+int hicma_tlr_rank_gather(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, int *rank_array, int band_size);
+
+/* HICMA_get_stat2 (hicma_parsec/hicma_internal.c:52-71). */
+int hicma_tlr_rank_stat(const int *rank_array, int NT, int band_size, int *minrk, int *maxrk,
+                        double *avgrk);
+
+/* parsec_band_size_auto_tuning (hicma_parsec.h:111-115;
+ * band_size_auto_tuning.jdf:201-318).  Returns the tuned band size. */
+int hicma_tlr_band_autotune(const int *rank_array, int NT, int NB, int verbose);
+
+/* parsec_band_regenerate (hicma_parsec.h:94-100; band_regenerate.jdf:124-143):
+ * switch the descriptor to band_size and regenerate the dense band tiles. */
+int hicma_tlr_band_regenerate(hicma_tlr_ctx *ctx, int uplo, hicma_tlr_desc *A,
+                              const hicma_tlr_problem *prob, int band_size);
+
+/* --------------------------------------------------------- factorization -- */
+
+/* HiCMA_dpotrf_L (hicma_parsec/hicma_parsec.h:38-56; hicma_parsec.c:463-646).
+ * Lower TLR Cholesky in place.  Ar (host, may be NULL) receives the final
+ * rank map.  tileopcounters (NT*NT) and opcounters (>= 1) are incremented
+ * with the reference's op_counts model (hicma_parsec/op_counts.h).
+ * critical_path_time[6] receives seconds spent in POTRF, TRSM and SYRK of the
+ * panel critical path, then total factorization, TRSM+SYRK+GEMM of all
+ * panels and the recompression share.  hmb is accepted and ignored (the
+ * recursive sub-tiling of the reference is replaced by multi-CTA kernels).
+ * Returns the reference's info (0, k*NB+i) or a negative error code. */
+int hicma_tlr_dpotrf_L(hicma_tlr_ctx *ctx, int uplo, hicma_tlr_desc *A, int *Ar,
+                       double acc, int fixed_rank, int maxrank, int *lookahead,
+                       int band_size, int hmb, int compmaxrank, int send_full_tile,
+                       int *two_flow, unsigned long *tileopcounters,
+                       unsigned long *opcounters, double *critical_path_time, int verbose);
+
+/* Precision policy for later hicma_tlr_dpotrf_L calls on this context. */
+int hicma_tlr_set_precision(hicma_tlr_ctx *ctx, int precision);
+
+/* Asynchronous form (HiCMA_dpotrf_L_2flow_New / _Destruct,
+ * hicma_parsec/hicma_parsec_internal.h:295-315): _start enqueues, _wait
+ * completes and returns the info. */
+int hicma_tlr_dpotrf_L_start(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, double acc, int fixed_rank,
+                             int maxrank);
+int hicma_tlr_dpotrf_L_wait(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, int *Ar);
+
+/* ------------------------------------------------------ check / results -- */
+
+/* STARSH_check (hicma_parsec.h:162-169; STARSH_check.jdf:90-143): expand the
+ * lower triangle to a dense host N x N column-major matrix (leading dim ld). */
+int hicma_tlr_uncompress(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, double *dense, long ld);
+
+/* Host copy of one tile.  Dense tiles: NB*NB doubles.  Low-rank tiles: the
+ * reference's packed [U, V] (2*NB*rank doubles); *rank receives the rank
+ * (-1 for dense tiles).  buf may be NULL to query the rank only. */
+int hicma_tlr_tile_get(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, int m, int n, double *buf,
+                       int *rank);
+int hicma_tlr_tile_set(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, int m, int n, const double *buf,
+                       int rank);
+
+/* Whole-matrix host <-> device transfer in the reference's layout: all band
+ * tiles (row m, then n = m-band+1..m) followed by the packed [U,V] of every
+ * off-band tile (row m, then n = 0..m-band), each packed with its own rank.
+ * bytes_needed returns the buffer size for the current ranks. */
+int hicma_tlr_store_bytes(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, size_t *bytes_needed);
+int hicma_tlr_store_get(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, double *buf, int *Ar);
+int hicma_tlr_store_set(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, const double *buf, const int *Ar);
+
+/* North-star additions (no reference counterpart; testing_dpotrf.c stops at
+ * the factor).  Require a factored descriptor. */
+int hicma_tlr_logdet(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, double *logdet);
+/* Solve A X = B in place; B is host N x nrhs column-major (leading dim ldb). */
+int hicma_tlr_solve(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, int nrhs, double *B, long ldb);
+/* Gaussian log-likelihood -1/2 (y^T A^-1 y + log det A + N log 2 pi). */
+int hicma_tlr_loglik(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, const double *y, double *loglik,
+                     double *logdet, double *x);
+
+/* Statistics of the last factorization on A: [0] seconds, [1] TLR flops
+ * (op_counts model), [2] recompressions capped at maxrank, [3] number of
+ * launches of library kernels, [4] POTRF s, [5] TRSM s, [6] SYRK s,
+ * [7] GEMM/recompression s. */
+int hicma_tlr_last_stats(hicma_tlr_desc *A, double *stats, int nstats);
+
+/* ------------------------------------------- kernel-level entry points -- */
+/* Device pointers; used by the parity tests and by callers that manage their
+ * own memory.  stream may be NULL for the context stream.  These replace the
+ * per-tile bodies of the reference's task classes. */
+
+/* STARS-H block kernel (call shape of STARSH_gen.jdf:70-72): out[nr x nc],
+ * ld, of global rows r0.., cols c0.. from device points [ndim][N]. */
+int hicma_tlr_k_cov(const hicma_tlr_problem *prob, const double *d_points, int N, int r0,
+                    int nr, int c0, int nc, double *d_out, int ld, void *stream);
+
+/* C = alpha op(A) op(B) + beta C on the FP64 tensor cores (CORE_dgemm). */
+int hicma_tlr_k_dgemm(int transA, int transB, int m, int n, int k, double alpha,
+                      const double *d_A, int lda, const double *d_B, int ldb, double beta,
+                      double *d_C, int ldc, void *stream);
+
+/* Lower Cholesky of an n x n tile in place (HCORE_dpotrf,
+ * HiCMA_dpotrf_L_2flow.jdf:233); *d_info (device int) gets the 1-based
+ * order of the first failing minor plus info_offset.  d_linv (n x n, may be
+ * NULL) receives L^-1.  Uses ctx workspace. */
+int hicma_tlr_k_potrf(hicma_tlr_ctx *ctx, int n, double *d_A, int lda, double *d_linv,
+                      int *d_info, int info_offset);
+
+/* Low-rank GEMM update with recompression of one tile
+ * (HCORE_dgemm_qr_svd + HCORE_dgemm_ormqr, HiCMA_dpotrf_L_2flow.jdf:985-1058):
+ * C = Cu Cv^T - Au (Bu (Bv^T Av))^T recompressed to absolute accuracy acc,
+ * rank capped at maxrank.  If d_Bv is NULL, B is dense NB x NB in d_Bu
+ * (HCORE_dgemm_qr_svd_b_dense, :830-903).  d_Cu/d_Cv have capacity maxrank
+ * columns; *rc (host) is updated.  Returns 0 or an error code. */
+int hicma_tlr_k_lr_update(hicma_tlr_ctx *ctx, int nb, const double *d_Au, const double *d_Av,
+                          int ra, const double *d_Bu, const double *d_Bv, int rb, double *d_Cu,
+                          double *d_Cv, int *rc, double acc, int maxrank, int fixed_rank);
+
+/* Compress a dense nb x nb tile (starsh_dense_dlrrsdd, STARSH_gen.jdf:162-163):
+ * randomized range finder with maxrank+10 samples, relative Frobenius
+ * truncation at tol; *rank = -1 when rejected. */
+int hicma_tlr_k_compress(hicma_tlr_ctx *ctx, int nb, const double *d_A, double *d_U, double *d_V,
+                         int maxrank, double tol, int *rank);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HICMA_TLR_H */

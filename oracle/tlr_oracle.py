@@ -1,0 +1,643 @@
+"""CPU oracle for the tile-low-rank (TLR) Cholesky path of HiCMA-PaRSEC.
+
+TEST INFRASTRUCTURE ONLY.  Nothing in the shipped library imports this module:
+only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline legs of
+``bench.py`` use it, and only as the checker (or as the timed CPU restatement).
+
+PARITY UNPINNED.  The arithmetic of the reference lives in three git
+submodules that are empty in the reference tree (``dplasma``, ``hcore``,
+``stars-h``; ``.gitmodules:1-10``) and no commit of them is pinned.  The
+reference ships no golden vectors or known-answer files either (its two CTest
+entries, ``hicma_parsec/CMakeLists.txt:59-62``, only run ``--check`` against a
+dense factorization at run time).  This module therefore restates:
+
+* the task graph, case selection, rank-0 skips and association orders of
+  ``hicma_parsec/HiCMA_dpotrf_L_2flow.jdf`` exactly;
+* the generation graph of ``hicma_parsec/STARSH_gen.jdf`` (band tiles dense,
+  off-band tiles compressed to a packed ``[U, V]`` pair plus a rank);
+* the band auto-tuning rule of ``hicma_parsec/band_size_auto_tuning.jdf``;
+* the flop model of ``hicma_parsec/op_counts.h`` (including its float32 casts);
+* the checks of ``hicma_parsec/testing_dpotrf.c:111-230``;
+
+and restates from their published mathematics the absent third-party pieces:
+
+* STARS-H point placement (jittered grid + Morton order) and the squared
+  exponential / exponential covariance kernels (call sites
+  ``testing_dpotrf.c:336-358``);
+* STARS-H ``starsh_dense_dlrrsdd`` rank rule: the smallest rank whose
+  discarded singular values have Frobenius norm <= tol * (Frobenius norm of the
+  sampled spectrum); a tile is rejected (rank -1, ``STARSH_gen.jdf:169-171``)
+  when that rank is >= min(m, n)/2 or > maxrank;
+* HCORE ``dgemm_qr_svd``/``dgemm_ormqr`` recompression: QR of the stacked
+  ``[Cu, Au]`` and ``[Cv, -Y]``, SVD of ``R_U R_V^T`` and an absolute
+  truncation sigma_i >= acc (or a fixed rank when ``fixed_rank > 0``), capped
+  at the storage maxrank.
+
+Conventions (shared with the CUDA path): a low-rank tile is A(m,n) = U V^T
+with U (NB x r) having orthonormal columns and V (NB x r) carrying the
+singular values.  Rank arrays are column-major NT x NT int arrays,
+``G[n*NT + m]`` for tile (m, n) (``band_size_auto_tuning.jdf:48``).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.linalg as sla
+
+# Problem kinds (``-D``), numbering of ``testing_dpotrf.c:12``.
+KIND_SQEXP_2D = 2
+KIND_SQEXP_3D = 3
+KIND_EXP_3D = 4
+KIND_NAMES = {KIND_SQEXP_2D: "st-2d-sqexp", KIND_SQEXP_3D: "st-3d-sqexp",
+              KIND_EXP_3D: "st-3d-exp"}
+KIND_NDIM = {KIND_SQEXP_2D: 2, KIND_SQEXP_3D: 3, KIND_EXP_3D: 3}
+
+FLUCTUATION = 0.66666667          # hicma_parsec_internal.h:107
+MORTON_BITS = 21
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+# --------------------------------------------------------------------------
+# Points (STARS-H ``STARSH_PARTICLES_UNIFORM`` + Morton sort, restated)
+# --------------------------------------------------------------------------
+def _mix64(x):
+    """splitmix64 finaliser on uint64 arrays (wrapping arithmetic)."""
+    with np.errstate(over="ignore"):
+        z = np.asarray(x, dtype=np.uint64) + _GOLDEN
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform01(seed: int, counters) -> np.ndarray:
+    """Counter-based uniform doubles in [0, 1): 53 high bits of
+    mix64(mix64(seed) + counter)."""
+    base = _mix64(np.array([seed], dtype=np.uint64))[0]
+    with np.errstate(over="ignore"):
+        z = _mix64(base + np.asarray(counters, dtype=np.uint64))
+    return (z >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
+
+
+def grid_side(n: int, ndim: int) -> int:
+    """Smallest s with s**ndim >= n."""
+    s = max(1, int(round(n ** (1.0 / ndim))))
+    while s ** ndim < n:
+        s += 1
+    while s > 1 and (s - 1) ** ndim >= n:
+        s -= 1
+    return s
+
+
+def morton_codes(pts: np.ndarray) -> np.ndarray:
+    ndim = pts.shape[1]
+    q = np.floor(pts * float(1 << MORTON_BITS)).astype(np.int64)
+    q = np.clip(q, 0, (1 << MORTON_BITS) - 1).astype(np.uint64)
+    code = np.zeros(pts.shape[0], dtype=np.uint64)
+    for b in range(MORTON_BITS):
+        for a in range(ndim):
+            code |= ((q[:, a] >> np.uint64(b)) & np.uint64(1)) << np.uint64(b * ndim + a)
+    return code
+
+
+def gen_points(n: int, ndim: int, seed: int = 0) -> np.ndarray:
+    """n points in [0,1]^ndim: a side^ndim grid (side = ceil(n^(1/ndim))),
+    each point jittered uniformly by +/-0.4 of the spacing, Morton-sorted
+    (stable), first n kept.  Returns an (n, ndim) float64 array.
+
+    Restates STARS-H's uniform particle placement called at
+    ``testing_dpotrf.c:336-358`` (seeded by ``srand(0)``, ``:312``); the
+    generator here is a documented counter-based one so that the CUDA host
+    code reproduces it bit for bit.
+    """
+    side = grid_side(n, ndim)
+    total = side ** ndim
+    idx = np.arange(total, dtype=np.int64)
+    pts = np.empty((total, ndim), dtype=np.float64)
+    for a in range(ndim):
+        c = (idx // (side ** a)) % side
+        u = uniform01(seed, idx * ndim + a)
+        pts[:, a] = ((c.astype(np.float64) + 0.1) + 0.8 * u) / float(side)
+    order = np.argsort(morton_codes(pts), kind="stable")
+    return np.ascontiguousarray(pts[order[:n]])
+
+
+# --------------------------------------------------------------------------
+# Covariance kernels (STARS-H ssdata block kernels, restated)
+# --------------------------------------------------------------------------
+@dataclass
+class Problem:
+    kind: int = KIND_SQEXP_2D
+    beta: float = 0.1          # testing_dpotrf.c:303
+    nu: float = 0.5            # testing_dpotrf.c:304 (unused by sqexp/exp)
+    noise: float = 0.1         # testing_dpotrf.c:305 (the reference's nugget)
+    sigma: float = 1.0         # testing_dpotrf.c:306
+    seed: int = 0
+
+    @property
+    def ndim(self) -> int:
+        return KIND_NDIM[self.kind]
+
+
+def cov_block(prob: Problem, pts: np.ndarray, r0: int, nr: int, c0: int, nc: int) -> np.ndarray:
+    """Column-major covariance block A[r0:r0+nr, c0:c0+nc]; the nugget is
+    added where the global row and column indices coincide.  Same call shape
+    as ``kernel(nrows, ncols, irow, icol, data, data, out, ld)``
+    (``STARSH_gen.jdf:70-72``)."""
+    X = pts[r0:r0 + nr]
+    Y = pts[c0:c0 + nc]
+    r2 = np.zeros((nr, nc))
+    for a in range(pts.shape[1]):
+        d = X[:, a][:, None] - Y[:, a][None, :]
+        r2 = r2 + d * d
+    if prob.kind == KIND_EXP_3D:
+        A = prob.sigma * np.exp(-np.sqrt(r2) / prob.beta)
+    else:
+        A = prob.sigma * np.exp(-r2 / (2.0 * prob.beta * prob.beta))
+    lo, hi = max(r0, c0), min(r0 + nr, c0 + nc)
+    if lo < hi:
+        i = np.arange(lo, hi)
+        A[i - r0, i - c0] += prob.noise
+    return A
+
+
+def dense_matrix(prob: Problem, pts: np.ndarray) -> np.ndarray:
+    n = pts.shape[0]
+    return cov_block(prob, pts, 0, n, 0, n)
+
+
+# --------------------------------------------------------------------------
+# op_counts.h restated (integer/float quirks kept)
+# --------------------------------------------------------------------------
+_U64 = (1 << 64) - 1
+
+
+def _f32(x) -> float:
+    return float(np.float32(x))
+
+
+def op_counts(op: str, a: int, b: int, c: int, d: int) -> int:
+    """``op_counts`` of ``hicma_parsec/op_counts.h:10-72`` with unsigned long
+    wrap-around and its float32 casts in the geqrf branch."""
+    if op == "q":
+        m, n = a, b
+        t1 = (2 * m * n * n) & _U64
+        t2 = int(_f32(_f32((2 * n * n * n) & _U64) / np.float32(3.0)))
+        t3 = (2 * m * n) & _U64
+        t4 = int(_f32(_f32((17 * n) & _U64) / np.float32(3.0)))
+        return (t1 - t2 + t3 + t4) & _U64
+    if op == "c":
+        n = a
+        v = float((n * n * n) // 3) - float(n * n) / 2.0 + float(n // 6)
+        return int(v) & _U64
+    if op == "t":
+        m, n, side = a, b, c
+        return (n * m * m) & _U64 if side == 1 else (m * n * n) & _U64
+    if op == "m":
+        return (a * b * c * 2) & _U64
+    if op == "s":
+        return (22 * a * a * a) & _U64
+    if op == "o":
+        m, n, k, side = a, b, c, d
+        if side == 1:
+            return (4 * n * m * k - 2 * n * k * k + 3 * n * k) & _U64
+        return (4 * n * m * k - 2 * m * k * k + 2 * m * k + n * k - (k * k) // 2 + k // 2) & _U64
+    if op == "r":
+        m, n, side = a, b, c
+        return (m * m * n) & _U64 if side == 1 else (m * n * n) & _U64
+    raise ValueError(op)
+
+
+def flops_dpotrf(n: float) -> float:
+    """FLOPS_DPOTRF of ``flops.h:86-87,272`` (dense-equivalent flop count)."""
+    n = float(n)
+    fmuls = n * (((1.0 / 6.0) * n + 0.5) * n + (1.0 / 3.0))
+    fadds = n * (((1.0 / 6.0) * n) * n - (1.0 / 6.0))
+    return fmuls + fadds
+
+
+def gemm_lr_opcount(nb: int, ra: int, rb: int, rc_old: int, rc_new: int, b_dense: bool) -> int:
+    """Op count of a low-rank-C GEMM task, ``HiCMA_dpotrf_L_2flow.jdf:909-924``
+    (B dense) and ``:1076-1092`` (B low rank)."""
+    ka = rc_old + ra
+    qra = op_counts("q", nb, ka, 0, 0)
+    if b_dense:
+        qrb = op_counts("q", nb, ka, 0, 0) + op_counts("m", ra, nb, nb, 0)
+    else:
+        qrb = op_counts("m", ra, rb, nb, 0) + op_counts("m", ra, nb, rb, 0) + op_counts("q", nb, ka, 0, 0)
+    svd = op_counts("r", ka, ka, 2, 0) + op_counts("s", ka, 0, 0, 0) + ka * rc_new
+    newu = op_counts("o", nb, rc_new, ka, 1)
+    newv = op_counts("o", rc_new, nb, ka, 2)
+    return (qra + qrb + svd + newu + newv) & _U64
+
+
+# --------------------------------------------------------------------------
+# TLR matrix
+# --------------------------------------------------------------------------
+@dataclass
+class TLRMatrix:
+    n: int
+    nb: int
+    band: int
+    maxrank: int
+    dense: dict = field(default_factory=dict)   # (m, n) -> NB x NB array
+    U: dict = field(default_factory=dict)       # (m, n) -> NB x r
+    V: dict = field(default_factory=dict)       # (m, n) -> NB x r
+
+    @property
+    def nt(self) -> int:
+        return self.n // self.nb
+
+    def is_dense(self, m: int, n: int) -> bool:
+        return m - n < self.band
+
+    def rank(self, m: int, n: int) -> int:
+        return -1 if self.is_dense(m, n) else self.U[(m, n)].shape[1]
+
+    def rank_array(self) -> np.ndarray:
+        """Column-major NT x NT map, -1 on the band and the upper triangle
+        (``testing_dpotrf.c:450-453``)."""
+        nt = self.nt
+        G = -np.ones(nt * nt, dtype=np.int32)
+        for (m, n), u in self.U.items():
+            G[n * nt + m] = u.shape[1]
+        return G
+
+    def copy(self) -> "TLRMatrix":
+        return TLRMatrix(self.n, self.nb, self.band, self.maxrank,
+                         {k: v.copy() for k, v in self.dense.items()},
+                         {k: v.copy() for k, v in self.U.items()},
+                         {k: v.copy() for k, v in self.V.items()})
+
+
+def truncation_rank_relfro(s: np.ndarray, tol: float) -> int:
+    """Smallest r with ||s[r:]||_2 <= tol * ||s||_2 (restated STARS-H rule)."""
+    s2 = s.astype(np.float64) ** 2
+    total = float(s2.sum())
+    if total == 0.0:
+        return 0
+    thr = tol * tol * total
+    tail = 0.0
+    r = len(s)
+    while r > 0 and tail + s2[r - 1] <= thr:
+        tail += s2[r - 1]
+        r -= 1
+    return r
+
+
+def compress_tile(A: np.ndarray, tol: float, maxrank: int, oversample: int = 10):
+    """Compress one off-band tile (``STARSH_gen.jdf:127-213``): returns
+    (U, V, rank) with rank -1 when the tile is rejected.  The spectrum is
+    restricted to the ``min(maxrank + oversample, NB)`` leading values, the
+    sample size the reference sizes its workspace for (``:262-266``)."""
+    m, n = A.shape
+    u, s, vt = np.linalg.svd(A, full_matrices=False)
+    ns = min(maxrank + oversample, min(m, n))
+    s = s[:ns]
+    r = truncation_rank_relfro(s, tol)
+    if not (r < min(m, n) / 2 and r <= maxrank):
+        return None, None, -1
+    U = np.ascontiguousarray(u[:, :r])
+    V = np.ascontiguousarray(vt[:r].T * s[:r])
+    return U, V, r
+
+
+def generate(prob: Problem, n: int, nb: int, tol: float, maxrank: int, band: int = 1,
+             pts: np.ndarray | None = None):
+    """``STARSH_gen`` (``STARSH_gen.jdf:342-369``): dense band tiles
+    ``m - band < n <= m`` (``:45-83``) and compressed off-band tiles
+    (``:127-213``).  Returns (TLRMatrix, info) with info = -1 if a tile was
+    rejected."""
+    if n % nb != 0:
+        raise ValueError("N must be a multiple of NB")
+    if pts is None:
+        pts = gen_points(n, prob.ndim, prob.seed)
+    T = TLRMatrix(n, nb, band, maxrank)
+    nt = n // nb
+    info = 0
+    for m in range(nt):
+        for c in range(max(m - band + 1, 0), m + 1):
+            T.dense[(m, c)] = cov_block(prob, pts, m * nb, nb, c * nb, nb)
+    for m in range(band, nt):
+        for c in range(0, m - band + 1):
+            U, V, r = compress_tile(cov_block(prob, pts, m * nb, nb, c * nb, nb), tol, maxrank)
+            if r < 0:
+                info = -1
+                U = np.zeros((nb, 0))
+                V = np.zeros((nb, 0))
+            T.U[(m, c)] = U
+            T.V[(m, c)] = V
+    return T, info
+
+
+def band_regenerate(T: TLRMatrix, prob: Problem, pts: np.ndarray, band: int) -> None:
+    """``parsec_band_regenerate`` (``band_regenerate.jdf:27-64``): tiles with
+    ``m - n < band`` become dense kernel tiles; the others keep their [U,V]."""
+    nt, nb = T.nt, T.nb
+    for m in range(nt):
+        for c in range(max(m - band + 1, 0), m + 1):
+            T.dense[(m, c)] = cov_block(prob, pts, m * nb, nb, c * nb, nb)
+            T.U.pop((m, c), None)
+            T.V.pop((m, c), None)
+    T.band = band
+
+
+# --------------------------------------------------------------------------
+# Rank statistics and band auto-tuning
+# --------------------------------------------------------------------------
+def rank_stat(G: np.ndarray, nt: int, band: int):
+    """``HICMA_get_stat2`` (``hicma_internal.c:52-71``): (min, max, avg) over
+    tiles i >= band, j <= i - band."""
+    vals = [int(G[j * nt + i]) for i in range(band, nt) for j in range(0, i - band + 1)]
+    if not vals:
+        return 2**31 - 1, 0, float("nan")
+    return min(vals), max(vals), float(sum(vals)) / len(vals)
+
+
+def band_autotune(G: np.ndarray, nt: int, nb: int, verbose: bool = False) -> int:
+    """``parsec_band_size_auto_tuning`` (``band_size_auto_tuning.jdf:201-318``).
+
+    For band b = 2..NT-1 it sums the modelled TLR and dense flops of the TRSMs
+    (``:36-65``) and GEMMs (``:70-127``) on sub-diagonal b-1.  It records
+    ``opt_min = b - 1`` at the first b with ``tlr * FLUCTUATION <= dense`` and
+    returns ``opt_min`` at the first b with ``tlr <= dense`` (``:290-313``),
+    else NT.  The reference keeps ``opt_min`` in file-static variables that
+    are never reset between calls; this restatement resets them per call.
+    """
+    indicator_min = 0
+    opt_min = 0
+    for band in range(2, nt):
+        t_tlr = t_dense = g_tlr = g_dense = 0
+        for m in range(band - 1, nt):
+            k = m + 1 - band
+            ar = int(G[k * nt + m])
+            t_tlr += nb * nb * ar
+            t_dense += nb * nb * nb
+        for k in range(0, nt - 2):
+            for m in range(k + band, nt):
+                n = m + 1 - band
+                ar = int(G[k * nt + m])
+                br = int(G[k * nt + n])
+                cr = int(G[n * nt + m])
+                ca = cr + ar
+                qra = op_counts("q", nb, ca, 0, 0)
+                qrb = op_counts("m", ar, br, nb, 0) + op_counts("m", ar, nb, br, 0) + op_counts("q", nb, ca, 0, 0)
+                svd = op_counts("r", ca, ca, 2, 0) + op_counts("s", ca, 0, 0, 0) + ca * cr
+                newu = op_counts("o", nb, cr, ca, 1)
+                newv = op_counts("o", cr, nb, ca, 2)
+                g_tlr += (qra + qrb + svd + newu + newv) & _U64
+                if m - k < band:
+                    g_dense += 2 * nb * nb * nb
+                elif n - k < band and m - n < band:
+                    g_dense += 4 * nb * nb * ar
+                elif m - n < band:
+                    g_dense += 2 * nb * nb * min(ar, br) + 4 * nb * ar * br
+        s_tlr = t_tlr + g_tlr
+        s_dense = t_dense + g_dense
+        if verbose:
+            print(f"band_size: {band}, ops_sum_tlr: {float(s_tlr):e}, ops_sum_dense: {float(s_dense):e}")
+        if float(s_tlr) * FLUCTUATION <= float(s_dense) and indicator_min == 0:
+            indicator_min = 1
+            opt_min = band - 1
+        if s_tlr <= s_dense:
+            return opt_min
+    return nt
+
+
+# --------------------------------------------------------------------------
+# Tile kernels (HCORE / CORE_d* restated)
+# --------------------------------------------------------------------------
+def recompress(Cu, Cv, Au, Y, acc, maxrank, fixed_rank=0):
+    """C_new = [Cu, Au] [Cv, -Y]^T recompressed (restated
+    ``HCORE_dgemm_qr_svd`` + ``HCORE_dgemm_ormqr``, call sites
+    ``HiCMA_dpotrf_L_2flow.jdf:830-903,985-1058``).  Returns
+    (U, V, rank, overflow)."""
+    Us = np.hstack([Cu, Au])
+    Vs = np.hstack([Cv, -Y])
+    nb, K = Us.shape
+    if K == 0:
+        return np.zeros((nb, 0)), np.zeros((nb, 0)), 0, False
+    Qu, Ru = np.linalg.qr(Us)
+    Qv, Rv = np.linalg.qr(Vs)
+    u, s, vt = np.linalg.svd(Ru @ Rv.T)
+    if fixed_rank > 0:
+        r = min(fixed_rank, K)
+    else:
+        r = int(np.count_nonzero(s >= acc))
+    overflow = r > maxrank
+    r = min(r, maxrank)
+    return (np.ascontiguousarray(Qu @ u[:, :r]),
+            np.ascontiguousarray(Qv @ (vt[:r].T * s[:r])), r, overflow)
+
+
+@dataclass
+class FactorStats:
+    info: int = 0
+    overflow: int = 0
+    tileopcounters: np.ndarray | None = None
+    op_band: int = 0
+    op_offband: int = 0
+    op_path: int = 0
+    op_offpath: int = 0
+
+    @property
+    def total(self) -> int:
+        return int(self.tileopcounters.sum())
+
+
+def potrf_tile(A: np.ndarray):
+    """Lower Cholesky of a dense tile; returns (L, iinfo) with iinfo the
+    1-based order of the first non-positive leading minor (0 on success)."""
+    try:
+        return np.linalg.cholesky(A), 0
+    except np.linalg.LinAlgError:
+        n = A.shape[0]
+        L = np.tril(A).copy()
+        for j in range(n):
+            d = L[j, j] - np.dot(L[j, :j], L[j, :j])
+            if not d > 0.0:
+                return L, j + 1
+            L[j, j] = math.sqrt(d)
+            L[j + 1:, j] = (L[j + 1:, j] - L[j + 1:, :j] @ L[j, :j]) / L[j, j]
+        return L, 0
+
+
+def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool = True) -> FactorStats:
+    """In-place 2-flow TLR Cholesky (``HiCMA_dpotrf_L_2flow.jdf:175-1113``)
+    run in a sequential order compatible with its data flow."""
+    nt, nb, band = T.nt, T.nb, T.band
+    st = FactorStats(tileopcounters=np.zeros((nt, nt), dtype=np.uint64))
+    tile_ops = st.tileopcounters
+
+    def log(cnt, i, j, region, path):
+        tile_ops[i, j] += np.uint64(cnt & _U64)
+        if region == "band":
+            st.op_band += cnt
+        else:
+            st.op_offband += cnt
+        if path:
+            st.op_path += cnt
+        else:
+            st.op_offpath += cnt
+
+    for k in range(nt):
+        # potrf_dpotrf(k): :175-245
+        log(op_counts("c", nb, 0, 0, 0), k, k, "band", True)
+        L, iinfo = potrf_tile(T.dense[(k, k)])
+        T.dense[(k, k)] = np.tril(L)
+        if iinfo != 0:
+            if st.info == 0:
+                st.info = k * nb + iinfo
+            if stop_on_error:
+                return st
+        Lkk = T.dense[(k, k)]
+        # potrf_dtrsm(m, k): :366-401
+        for m in range(k + 1, nt):
+            if m - k < band:
+                log(op_counts("t", nb, nb, 1, 0), m, k, "band", m - k == 1)
+                T.dense[(m, k)] = sla.solve_triangular(Lkk, T.dense[(m, k)].T, lower=True).T
+            else:
+                r = T.U[(m, k)].shape[1]
+                log(op_counts("t", nb, r, 1, 0), m, k, "offband", m - k == 1)
+                if r == 0:
+                    continue
+                T.V[(m, k)] = sla.solve_triangular(Lkk, T.V[(m, k)], lower=True)
+        # potrf_dsyrk(k, m): :503-565
+        for m in range(k + 1, nt):
+            if m - k < band:
+                A = T.dense[(m, k)]
+                log(op_counts("m", nb, nb, nb, 0), m, m, "band", m - k == 1)
+                T.dense[(m, m)] = T.dense[(m, m)] - A @ A.T
+            else:
+                U, V = T.U[(m, k)], T.V[(m, k)]
+                r = U.shape[1]
+                cnt = op_counts("m", r, r, nb, 0) + op_counts("m", nb, r, r, 0) + op_counts("m", nb, nb, r, 0)
+                log(cnt, m, m, "band", m - k == 1)
+                if r == 0:
+                    continue
+                T.dense[(m, m)] = T.dense[(m, m)] - U @ ((V.T @ V) @ U.T)
+        # potrf_dgemm(m, n, k): :699-1097
+        for m in range(k + 2, nt):
+            for n in range(k + 1, m):
+                if m - k < band:                                   # (i) :699-708
+                    log(op_counts("m", nb, nb, nb, 0), m, n, "band", False)
+                    T.dense[(m, n)] = T.dense[(m, n)] - T.dense[(m, k)] @ T.dense[(n, k)].T
+                elif n - k < band and m - n < band:                # (ii) :710-730
+                    Au, Av = T.U[(m, k)], T.V[(m, k)]
+                    ra = Au.shape[1]
+                    log(op_counts("m", nb, nb, ra, 0) * 2, m, n, "band", False)
+                    tmp = Av.T @ T.dense[(n, k)].T
+                    T.dense[(m, n)] = T.dense[(m, n)] - Au @ tmp
+                elif m - n < band:                                 # (iii) :732-782
+                    Au, Av = T.U[(m, k)], T.V[(m, k)]
+                    Bu, Bv = T.U[(n, k)], T.V[(n, k)]
+                    ra, rb = Au.shape[1], Bu.shape[1]
+                    log(op_counts("m", nb, nb, min(ra, rb), 0) + op_counts("m", nb, ra, rb, 0) * 2,
+                        m, n, "band", False)
+                    rr = Av.T @ Bv
+                    if ra > rb:
+                        T.dense[(m, n)] = T.dense[(m, n)] - (Au @ rr) @ Bu.T
+                    else:
+                        T.dense[(m, n)] = T.dense[(m, n)] - Au @ (rr @ Bu.T)
+                elif n - k < band:                                 # (iv) :784-927
+                    Au, Av = T.U[(m, k)], T.V[(m, k)]
+                    ra = Au.shape[1]
+                    rc_old = T.U[(m, n)].shape[1]
+                    Y = T.dense[(n, k)] @ Av
+                    U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank)
+                    st.overflow += int(ov)
+                    T.U[(m, n)], T.V[(m, n)] = U, V
+                    log(gemm_lr_opcount(nb, ra, 0, rc_old, r, True), m, n, "offband", False)
+                else:                                              # (v) :929-1097
+                    Au, Av = T.U[(m, k)], T.V[(m, k)]
+                    Bu, Bv = T.U[(n, k)], T.V[(n, k)]
+                    ra, rb = Au.shape[1], Bu.shape[1]
+                    if ra == 0 or rb == 0:
+                        continue
+                    rc_old = T.U[(m, n)].shape[1]
+                    Y = Bu @ (Bv.T @ Av)
+                    U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank)
+                    st.overflow += int(ov)
+                    T.U[(m, n)], T.V[(m, n)] = U, V
+                    log(gemm_lr_opcount(nb, ra, rb, rc_old, r, False), m, n, "offband", False)
+    return st
+
+
+# --------------------------------------------------------------------------
+# Checks, log-determinant, solve, likelihood
+# --------------------------------------------------------------------------
+def uncompress(T: TLRMatrix) -> np.ndarray:
+    """Lower-triangular dense N x N matrix from the TLR storage
+    (``STARSH_check.jdf:90-143``: band tiles copied, ``U V^T`` expanded)."""
+    nb, nt = T.nb, T.nt
+    D = np.zeros((T.n, T.n))
+    for (m, n), t in T.dense.items():
+        D[m * nb:(m + 1) * nb, n * nb:(n + 1) * nb] = t
+    for (m, n), u in T.U.items():
+        D[m * nb:(m + 1) * nb, n * nb:(n + 1) * nb] = u @ T.V[(m, n)].T
+    return np.tril(D)
+
+
+def sym_fro_lower(X: np.ndarray) -> float:
+    """Frobenius norm of the symmetric matrix whose lower triangle is
+    tril(X) (``dplasma_dlansy(Frobenius, Lower)``)."""
+    L = np.tril(X)
+    d = np.diag(L)
+    off = L - np.diag(d)
+    return math.sqrt(float(np.sum(d * d) + 2.0 * np.sum(off * off)))
+
+
+def check_dpotrf2(L: np.ndarray, A: np.ndarray) -> float:
+    """||L L^T - A||_F / ||A||_F as ``check_dpotrf2`` (``testing_dpotrf.c:111-180``)."""
+    L = np.tril(L)
+    return sym_fro_lower(L @ L.T - A) / sym_fro_lower(A)
+
+
+def check_diff(L: np.ndarray, L0: np.ndarray) -> float:
+    """||L - L0|| / ||L|| as ``check_diff`` (``testing_dpotrf.c:183-230``)."""
+    return sym_fro_lower(np.tril(L) - np.tril(L0)) / sym_fro_lower(L)
+
+
+def logdet(T: TLRMatrix) -> float:
+    """log det(A) = 2 sum log L_ii over the diagonal tiles."""
+    return float(sum(2.0 * np.sum(np.log(np.diag(T.dense[(k, k)]))) for k in range(T.nt)))
+
+
+def solve(T: TLRMatrix, y: np.ndarray) -> np.ndarray:
+    """x = A^{-1} y from the TLR factor: forward L z = y, backward L^T x = z."""
+    nb, nt = T.nb, T.nt
+    y = np.asarray(y, dtype=np.float64)
+    squeeze = y.ndim == 1
+    Y = y.reshape(T.n, -1).copy()
+
+    def blk(i):
+        return slice(i * nb, (i + 1) * nb)
+
+    for k in range(nt):
+        for j in range(k):
+            if T.is_dense(k, j):
+                Y[blk(k)] -= T.dense[(k, j)] @ Y[blk(j)]
+            else:
+                Y[blk(k)] -= T.U[(k, j)] @ (T.V[(k, j)].T @ Y[blk(j)])
+        Y[blk(k)] = sla.solve_triangular(T.dense[(k, k)], Y[blk(k)], lower=True)
+    for k in reversed(range(nt)):
+        for m in range(k + 1, nt):
+            if T.is_dense(m, k):
+                Y[blk(k)] -= T.dense[(m, k)].T @ Y[blk(m)]
+            else:
+                Y[blk(k)] -= T.V[(m, k)] @ (T.U[(m, k)].T @ Y[blk(m)])
+        Y[blk(k)] = sla.solve_triangular(T.dense[(k, k)], Y[blk(k)], lower=True, trans="T")
+    return Y[:, 0] if squeeze else Y
+
+
+def loglik(T: TLRMatrix, y: np.ndarray):
+    """Gaussian log-likelihood -1/2 (y^T A^{-1} y + log det A + N log 2 pi);
+    returns (loglik, logdet, x)."""
+    x = solve(T, y)
+    ld = logdet(T)
+    q = float(np.dot(np.asarray(y).ravel(), x.ravel()))
+    return -0.5 * (q + ld + T.n * math.log(2.0 * math.pi)), ld, x

@@ -1,0 +1,139 @@
+"""End-to-end parity of the TLR Cholesky on the reference's own test case.
+
+The reference's CTest entries (hicma_parsec/CMakeLists.txt:59-62) run
+``testing_dpotrf_tlr -N 2700 -t 270 -e 1e-8 -u 130 -D 2 --check``: 2D
+squared-exponential covariance, tile 270, accuracy 1e-8, maxrank 130.  Its
+pass criteria are ``check_dpotrf2`` and ``check_diff`` <= tol
+(testing_dpotrf.c:851-853,891-893).  The north star adds: residual <= 10 e,
+log-determinant relative error <= 1e-8, per-tile ranks within +/-2 of the
+oracle's TLR run.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import tlr_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+N, NB, TOL, MAXRANK = 2700, 270, 1e-8, 130
+
+
+def _gpu_run(ctx, prob_kw, band=1, autoband=False):
+    from hicma_parsec_b200 import tlr
+    prob = tlr.Problem(**prob_kw)
+    A = tlr.TLRMatrix(ctx, N, NB, MAXRANK, band)
+    info = A.generate(prob, TOL, MAXRANK)
+    assert info == 0
+    G0 = A.rank_map()
+    if autoband:
+        b = tlr.parsec_band_size_auto_tuning(G0, N // NB, NB)
+        if b != 1:
+            A.band_regenerate(prob, b)
+    return A, G0, prob
+
+
+@pytest.mark.parametrize("noise", [0.1, 1e-4])
+def test_c1_factorization_matches_oracle(ctx, noise):
+    from hicma_parsec_b200 import tlr
+    A, G0, prob = _gpu_run(ctx, dict(kind=2, noise=noise))
+    oprob = O.Problem(kind=2, noise=noise)
+    pts = O.gen_points(N, 2)
+    T, _ = O.generate(oprob, N, NB, TOL, MAXRANK, 1, pts)
+    Gref = T.rank_array()
+    off = Gref >= 0
+    # generation ranks within +/-2 of the oracle (randomized range finder vs exact SVD)
+    assert np.max(np.abs(G0[off] - Gref[off])) <= 2
+    info, tileops, total_ops, cpt = tlr.HiCMA_dpotrf_L(ctx, tlr.LOWER, A, TOL, 0, MAXRANK)
+    assert info == 0
+    st = O.tlr_potrf(T, TOL)
+    G1 = A.rank_map()
+    Gref1 = T.rank_array()
+    assert np.max(np.abs(G1[off] - Gref1[off])) <= 2
+    # op counts follow the reference formulas with the actual ranks
+    assert abs(total_ops - st.total) <= 0.02 * st.total
+    L = A.uncompress()
+    Aexact = O.dense_matrix(oprob, pts)
+    res = O.check_dpotrf2(L, Aexact)
+    assert res <= 10 * TOL, res
+    if noise == 0.1:
+        # the reference's own threshold (testing_dpotrf.c:891-893)
+        assert res <= TOL
+        A0 = O.uncompress(O.generate(oprob, N, NB, TOL, MAXRANK, 1, pts)[0])
+        L0 = np.linalg.cholesky(A0 + np.tril(A0, -1).T)
+        assert O.check_diff(L, L0) <= TOL
+    ld = A.logdet()
+    ld_exact = 2.0 * np.sum(np.log(np.diag(np.linalg.cholesky(Aexact))))
+    assert abs(ld - ld_exact) / abs(ld_exact) <= 1e-8
+    assert abs(ld - O.logdet(T)) / abs(ld_exact) <= 1e-9
+    y = np.random.default_rng(7).standard_normal(N)
+    ll, ld2, x = A.loglik(y)
+    llo, _, xo = O.loglik(T, y)
+    assert abs(ld2 - ld) <= 1e-12 * abs(ld)
+    assert abs(ll - llo) / abs(llo) <= 1e-8
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-6
+
+
+def test_c1_autoband(ctx):
+    """-E 1 path: rank gather -> band auto-tuning -> band regeneration -> potrf."""
+    from hicma_parsec_b200 import tlr
+    A, G0, prob = _gpu_run(ctx, dict(kind=2, noise=0.1), autoband=True)
+    pts = O.gen_points(N, 2)
+    oprob = O.Problem(kind=2, noise=0.1)
+    T, _ = O.generate(oprob, N, NB, TOL, MAXRANK, 1, pts)
+    b_ref = O.band_autotune(T.rank_array(), N // NB, NB)
+    b = A.band_size
+    assert b == tlr.parsec_band_size_auto_tuning(G0, N // NB, NB)
+    assert abs(b - b_ref) <= 1
+    info = A.potrf(TOL)
+    assert info == 0
+    L = A.uncompress()
+    res = O.check_dpotrf2(L, O.dense_matrix(oprob, pts))
+    assert res <= TOL, res
+
+
+def test_3d_exp_small(ctx):
+    """3D exponential kernel (-D 4) with a dense band, scaled down."""
+    from hicma_parsec_b200 import tlr
+    n, nb, mr = 4000, 400, 200
+    prob = tlr.Problem(kind=4, noise=1e-4)
+    A = tlr.TLRMatrix(ctx, n, nb, mr, 2)
+    assert A.generate(prob, TOL, mr) == 0
+    assert A.potrf(TOL) == 0
+    pts = O.gen_points(n, 3)
+    Aex = O.dense_matrix(O.Problem(kind=4, noise=1e-4), pts)
+    res = O.check_dpotrf2(A.uncompress(), Aex)
+    assert res <= 10 * TOL, res
+    ld_exact = 2.0 * np.sum(np.log(np.diag(np.linalg.cholesky(Aex))))
+    assert abs(A.logdet() - ld_exact) / abs(ld_exact) <= 1e-8
+
+
+def test_not_spd_returns_info(ctx):
+    from hicma_parsec_b200 import tlr
+    prob = tlr.Problem(kind=2, noise=0.1)
+    A = tlr.TLRMatrix(ctx, N, NB, MAXRANK, 1)
+    assert A.generate(prob, TOL, MAXRANK) == 0
+    D = A.tile(3, 3)
+    D[100, 100] = -1.0
+    A.set_tile(3, 3, D)
+    info = A.potrf(TOL)
+    assert info > 0
+    assert info // NB <= 3           # first failure in panel <= 3 (k*NB + iinfo)
+    with pytest.raises(tlr.TLRError):
+        A.logdet()                   # not factored
+
+
+def test_argument_errors(ctx):
+    from hicma_parsec_b200 import tlr
+    with pytest.raises(tlr.TLRError) as e:
+        tlr.TLRMatrix(ctx, 2701, 270, 130)
+    assert e.value.code == tlr.ERR_NOT_SUPPORTED
+    A = tlr.TLRMatrix(ctx, N, NB, MAXRANK, 1)
+    A.generate(tlr.Problem(kind=2), TOL, MAXRANK)
+    with pytest.raises(tlr.TLRError) as e:
+        tlr.HiCMA_dpotrf_L(ctx, tlr.UPPER, A, TOL, 0, MAXRANK)
+    assert e.value.code == tlr.ERR_NOT_SUPPORTED
+    with pytest.raises(tlr.TLRError) as e:
+        tlr.HiCMA_dpotrf_L(ctx, tlr.LOWER, A, TOL, 0, NB)     # maxrank > NB/2
+    assert e.value.code == tlr.ERR_ARG
