@@ -1,0 +1,410 @@
+"""Benchmark of the TLR Cholesky (seconds per factorization) on B200.
+
+Default workload: 2D squared-exponential covariance, N = 270,000, tile 2700
+(100 x 100 tiles), accuracy e = 1e-8, maxrank 150, band 1, FP64 throughout,
+nugget 1e-4, points on a jittered 520 x 520 grid in Morton order (seeded).
+The compressed matrix is generated once (untimed) and kept resident in HBM;
+one step = restore the pristine compressed matrix (device-to-device copy, the
+factorization is in place) + the full TLR factorization.
+
+Printed JSON line (rank 0): metric/value (s/factor, lower is better), the
+end-to-end number through the C ABI with host buffers (pinned host copy of
+the compressed matrix in, factor out), the roofline of the dominant kernel
+class (measured with CUDA events on the library's stream), the CPU
+restatement timed on a bounded sample, and the SM clocks seen during the
+timed region.
+
+``--impl reference`` times the CPU restatement of the reference algorithm
+(the oracle port; the reference itself cannot be built here) on a bounded
+sample of the same workload and extrapolates to seconds per factorization.
+Multi-GPU (torchrun): independent replicas, no collectives.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # name: (kind, N, NB, maxrank, acc, nugget, band, autoband)
+    "c2": dict(kind=2, n=270000, nb=2700, maxrank=150, acc=1e-8, noise=1e-4, band=1, autoband=False,
+               workload="2D sqexp N=270000 NB=2700 (100x100 tiles) e=1e-8 maxrank=150 band=1 FP64"),
+    "c1": dict(kind=2, n=2700, nb=270, maxrank=130, acc=1e-8, noise=1e-4, band=1, autoband=False,
+               workload="2D sqexp N=2700 NB=270 e=1e-8 maxrank=130 band=1 FP64"),
+    "c2s": dict(kind=2, n=27000, nb=2700, maxrank=150, acc=1e-8, noise=1e-4, band=1, autoband=False,
+                workload="2D sqexp N=27000 NB=2700 e=1e-8 maxrank=150 band=1 FP64 (scaled twin of N=270000)"),
+    "c3": dict(kind=4, n=108000, nb=2700, maxrank=1350, acc=1e-8, noise=1e-4, band=1, autoband=True,
+               workload="3D exp N=108000 NB=2700 e=1e-8 maxrank=1350 band auto FP64"),
+    "c4": dict(kind=3, n=216000, nb=2700, maxrank=500, acc=1e-8, noise=1e-4, band=1, autoband=True,
+               workload="3D sqexp N=216000 NB=2700 e=1e-8 maxrank=500 band auto FP64"),
+}
+METRIC = "TLR Cholesky s/factor at e=1e-8"
+UNIT = "s/factor"
+CPU_SAMPLE_ROWS = 12      # panel-0 sample: tiles (m, n) with n < m < 12
+WORK_FIXTURE = os.path.join(ROOT, "oracle", "workload_ops.json")
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        load = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------- CPU sample --
+def cpu_sample_tasks(tiles: dict, nb: int, S: int, acc: float, maxrank: int, threads: int):
+    """Time the panel-0 tasks of the TLR Cholesky restricted to tiles (m, n)
+    with n < m < S on the host cores (oracle restatement, one BLAS thread per
+    task, tasks of a class in parallel as the reference's PaRSEC workers
+    would run them).  Returns (seconds, algorithmic ops of the sample)."""
+    from concurrent.futures import ThreadPoolExecutor
+    import scipy.linalg as sla
+    from threadpoolctl import threadpool_limits
+    from oracle import tlr_oracle as O
+    ops = 0
+    with threadpool_limits(limits=1):
+        t0 = time.perf_counter()
+        L, _ = O.potrf_tile(tiles[(0, 0)])
+        ops += O.op_counts("c", nb, 0, 0, 0)
+
+        def trsm(m):
+            U, V = tiles[(m, 0)]
+            return m, (U, sla.solve_triangular(L, V, lower=True))
+
+        with ThreadPoolExecutor(threads) as ex:
+            res = dict(ex.map(trsm, range(1, S)))
+            for m in range(1, S):
+                ops += O.op_counts("t", nb, res[m][0].shape[1], 1, 0)
+
+            def syrk(m):
+                U, V = res[m]
+                D = tiles[(m, m)] - U @ ((V.T @ V) @ U.T)
+                return D.shape[0]
+
+            list(ex.map(syrk, range(1, S)))
+            for m in range(1, S):
+                r = res[m][0].shape[1]
+                ops += O.op_counts("m", r, r, nb, 0) + O.op_counts("m", nb, r, r, 0) + O.op_counts("m", nb, nb, r, 0)
+
+            def gemm(mn):
+                m, n = mn
+                Au, Av = res[m]
+                Bu, Bv = res[n]
+                Cu, Cv = tiles[(m, n)]
+                if Au.shape[1] == 0 or Bu.shape[1] == 0:
+                    return 0
+                Y = Bu @ (Bv.T @ Av)
+                U, V, r, _ = O.recompress(Cu, Cv, Au, Y, acc, maxrank)
+                return O.gemm_lr_opcount(nb, Au.shape[1], Bu.shape[1], Cu.shape[1], r, False)
+
+            ops += sum(ex.map(gemm, [(m, n) for m in range(2, S) for n in range(1, m)]))
+        secs = time.perf_counter() - t0
+    return secs, ops
+
+
+def load_work_fixture(cfg_name: str):
+    try:
+        with open(WORK_FIXTURE) as f:
+            return json.load(f).get(cfg_name)
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------------ arms ----
+def run_reference(args, cfg):
+    """CPU restatement on a bounded sample; rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import tlr_oracle as O
+    threads = os.cpu_count() or 1
+    nb, S = cfg["nb"], min(CPU_SAMPLE_ROWS, cfg["n"] // cfg["nb"])
+    prob = O.Problem(kind=cfg["kind"], noise=cfg["noise"])
+    pts = O.gen_points(cfg["n"], prob.ndim, 0)
+    tiles = {}
+    for m in range(S):
+        tiles[(m, m)] = O.cov_block(prob, pts, m * nb, nb, m * nb, nb)
+        for n in range(m):
+            U, V, r = O.compress_tile_rsvd(O.cov_block(prob, pts, m * nb, nb, n * nb, nb), cfg["acc"], cfg["maxrank"])
+            tiles[(m, n)] = (U, V)
+    fx = load_work_fixture(args.config)
+    times = []
+    sample_ops = 0
+    for i in range(args.warmup + args.steps):
+        secs, sample_ops = cpu_sample_tasks(tiles, nb, S, cfg["acc"], cfg["maxrank"], threads)
+        if i >= args.warmup:
+            times.append(secs)
+    t = statistics.median(times)
+    if fx and fx.get("total_ops"):
+        scale = fx["total_ops"] / sample_ops
+        value = t * scale
+        how = (f"panel-0 tasks on tiles (m,n), n<m<{S} ({sample_ops:.3e} op_counts flops, {t:.2f} s); "
+               f"scaled by the workload's {fx['total_ops']:.3e} op_counts flops")
+    else:
+        value = None
+        how = "panel-0 sample; workload op total unknown (no fixture)"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "sample": how},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": how},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def measure_dgemm_peak(torch, dev) -> float:
+    """FP64 DGEMM TF/s (cuBLAS via torch.matmul), best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    best = 1e9
+    for _ in range(6):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def run_ours(args, cfg):
+    import torch
+    import torch.distributed as dist
+    from hicma_parsec_b200 import tlr
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=1800))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    meas = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    fp64_peak = measure_dgemm_peak(torch, dev)
+
+    ctx = tlr.Context(local, int(args.workspace_gb * (1 << 30)))
+    ctx.set_precision(tlr.PREC_MIXED if args.precision == "mixed" else tlr.PREC_FP64)
+    prob = tlr.Problem(kind=cfg["kind"], noise=cfg["noise"], beta=0.1, sigma=1.0, seed=0)
+    n, nb, mr, acc = cfg["n"], cfg["nb"], cfg["maxrank"], cfg["acc"]
+    A0 = tlr.TLRMatrix(ctx, n, nb, mr, cfg["band"])
+    t0 = time.perf_counter()
+    info = A0.generate(prob, acc, mr)
+    t_gen = time.perf_counter() - t0
+    if info != 0:
+        raise SystemExit(f"generation rejected a tile (info={info})")
+    G0 = A0.rank_map()
+    band = cfg["band"]
+    if cfg["autoband"]:
+        band = tlr.parsec_band_size_auto_tuning(G0, n // nb, nb)
+        if band != 1:
+            A0.band_regenerate(prob, band)
+    rmin, rmax, ravg = tlr.HICMA_get_stat2(A0.rank_map(), n // nb, A0.band_size)
+
+    # CPU sample tiles come from the generated matrix before any factorization
+    cpu = None
+    S = min(CPU_SAMPLE_ROWS, n // nb)
+    tiles = {}
+    if rank == 0 and world == 1 and not args.no_cpu and A0.band_size == 1:
+        for m in range(S):
+            tiles[(m, m)] = A0.tile(m, m)
+            for c in range(m):
+                tiles[(m, c)] = A0.tile(m, c)
+
+    W = tlr.TLRMatrix(ctx, n, nb, mr, A0.band_size)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    def step():
+        W.copy_from(A0)
+        inf = W.potrf(acc, mr)
+        if inf != 0:
+            raise SystemExit(f"factorization failed, info={inf}")
+
+    for _ in range(args.warmup):
+        step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    secs = e0.elapsed_time(e1) * 1e-3
+    if world > 1:
+        tt = torch.tensor([secs], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        secs = float(tt.item())
+        dist.barrier()
+    s_per_factor = secs / (args.steps * world)
+    st = W.stats()
+    total_ops = st[1]
+
+    # profiling pass (one extra step, not part of value): per-kernel-class event timing
+    ctx.prof_enable(True)
+    step()
+    prof = ctx.prof_read()
+    ctx.prof_enable(False)
+    dom = max(prof, key=lambda k: prof[k]["seconds"])
+    pd = prof[dom]
+    launches = int(sum(v["launches"] for v in prof.values()))
+    roof = None
+    if pd["launches"]:
+        t_launch = pd["seconds"] / pd["launches"]
+        if pd["flops"] > 0:
+            ach = pd["flops"] / pd["launches"] / t_launch / 1e12
+            roof = {"kernel": dom, "bound": "tensor", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+                    "frac": ach / fp64_peak, "traffic": None,
+                    "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+                    "avg_launch_ms": t_launch * 1e3, "launches": pd["launches"],
+                    "algorithmic_flops_per_launch": pd["flops"] / pd["launches"]}
+        else:
+            peak = meas.get("hbm_gbs", 6650.0)
+            ach = pd["bytes"] / pd["launches"] / t_launch / 1e9
+            roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": ach / peak, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                    "avg_launch_ms": t_launch * 1e3, "launches": pd["launches"]}
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        nbytes = A0.store_bytes()
+        host = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
+        ranks = np.empty((n // nb) ** 2, dtype=np.int32)
+        A0.store_get(host.data_ptr(), ranks)
+        out = torch.empty(nbytes // 8 + (n // nb) ** 2 * nb * 2 * mr, dtype=torch.float64, pin_memory=True)
+        torch.cuda.synchronize()
+        ts = []
+        d2h = 0
+        for i in range(max(1, args.e2e_steps)):
+            q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            q0.record(stream)
+            W.store_set(host.data_ptr(), ranks)
+            inf = W.potrf(acc, mr)
+            assert inf == 0
+            d2h = W.store_bytes()
+            W.store_get(out.data_ptr(), None)
+            q1.record(stream)
+            q1.synchronize()
+            ts.append(q0.elapsed_time(q1) * 1e-3)
+        e2e = {"value": statistics.median(ts), "unit": UNIT, "h2d_bytes_per_step": int(nbytes),
+               "d2h_bytes_per_step": int(d2h), "steps": len(ts),
+               "path": "hicma_tlr_store_set (pinned host -> HBM) + hicma_tlr_dpotrf_L + hicma_tlr_store_get"}
+        del host, out
+
+    if tiles:
+        threads = os.cpu_count() or 1
+        csecs, cops = cpu_sample_tasks(tiles, nb, S, acc, mr, threads)
+        cpu = {"value": csecs * total_ops / cops, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"panel-0 tasks on tiles (m,n), n<m<{S}: {cops:.3e} op_counts flops in {csecs:.2f} s, "
+                         f"scaled to this run's {total_ops:.3e} op_counts flops"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": s_per_factor, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": cfg["workload"], "N": n, "NB": nb, "maxrank": mr, "acc": acc,
+                           "band": int(A0.band_size), "nugget": cfg["noise"], "precision": args.precision,
+                           "parallelism": "replicas" if world > 1 else "single GPU",
+                           "l2": "inputs larger than L2 (compressed matrix ~%.1f GB resident)" % (A0.store_bytes() / 1e9),
+                           "step": "device copy of the pristine compressed matrix + full TLR factorization",
+                           "generation_s": t_gen, "rank_min_max_avg": [rmin, rmax, ravg],
+                           "final_rank_min_max_avg": list(tlr.HICMA_get_stat2(W.rank_map(), n // nb, W.band_size))},
+                "tlr_tflops": total_ops / s_per_factor / world / 1e12 if world else None,
+                "op_counts_flops": total_ops,
+                "dense_equiv_gflops": (n ** 3 / 3.0) / s_per_factor / 1e9,
+                "phase_s": {"potrf": st[4], "trsm": st[5], "syrk": st[6], "gemm_recompress": st[7]},
+                "jacobi_sweeps_total": st[8],
+                "kernel_classes": prof, "gpu_launches": launches * args.steps,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    W.close()
+    A0.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workspace-gb", type=float, default=16.0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

@@ -70,9 +70,14 @@ __device__ __forceinline__ void load_stage(Smem &sm, int s, const GemmTask &t, i
     cp_async_commit();
 }
 
-__device__ __forceinline__ void gemm_tile(Smem &sm, const GemmTask &t, int tm, int tn) {
+__device__ __forceinline__ void gemm_tile(Smem &sm, GemmTask t, int tm, int tn) {
     const int i0 = tm * BM, j0 = tn * BN;
     if (t.lower && j0 >= i0 + BM) return;
+    if (t.n_dev) {
+        const int nd = *t.n_dev;
+        t.n = nd < t.n ? nd : t.n;
+    }
+    if (j0 >= t.n) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, tig = lane & 3;
     const int wm = warp & 1, wn = warp >> 1;
@@ -163,10 +168,15 @@ __global__ void __launch_bounds__(256) k_sgemm_batched(const GemmTask *__restric
         const int mid = (lo + hi + 1) >> 1;
         if (tile_off[mid] <= bid) lo = mid; else hi = mid - 1;
     }
-    const GemmTask t = tasks[lo];
+    GemmTask t = tasks[lo];
     const int local = bid - tile_off[lo];
     const int i0 = (local % t.tiles_m) * FB, j0 = (local / t.tiles_m) * FB;
     if (t.lower && j0 >= i0 + FB) return;
+    if (t.n_dev) {
+        const int nd = *t.n_dev;
+        t.n = nd < t.n ? nd : t.n;
+    }
+    if (j0 >= t.n) return;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     float acc[4][4] = {};
     for (int k0 = 0; k0 < t.k; k0 += FK) {

@@ -17,8 +17,7 @@
 namespace tlr {
 namespace {
 
-constexpr int QT = 256;            // threads per CTA
-constexpr int QW = QT / 32;        // warps
+constexpr int QW_MAX = 16;         // warps of the largest CTA (reduction scratch)
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -32,16 +31,66 @@ __device__ __forceinline__ double vref(const double *P, int mr, int i, int r) {
     return r > i ? P[i * mr + r] : (r == i ? 1.0 : 0.0);
 }
 
+// w[i] = sum_r v_i(r) y[r] over the panel rows (warp-wide, 4 rows in flight per lane)
 template <int PB>
+__device__ __forceinline__ void panel_dots(const double *P, int mr, int jb, const double *y, int lane, double (&w)[PB]) {
+#pragma unroll
+    for (int i = 0; i < PB; ++i) w[i] = 0.0;
+    int r = lane;
+    for (; r + 96 < mr; r += 128) {
+        const double x0 = y[r], x1 = y[r + 32], x2 = y[r + 64], x3 = y[r + 96];
+#pragma unroll
+        for (int i = 0; i < PB; ++i)
+            if (i < jb)
+                w[i] += vref(P, mr, i, r) * x0 + vref(P, mr, i, r + 32) * x1 + vref(P, mr, i, r + 64) * x2 +
+                        vref(P, mr, i, r + 96) * x3;
+    }
+    for (; r < mr; r += 32) {
+        const double x = y[r];
+#pragma unroll
+        for (int i = 0; i < PB; ++i)
+            if (i < jb) w[i] += vref(P, mr, i, r) * x;
+    }
+#pragma unroll
+    for (int i = 0; i < PB; ++i) w[i] = warp_sum(w[i]);
+}
+
+// y[r] -= sum_i v_i(r) w2[i]
+template <int PB>
+__device__ __forceinline__ void panel_update(const double *P, int mr, int jb, double *y, int lane, const double (&w2)[PB]) {
+    int r = lane;
+    for (; r + 96 < mr; r += 128) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+        for (int i = 0; i < PB; ++i)
+            if (i < jb) {
+                a0 += vref(P, mr, i, r) * w2[i];
+                a1 += vref(P, mr, i, r + 32) * w2[i];
+                a2 += vref(P, mr, i, r + 64) * w2[i];
+                a3 += vref(P, mr, i, r + 96) * w2[i];
+            }
+        y[r] -= a0; y[r + 32] -= a1; y[r + 64] -= a2; y[r + 96] -= a3;
+    }
+    for (; r < mr; r += 32) {
+        double a = 0.0;
+#pragma unroll
+        for (int i = 0; i < PB; ++i)
+            if (i < jb) a += vref(P, mr, i, r) * w2[i];
+        y[r] -= a;
+    }
+}
+
+template <int PB, int QT>
 __global__ void __launch_bounds__(QT) k_qr(const QRTask *__restrict__ tasks) {
+    constexpr int QW = QT / 32;
     extern __shared__ double sm[];
     const QRTask t = tasks[blockIdx.x];
     const int m = t.m, K = t.K, ld = t.ld;
     if (K <= 0) return;
     double *X = t.X;
     double *P = sm;                       // PB * m
-    double *red = P + PB * m;             // QW * PB
-    double *Ts = red + QW * PB;           // PB * PB
+    double *red = P + PB * m;             // QW_MAX * PB
+    double *Ts = red + QW_MAX * PB;       // PB * PB
     double *wsm = Ts + PB * PB;           // PB
     double *sc = wsm + PB;                // 4 scalars
     double *G = sc + 4;                   // PB * PB gram of the panel reflectors
@@ -144,16 +193,7 @@ __global__ void __launch_bounds__(QT) k_qr(const QRTask *__restrict__ tasks) {
         for (int col = j0 + jb + warp; col < K; col += QW) {
             double *xcol = X + (size_t)col * ld + j0;
             double w[PB];
-#pragma unroll
-            for (int i = 0; i < PB; ++i) w[i] = 0.0;
-            for (int r = lane; r < mr; r += 32) {
-                const double x = xcol[r];
-#pragma unroll
-                for (int i = 0; i < PB; ++i)
-                    if (i < jb) w[i] += vref(P, mr, i, r) * x;
-            }
-#pragma unroll
-            for (int i = 0; i < PB; ++i) w[i] = warp_sum(w[i]);
+            panel_dots<PB>(P, mr, jb, xcol, lane, w);
             double w2[PB];
 #pragma unroll
             for (int i = 0; i < PB; ++i) {
@@ -163,20 +203,15 @@ __global__ void __launch_bounds__(QT) k_qr(const QRTask *__restrict__ tasks) {
                     if (l <= i) z += Ts[l + i * PB] * w[l];
                 w2[i] = z;
             }
-            for (int r = lane; r < mr; r += 32) {
-                double a = 0.0;
-#pragma unroll
-                for (int i = 0; i < PB; ++i)
-                    if (i < jb) a += vref(P, mr, i, r) * w2[i];
-                xcol[r] -= a;
-            }
+            panel_update<PB>(P, mr, jb, xcol, lane, w2);
         }
         __syncthreads();
     }
 }
 
-template <int PB>
+template <int PB, int QT>
 __global__ void __launch_bounds__(QT) k_qapply(const QApplyTask *__restrict__ tasks) {
+    constexpr int QW = QT / 32;
     extern __shared__ double sm[];
     const QApplyTask t = tasks[blockIdx.x];
     int r = t.r_dev ? *t.r_dev : t.r_cap;
@@ -205,16 +240,7 @@ __global__ void __launch_bounds__(QT) k_qapply(const QApplyTask *__restrict__ ta
         for (int col = warp; col < r; col += QW) {
             double *y = t.out + (size_t)col * t.ldo + j0;
             double w[PB];
-#pragma unroll
-            for (int i = 0; i < PB; ++i) w[i] = 0.0;
-            for (int rr = lane; rr < mr; rr += 32) {
-                const double x = y[rr];
-#pragma unroll
-                for (int i = 0; i < PB; ++i)
-                    if (i < jb) w[i] += vref(P, mr, i, rr) * x;
-            }
-#pragma unroll
-            for (int i = 0; i < PB; ++i) w[i] = warp_sum(w[i]);
+            panel_dots<PB>(P, mr, jb, y, lane, w);
             double w2[PB];
 #pragma unroll
             for (int i = 0; i < PB; ++i) {
@@ -224,33 +250,33 @@ __global__ void __launch_bounds__(QT) k_qapply(const QApplyTask *__restrict__ ta
                     if (l >= i) z += Ts[i + l * PB] * w[l];
                 w2[i] = z;
             }
-            for (int rr = lane; rr < mr; rr += 32) {
-                double a = 0.0;
-#pragma unroll
-                for (int i = 0; i < PB; ++i)
-                    if (i < jb) a += vref(P, mr, i, rr) * w2[i];
-                y[rr] -= a;
-            }
+            panel_update<PB>(P, mr, jb, y, lane, w2);
         }
         __syncthreads();
     }
 }
 
 template <int PB>
-size_t qr_smem(int m) { return sizeof(double) * ((size_t)PB * m + QW * PB + 2 * PB * PB + PB + 4); }
+size_t qr_smem(int m) { return sizeof(double) * ((size_t)PB * m + QW_MAX * PB + 2 * PB * PB + PB + 4); }
+
+// 512 threads where the register budget allows it (PB <= 16), else 256
+template <int PB>
+constexpr int qr_threads() { return PB <= 16 ? 512 : 256; }
 
 template <int PB>
 void launch_qr_pb(const QRTask *d_tasks, int ntasks, int m_max, cudaStream_t st) {
     const size_t smem = qr_smem<PB>(m_max);
-    cudaFuncSetAttribute(k_qr<PB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_qr<PB><<<ntasks, QT, smem, st>>>(d_tasks);
+    constexpr int T = qr_threads<PB>();
+    cudaFuncSetAttribute(k_qr<PB, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_qr<PB, T><<<ntasks, T, smem, st>>>(d_tasks);
 }
 
 template <int PB>
 void launch_qapply_pb(const QApplyTask *d_tasks, int ntasks, int m_max, cudaStream_t st) {
     const size_t smem = sizeof(double) * ((size_t)PB * m_max + PB * PB);
-    cudaFuncSetAttribute(k_qapply<PB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_qapply<PB><<<ntasks, QT, smem, st>>>(d_tasks);
+    constexpr int T = qr_threads<PB>();
+    cudaFuncSetAttribute(k_qapply<PB, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_qapply<PB, T><<<ntasks, T, smem, st>>>(d_tasks);
 }
 
 }  // namespace

@@ -1,37 +1,40 @@
 // Batched small-core SVD and rank truncation, FP64.
 //
-// Replaces the SVD + truncation step inside HCORE_dgemm_qr_svd (the r x r
-// core R_U R_V^T of a recompression, call sites
+// Replaces the SVD + truncation step inside HCORE_dgemm_qr_svd (the core
+// R_U R_V^T of a recompression, call sites
 // hicma_parsec/HiCMA_dpotrf_L_2flow.jdf:830-903,985-1058) and the rank rule of
 // starsh_dense_dlrrsdd (STARSH_gen.jdf:162-171).
 //
-// One CTA per core.  M = R_U R_V^T is formed in shared memory (global scratch
-// when K is too large), then a one-sided (Hestenes) Jacobi SVD orthogonalises
-// its columns with a round-robin tournament ordering: every round K/2
-// disjoint column pairs are rotated in parallel, one warp per pair, the three
-// dot products of a pair reduced with warp shuffles.  One-sided Jacobi gives
-// small singular values to high relative accuracy, which is what the
-// absolute truncation threshold needs.  The truncation decision is FP64.
+// One CTA per core.  M = R_U R_V^T is formed in shared memory (global
+// scratch when K is large) and a one-sided (Hestenes) Jacobi SVD
+// orthogonalises its columns, W = M J = U Sigma, with a round-robin
+// tournament ordering: each round rotates K/2 disjoint column pairs in
+// parallel, LP lanes per pair, the three dot products of a pair reduced with
+// warp shuffles.  The rotations are not accumulated: the caller recovers
+// V Sigma = M^T U = R_V (R_U^T U) with two GEMMs, so only W lives on chip.
+// One-sided Jacobi resolves small singular values to high relative accuracy,
+// which the absolute truncation threshold needs; the decision is FP64.
 #include "tlr_internal.h"
 
 namespace tlr {
 namespace {
 
-constexpr int CT = 512;
-constexpr int CW = CT / 32;
-constexpr int KMAX_SMEM = 112;
+constexpr int CT = 256;
+constexpr int KMAX_SMEM = 160;
 constexpr int MAX_SWEEPS = 40;
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
 __device__ __forceinline__ int tourney(int slot, int round, int Kp) {
     return slot == 0 ? 0 : 1 + ((slot - 1 + round) % (Kp - 1));
 }
 
+template <int LP>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+    for (int o = LP / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int LP>
 __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ tasks, CoreParams p) {
     extern __shared__ double sm[];
     __shared__ int rotated;
@@ -47,12 +50,11 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
         return;
     }
     const bool in_smem = K <= KMAX_SMEM;
-    double *M = in_smem ? sm : t.work;
-    double *V = in_smem ? sm + (size_t)K * K : t.work + (size_t)K * K;
-    double *sig = in_smem ? sm + 2 * (size_t)K * K : sm;
+    double *W = in_smem ? sm : t.work;
+    double *sig = in_smem ? sm + (size_t)K * K : sm;
     int *order = (int *)(sig + K);
 
-    // M = RU RV^T with RU, RV upper triangular (RU null: identity)
+    // M = RU RV^T (RU, RV upper triangular; RU null: identity); clean copy of RU
     for (long long idx = tid; idx < (long long)K * K; idx += CT) {
         const int i = (int)(idx % K), j = (int)(idx / K);
         double s = 0.0;
@@ -60,51 +62,87 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
             const int l0 = i > j ? i : j;
             for (int l = l0; l < K; ++l)
                 s += t.RU[(size_t)i + (size_t)l * t.ldru] * t.RV[(size_t)j + (size_t)l * t.ldrv];
+            if (t.RUc) t.RUc[idx] = (i <= j) ? t.RU[(size_t)i + (size_t)j * t.ldru] : 0.0;
         } else {
             s = (j <= i) ? t.RV[(size_t)j + (size_t)i * t.ldrv] : 0.0;
         }
-        M[idx] = s;
-        V[idx] = (i == j) ? 1.0 : 0.0;
+        W[idx] = s;
     }
     __syncthreads();
 
+    // Columns whose norm is below tau can only move the result by O(tau) and
+    // are truncated anyway: pairs involving them are not rotated.  tau is
+    // 1e-3 of the absolute threshold (recompression) or of tol * ||M||_F
+    // (generation); fixed-rank mode keeps every rotation.
+    __shared__ double tau2_sh;
+    if (tid == 0) {
+        double tau = 0.0;
+        if (p.mode == 0 && p.fixed_rank <= 0) tau = 1e-3 * p.tol;
+        tau2_sh = tau * tau;
+    }
+    if (p.mode == 1) {
+        double s2 = 0.0;
+        for (long long idx = tid; idx < (long long)K * K; idx += CT) s2 += W[idx] * W[idx];
+        s2 = group_sum<32>(s2);
+        __shared__ double red[CT / 32];
+        if (lane == 0) red[warp] = s2;
+        __syncthreads();
+        if (tid == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < CT / 32; ++w) tot += red[w];
+            tau2_sh = 1e-6 * p.tol * p.tol * tot;
+        }
+    }
+    __syncthreads();
+    const double tau2 = tau2_sh;
+
+    constexpr int GPW = 32 / LP;                 // pair groups per warp
+    const int groups = (CT / 32) * GPW;          // pair groups per CTA
+    const int gsub = lane / LP, gl = lane % LP;
     const int Kp = K + (K & 1);
     const double tolj = 2.3e-16 * sqrt((double)K);
+    int sweeps = 0;
     if (K > 1) {
         for (int sweep = 0; sweep < MAX_SWEEPS; ++sweep) {
             if (tid == 0) rotated = 0;
             __syncthreads();
+            ++sweeps;
             for (int round = 0; round < Kp - 1; ++round) {
-                for (int pr = warp; pr < Kp / 2; pr += CW) {
-                    int a = tourney(pr, round, Kp), b = tourney(Kp - 1 - pr, round, Kp);
-                    if (a >= K || b >= K) continue;
-                    if (a > b) { const int tmp = a; a = b; b = tmp; }
-                    double *mp = M + (size_t)a * K, *mq = M + (size_t)b * K;
-                    double aa = 0.0, bb = 0.0, cc = 0.0;
-                    for (int r = lane; r < K; r += 32) {
-                        const double x = mp[r], y = mq[r];
-                        aa += x * x; bb += y * y; cc += x * y;
+                // uniform trip count per warp: every lane reaches the shuffles
+                for (int base = warp * GPW; base < Kp / 2; base += groups) {
+                    const int pr = base + gsub;
+                    int a = 0, b = 0;
+                    bool valid = pr < Kp / 2;
+                    if (valid) {
+                        a = tourney(pr, round, Kp);
+                        b = tourney(Kp - 1 - pr, round, Kp);
+                        if (a > b) { const int tmp = a; a = b; b = tmp; }
+                        valid = b < K;
                     }
-                    aa = warp_sum(aa); bb = warp_sum(bb); cc = warp_sum(cc);
-                    if (cc == 0.0 || aa < 1e-290 || bb < 1e-290) continue;
+                    double aa = 0.0, bb = 0.0, cc = 0.0;
+                    double *mp = W + (size_t)a * K, *mq = W + (size_t)b * K;
+                    if (valid) {
+                        for (int r = gl; r < K; r += LP) {
+                            const double x = mp[r], y = mq[r];
+                            aa += x * x; bb += y * y; cc += x * y;
+                        }
+                    }
+                    aa = group_sum<LP>(aa);
+                    bb = group_sum<LP>(bb);
+                    cc = group_sum<LP>(cc);
+                    if (!valid || cc == 0.0 || aa <= tau2 || bb <= tau2 || aa < 1e-290 || bb < 1e-290) continue;
                     if (fabs(cc) <= tolj * sqrt(aa) * sqrt(bb)) continue;
                     const double zeta = (bb - aa) / (2.0 * cc);
                     double tt;
                     if (fabs(zeta) > 1e150) tt = 0.5 / zeta;
                     else tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
                     const double cs = 1.0 / sqrt(1.0 + tt * tt), sn = cs * tt;
-                    for (int r = lane; r < K; r += 32) {
+                    for (int r = gl; r < K; r += LP) {
                         const double x = mp[r], y = mq[r];
                         mp[r] = cs * x - sn * y;
                         mq[r] = sn * x + cs * y;
                     }
-                    double *vp = V + (size_t)a * K, *vq = V + (size_t)b * K;
-                    for (int r = lane; r < K; r += 32) {
-                        const double x = vp[r], y = vq[r];
-                        vp[r] = cs * x - sn * y;
-                        vq[r] = sn * x + cs * y;
-                    }
-                    if (lane == 0) rotated = 1;
+                    if (gl == 0) rotated = 1;
                 }
                 __syncthreads();
             }
@@ -114,10 +152,10 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
     }
 
     // singular values and descending order
-    for (int c = warp; c < K; c += CW) {
+    for (int c = warp; c < K; c += CT / 32) {
         double s = 0.0;
-        for (int r = lane; r < K; r += 32) s += M[(size_t)c * K + r] * M[(size_t)c * K + r];
-        s = warp_sum(s);
+        for (int r = lane; r < K; r += 32) s += W[(size_t)c * K + r] * W[(size_t)c * K + r];
+        s = group_sum<32>(s);
         if (lane == 0) sig[c] = sqrt(s);
     }
     __syncthreads();
@@ -165,16 +203,22 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
         rank_sh = r;
         if (t.rank_out) *t.rank_out = r;
         if (t.rank_task) *t.rank_task = r;
+        if (p.sweeps) atomicAdd(p.sweeps, sweeps);
     }
     __syncthreads();
-    const int r = rank_sh;
-    for (long long idx = tid; idx < (long long)K * (r > 0 ? r : 0); idx += CT) {
+    // left singular vectors, all K columns in decreasing sigma order
+    for (long long idx = tid; idx < (long long)K * K; idx += CT) {
         const int row = (int)(idx % K), i = (int)(idx / K);
         const int c = order[i];
         const double s = sig[c];
-        t.SU[(size_t)row + (size_t)i * K] = s > 0.0 ? M[(size_t)c * K + row] / s : 0.0;
-        t.SV[(size_t)row + (size_t)i * K] = V[(size_t)c * K + row] * s;
+        t.SU[idx] = s > 0.0 ? W[(size_t)c * K + row] / s : 0.0;
     }
+}
+
+template <int LP>
+void launch_lp(const CoreTask *d, int n, size_t smem, const CoreParams &p, cudaStream_t st) {
+    cudaFuncSetAttribute(k_core_svd<LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_core_svd<LP><<<n, CT, smem, st>>>(d, p);
 }
 
 }  // namespace
@@ -184,18 +228,16 @@ int core_smem_kmax() { return KMAX_SMEM; }
 void launch_core_svd_batched(const CoreTask *d_tasks, int ntasks, int kmax, const CoreParams &p,
                              cudaStream_t st) {
     if (ntasks <= 0) return;
+    if (kmax < 1) kmax = 1;
     size_t smem;
     if (kmax <= KMAX_SMEM)
-        smem = sizeof(double) * (2 * (size_t)kmax * kmax + (size_t)kmax) + sizeof(int) * kmax;
+        smem = sizeof(double) * ((size_t)kmax * kmax + kmax) + sizeof(int) * kmax;
     else
         smem = sizeof(double) * (size_t)kmax + sizeof(int) * kmax;
-    // tasks with K <= KMAX_SMEM keep M and V in shared memory
-    const size_t smem_small = sizeof(double) * (2 * (size_t)KMAX_SMEM * KMAX_SMEM + KMAX_SMEM) +
-                              sizeof(int) * KMAX_SMEM;
-    if (smem < smem_small && kmax > KMAX_SMEM) smem = smem_small;
-    if (kmax > KMAX_SMEM) smem = smem > smem_small ? smem : smem_small;
-    cudaFuncSetAttribute(k_core_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_core_svd<<<ntasks, CT, smem, st>>>(d_tasks, p);
+    smem = (smem + 15) / 16 * 16;
+    if (kmax <= 32) launch_lp<8>(d_tasks, ntasks, smem, p, st);
+    else if (kmax <= 96) launch_lp<16>(d_tasks, ntasks, smem, p, st);
+    else launch_lp<32>(d_tasks, ntasks, smem, p, st);
 }
 
 }  // namespace tlr

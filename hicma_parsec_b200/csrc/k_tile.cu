@@ -115,7 +115,52 @@ __global__ void __launch_bounds__(1024) k_logdiag_sum(const double *const *tiles
     if (threadIdx.x == 0) *out = red[0];
 }
 
+// Sum of squares of (X - Y) (Y may be null) over an m x n column-major
+// matrix; sym_lower counts only the lower triangle with off-diagonal
+// entries twice (Frobenius norm of the symmetric matrix stored in the lower
+// triangle, as dplasma_dlansy(Frobenius, Lower)).  Per-block partials.
+__global__ void __launch_bounds__(256) k_sumsq(const double *X, const double *Y, int m, int n, long long ld,
+                                               int sym_lower, double *partial) {
+    __shared__ double red[256];
+    double s = 0.0;
+    const long long total = (long long)m * n;
+    for (long long i = blockIdx.x * 256LL + threadIdx.x; i < total; i += (long long)gridDim.x * 256) {
+        const int r = (int)(i % m), c = (int)(i / m);
+        if (sym_lower && r < c) continue;
+        double v = X[(size_t)r + (size_t)c * ld];
+        if (Y) v -= Y[(size_t)r + (size_t)c * ld];
+        v *= v;
+        s += (sym_lower && r > c) ? 2.0 * v : v;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
+__global__ void k_sum_final(const double *partial, int n, double *out) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += 256) s += partial[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = red[0];
+}
+
 }  // namespace
+
+void launch_sumsq(const double *X, const double *Y, int m, int n, long long ld, int sym_lower, double *partial,
+                  int nblocks, double *out, cudaStream_t st) {
+    k_sumsq<<<nblocks, 256, 0, st>>>(X, Y, m, n, ld, sym_lower, partial);
+    k_sum_final<<<1, 256, 0, st>>>(partial, nblocks, out);
+}
 
 void launch_cov_batched(const CovParams &p, const CovTask *d_tasks, int ntasks, int max_nr, int max_nc,
                         cudaStream_t st) {

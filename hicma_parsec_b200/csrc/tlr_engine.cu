@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -61,11 +62,20 @@ extern "C" const char *hicma_tlr_last_error(void) { return g_err.c_str(); }
     } while (0)
 
 // --------------------------------------------------------------- context ---
+struct Arena {
+    char *base = nullptr;
+    size_t bytes = 0, off = 0;
+};
+
 struct hicma_tlr_ctx_s {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;      // bulk work
+    cudaStream_t stream_hi = nullptr;   // critical path (high priority): SYRK(k,k+1) + POTRF(k+1)
+    cudaStream_t cur = nullptr;         // stream the helpers launch on
     char *d_ws = nullptr;
-    size_t ws_bytes = 0, ws_off = 0;
+    size_t ws_bytes = 0;
+    Arena main_ar, hi_ar;               // workspace of `stream` / `stream_hi`
+    Arena *ar = nullptr;                // arena of `cur`
     char *h_stage = nullptr, *d_stage = nullptr;
     size_t stage_bytes = 0, stage_off = 0;
     int *d_flags = nullptr;     // [0] info, [1] overflow count
@@ -75,6 +85,13 @@ struct hicma_tlr_ctx_s {
     std::recursive_mutex mu;
     std::thread async_thread;
     int async_ret = 0;
+    std::set<hicma_tlr_desc_s *> descs;   // live descriptors, orphaned by fini
+    // per-kernel-class profiling (CUDA events around launches on `stream`)
+    bool prof = false;
+    struct ProfRec { int cls; cudaEvent_t a, b; double flops, bytes; };
+    std::vector<ProfRec> prof_recs;
+    std::vector<cudaEvent_t> ev_pool;
+    double prof_acc[8][4] = {};
 };
 
 struct hicma_tlr_desc_s {
@@ -89,7 +106,7 @@ struct hicma_tlr_desc_s {
     std::vector<int> h_rank;
     double *d_linv = nullptr;
     bool factored = false;
-    double stats[8] = {0};
+    double stats[12] = {0};
     double async_acc = 0;
     int async_fixed = 0, async_maxrank = 0;
 
@@ -112,21 +129,29 @@ namespace {
 size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
 int ctx_sync(hicma_tlr_ctx *c) {
+    CUDA_TRY(cudaStreamSynchronize(c->stream_hi));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->stage_off = 0;
     return 0;
 }
 
-void ws_reset(hicma_tlr_ctx *c) { c->ws_off = 0; }
+void ws_reset(hicma_tlr_ctx *c) { c->ar->off = 0; }
 template <class T>
 T *ws_alloc(hicma_tlr_ctx *c, size_t n) {
     const size_t bytes = align_up(n * sizeof(T) + 1);
-    if (c->ws_off + bytes > c->ws_bytes) return nullptr;
-    T *p = (T *)(c->d_ws + c->ws_off);
-    c->ws_off += bytes;
+    if (c->ar->off + bytes > c->ar->bytes) return nullptr;
+    T *p = (T *)(c->ar->base + c->ar->off);
+    c->ar->off += bytes;
     return p;
 }
-size_t ws_free(hicma_tlr_ctx *c) { return c->ws_bytes - c->ws_off; }
+size_t ws_free(hicma_tlr_ctx *c) { return c->ar->bytes - c->ar->off; }
+
+// Switch the helpers to the critical-path stream/arena and back.
+struct OnHi {
+    hicma_tlr_ctx *c;
+    explicit OnHi(hicma_tlr_ctx *ctx) : c(ctx) { c->cur = c->stream_hi; c->ar = &c->hi_ar; }
+    ~OnHi() { c->cur = c->stream; c->ar = &c->main_ar; }
+};
 
 template <class T>
 T *stage(hicma_tlr_ctx *c, const T *src, size_t n) {
@@ -134,22 +159,115 @@ T *stage(hicma_tlr_ctx *c, const T *src, size_t n) {
     const size_t bytes = align_up(raw + 1);
     if (bytes > c->stage_bytes) return nullptr;
     if (c->stage_off + bytes > c->stage_bytes) {
+        if (cudaStreamSynchronize(c->stream_hi) != cudaSuccess) return nullptr;
         if (cudaStreamSynchronize(c->stream) != cudaSuccess) return nullptr;
         c->stage_off = 0;
     }
     std::memcpy(c->h_stage + c->stage_off, src, raw);
     if (cudaMemcpyAsync(c->d_stage + c->stage_off, c->h_stage + c->stage_off, raw,
-                        cudaMemcpyHostToDevice, c->stream) != cudaSuccess)
+                        cudaMemcpyHostToDevice, c->cur) != cudaSuccess)
         return nullptr;
     T *d = (T *)(c->d_stage + c->stage_off);
     c->stage_off += bytes;
     return d;
 }
 
+enum { P_GEMM = 0, P_QR, P_QAPPLY, P_CORE, P_POTRF, P_COV, P_COPY, P_OTHER, P_NCLASS };
+
+cudaEvent_t pool_event(hicma_tlr_ctx *c) {
+    if (!c->ev_pool.empty()) {
+        cudaEvent_t e = c->ev_pool.back();
+        c->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+// Records the device time of the launches issued in its scope (profiling on).
+struct Prof {
+    hicma_tlr_ctx *c;
+    int cls;
+    double flops, bytes;
+    cudaEvent_t a = nullptr;
+    Prof(hicma_tlr_ctx *ctx, int k, double f, double b) : c(ctx), cls(k), flops(f), bytes(b) {
+        if (c->prof) {
+            a = pool_event(c);
+            cudaEventRecord(a, c->cur);
+        }
+    }
+    ~Prof() {
+        if (a) {
+            cudaEvent_t b2 = pool_event(c);
+            cudaEventRecord(b2, c->cur);
+            c->prof_recs.push_back({cls, a, b2, flops, bytes});
+        }
+    }
+};
+
+void prof_flush(hicma_tlr_ctx *c) {
+    for (auto &r : c->prof_recs) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(r.b) == cudaSuccess && cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            c->prof_acc[r.cls][0] += 1;
+            c->prof_acc[r.cls][1] += ms * 1e-3;
+            c->prof_acc[r.cls][2] += r.flops;
+            c->prof_acc[r.cls][3] += r.bytes;
+        }
+        c->ev_pool.push_back(r.a);
+        c->ev_pool.push_back(r.b);
+    }
+    c->prof_recs.clear();
+}
+
 int check_launch(hicma_tlr_ctx *c) {
     c->launches++;
     CUDA_TRY(cudaGetLastError());
     return 0;
+}
+
+int run_qr(hicma_tlr_ctx *c, std::vector<QRTask> &v, int m_max) {
+    if (v.empty()) return 0;
+    QRTask *d = stage(c, v.data(), v.size());
+    if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+    double fl = 0, by = 0;
+    for (auto &t : v) {
+        fl += 2.0 * t.m * (double)t.K * t.K - 2.0 / 3.0 * (double)t.K * t.K * t.K;
+        by += 16.0 * t.m * (double)t.K;
+    }
+    {
+        Prof pf(c, P_QR, fl, by);
+        launch_qr_batched(d, (int)v.size(), m_max, c->cur);
+    }
+    v.clear();
+    return check_launch(c);
+}
+
+int run_qapply(hicma_tlr_ctx *c, std::vector<QApplyTask> &v, int m_max) {
+    if (v.empty()) return 0;
+    QApplyTask *d = stage(c, v.data(), v.size());
+    if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+    double by = 0;
+    for (auto &t : v) by += 8.0 * t.m * (double)t.K;
+    {
+        Prof pf(c, P_QAPPLY, 0, by);
+        launch_qapply_batched(d, (int)v.size(), m_max, c->cur);
+    }
+    v.clear();
+    return check_launch(c);
+}
+
+int run_core(hicma_tlr_ctx *c, std::vector<CoreTask> &v, int kmax, const CoreParams &cp) {
+    if (v.empty()) return 0;
+    CoreTask *d = stage(c, v.data(), v.size());
+    if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+    {
+        Prof pf(c, P_CORE, 0, 0);
+        launch_core_svd_batched(d, (int)v.size(), std::max(kmax, 1), cp, c->cur);
+    }
+    v.clear();
+    return check_launch(c);
 }
 
 int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false) {
@@ -161,7 +279,13 @@ int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false) {
     GemmTask *dt = stage(c, v.data(), v.size());
     int *doff = stage(c, off.data(), off.size());
     if (!dt || !doff) { set_err("task staging failed"); return HICMA_TLR_ERR_CUDA; }
-    launch_gemm_batched(dt, doff, (int)v.size(), off.back(), c->stream, fp32);
+    double fl = 0, by = 0;
+    for (auto &t : v) {
+        fl += 2.0 * t.m * (double)t.n * t.k;
+        by += 8.0 * ((double)t.m * t.k + (double)t.k * t.n + (t.beta != 0.0 ? 2.0 : 1.0) * t.m * (double)t.n);
+    }
+    Prof pf(c, P_GEMM, fl, by);
+    launch_gemm_batched(dt, doff, (int)v.size(), off.back(), c->cur, fp32);
     v.clear();
     return check_launch(c);
 }
@@ -172,7 +296,10 @@ int run_copies(hicma_tlr_ctx *c, std::vector<CopyTask> &v) {
     for (auto &t : v) maxc = std::max(maxc, t.cols);
     CopyTask *dt = stage(c, v.data(), v.size());
     if (!dt) { set_err("task staging failed"); return HICMA_TLR_ERR_CUDA; }
-    launch_copy_batched(dt, (int)v.size(), maxc, c->stream);
+    double by = 0;
+    for (auto &t : v) by += 16.0 * t.rows * (double)t.cols;
+    Prof pf(c, P_COPY, 0, by);
+    launch_copy_batched(dt, (int)v.size(), maxc, c->cur);
     v.clear();
     return check_launch(c);
 }
@@ -191,8 +318,9 @@ CopyTask make_copy(const double *src, int lds, double *dst, int ldd, int rows, i
 int potrf_tile(hicma_tlr_ctx *c, double *A, int n, int lda, double *Linv, int ldl, int *d_info,
                int info_base) {
     const int DBK = 64;
-    cudaStream_t st = c->stream;
-    const size_t mark = c->ws_off;
+    cudaStream_t st = c->cur;
+    const size_t mark = c->ar->off;
+    Prof pf(c, P_POTRF, (double)n * n * n / 3.0 * (Linv ? 2.0 : 1.0), 8.0 * n * (double)n * (Linv ? 3.0 : 2.0));
     double *dscr = nullptr;
     if (!Linv) {
         dscr = ws_alloc<double>(c, DBK * DBK);
@@ -232,7 +360,7 @@ int potrf_tile(hicma_tlr_ctx *c, double *A, int n, int lda, double *Linv, int ld
             TRY(check_launch(c));
         }
     }
-    c->ws_off = mark;
+    c->ar->off = mark;
     return 0;
 }
 
@@ -255,29 +383,43 @@ size_t recomp_ws_bytes(int nb, const RecompTask &t) {
     const int pb = qr_panel_width(nb);
     const size_t npan = (size_t)(K + pb - 1) / pb + 1;
     size_t b = 0;
-    b += align_up(sizeof(double) * (size_t)nb * K + 1) * 2;        // Us, Vs
+    b += align_up(sizeof(double) * (size_t)nb * K + 1) * 3;        // Us, Vs, Vkeep
     b += align_up(sizeof(double) * (size_t)K + 1) * 2;             // tau
     b += align_up(sizeof(double) * npan * pb * pb + 1) * 2;        // T factors
-    b += align_up(sizeof(double) * (size_t)K * K + 1) * 2;         // SU, SV
-    if (K > core_smem_kmax()) b += align_up(sizeof(double) * 2 * (size_t)K * K + 1);
+    b += align_up(sizeof(double) * (size_t)K * K + 1) * 3;         // SU, RUc, T1
+    if (K > core_smem_kmax()) b += align_up(sizeof(double) * (size_t)K * K + 1);
     if (t.Bv) b += align_up(sizeof(double) * (size_t)t.rb * t.ra + 1);
     return b + 1024;
+}
+
+// Core-SVD launches bucketed by K so that small cores run several CTAs per SM.
+int run_core_buckets(hicma_tlr_ctx *c, std::vector<CoreTask> &cores, const CoreParams &cp) {
+    static const int edges[] = {32, 64, 96, 128, 160, 1 << 30};
+    std::vector<CoreTask> bucket;
+    int lo = -1;
+    for (int e : edges) {
+        int kmax = 0;
+        for (auto &t : cores)
+            if (t.K > lo && t.K <= e) { bucket.push_back(t); kmax = std::max(kmax, t.K); }
+        if (!bucket.empty()) TRY(run_core(c, bucket, kmax, cp));
+        lo = e;
+    }
+    cores.clear();
+    return 0;
 }
 
 int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, double acc, int maxrank,
                    int fixed_rank, int *d_rank_task_base, bool fp32) {
     if (tasks.empty()) return 0;
-    cudaStream_t st = c->stream;
-    const size_t mark = c->ws_off;
+    const size_t mark = c->ar->off;
     size_t i0 = 0;
     while (i0 < tasks.size()) {
-        c->ws_off = mark;
-        std::vector<CopyTask> copies;
-        std::vector<GemmTask> g1, g2;
+        c->ar->off = mark;
+        std::vector<CopyTask> copies, keeps;
+        std::vector<GemmTask> g1, g2, g3, g4;
         std::vector<QRTask> qrs;
         std::vector<CoreTask> cores;
         std::vector<QApplyTask> apps;
-        int kmax = 0;
         size_t i = i0;
         int *rank_task = d_rank_task_base;
         for (; i < tasks.size(); ++i) {
@@ -297,10 +439,12 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             const size_t npan = (size_t)(K + pb - 1) / pb + 1;
             double *Us = ws_alloc<double>(c, (size_t)nb * K);
             double *Vs = ws_alloc<double>(c, (size_t)nb * K);
+            double *Vk = ws_alloc<double>(c, (size_t)nb * K);
             double *tauU = ws_alloc<double>(c, K), *tauV = ws_alloc<double>(c, K);
             double *TU = ws_alloc<double>(c, npan * pb * pb), *TV = ws_alloc<double>(c, npan * pb * pb);
-            double *SU = ws_alloc<double>(c, (size_t)K * K), *SV = ws_alloc<double>(c, (size_t)K * K);
-            double *work = K > core_smem_kmax() ? ws_alloc<double>(c, 2 * (size_t)K * K) : nullptr;
+            double *SU = ws_alloc<double>(c, (size_t)K * K), *RUc = ws_alloc<double>(c, (size_t)K * K);
+            double *T1 = ws_alloc<double>(c, (size_t)K * K);
+            double *work = K > core_smem_kmax() ? ws_alloc<double>(c, (size_t)K * K) : nullptr;
             if (t.rc > 0) {
                 copies.push_back(make_copy(t.Cu, nb, Us, nb, nb, t.rc));
                 copies.push_back(make_copy(t.Cv, nb, Vs, nb, nb, t.rc));
@@ -316,40 +460,34 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                     g1.push_back(make_gemm(0, 0, nb, t.ra, nb, -1.0, t.Bu, nb, t.Av, nb, 0.0, Y, nb));
                 }
             }
+            keeps.push_back(make_copy(Vs, nb, Vk, nb, nb, K));
             qrs.push_back(QRTask{Us, tauU, TU, nb, K, nb});
             qrs.push_back(QRTask{Vs, tauV, TV, nb, K, nb});
             ct.RU = Us; ct.RV = Vs; ct.ldru = nb; ct.ldrv = nb;
-            ct.SU = SU; ct.SV = SV; ct.work = work;
+            ct.SU = SU; ct.RUc = RUc; ct.work = work;
             cores.push_back(ct);
-            QApplyTask au{Us, TU, SU, t.outU, ct.rank_task, nb, K, nb, K, nb, maxrank};
-            QApplyTask av{Vs, TV, SV, t.outV, ct.rank_task, nb, K, nb, K, nb, maxrank};
-            apps.push_back(au);
-            apps.push_back(av);
-            kmax = std::max(kmax, K);
+            apps.push_back(QApplyTask{Us, TU, SU, t.outU, ct.rank_task, nb, K, nb, K, nb, maxrank});
+            // V Sigma = M^T U = R_V (R_U^T U): new V = Vs_orig (R_U^T U_r)
+            GemmTask a = make_gemm(1, 0, K, K, K, 1.0, RUc, K, SU, K, 0.0, T1, K);
+            a.n_dev = ct.rank_task;
+            g3.push_back(a);
+            GemmTask b = make_gemm(0, 0, nb, maxrank, K, 1.0, Vk, nb, T1, K, 0.0, t.outV, nb);
+            b.n_dev = ct.rank_task;
+            g4.push_back(b);
         }
         TRY(run_copies(c, copies));
         TRY(run_gemms(c, g1, fp32));
         TRY(run_gemms(c, g2, fp32));
-        if (!qrs.empty()) {
-            QRTask *dq = stage(c, qrs.data(), qrs.size());
-            if (!dq) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
-            launch_qr_batched(dq, (int)qrs.size(), nb, st);
-            TRY(check_launch(c));
-        }
-        CoreParams cp{0, acc, maxrank, fixed_rank, nb, c->d_flags + 1};
-        CoreTask *dc = stage(c, cores.data(), cores.size());
-        if (!dc) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
-        launch_core_svd_batched(dc, (int)cores.size(), std::max(kmax, 1), cp, st);
-        TRY(check_launch(c));
-        if (!apps.empty()) {
-            QApplyTask *da = stage(c, apps.data(), apps.size());
-            if (!da) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
-            launch_qapply_batched(da, (int)apps.size(), nb, st);
-            TRY(check_launch(c));
-        }
+        TRY(run_copies(c, keeps));
+        TRY(run_qr(c, qrs, nb));
+        CoreParams cp{0, acc, maxrank, fixed_rank, nb, c->d_flags + 1, c->d_flags + 2};
+        TRY(run_core_buckets(c, cores, cp));
+        TRY(run_qapply(c, apps, nb));
+        TRY(run_gemms(c, g3));
+        TRY(run_gemms(c, g4));
         i0 = i;
     }
-    c->ws_off = mark;
+    c->ar->off = mark;
     return 0;
 }
 
@@ -470,6 +608,10 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     auto *c = new hicma_tlr_ctx_s();
     c->device = device;
     CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    int prio_lo = 0, prio_hi = 0;
+    CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    CUDA_TRY(cudaStreamCreateWithPriority(&c->stream_hi, cudaStreamNonBlocking, prio_hi));
+    c->cur = c->stream;
     size_t free_b = 0, total_b = 0;
     CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
     if (workspace_bytes == 0) {
@@ -483,6 +625,14 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
         delete c;
         return HICMA_TLR_ERR_OOM;
     }
+    {
+        const size_t hi = std::min<size_t>(c->ws_bytes / 8, (size_t)512 << 20);
+        c->hi_ar.base = c->d_ws;
+        c->hi_ar.bytes = hi;
+        c->main_ar.base = c->d_ws + hi;
+        c->main_ar.bytes = c->ws_bytes - hi;
+        c->ar = &c->main_ar;
+    }
     c->stage_bytes = (size_t)64 << 20;
     CUDA_TRY(cudaMallocHost(&c->h_stage, c->stage_bytes));
     CUDA_TRY(cudaMalloc(&c->d_stage, c->stage_bytes));
@@ -493,16 +643,33 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     return 0;
 }
 
+static void desc_free_device(hicma_tlr_desc *A) {
+    cudaFree(A->d_pts);
+    cudaFree(A->d_band);
+    cudaFree(A->d_lr);
+    cudaFree(A->d_rank);
+    cudaFree(A->d_linv);
+    A->d_pts = A->d_band = A->d_lr = A->d_linv = nullptr;
+    A->d_rank = nullptr;
+}
+
 int hicma_tlr_fini(hicma_tlr_ctx *c) {
     if (!c) return 0;
     if (c->async_thread.joinable()) c->async_thread.join();
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    for (hicma_tlr_desc *A : c->descs) {   // descriptors outliving their context
+        desc_free_device(A);
+        A->ctx = nullptr;
+    }
+    c->descs.clear();
     cudaFree(c->d_ws);
     cudaFree(c->d_stage);
     cudaFreeHost(c->h_stage);
     cudaFree(c->d_flags);
     cudaFree(c->d_scal);
+    cudaStreamSynchronize(c->stream_hi);
+    cudaStreamDestroy(c->stream_hi);
     cudaStreamDestroy(c->stream);
     delete c;
     return 0;
@@ -551,19 +718,21 @@ int hicma_tlr_desc_create(hicma_tlr_ctx *c, int N, int NB, int maxrank, int band
     for (int m = 0; m < NT; ++m)
         for (int n = 0; n <= m - A->band; ++n) A->h_rank[(size_t)n * NT + m] = 0;
     CUDA_TRY(cudaMemcpy(A->d_rank, A->h_rank.data(), (size_t)NT * NT * sizeof(int), cudaMemcpyHostToDevice));
+    c->descs.insert(A);
     *out = A;
     return 0;
 }
 
 int hicma_tlr_desc_destroy(hicma_tlr_desc *A) {
     if (!A) return 0;
-    cudaSetDevice(A->ctx->device);
-    cudaStreamSynchronize(A->ctx->stream);
-    cudaFree(A->d_pts);
-    cudaFree(A->d_band);
-    cudaFree(A->d_lr);
-    cudaFree(A->d_rank);
-    cudaFree(A->d_linv);
+    if (A->ctx) {
+        hicma_tlr_ctx *c = A->ctx;
+        std::lock_guard<std::recursive_mutex> lk(c->mu);
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->stream);
+        desc_free_device(A);
+        c->descs.erase(A);
+    }
     delete A;
     return 0;
 }
@@ -644,6 +813,7 @@ static int gen_band_tiles(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_p
             tasks.push_back(CovTask{A->dense(m, n), A->NB, m * A->NB, n * A->NB, A->NB, A->NB});
     CovTask *dt = stage(c, tasks.data(), tasks.size());
     if (!dt) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+    Prof pf(c, P_COV, 0, 8.0 * tasks.size() * (double)A->NB * A->NB);
     launch_cov_batched(cov_params(A, prob), dt, (int)tasks.size(), A->NB, A->NB, c->stream);
     return check_launch(c);
 }
@@ -662,24 +832,24 @@ static size_t compress_ws_bytes(int nb, int s) {
     const int pb = qr_panel_width(nb);
     const size_t npan = (size_t)(s + pb - 1) / pb + 1;
     size_t b = 0;
-    b += align_up(sizeof(double) * (size_t)nb * s + 1) * 3;   // Y, Q, W
+    b += align_up(sizeof(double) * (size_t)nb * s + 1) * 4;   // Y, Q, W, Wkeep
     b += align_up(sizeof(double) * (size_t)s + 1) * 2;
     b += align_up(sizeof(double) * npan * pb * pb + 1) * 2;
-    b += align_up(sizeof(double) * (size_t)s * s + 1) * 2;
-    if (s > core_smem_kmax()) b += align_up(sizeof(double) * 2 * (size_t)s * s + 1);
+    b += align_up(sizeof(double) * (size_t)s * s + 1);
+    if (s > core_smem_kmax()) b += align_up(sizeof(double) * (size_t)s * s + 1);
     return b + 1024;
 }
 
 static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const double *Omega, int s,
                         std::vector<CompressTask> &tasks, const double *d_identity, int *d_rank_task_base) {
-    cudaStream_t st = c->stream;
     const int pb = qr_panel_width(nb);
     const size_t npan = (size_t)(s + pb - 1) / pb + 1;
-    const size_t mark = c->ws_off;
+    const size_t mark = c->ar->off;
     size_t i0 = 0;
     while (i0 < tasks.size()) {
-        c->ws_off = mark;
-        std::vector<GemmTask> gy, gw;
+        c->ar->off = mark;
+        std::vector<GemmTask> gy, gw, gv;
+        std::vector<CopyTask> keeps;
         std::vector<QRTask> qy, qw;
         std::vector<QApplyTask> aq, au;
         std::vector<CoreTask> cores;
@@ -693,46 +863,42 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
             double *Y = ws_alloc<double>(c, (size_t)nb * s);
             double *Q = ws_alloc<double>(c, (size_t)nb * s);
             double *W = ws_alloc<double>(c, (size_t)nb * s);
+            double *Wk = ws_alloc<double>(c, (size_t)nb * s);
             double *tauY = ws_alloc<double>(c, s), *tauW = ws_alloc<double>(c, s);
             double *TY = ws_alloc<double>(c, npan * pb * pb), *TW = ws_alloc<double>(c, npan * pb * pb);
-            double *SU = ws_alloc<double>(c, (size_t)s * s), *SV = ws_alloc<double>(c, (size_t)s * s);
-            double *work = s > core_smem_kmax() ? ws_alloc<double>(c, 2 * (size_t)s * s) : nullptr;
+            double *SU = ws_alloc<double>(c, (size_t)s * s);
+            double *work = s > core_smem_kmax() ? ws_alloc<double>(c, (size_t)s * s) : nullptr;
             int *rt = d_rank_task_base + (i - i0);
             gy.push_back(make_gemm(0, 0, nb, s, nb, 1.0, t.A, nb, Omega, nb, 0.0, Y, nb));
             qy.push_back(QRTask{Y, tauY, TY, nb, s, nb});
             aq.push_back(QApplyTask{Y, TY, d_identity, Q, nullptr, nb, s, nb, s, nb, s});
             gw.push_back(make_gemm(1, 0, nb, s, nb, 1.0, t.A, nb, Q, nb, 0.0, W, nb));
+            keeps.push_back(make_copy(W, nb, Wk, nb, nb, s));
             qw.push_back(QRTask{W, tauW, TW, nb, s, nb});
             CoreTask ct{};
             ct.RU = nullptr; ct.RV = W; ct.ldru = nb; ct.ldrv = nb;
-            ct.SU = SU; ct.SV = SV; ct.work = work;
+            ct.SU = SU; ct.RUc = nullptr; ct.work = work;
             ct.rank_out = t.rank_dst; ct.rank_task = rt; ct.K = s;
             cores.push_back(ct);
             au.push_back(QApplyTask{Y, TY, SU, t.outU, rt, nb, s, nb, s, nb, maxrank});
-            au.push_back(QApplyTask{W, TW, SV, t.outV, rt, nb, s, nb, s, nb, maxrank});
+            // V Sigma = (A^T Q) U_r  (R_U = I)
+            GemmTask g = make_gemm(0, 0, nb, maxrank, s, 1.0, Wk, nb, SU, s, 0.0, t.outV, nb);
+            g.n_dev = rt;
+            gv.push_back(g);
         }
         TRY(run_gemms(c, gy));
-        QRTask *d1 = stage(c, qy.data(), qy.size());
-        launch_qr_batched(d1, (int)qy.size(), nb, st);
-        TRY(check_launch(c));
-        QApplyTask *d2 = stage(c, aq.data(), aq.size());
-        launch_qapply_batched(d2, (int)aq.size(), nb, st);
-        TRY(check_launch(c));
+        TRY(run_qr(c, qy, nb));
+        TRY(run_qapply(c, aq, nb));
         TRY(run_gemms(c, gw));
-        QRTask *d3 = stage(c, qw.data(), qw.size());
-        launch_qr_batched(d3, (int)qw.size(), nb, st);
-        TRY(check_launch(c));
-        CoreParams cp{1, tol, maxrank, 0, nb, nullptr};
-        CoreTask *d4 = stage(c, cores.data(), cores.size());
-        launch_core_svd_batched(d4, (int)cores.size(), s, cp, st);
-        TRY(check_launch(c));
-        QApplyTask *d5 = stage(c, au.data(), au.size());
-        launch_qapply_batched(d5, (int)au.size(), nb, st);
-        TRY(check_launch(c));
-        if (!d1 || !d2 || !d3 || !d4 || !d5) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+        TRY(run_copies(c, keeps));
+        TRY(run_qr(c, qw, nb));
+        CoreParams cp{1, tol, maxrank, 0, nb, nullptr, nullptr};
+        TRY(run_core_buckets(c, cores, cp));
+        TRY(run_qapply(c, au, nb));
+        TRY(run_gemms(c, gv));
         i0 = i;
     }
-    c->ws_off = mark;
+    c->ar->off = mark;
     return 0;
 }
 
@@ -771,7 +937,7 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
     const CovParams cp = cov_params(A, prob);
     for (size_t t0 = 0; t0 < tiles.size(); t0 += chunk) {
         const size_t t1 = std::min(tiles.size(), t0 + chunk);
-        const size_t mark = c->ws_off;
+        const size_t mark = c->ar->off;
         std::vector<CovTask> cov;
         std::vector<CompressTask> comp;
         for (size_t i = t0; i < t1; ++i) {
@@ -782,10 +948,13 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
         }
         CovTask *dcov = stage(c, cov.data(), cov.size());
         if (!dcov) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
-        launch_cov_batched(cp, dcov, (int)cov.size(), NB, NB, c->stream);
+        {
+            Prof pf(c, P_COV, 0, 8.0 * cov.size() * (double)NB * NB);
+            launch_cov_batched(cp, dcov, (int)cov.size(), NB, NB, c->stream);
+        }
         TRY(check_launch(c));
         TRY(run_compress(c, NB, maxrank, tol, Omega, s, comp, Ident, rtask));
-        c->ws_off = mark;
+        c->ar->off = mark;
     }
     TRY(ctx_sync(c));
     CUDA_TRY(cudaMemcpy(A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
@@ -908,10 +1077,55 @@ int hicma_tlr_band_regenerate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, con
 }
 
 // ------------------------------------------------------- factorization -----
+// SYRK(k, m) for the listed m on the current stream/arena:
+// dense T -= A A^T (CORE_dsyrk), low rank T -= U (V^T V) U^T (HCORE_dsyrk),
+// HiCMA_dpotrf_L_2flow.jdf:503-565; rank 0 skips (:511-513).
+static int run_syrk(hicma_tlr_ctx *c, hicma_tlr_desc *A, int k, const std::vector<int> &ms) {
+    const int NB = A->NB;
+    const size_t mark = c->ar->off;
+    std::vector<GemmTask> g1, g2, g3;
+    for (int m : ms) {
+        if (A->is_dense(m, k)) {
+            g1.push_back(make_gemm(0, 1, NB, NB, NB, -1.0, A->dense(m, k), NB, A->dense(m, k), NB, 1.0,
+                                   A->dense(m, m), NB));
+            continue;
+        }
+        const int r = A->rank(m, k);
+        if (r == 0) continue;
+        double *W = ws_alloc<double>(c, (size_t)r * r);
+        double *X = ws_alloc<double>(c, (size_t)NB * r);
+        if (!W || !X) {
+            TRY(run_gemms(c, g1)); TRY(run_gemms(c, g2)); TRY(run_gemms(c, g3));
+            c->ar->off = mark;
+            W = ws_alloc<double>(c, (size_t)r * r);
+            X = ws_alloc<double>(c, (size_t)NB * r);
+            if (!W || !X) { set_err("workspace too small (syrk)"); return HICMA_TLR_ERR_OOM; }
+        }
+        g1.push_back(make_gemm(1, 0, r, r, NB, 1.0, A->V(m, k), NB, A->V(m, k), NB, 0.0, W, r));
+        g2.push_back(make_gemm(0, 0, NB, r, r, 1.0, A->U(m, k), NB, W, r, 0.0, X, NB));
+        g3.push_back(make_gemm(0, 1, NB, NB, r, -1.0, X, NB, A->U(m, k), NB, 1.0, A->dense(m, m), NB));
+    }
+    TRY(run_gemms(c, g1));
+    TRY(run_gemms(c, g2));
+    TRY(run_gemms(c, g3));
+    c->ar->off = mark;
+    return 0;
+}
+
+static unsigned long syrk_ops(const hicma_tlr_desc *A, int k, int m) {
+    const unsigned long NB = A->NB;
+    if (A->is_dense(m, k)) return op_counts('m', NB, NB, NB, 0);
+    const unsigned long r = A->rank(m, k);
+    return op_counts('m', r, r, NB, 0) + op_counts('m', NB, r, r, 0) + op_counts('m', NB, NB, r, 0);
+}
+
+// Per-panel schedule with a one-panel lookahead: the critical chain
+// TRSM(k+1,k) -> SYRK(k,k+1) -> POTRF(k+1) runs on the high-priority stream
+// and overlaps the remaining SYRK/GEMM work of panel k on the bulk stream.
 static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_rank, int maxrank,
-                     unsigned long *tileops, unsigned long *opcounters, double *cpt, int verbose) {
+                     unsigned long *tileops, unsigned long *opcounters, double *cpt, int verbose,
+                     bool lookahead) {
     const int NT = A->NT, NB = A->NB, band = A->band;
-    cudaStream_t st = c->stream;
     const bool mixed = c->precision == HICMA_TLR_PREC_MIXED;
     if (!A->d_linv) {
         if (cudaMalloc(&A->d_linv, (size_t)NT * NB * NB * sizeof(double)) != cudaSuccess) {
@@ -920,16 +1134,23 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             return HICMA_TLR_ERR_OOM;
         }
     }
-    ws_reset(c);
-    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 2 * sizeof(int), st));
+    c->cur = c->stream;
+    c->ar = &c->main_ar;
+    c->main_ar.off = 0;
+    c->hi_ar.off = 0;
+    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 3 * sizeof(int), c->stream));
+    TRY(ctx_sync(c));
     int *d_info = c->d_flags;
     int *rtask = ws_alloc<int>(c, (size_t)NT * NT + 16);
     if (!rtask) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
-    const size_t base_mark = c->ws_off;
+    const size_t base_mark = c->ar->off;
     std::vector<unsigned long> tops((size_t)NT * NT, 0);
     unsigned long op_total = 0;
-    cudaEvent_t ev[5];
+    enum { P0, P1, T0, T1, S0, S1, G0, G1, NEV };
+    cudaEvent_t ev[NEV], evP, evT;
     for (auto &e : ev) CUDA_TRY(cudaEventCreate(&e));
+    CUDA_TRY(cudaEventCreateWithFlags(&evP, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&evT, cudaEventDisableTiming));
     double t_phase[4] = {0, 0, 0, 0};
     const auto t_start = std::chrono::steady_clock::now();
     const long long launches0 = c->launches;
@@ -938,41 +1159,48 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         tops[(size_t)i * NT + j] += cnt;
         op_total += cnt;
     };
+    auto elapsed = [&](cudaEvent_t a, cudaEvent_t b) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms * 1e-3;
+    };
+    // POTRF(0)
+    {
+        OnHi h(c);
+        c->ar->off = 0;
+        CUDA_TRY(cudaEventRecord(ev[P0], c->cur));
+        TRY(potrf_tile(c, A->dense(0, 0), NB, NB, A->linv(0), NB, d_info, 0));
+        CUDA_TRY(cudaEventRecord(ev[P1], c->cur));
+        CUDA_TRY(cudaEventRecord(evP, c->cur));
+    }
+    log_op(op_counts('c', NB, 0, 0, 0), 0, 0);
+    CUDA_TRY(cudaEventSynchronize(ev[P1]));
+    t_phase[0] += elapsed(ev[P0], ev[P1]);
     for (int k = 0; k < NT; ++k) {
-        CUDA_TRY(cudaEventRecord(ev[0], st));
-        // ---- POTRF(k)
-        log_op(op_counts('c', NB, 0, 0, 0), k, k);
-        TRY(potrf_tile(c, A->dense(k, k), NB, NB, A->linv(k), NB, d_info, k * NB));
-        CUDA_TRY(cudaEventRecord(ev[1], st));
         const double *Li = A->linv(k);
-        // ---- TRSM(m, k): dense C <- C L^-T ; low rank V <- L^-1 V
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, evP, 0));
+        // ---- TRSM(m, k): dense C <- C L^-T ; low rank V <- L^-1 V (:366-401)
+        CUDA_TRY(cudaEventRecord(ev[T0], c->stream));
         {
-            c->ws_off = base_mark;
+            c->ar->off = base_mark;
             std::vector<GemmTask> g;
             std::vector<CopyTask> cp;
             for (int m = k + 1; m < NT; ++m) {
-                if (A->is_dense(m, k)) {
-                    log_op(op_counts('t', NB, NB, 1, 0), m, k);
-                    double *tmp = ws_alloc<double>(c, (size_t)NB * NB);
-                    if (!tmp) {
-                        TRY(run_gemms(c, g)); TRY(run_copies(c, cp));
-                        c->ws_off = base_mark;
-                        tmp = ws_alloc<double>(c, (size_t)NB * NB);
-                        if (!tmp) { set_err("workspace too small (trsm)"); return HICMA_TLR_ERR_OOM; }
-                    }
+                const bool dense = A->is_dense(m, k);
+                const int r = dense ? NB : A->rank(m, k);
+                log_op(op_counts('t', NB, r, 1, 0), m, k);
+                if (r == 0) continue;
+                double *tmp = ws_alloc<double>(c, (size_t)NB * r);
+                if (!tmp) {
+                    TRY(run_gemms(c, g)); TRY(run_copies(c, cp));
+                    c->ar->off = base_mark;
+                    tmp = ws_alloc<double>(c, (size_t)NB * r);
+                    if (!tmp) { set_err("workspace too small (trsm)"); return HICMA_TLR_ERR_OOM; }
+                }
+                if (dense) {
                     g.push_back(make_gemm(0, 1, NB, NB, NB, 1.0, A->dense(m, k), NB, Li, NB, 0.0, tmp, NB));
                     cp.push_back(make_copy(tmp, NB, A->dense(m, k), NB, NB, NB));
                 } else {
-                    const int r = A->rank(m, k);
-                    log_op(op_counts('t', NB, r, 1, 0), m, k);
-                    if (r == 0) continue;
-                    double *tmp = ws_alloc<double>(c, (size_t)NB * r);
-                    if (!tmp) {
-                        TRY(run_gemms(c, g)); TRY(run_copies(c, cp));
-                        c->ws_off = base_mark;
-                        tmp = ws_alloc<double>(c, (size_t)NB * r);
-                        if (!tmp) { set_err("workspace too small (trsm)"); return HICMA_TLR_ERR_OOM; }
-                    }
                     g.push_back(make_gemm(0, 0, NB, r, NB, 1.0, Li, NB, A->V(m, k), NB, 0.0, tmp, NB));
                     cp.push_back(make_copy(tmp, NB, A->V(m, k), NB, NB, r));
                 }
@@ -980,45 +1208,39 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             TRY(run_gemms(c, g));
             TRY(run_copies(c, cp));
         }
-        CUDA_TRY(cudaEventRecord(ev[2], st));
-        // ---- SYRK(k, m)
-        {
-            c->ws_off = base_mark;
-            std::vector<GemmTask> g1, g2, g3;
-            for (int m = k + 1; m < NT; ++m) {
-                if (A->is_dense(m, k)) {
-                    log_op(op_counts('m', NB, NB, NB, 0), m, m);
-                    g1.push_back(make_gemm(0, 1, NB, NB, NB, -1.0, A->dense(m, k), NB, A->dense(m, k), NB, 1.0,
-                                           A->dense(m, m), NB));
-                } else {
-                    const int r = A->rank(m, k);
-                    log_op(op_counts('m', r, r, NB, 0) + op_counts('m', NB, r, r, 0) + op_counts('m', NB, NB, r, 0), m, m);
-                    if (r == 0) continue;
-                    double *W = ws_alloc<double>(c, (size_t)r * r);
-                    double *X = ws_alloc<double>(c, (size_t)NB * r);
-                    if (!W || !X) {
-                        TRY(run_gemms(c, g1)); TRY(run_gemms(c, g2)); TRY(run_gemms(c, g3));
-                        c->ws_off = base_mark;
-                        W = ws_alloc<double>(c, (size_t)r * r);
-                        X = ws_alloc<double>(c, (size_t)NB * r);
-                        if (!W || !X) { set_err("workspace too small (syrk)"); return HICMA_TLR_ERR_OOM; }
-                    }
-                    g1.push_back(make_gemm(1, 0, r, r, NB, 1.0, A->V(m, k), NB, A->V(m, k), NB, 0.0, W, r));
-                    g2.push_back(make_gemm(0, 0, NB, r, r, 1.0, A->U(m, k), NB, W, r, 0.0, X, NB));
-                    g3.push_back(make_gemm(0, 1, NB, NB, r, -1.0, X, NB, A->U(m, k), NB, 1.0, A->dense(m, m), NB));
-                }
-            }
-            TRY(run_gemms(c, g1));
-            TRY(run_gemms(c, g2));
-            TRY(run_gemms(c, g3));
-        }
-        CUDA_TRY(cudaEventRecord(ev[3], st));
-        // ---- GEMM(m, n, k)
+        CUDA_TRY(cudaEventRecord(ev[T1], c->stream));
+        CUDA_TRY(cudaEventRecord(evT, c->stream));
         std::vector<RecompTask> rec;
-        std::vector<int> rec_case;   // 0: B low rank, 1: B dense
+        std::vector<int> rec_case;
         std::vector<std::array<int, 5>> rec_meta;
-        {
-            c->ws_off = base_mark;
+        if (k + 1 < NT) {
+            // ---- critical chain: SYRK(k, k+1) + POTRF(k+1)
+            log_op(syrk_ops(A, k, k + 1), k + 1, k + 1);
+            log_op(op_counts('c', NB, 0, 0, 0), k + 1, k + 1);
+            {
+                OnHi h(c);
+                if (!lookahead) c->cur = c->stream;
+                c->ar->off = 0;
+                CUDA_TRY(cudaStreamWaitEvent(c->cur, evT, 0));
+                TRY(run_syrk(c, A, k, std::vector<int>{k + 1}));
+                CUDA_TRY(cudaEventRecord(ev[P0], c->cur));
+                TRY(potrf_tile(c, A->dense(k + 1, k + 1), NB, NB, A->linv(k + 1), NB, d_info, (k + 1) * NB));
+                CUDA_TRY(cudaEventRecord(ev[P1], c->cur));
+                CUDA_TRY(cudaEventRecord(evP, c->cur));
+            }
+            // ---- SYRK(k, m), m > k+1
+            CUDA_TRY(cudaEventRecord(ev[S0], c->stream));
+            c->ar->off = base_mark;
+            std::vector<int> ms;
+            for (int m = k + 2; m < NT; ++m) {
+                ms.push_back(m);
+                log_op(syrk_ops(A, k, m), m, m);
+            }
+            TRY(run_syrk(c, A, k, ms));
+            CUDA_TRY(cudaEventRecord(ev[S1], c->stream));
+            // ---- GEMM(m, n, k) (:699-1097)
+            CUDA_TRY(cudaEventRecord(ev[G0], c->stream));
+            c->ar->off = base_mark;
             std::vector<GemmTask> g1, g2, g3;
             for (int m = k + 2; m < NT; ++m) {
                 for (int n = k + 1; n < m; ++n) {
@@ -1033,7 +1255,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                         double *tmp = ws_alloc<double>(c, (size_t)ra * NB);
                         if (!tmp) {
                             TRY(run_gemms(c, g1)); TRY(run_gemms(c, g2)); TRY(run_gemms(c, g3));
-                            c->ws_off = base_mark;
+                            c->ar->off = base_mark;
                             tmp = ws_alloc<double>(c, (size_t)ra * NB);
                             if (!tmp) { set_err("workspace too small (gemm)"); return HICMA_TLR_ERR_OOM; }
                         }
@@ -1047,7 +1269,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                         double *tmp = ws_alloc<double>(c, (size_t)NB * std::max(ra, rb));
                         if (!rr || !tmp) {
                             TRY(run_gemms(c, g1)); TRY(run_gemms(c, g2)); TRY(run_gemms(c, g3));
-                            c->ws_off = base_mark;
+                            c->ar->off = base_mark;
                             rr = ws_alloc<double>(c, (size_t)ra * rb);
                             tmp = ws_alloc<double>(c, (size_t)NB * std::max(ra, rb));
                             if (!rr || !tmp) { set_err("workspace too small (gemm)"); return HICMA_TLR_ERR_OOM; }
@@ -1081,10 +1303,10 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             TRY(run_gemms(c, g1));
             TRY(run_gemms(c, g2));
             TRY(run_gemms(c, g3));
-            c->ws_off = base_mark;
+            c->ar->off = base_mark;
             TRY(run_recompress(c, NB, rec, acc, maxrank, fixed_rank, rtask, mixed));
+            CUDA_TRY(cudaEventRecord(ev[G1], c->stream));
         }
-        CUDA_TRY(cudaEventRecord(ev[4], st));
         // ---- panel end: info, ranks, timings
         TRY(ctx_sync(c));
         int hinfo = 0;
@@ -1093,13 +1315,13 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             CUDA_TRY(cudaMemcpy(A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
         for (size_t i = 0; i < rec.size(); ++i) {
             const auto &mt = rec_meta[i];
-            const int rnew = A->rank(mt[0], mt[1]);
-            log_op(gemm_lr_ops(NB, mt[2], mt[3], mt[4], rnew, rec_case[i] == 1), mt[0], mt[1]);
+            log_op(gemm_lr_ops(NB, mt[2], mt[3], mt[4], A->rank(mt[0], mt[1]), rec_case[i] == 1), mt[0], mt[1]);
         }
-        float ms;
-        for (int p = 0; p < 4; ++p) {
-            CUDA_TRY(cudaEventElapsedTime(&ms, ev[p], ev[p + 1]));
-            t_phase[p] += ms * 1e-3;
+        t_phase[1] += elapsed(ev[T0], ev[T1]);
+        if (k + 1 < NT) {
+            t_phase[0] += elapsed(ev[P0], ev[P1]);
+            t_phase[2] += elapsed(ev[S0], ev[S1]);
+            t_phase[3] += elapsed(ev[G0], ev[G1]);
         }
         if (hinfo != 0) {
             info = hinfo;
@@ -1109,9 +1331,13 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         if (verbose > 1) fprintf(stderr, "panel %d done\n", k);
     }
     for (auto &e : ev) cudaEventDestroy(e);
+    cudaEventDestroy(evP);
+    cudaEventDestroy(evT);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-    int overflow = 0;
-    CUDA_TRY(cudaMemcpy(&overflow, c->d_flags + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    int flags_h[3] = {0, 0, 0};
+    CUDA_TRY(cudaMemcpy(flags_h, c->d_flags, 3 * sizeof(int), cudaMemcpyDeviceToHost));
+    const int overflow = flags_h[1];
+    A->stats[8] = flags_h[2];
     if (tileops)
         for (size_t i = 0; i < tops.size(); ++i) tileops[i] += tops[i];
     if (opcounters) opcounters[0] += op_total;
@@ -1125,7 +1351,8 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     A->stats[3] = (double)(c->launches - launches0);
     A->stats[4] = t_phase[0]; A->stats[5] = t_phase[1]; A->stats[6] = t_phase[2]; A->stats[7] = t_phase[3];
     A->factored = (info == 0);
-    ws_reset(c);
+    c->main_ar.off = 0;
+    c->hi_ar.off = 0;
     return info;
 }
 
@@ -1150,7 +1377,8 @@ int hicma_tlr_dpotrf_L(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, d
     if (two_flow) *two_flow = 1;
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     CUDA_TRY(cudaSetDevice(c->device));
-    const int info = factorize(c, A, acc, fixed_rank, maxrank, tileopcounters, opcounters, critical_path_time, verbose);
+    const bool la = !(lookahead && *lookahead == 0);
+    const int info = factorize(c, A, acc, fixed_rank, maxrank, tileopcounters, opcounters, critical_path_time, verbose, la);
     if (Ar) std::memcpy(Ar, A->h_rank.data(), (size_t)A->NT * A->NT * sizeof(int));
     return info;
 }
@@ -1176,7 +1404,7 @@ int hicma_tlr_dpotrf_L_wait(hicma_tlr_ctx *c, hicma_tlr_desc *A, int *Ar) {
 
 int hicma_tlr_last_stats(hicma_tlr_desc *A, double *stats, int nstats) {
     ARG_CHECK(A && stats, "null");
-    for (int i = 0; i < nstats && i < 8; ++i) stats[i] = A->stats[i];
+    for (int i = 0; i < nstats && i < 12; ++i) stats[i] = A->stats[i];
     return 0;
 }
 
@@ -1425,6 +1653,108 @@ int hicma_tlr_loglik(hicma_tlr_ctx *c, hicma_tlr_desc *A, const double *y, doubl
     if (loglik) *loglik = -0.5 * (q + ld + A->N * std::log(2.0 * M_PI));
     if (logdet) *logdet = ld;
     if (x) std::memcpy(x, xs.data(), sizeof(double) * A->N);
+    return 0;
+}
+
+// ------------------------------------------------------------ profiling ----
+int hicma_tlr_prof_enable(hicma_tlr_ctx *c, int on) {
+    ARG_CHECK(c, "null");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    prof_flush(c);
+    std::memset(c->prof_acc, 0, sizeof c->prof_acc);
+    c->prof = on != 0;
+    return 0;
+}
+
+int hicma_tlr_prof_read(hicma_tlr_ctx *c, double *out, int nclass) {
+    ARG_CHECK(c && out, "null");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    prof_flush(c);
+    for (int k = 0; k < nclass && k < P_NCLASS; ++k)
+        for (int j = 0; j < 4; ++j) out[k * 4 + j] = c->prof_acc[k][j];
+    return 0;
+}
+
+// ---------------------------------------------------------------- check ----
+// Dense device copy (lower triangle, ld N) of a TLR descriptor.
+static int densify(hicma_tlr_ctx *c, hicma_tlr_desc *A, double *D) {
+    const int NT = A->NT, NB = A->NB;
+    const size_t N = A->N;
+    CUDA_TRY(cudaMemsetAsync(D, 0, N * N * sizeof(double), c->stream));
+    std::vector<GemmTask> g;
+    std::vector<CopyTask> cp;
+    for (int n = 0; n < NT; ++n)
+        for (int m = n; m < NT; ++m) {
+            double *dst = D + (size_t)m * NB + (size_t)n * NB * N;
+            if (A->is_dense(m, n)) {
+                cp.push_back(make_copy(A->dense(m, n), NB, dst, (int)N, NB, NB));
+            } else {
+                const int r = A->rank(m, n);
+                if (r > 0) g.push_back(make_gemm(0, 1, NB, NB, r, 1.0, A->U(m, n), NB, A->V(m, n), NB, 0.0, dst, (int)N));
+            }
+        }
+    TRY(run_copies(c, cp));
+    TRY(run_gemms(c, g));
+    for (int k = 0; k < NT; ++k) {
+        launch_zero_upper(D + (size_t)k * NB + (size_t)k * NB * N, NB, (int)N, c->stream);
+        TRY(check_launch(c));
+    }
+    return 0;
+}
+
+int hicma_tlr_check(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_problem *prob, hicma_tlr_desc *A0,
+                    double *res_llt, double *res_diff) {
+    ARG_CHECK(c && L && prob, "null");
+    if (!L->factored) { set_err("descriptor is not factored"); return HICMA_TLR_ERR_STATE; }
+    ARG_CHECK(L->d_pts, "no points");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t N = L->N;
+    double *DL = nullptr, *DA = nullptr, *D0 = nullptr, *part = nullptr, *sc = nullptr;
+    int *dinfo = nullptr;
+    auto cleanup = [&]() { cudaFree(DL); cudaFree(DA); cudaFree(D0); cudaFree(part); cudaFree(sc); cudaFree(dinfo); };
+    const int nblk = 1024;
+    if (cudaMalloc(&DL, N * N * sizeof(double)) != cudaSuccess || cudaMalloc(&DA, N * N * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&part, nblk * sizeof(double)) != cudaSuccess || cudaMalloc(&sc, 8 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&dinfo, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        set_err("check: allocation of dense N x N buffers failed (N = %zu)", N);
+        return HICMA_TLR_ERR_OOM;
+    }
+    int rc = densify(c, L, DL);
+    if (rc) { cleanup(); return rc; }
+    // exact A (check_dpotrf2 uses the unapproximated matrix, testing_dpotrf.c:856-893)
+    CovTask ct{DA, (int)N, 0, 0, (int)N, (int)N};
+    CovTask *dct = stage(c, &ct, 1);
+    launch_cov_batched(cov_params(L, prob), dct, 1, (int)N, (int)N, c->stream);
+    launch_sumsq(DA, nullptr, (int)N, (int)N, (long long)N, 0, part, nblk, sc + 0, c->stream);
+    // DA <- L L^T - A
+    launch_gemm_single(make_gemm(0, 1, (int)N, (int)N, (int)N, 1.0, DL, (int)N, DL, (int)N, -1.0, DA, (int)N), c->stream);
+    launch_sumsq(DA, nullptr, (int)N, (int)N, (long long)N, 0, part, nblk, sc + 1, c->stream);
+    double h[4] = {0, 0, 0, 0};
+    if (A0 && res_diff) {
+        if (cudaMalloc(&D0, N * N * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            cleanup();
+            set_err("check: allocation failed");
+            return HICMA_TLR_ERR_OOM;
+        }
+        rc = densify(c, A0, D0);
+        if (rc) { cleanup(); return rc; }
+        cudaMemsetAsync(dinfo, 0, sizeof(int), c->stream);
+        rc = potrf_tile(c, D0, (int)N, (int)N, nullptr, 0, dinfo, 0);
+        if (rc) { cleanup(); return rc; }
+        launch_sumsq(DL, D0, (int)N, (int)N, (long long)N, 1, part, nblk, sc + 2, c->stream);
+        launch_sumsq(DL, nullptr, (int)N, (int)N, (long long)N, 1, part, nblk, sc + 3, c->stream);
+    }
+    cudaError_t e = cudaMemcpyAsync(h, sc, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    c->stage_off = 0;
+    cleanup();
+    if (e != cudaSuccess) { set_err("check: %s", cudaGetErrorString(e)); return HICMA_TLR_ERR_CUDA; }
+    if (res_llt) *res_llt = std::sqrt(h[1]) / std::sqrt(h[0]);
+    if (res_diff) *res_diff = (A0 ? std::sqrt(h[2]) / std::sqrt(h[3]) : NAN);
     return 0;
 }
 

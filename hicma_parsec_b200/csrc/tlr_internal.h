@@ -22,6 +22,7 @@ struct GemmTask {
     int lower;          // skip output tiles strictly above the diagonal
     int tiles_m;        // ceil(m / 64)
     double alpha, beta;
+    const int *n_dev;   // if set, n = min(n, *n_dev) at run time (rank known on device only)
 };
 
 // Single-precision variant used by the mixed-precision policy: operands are
@@ -43,6 +44,7 @@ inline GemmTask make_gemm(int opA, int opB, int m, int n, int k, double alpha, c
     t.opA = opA; t.opB = opB; t.lower = lower;
     t.tiles_m = gemm_tiles_m(m);
     t.alpha = alpha; t.beta = beta;
+    t.n_dev = nullptr;
     return t;
 }
 
@@ -116,13 +118,13 @@ void launch_qapply_batched(const QApplyTask *d_tasks, int ntasks, int m_max, cud
 // (K x r each, ld K).  mode 0: absolute sigma >= tol (recompression);
 // mode 1: relative Frobenius tol (generation, with reject rules).
 struct CoreTask {
-    const double *RU;
-    const double *RV;
-    double *SU;
-    double *SV;
-    double *work;        // 2*K*K doubles when K > core_smem_kmax()
+    const double *RU;    // K x K upper (ld ldru), nullptr = identity
+    const double *RV;    // K x K upper (ld ldrv)
+    double *SU;          // out: K x K, left singular vectors sorted by decreasing sigma
+    double *RUc;         // out (if RU): clean copy of RU, K x K, zeros below the diagonal
+    double *work;        // K*K doubles when K > core_smem_kmax()
     int *rank_out;       // rank map entry (may be null)
-    int *rank_task;      // per-task rank for the Q-apply step
+    int *rank_task;      // per-task rank for the apply steps
     int K, ldru, ldrv;
 };
 struct CoreParams {
@@ -132,8 +134,10 @@ struct CoreParams {
     int fixed_rank;
     int nb;              // tile size (generation reject rule r >= nb/2)
     int *overflow;       // device counter of capped recompressions
+    int *sweeps;         // device counter of Jacobi sweeps (diagnostics, may be null)
 };
 int core_smem_kmax();
+// All tasks of one launch should have K <= kmax; shared memory is sized from kmax.
 void launch_core_svd_batched(const CoreTask *d_tasks, int ntasks, int kmax, const CoreParams &p,
                              cudaStream_t st);
 
@@ -142,5 +146,8 @@ void launch_core_svd_batched(const CoreTask *d_tasks, int ntasks, int kmax, cons
 void launch_logdiag_sum(const double *const *d_tiles, int ntiles, int n, int ld, double *out,
                         cudaStream_t st);
 
-// Device-side helpers for pointer arrays are built by the host engine.
+// sum of squares of X - Y (Y may be null) into *out (nblocks partials in
+// `partial`); sym_lower: Frobenius^2 of the symmetric matrix in the lower part
+void launch_sumsq(const double *X, const double *Y, int m, int n, long long ld, int sym_lower, double *partial,
+                  int nblocks, double *out, cudaStream_t st);
 }  // namespace tlr

@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -104,6 +105,9 @@ def load_library(path: str | None = None):
         "hicma_tlr_solve": (i, [vp, vp, i, vp, C.c_long]),
         "hicma_tlr_loglik": (i, [vp, vp, vp, dp, dp, vp]),
         "hicma_tlr_last_stats": (i, [vp, vp, i]),
+        "hicma_tlr_check": (i, [vp, vp, C.POINTER(CProblem), vp, dp, dp]),
+        "hicma_tlr_prof_enable": (i, [vp, i]),
+        "hicma_tlr_prof_read": (i, [vp, vp, i]),
         "hicma_tlr_k_cov": (i, [C.POINTER(CProblem), vp, i, i, i, i, i, vp, i, vp]),
         "hicma_tlr_k_dgemm": (i, [i, i, i, i, i, d, vp, i, vp, i, d, vp, i, vp]),
         "hicma_tlr_k_potrf": (i, [vp, i, vp, i, vp, vp, i]),
@@ -131,6 +135,8 @@ def _check(code: int, where: str) -> int:
 def points(prob: Problem, n: int) -> np.ndarray:
     """Points [ndim][n] of the problem (host generator of the library)."""
     lib = load_library()
+    if prob.kind not in KIND_NDIM:
+        raise TLRError(ERR_ARG, "hicma_tlr_points", f"unsupported problem kind {prob.kind}")
     out = np.empty((prob.ndim, n), dtype=np.float64)
     cp = prob.c()
     _check(lib.hicma_tlr_points(C.byref(cp), n, _p(out)), "hicma_tlr_points")
@@ -145,16 +151,31 @@ class Context:
         h = C.c_void_p()
         _check(self.lib.hicma_tlr_init(device, workspace_bytes, C.byref(h)), "hicma_tlr_init")
         self.h = h
+        self._mats = weakref.WeakSet()
 
     @property
     def stream(self) -> int:
         return self.lib.hicma_tlr_stream(self.h) or 0
+
+    PROF_CLASSES = ("gemm", "qr", "qapply", "core_svd", "potrf", "cov", "copy", "other")
+
+    def prof_enable(self, on: bool = True) -> None:
+        _check(self.lib.hicma_tlr_prof_enable(self.h, int(on)), "hicma_tlr_prof_enable")
+
+    def prof_read(self) -> dict:
+        out = np.zeros(32)
+        _check(self.lib.hicma_tlr_prof_read(self.h, _p(out), 8), "hicma_tlr_prof_read")
+        o = out.reshape(8, 4)
+        return {name: {"launches": int(o[k, 0]), "seconds": float(o[k, 1]), "flops": float(o[k, 2]),
+                       "bytes": float(o[k, 3])} for k, name in enumerate(self.PROF_CLASSES)}
 
     def set_precision(self, prec: int) -> None:
         _check(self.lib.hicma_tlr_set_precision(self.h, prec), "hicma_tlr_set_precision")
 
     def close(self) -> None:
         if self.h:
+            for m in list(self._mats):
+                m.close()
             self.lib.hicma_tlr_fini(self.h)
             self.h = None
 
@@ -180,6 +201,7 @@ class TLRMatrix:
         h = C.c_void_p()
         _check(self.lib.hicma_tlr_desc_create(ctx.h, n, nb, maxrank, band_size, C.byref(h)), "hicma_tlr_desc_create")
         self.h = h
+        ctx._mats.add(self)
         self.n, self.nb, self.maxrank = n, nb, maxrank
         self.nt = n // nb
 
@@ -240,8 +262,8 @@ class TLRMatrix:
         return info
 
     def stats(self) -> np.ndarray:
-        s = np.zeros(8)
-        _check(self.lib.hicma_tlr_last_stats(self.h, _p(s), 8), "hicma_tlr_last_stats")
+        s = np.zeros(12)
+        _check(self.lib.hicma_tlr_last_stats(self.h, _p(s), 12), "hicma_tlr_last_stats")
         return s
 
     def copy_from(self, other: "TLRMatrix") -> None:
@@ -284,6 +306,14 @@ class TLRMatrix:
 
     def store_set(self, buf_ptr: int, ranks: np.ndarray) -> None:
         _check(self.lib.hicma_tlr_store_set(self.ctx.h, self.h, C.c_void_p(buf_ptr), _p(ranks)), "hicma_tlr_store_set")
+
+    def check(self, prob: Problem, approx: "TLRMatrix | None" = None):
+        """(||L L^T - A|| / ||A||, ||L - L0|| / ||L||) on the device."""
+        r1, r2 = C.c_double(), C.c_double()
+        cp = prob.c()
+        _check(self.lib.hicma_tlr_check(self.ctx.h, self.h, C.byref(cp), approx.h if approx else None,
+                                        C.byref(r1), C.byref(r2)), "hicma_tlr_check")
+        return r1.value, r2.value
 
     def logdet(self) -> float:
         v = C.c_double()

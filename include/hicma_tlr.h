@@ -184,8 +184,25 @@ int hicma_tlr_loglik(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, const double *y, dou
 /* Statistics of the last factorization on A: [0] seconds, [1] TLR flops
  * (op_counts model), [2] recompressions capped at maxrank, [3] number of
  * launches of library kernels, [4] POTRF s, [5] TRSM s, [6] SYRK s,
- * [7] GEMM/recompression s. */
+ * [7] GEMM/recompression s, [8] Jacobi sweeps summed over all cores.
+ * nstats <= 12. */
 int hicma_tlr_last_stats(hicma_tlr_desc *A, double *stats, int nstats);
+
+/* --check of the reference driver (check_dpotrf2 and check_diff,
+ * hicma_parsec/testing_dpotrf.c:111-230, flow :642-903) on the device:
+ * res_llt = ||L L^T - A||_F / ||A||_F against the exact (unapproximated)
+ * covariance; res_diff = ||L - L0|| / ||L|| with L0 the dense Cholesky of the
+ * approximate matrix held (unfactored) in A0 (A0 may be NULL).  Allocates
+ * three dense N x N device buffers, so it is meant for moderate N. */
+int hicma_tlr_check(hicma_tlr_ctx *ctx, hicma_tlr_desc *L, const hicma_tlr_problem *prob,
+                    hicma_tlr_desc *A0, double *res_llt, double *res_diff);
+
+/* Per-kernel-class device timing (CUDA events around launches on the context
+ * stream).  Classes: 0 GEMM, 1 QR, 2 Q-apply, 3 core SVD, 4 tile POTRF,
+ * 5 covariance generation, 6 copies.  out[4*k + j]: j = 0 launches,
+ * 1 seconds, 2 algorithmic flops, 3 algorithmic bytes.  Enabling resets. */
+int hicma_tlr_prof_enable(hicma_tlr_ctx *ctx, int on);
+int hicma_tlr_prof_read(hicma_tlr_ctx *ctx, double *out, int nclass);
 
 /* ------------------------------------------- kernel-level entry points -- */
 /* Device pointers; used by the parity tests and by callers that manage their

@@ -306,6 +306,22 @@ def compress_tile(A: np.ndarray, tol: float, maxrank: int, oversample: int = 10)
     return U, V, r
 
 
+def compress_tile_rsvd(A: np.ndarray, tol: float, maxrank: int, oversample: int = 10, seed: int = 0):
+    """Randomized variant of :func:`compress_tile` (range finder with
+    ``min(maxrank + oversample, NB)`` Gaussian samples, then an exact SVD of
+    the projected tile), the algorithm the CUDA generator implements."""
+    m, n = A.shape
+    s = min(maxrank + oversample, min(m, n))
+    Om = np.random.default_rng(seed).standard_normal((n, s))
+    Q, _ = np.linalg.qr(A @ Om)
+    Qw, Rw = np.linalg.qr(A.T @ Q)
+    u, sv, vt = np.linalg.svd(Rw.T)
+    r = truncation_rank_relfro(sv, tol)
+    if not (r < min(m, n) / 2 and r <= maxrank):
+        return None, None, -1
+    return (np.ascontiguousarray(Q @ u[:, :r]), np.ascontiguousarray(Qw @ (vt[:r].T * sv[:r])), r)
+
+
 def generate(prob: Problem, n: int, nb: int, tol: float, maxrank: int, band: int = 1,
              pts: np.ndarray | None = None):
     """``STARSH_gen`` (``STARSH_gen.jdf:342-369``): dense band tiles

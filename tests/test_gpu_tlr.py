@@ -96,10 +96,13 @@ def test_c1_autoband(ctx):
 def test_3d_exp_small(ctx):
     """3D exponential kernel (-D 4) with a dense band, scaled down."""
     from hicma_parsec_b200 import tlr
-    n, nb, mr = 4000, 400, 200
+    n, nb, mr = 8000, 1000, 499
     prob = tlr.Problem(kind=4, noise=1e-4)
-    A = tlr.TLRMatrix(ctx, n, nb, mr, 2)
+    A = tlr.TLRMatrix(ctx, n, nb, mr, 1)
     assert A.generate(prob, TOL, mr) == 0
+    b = tlr.parsec_band_size_auto_tuning(A.rank_map(), n // nb, nb)
+    if b > 1:
+        A.band_regenerate(prob, b)
     assert A.potrf(TOL) == 0
     pts = O.gen_points(n, 3)
     Aex = O.dense_matrix(O.Problem(kind=4, noise=1e-4), pts)

@@ -1,0 +1,75 @@
+"""The C-ABI library loads on a machine without a GPU, exports every entry
+point declared in include/hicma_tlr.h, and its host-only functions (point
+placement, band auto-tuning, rank statistics) agree with the oracle bit for
+bit.  No device work is launched here."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import tlr_oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "hicma_tlr.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(hicma_tlr_\w+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from hicma_parsec_b200 import tlr
+    return tlr.load_library()
+
+
+def test_exports_every_declared_symbol(lib):
+    syms = declared_symbols()
+    assert len(syms) >= 30
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_library_is_sm100a(lib):
+    from hicma_parsec_b200 import build
+    assert "arch=compute_100a,code=sm_100a" in " ".join(build.ARCH)
+    assert os.path.exists(build.LIB)
+
+
+@pytest.mark.parametrize("kind,n", [(2, 2700), (2, 10000), (3, 1000), (4, 4913), (3, 999)])
+def test_points_bit_identical(kind, n):
+    from hicma_parsec_b200 import tlr
+    P = tlr.points(tlr.Problem(kind=kind, seed=0), n)
+    Q = O.gen_points(n, O.KIND_NDIM[kind], 0)
+    np.testing.assert_array_equal(P, Q.T)
+
+
+def test_band_autotune_matches_oracle():
+    from hicma_parsec_b200 import tlr
+    rng = np.random.default_rng(11)
+    for _ in range(100):
+        nt, nb = int(rng.integers(3, 25)), int(rng.integers(50, 3000))
+        G = rng.integers(0, nb // 2, size=nt * nt).astype(np.int32)
+        assert tlr.parsec_band_size_auto_tuning(G, nt, nb) == O.band_autotune(G, nt, nb)
+
+
+def test_rank_stat_matches_oracle():
+    from hicma_parsec_b200 import tlr
+    rng = np.random.default_rng(5)
+    for band in (1, 2, 4):
+        G = rng.integers(0, 100, size=144).astype(np.int32)
+        mn, mx, av = tlr.HICMA_get_stat2(G, 12, band)
+        omn, omx, oav = O.rank_stat(G, 12, band)
+        assert (mn, mx) == (omn, omx) and av == pytest.approx(oav, rel=1e-15)
+
+
+def test_argument_errors_without_gpu(lib):
+    from hicma_parsec_b200 import tlr
+    with pytest.raises(tlr.TLRError):
+        tlr.points(tlr.Problem(kind=9), 10)
+    G = np.zeros(4, np.int32)
+    assert lib.hicma_tlr_band_autotune(None, 2, 10, 0) == tlr.ERR_ARG
