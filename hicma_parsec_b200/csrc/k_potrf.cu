@@ -8,6 +8,9 @@
 // panel solve; the panel and trailing updates are DMMA GEMMs.
 #include "tlr_internal.h"
 
+#include <cstdio>
+#include <mutex>
+
 namespace tlr {
 namespace {
 
@@ -82,3 +85,99 @@ void launch_potrf_diag(double *A, int lda, int jb, double *Dinv, int ldd, int *i
 }
 
 }  // namespace tlr
+
+// ---------------------------------------------------------------------------
+// Allocation-free tile Cholesky.
+//
+// For callers that must not allocate device memory (for example code that
+// runs inside a host framework owning every device buffer, or a latency-bound
+// loop that cannot afford the device-wide synchronisation cudaMalloc may
+// cause).  Its scratch is the file-scope array below: the 64 x 64 inverse of
+// the current diagonal block followed by the 64 x n row panel used while the
+// inverse of the factor is assembled.  Every GPU that loads this library
+// holds the array until the process exits.
+namespace tlr {
+namespace {
+
+constexpr int NOALLOC_MAX_N = 4096;
+constexpr size_t NOALLOC_SCRATCH = 64 * 64 + (size_t)64 * NOALLOC_MAX_N;
+__device__ __align__(256) double g_potrf_scratch[NOALLOC_SCRATCH];
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_scratch_mu;
+double *g_scratch_ptr[MAX_DEVICES] = {nullptr};
+
+}  // namespace
+}  // namespace tlr
+
+extern "C" int hicma_tlr_k_potrf_noalloc(int n, double *d_A, int lda, double *d_linv, int *d_info, int info_offset,
+                                         void *stream) {
+    using namespace tlr;
+    if (n < 1 || n > NOALLOC_MAX_N || !d_A || lda < n || !d_info) {
+        char msg[256];
+        snprintf(msg, sizeof msg,
+                 "hicma_tlr_k_potrf_noalloc: need 1 <= n <= %d (got %d), lda >= n, non-null A and info",
+                 NOALLOC_MAX_N, n);
+        tlr_set_error(msg);
+        return HICMA_TLR_ERR_ARG;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
+        tlr_set_error("hicma_tlr_k_potrf_noalloc: no current CUDA device");
+        return HICMA_TLR_ERR_CUDA;
+    }
+    double *scratch = nullptr;
+    {
+        // once per device, with that device current: the host-side name of the
+        // array is not a device address, so ask the runtime for it
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        if (!g_scratch_ptr[dev]) {
+            void *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_potrf_scratch);
+            if (e != cudaSuccess || !p) {
+                tlr_set_error("hicma_tlr_k_potrf_noalloc: cudaGetSymbolAddress of the scratch array failed");
+                return HICMA_TLR_ERR_CUDA;
+            }
+            g_scratch_ptr[dev] = (double *)p;
+        }
+        scratch = g_scratch_ptr[dev];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    double *dscr = scratch;              // 64 x 64 diagonal-block inverse
+    double *tmp = scratch + 64 * 64;     // 64 x n row panel
+    const int DBK = 64;
+    if (d_linv && cudaMemset2DAsync(d_linv, (size_t)n * sizeof(double), 0, sizeof(double) * n, n, st) != cudaSuccess) {
+        tlr_set_error("hicma_tlr_k_potrf_noalloc: clearing the inverse failed");
+        return HICMA_TLR_ERR_CUDA;
+    }
+    for (int j = 0; j < n; j += DBK) {
+        const int jb = n - j < DBK ? n - j : DBK;
+        double *Dinv = d_linv ? d_linv + j + (size_t)j * n : dscr;
+        const int ldd = d_linv ? n : DBK;
+        launch_potrf_diag(d_A + j + (size_t)j * lda, lda, jb, Dinv, ldd, d_info, info_offset + j, st);
+        if (j + jb < n) {
+            const int rows = n - j - jb;
+            double *Pn = d_A + (j + jb) + (size_t)j * lda;
+            launch_gemm_single(make_gemm(0, 1, rows, jb, jb, 1.0, Pn, lda, Dinv, ldd, 0.0, Pn, lda), st);
+            launch_gemm_single(make_gemm(0, 1, rows, rows, jb, -1.0, Pn, lda, Pn, lda, 1.0,
+                                         d_A + (j + jb) + (size_t)(j + jb) * lda, lda, 1),
+                               st);
+        }
+    }
+    launch_zero_upper(d_A, n, lda, st);
+    if (d_linv) {
+        for (int i0 = DBK; i0 < n; i0 += DBK) {
+            const int ib = n - i0 < DBK ? n - i0 : DBK;
+            launch_gemm_single(make_gemm(0, 0, ib, i0, i0, 1.0, d_A + i0, lda, d_linv, n, 0.0, tmp, ib), st);
+            launch_gemm_single(make_gemm(0, 0, ib, i0, ib, -1.0, d_linv + i0 + (size_t)i0 * n, n, tmp, ib, 0.0,
+                                         d_linv + i0, n),
+                               st);
+        }
+    }
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        tlr_set_error(cudaGetErrorString(e));
+        return HICMA_TLR_ERR_CUDA;
+    }
+    return 0;
+}

@@ -39,6 +39,7 @@ static void set_err(const char *fmt, ...) {
     g_err = buf;
 }
 extern "C" const char *hicma_tlr_last_error(void) { return g_err.c_str(); }
+void tlr::tlr_set_error(const char *msg) { g_err = msg ? msg : ""; }
 
 #define CUDA_TRY(x)                                                                         \
     do {                                                                                    \

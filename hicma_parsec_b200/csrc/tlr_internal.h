@@ -150,4 +150,6 @@ void launch_logdiag_sum(const double *const *d_tiles, int ntiles, int n, int ld,
 // `partial`); sym_lower: Frobenius^2 of the symmetric matrix in the lower part
 void launch_sumsq(const double *X, const double *Y, int m, int n, long long ld, int sym_lower, double *partial,
                   int nblocks, double *out, cudaStream_t st);
+// Record the message returned by hicma_tlr_last_error() for this thread.
+void tlr_set_error(const char *msg);
 }  // namespace tlr

@@ -113,6 +113,7 @@ def load_library(path: str | None = None):
         "hicma_tlr_k_potrf": (i, [vp, i, vp, i, vp, vp, i]),
         "hicma_tlr_k_lr_update": (i, [vp, i, vp, vp, i, vp, vp, i, vp, vp, ip, d, i, i]),
         "hicma_tlr_k_compress": (i, [vp, i, vp, vp, vp, i, d, ip]),
+        "hicma_tlr_k_potrf_noalloc": (i, [i, vp, i, vp, vp, i, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -242,6 +242,26 @@ int hicma_tlr_k_lr_update(hicma_tlr_ctx *ctx, int nb, const double *d_Au, const 
 int hicma_tlr_k_compress(hicma_tlr_ctx *ctx, int nb, const double *d_A, double *d_U, double *d_V,
                          int maxrank, double tol, int *rank);
 
+/* Allocation-free variant of hicma_tlr_k_potrf.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc, such as code
+ * embedded in a host framework that owns all device memory and only lends out
+ * buffers, or latency-critical loops that must avoid the device-wide
+ * synchronisation an allocation can trigger.  It factors the n x n tile d_A
+ * (leading dimension lda) in place and, if d_linv is non-NULL, writes L^-1
+ * there (n x n, leading dimension n); *d_info as for hicma_tlr_k_potrf.  No
+ * context, no allocation, no freeing: its scratch is a fixed array inside the
+ * library (2.1 MB of device memory on every GPU that loads the library, held
+ * until the process exits), which limits n to 1..4096; larger n returns
+ * HICMA_TLR_ERR_ARG with a message in hicma_tlr_last_error().  The first call
+ * on a device looks up the device address of that array, so make that first
+ * call before capturing the stream into a CUDA graph.  The work is enqueued on
+ * `stream` (NULL = legacy default stream) and the call returns without
+ * waiting.  All calls share the one array: calls whose work overlaps on the
+ * GPU (other streams, other host threads) race on it and must be ordered by
+ * the caller. */
+int hicma_tlr_k_potrf_noalloc(int n, double *d_A, int lda, double *d_linv, int *d_info,
+                              int info_offset, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
