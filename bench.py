@@ -386,6 +386,36 @@ def run_ours(args, cfg):
         dist.destroy_process_group()
 
 
+def run_serving(args):
+    """MLE serving stream: the same seeded requests served
+    sequentially on one slot and by the continuous-batching loop."""
+    import torch
+    from hicma_parsec_b200 import serving
+    reqs = serving.sample_requests(args.requests, seed=0, rate=args.rate, n_max=args.serving_nmax)
+    out = {"metric": "MLE solves/s (p50/p99 latency)", "unit": "solves/s", "higher_is_better": True,
+           "n_gpus": 1, "data": "synthetic", "dtype": "f64",
+           "config": {"workload": f"{len(reqs)} Poisson ML requests, N log-U[1e4,{args.serving_nmax}], tile 1000-2700, "
+                                  "2D/3D sqexp or 3D exp, e in {1e-6,1e-8,1e-9}", "rate_per_s": args.rate}}
+    for mode, slots, realtime in (("sequential", 1, False), ("continuous", args.slots, False),
+                                  ("continuous_poisson", args.slots, True)):
+        srv = serving.MLEServer(0, slots=slots, workspace_bytes=int(args.workspace_gb * (1 << 30) / max(slots, 1)))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = srv.run(reqs, realtime=realtime)
+        mk = time.perf_counter() - t0
+        srv.close()
+        out[mode] = serving.summarize(res, mk)
+        out[mode]["slots"] = slots
+        if mode == "sequential":
+            ref = res
+        else:
+            diff = max(abs(a.loglik - b.loglik) / abs(a.loglik) for a, b in zip(ref, res) if a.status == 0 and b.status == 0)
+            out[mode]["max_rel_diff_vs_sequential"] = diff
+    out["value"] = out["continuous"]["solves_per_s"]
+    out["speedup_vs_sequential"] = out["continuous"]["solves_per_s"] / out["sequential"]["solves_per_s"]
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -398,8 +428,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serving", action="store_true", help="run the MLE serving benchmark instead")
+    ap.add_argument("--requests", type=int, default=16)
+    ap.add_argument("--rate", type=float, default=1.0)
+    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--serving-nmax", type=int, default=200000)
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
+    if args.serving:
+        run_serving(args)
+        return
     if args.impl == "reference":
         run_reference(args, cfg)
     else:

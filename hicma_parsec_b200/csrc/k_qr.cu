@@ -105,32 +105,34 @@ __global__ void __launch_bounds__(QT) k_qr(const QRTask *__restrict__ tasks) {
         }
         __syncthreads();
 
+        // Column c: norm of P[c][c+1:] and dots with the later panel columns
+        // (reduced across the CTA), reflector from warp 0, then one fused pass
+        // that applies H_c to the later columns and accumulates the sums of
+        // column c+1 for the next step.
+        double s[PB];
+#pragma unroll
+        for (int i = 0; i < PB; ++i) s[i] = 0.0;
+        for (int r = 1 + tid; r < mr; r += QT) {
+            const double x = P[r];
+            s[0] += x * x;
+#pragma unroll
+            for (int cc = 1; cc < PB; ++cc)
+                if (cc < jb) s[cc] += x * P[cc * mr + r];
+        }
         for (int c = 0; c < jb; ++c) {
-            double s[PB];
-#pragma unroll
-            for (int i = 0; i < PB; ++i) s[i] = 0.0;
-            const double *xc = P + c * mr;
-            for (int r = c + 1 + tid; r < mr; r += QT) {
-                const double x = xc[r];
-                s[0] += x * x;
-#pragma unroll
-                for (int cc = 1; cc < PB; ++cc)
-                    if (cc > c && cc < jb) s[cc] += x * P[cc * mr + r];
-            }
 #pragma unroll
             for (int i = 0; i < PB; ++i) {
                 const double v = warp_sum(s[i]);
                 if (lane == 0) red[warp * PB + i] = v;
             }
             __syncthreads();
-            if (tid == 0) {
-                double acc[PB];
-#pragma unroll
-                for (int i = 0; i < PB; ++i) acc[i] = 0.0;
-                for (int w = 0; w < QW; ++w)
-#pragma unroll
-                    for (int i = 0; i < PB; ++i) acc[i] += red[w * PB + i];
-                const double alpha = xc[c], norm2 = acc[0];
+            if (warp == 0) {
+                // lane i sums entry i over the warps
+                double acc = 0.0;
+                if (lane < PB)
+                    for (int w = 0; w < QW; ++w) acc += red[w * PB + lane];
+                const double norm2 = __shfl_sync(0xffffffffu, acc, 0);
+                const double alpha = P[c * mr + c];
                 double tau, beta, scale;
                 if (norm2 == 0.0) {
                     tau = 0.0; beta = alpha; scale = 0.0;
@@ -139,20 +141,36 @@ __global__ void __launch_bounds__(QT) k_qr(const QRTask *__restrict__ tasks) {
                     tau = (beta - alpha) / beta;
                     scale = 1.0 / (alpha - beta);
                 }
-                sc[0] = tau; sc[1] = beta; sc[2] = scale;
-                for (int cc = c + 1; cc < jb; ++cc) wsm[cc] = P[cc * mr + c] + scale * acc[cc];
-                t.tau[j0 + c] = tau;
+                if (lane > c && lane < jb) wsm[lane] = P[lane * mr + c] + scale * acc;
+                if (lane == 0) {
+                    sc[0] = tau; sc[1] = beta; sc[2] = scale;
+                    t.tau[j0 + c] = tau;
+                }
             }
             __syncthreads();
             const double tau = sc[0], beta = sc[1], scale = sc[2];
+            const int c1 = c + 1;
+#pragma unroll
+            for (int i = 0; i < PB; ++i) s[i] = 0.0;
             for (int r = c + tid; r < mr; r += QT) {
                 double v;
                 if (r == c) { v = 1.0; P[c * mr + c] = beta; }
-                else        { v = xc[r] * scale; P[c * mr + r] = v; }
-                for (int cc = c + 1; cc < jb; ++cc) P[cc * mr + r] -= tau * v * wsm[cc];
+                else        { v = P[c * mr + r] * scale; P[c * mr + r] = v; }
+                const double tv = tau * v;
+                double xn = 0.0;
+#pragma unroll
+                for (int cc = 1; cc < PB; ++cc) {
+                    if (cc > c && cc < jb) {
+                        const double y = P[cc * mr + r] - tv * wsm[cc];
+                        P[cc * mr + r] = y;
+                        if (cc == c1) xn = y;
+                        else if (cc > c1 && r > c1) s[cc] += xn * y;
+                    }
+                }
+                if (r > c1 && c1 < jb) s[0] += xn * xn;
             }
-            __syncthreads();
         }
+        __syncthreads();
 
         // Gram of the panel reflectors: G[l][i] = v_l . v_i for l < i.
         const int npairs = jb * (jb - 1) / 2;

@@ -105,6 +105,14 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
     if (K > 1) {
         for (int sweep = 0; sweep < MAX_SWEEPS; ++sweep) {
             if (tid == 0) rotated = 0;
+            // exact squared column norms at the start of every sweep (sig is
+            // free until the sweeps end); rotations keep them up to date
+            for (int c = warp; c < K; c += CT / 32) {
+                double s2 = 0.0;
+                for (int r = lane; r < K; r += 32) s2 += W[(size_t)c * K + r] * W[(size_t)c * K + r];
+                s2 = group_sum<32>(s2);
+                if (lane == 0) sig[c] = s2;
+            }
             __syncthreads();
             ++sweeps;
             for (int round = 0; round < Kp - 1; ++round) {
@@ -117,7 +125,7 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
                         a = tourney(pr, round, Kp);
                         b = tourney(Kp - 1 - pr, round, Kp);
                         if (a > b) { const int tmp = a; a = b; b = tmp; }
-                        valid = b < K;
+                        valid = b < K && sig[a] > tau2 && sig[b] > tau2;
                     }
                     double aa = 0.0, bb = 0.0, cc = 0.0;
                     double *mp = W + (size_t)a * K, *mq = W + (size_t)b * K;
@@ -142,7 +150,11 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
                         mp[r] = cs * x - sn * y;
                         mq[r] = sn * x + cs * y;
                     }
-                    if (gl == 0) rotated = 1;
+                    if (gl == 0) {
+                        rotated = 1;
+                        sig[a] = aa - tt * cc;
+                        sig[b] = bb + tt * cc;
+                    }
                 }
                 __syncthreads();
             }

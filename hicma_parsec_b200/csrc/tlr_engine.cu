@@ -966,6 +966,10 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
                 if (bad < 4) fprintf(stderr, "Tile(%d, %d) is dense, try increasing NB or maxrank \n", m, n);
                 ++bad;
             }
+    // Ar reports rejected tiles as -1, the value the reference leaves in dcAr
+    // when starsh_dense_dlrrsdd returns rank -1 (STARSH_gen.jdf:169-175); the
+    // descriptor stores them with rank 0 so that no kernel reads their slots.
+    if (Ar) std::memcpy(Ar, A->h_rank.data(), (size_t)NT * NT * sizeof(int));
     if (bad) {
         for (int m = A->band; m < NT; ++m)
             for (int n = 0; n <= m - A->band; ++n)
@@ -974,7 +978,6 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
         if (info) *info = -1;
     }
     A->factored = false;
-    if (Ar) std::memcpy(Ar, A->h_rank.data(), (size_t)NT * NT * sizeof(int));
     return 0;
 }
 

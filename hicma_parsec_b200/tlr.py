@@ -230,10 +230,20 @@ class TLRMatrix:
         cp = prob.c()
         if pts is not None:
             pts = np.ascontiguousarray(pts, dtype=np.float64)
-        _check(self.lib.hicma_tlr_generate(self.ctx.h, LOWER, self.h, None, C.byref(cp), _p(pts), tol,
+        Ar = np.empty(self.nt * self.nt, dtype=np.int32)
+        _check(self.lib.hicma_tlr_generate(self.ctx.h, LOWER, self.h, _p(Ar), C.byref(cp), _p(pts), tol,
                                            maxrank or self.maxrank, self.band_size, 0, C.byref(info)),
                "hicma_tlr_generate")
+        self.gen_ranks = Ar    # rank map of the generation; rejected tiles are -1
         return info.value
+
+    def rejected_tiles(self) -> list:
+        """Off-band tiles the last generation rejected (rank rule), as (m, n)."""
+        G = getattr(self, "gen_ranks", None)
+        if G is None:
+            return []
+        b = self.band_size
+        return [(m, n) for m in range(b, self.nt) for n in range(0, m - b + 1) if G[n * self.nt + m] < 0]
 
     def rank_map(self) -> np.ndarray:
         G = np.empty(self.nt * self.nt, dtype=np.int32)

@@ -1,0 +1,78 @@
+"""Serving loop: each maximum-likelihood result is the same alone and in the
+mix (tolerance: 1e-12 relative on log det and log-likelihood; the kernels are
+deterministic so the values are expected to agree bit for bit), requests are
+admitted under an HBM budget, and a result is checked against the dense FP64
+oracle."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import tlr_oracle as O
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _requests():
+    from hicma_parsec_b200 import serving
+    reqs = serving.sample_requests(6, seed=3, rate=0.0, n_min=2000, n_max=6000, tiles=(500, 1000))
+    for r in reqs:
+        r.maxrank = r.nb // 2 - 1
+    return reqs
+
+
+def test_alone_equals_mix():
+    from hicma_parsec_b200 import serving
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    reqs = _requests()
+    seq = serving.MLEServer(0, slots=1, workspace_bytes=1 << 30)
+    alone = seq.run(reqs, realtime=False)
+    seq.close()
+    mix_srv = serving.MLEServer(0, slots=3, workspace_bytes=1 << 30)
+    mix = mix_srv.run(reqs, realtime=False)
+    mix_srv.close()
+    for a, b in zip(alone, mix):
+        assert a.status == 0 and b.status == 0, (a.error, b.error)
+        assert abs(a.logdet - b.logdet) <= 1e-12 * abs(a.logdet)
+        assert abs(a.loglik - b.loglik) <= 1e-12 * abs(a.loglik)
+        assert np.allclose(a.x, b.x, rtol=1e-12, atol=0)
+    # the concurrent run overlapped requests on the device
+    assert sum(1 for r in mix if r.t_admit < max(x.t_done for x in mix) * 0.5) >= 2
+
+
+def test_result_matches_dense_oracle():
+    from hicma_parsec_b200 import serving, tlr
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    req = serving.MLERequest(rid=0, kind=tlr.KIND_SQEXP_2D, n=4000, nb=500, beta=0.1, sigma=1.5, noise=1e-3,
+                             acc=1e-9, seed=5, maxrank=249)
+    srv = serving.MLEServer(0, slots=1, workspace_bytes=1 << 30)
+    (res,) = srv.run([req], realtime=False)
+    srv.close()
+    assert res.status == 0, res.error
+    pts = O.gen_points(req.n, 2, req.seed)
+    A = O.dense_matrix(O.Problem(kind=2, beta=0.1, sigma=1.5, noise=1e-3), pts)
+    L = np.linalg.cholesky(A)
+    y = req.rhs()
+    x = np.linalg.solve(A, y)
+    ld = 2.0 * np.sum(np.log(np.diag(L)))
+    ll = -0.5 * (y @ x + ld + req.n * math.log(2 * math.pi))
+    assert abs(res.logdet - ld) <= 1e-8 * abs(ld)
+    assert abs(res.loglik - ll) <= 1e-6 * abs(ll)
+
+
+def test_admission_under_tight_budget():
+    from hicma_parsec_b200 import serving
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    reqs = _requests()[:3]
+    srv = serving.MLEServer(0, slots=3, hbm_budget=1, workspace_bytes=1 << 30)
+    res = srv.run(reqs, realtime=False)
+    srv.close()
+    assert all(r.status == 0 for r in res)
+    # with a budget smaller than any request, requests ran one at a time
+    order = sorted(res, key=lambda r: r.t_admit)
+    for prev, nxt in zip(order, order[1:]):
+        assert nxt.t_admit >= prev.t_done - 1e-3
