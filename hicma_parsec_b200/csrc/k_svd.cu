@@ -19,7 +19,6 @@
 namespace tlr {
 namespace {
 
-constexpr int CT = 256;
 constexpr int KMAX_SMEM = 160;
 constexpr int MAX_SWEEPS = 40;
 
@@ -34,7 +33,7 @@ __device__ __forceinline__ double group_sum(double v) {
     return v;
 }
 
-template <int LP>
+template <int LP, int CT>
 __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ tasks, CoreParams p) {
     extern __shared__ double sm[];
     __shared__ int rotated;
@@ -100,7 +99,10 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
     const int groups = (CT / 32) * GPW;          // pair groups per CTA
     const int gsub = lane / LP, gl = lane % LP;
     const int Kp = K + (K & 1);
-    const double tolj = 2.3e-16 * sqrt((double)K);
+    // A pair counts as orthogonal when |c| <= tolj sqrt(a b).  The computed dot
+    // products of K-term columns carry a rounding error of about K eps, so a
+    // tighter threshold would keep rotating noise and never converge.
+    const double tolj = 4.4e-16 * (double)(K > 16 ? K : 16);
     int sweeps = 0;
     if (K > 1) {
         for (int sweep = 0; sweep < MAX_SWEEPS; ++sweep) {
@@ -227,10 +229,10 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
     }
 }
 
-template <int LP>
+template <int LP, int CT>
 void launch_lp(const CoreTask *d, int n, size_t smem, const CoreParams &p, cudaStream_t st) {
-    cudaFuncSetAttribute(k_core_svd<LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_core_svd<LP><<<n, CT, smem, st>>>(d, p);
+    cudaFuncSetAttribute(k_core_svd<LP, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_core_svd<LP, CT><<<n, CT, smem, st>>>(d, p);
 }
 
 }  // namespace
@@ -247,9 +249,11 @@ void launch_core_svd_batched(const CoreTask *d_tasks, int ntasks, int kmax, cons
     else
         smem = sizeof(double) * (size_t)kmax + sizeof(int) * kmax;
     smem = (smem + 15) / 16 * 16;
-    if (kmax <= 32) launch_lp<8>(d_tasks, ntasks, smem, p, st);
-    else if (kmax <= 96) launch_lp<16>(d_tasks, ntasks, smem, p, st);
-    else launch_lp<32>(d_tasks, ntasks, smem, p, st);
+    // lanes per pair ~ K/8 elements each; more pair groups per CTA for large K
+    if (kmax <= 64) launch_lp<8, 256>(d_tasks, ntasks, smem, p, st);
+    else if (kmax <= 96) launch_lp<16, 256>(d_tasks, ntasks, smem, p, st);
+    else if (kmax <= KMAX_SMEM) launch_lp<16, 512>(d_tasks, ntasks, smem, p, st);
+    else launch_lp<32, 512>(d_tasks, ntasks, smem, p, st);
 }
 
 }  // namespace tlr

@@ -79,7 +79,9 @@ __global__ void __launch_bounds__(256) k_copy_batched(const CopyTask *__restrict
     for (int c = c0; c < cend; ++c) {
         const double *s = t.src + (size_t)c * t.lds;
         double *d = t.dst + (size_t)c * t.ldd;
-        if (t.alpha == 1.0)
+        if (t.beta != 0.0)
+            for (int r = threadIdx.x; r < t.rows; r += blockDim.x) d[r] = t.alpha * s[r] + t.beta * d[r];
+        else if (t.alpha == 1.0)
             for (int r = threadIdx.x; r < t.rows; r += blockDim.x) d[r] = s[r];
         else
             for (int r = threadIdx.x; r < t.rows; r += blockDim.x) d[r] = t.alpha * s[r];
@@ -154,7 +156,27 @@ __global__ void k_sum_final(const double *partial, int n, double *out) {
     if (threadIdx.x == 0) *out = red[0];
 }
 
+__global__ void __launch_bounds__(256) k_assemble_r(const AssembleTask *__restrict__ tasks) {
+    const AssembleTask t = tasks[blockIdx.x];
+    const int rc = t.rc, ra = t.ra, K = rc + ra;
+    for (int idx = threadIdx.x; idx < K * K; idx += blockDim.x) {
+        const int i = idx % K, j = idx / K;
+        double u = 0.0;
+        if (i < rc) {
+            if (j < rc) u = (i == j) ? 1.0 : 0.0;
+            else u = t.Pu[(size_t)i + (size_t)(j - rc) * rc];
+        } else if (j >= i) {
+            u = t.Wu[(size_t)(i - rc) + (size_t)(j - rc) * t.nb];
+        }
+        t.RU[idx] = u;
+    }
+}
+
 }  // namespace
+
+void launch_assemble_r(const AssembleTask *d_tasks, int ntasks, cudaStream_t st) {
+    if (ntasks > 0) k_assemble_r<<<ntasks, 256, 0, st>>>(d_tasks);
+}
 
 void launch_sumsq(const double *X, const double *Y, int m, int n, long long ld, int sym_lower, double *partial,
                   int nblocks, double *out, cudaStream_t st) {

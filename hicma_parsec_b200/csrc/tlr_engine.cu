@@ -92,7 +92,7 @@ struct hicma_tlr_ctx_s {
     struct ProfRec { int cls; cudaEvent_t a, b; double flops, bytes; };
     std::vector<ProfRec> prof_recs;
     std::vector<cudaEvent_t> ev_pool;
-    double prof_acc[8][4] = {};
+    double prof_acc[9][4] = {};
 };
 
 struct hicma_tlr_desc_s {
@@ -173,7 +173,7 @@ T *stage(hicma_tlr_ctx *c, const T *src, size_t n) {
     return d;
 }
 
-enum { P_GEMM = 0, P_QR, P_QAPPLY, P_CORE, P_POTRF, P_COV, P_COPY, P_OTHER, P_NCLASS };
+enum { P_GEMM = 0, P_QR, P_QAPPLY, P_CORE, P_POTRF, P_COV, P_COPY, P_OTHER, P_PROJ, P_NCLASS };
 
 cudaEvent_t pool_event(hicma_tlr_ctx *c) {
     if (!c->ev_pool.empty()) {
@@ -305,9 +305,11 @@ int run_copies(hicma_tlr_ctx *c, std::vector<CopyTask> &v) {
     return check_launch(c);
 }
 
-CopyTask make_copy(const double *src, int lds, double *dst, int ldd, int rows, int cols, double alpha = 1.0) {
+CopyTask make_copy(const double *src, int lds, double *dst, int ldd, int rows, int cols, double alpha = 1.0,
+                   double beta = 0.0) {
     CopyTask t;
     t.src = src; t.dst = dst; t.lds = lds; t.ldd = ldd; t.rows = rows; t.cols = cols; t.alpha = alpha;
+    t.beta = beta;
     return t;
 }
 
@@ -379,17 +381,19 @@ struct RecompTask {
     int *rank_dst;
 };
 
+// Workspace of one low-rank update (K = rc + ra).
 size_t recomp_ws_bytes(int nb, const RecompTask &t) {
-    const int K = t.rc + t.ra;
+    const int K = t.rc + t.ra, rc = t.rc, ra = t.ra;
     const int pb = qr_panel_width(nb);
-    const size_t npan = (size_t)(K + pb - 1) / pb + 1;
+    const size_t npk = (size_t)(K + pb - 1) / pb + 1, npa = (size_t)(ra + pb - 1) / pb + 1;
+    auto A = [](size_t n) { return align_up(sizeof(double) * n + 1); };
     size_t b = 0;
-    b += align_up(sizeof(double) * (size_t)nb * K + 1) * 3;        // Us, Vs, Vkeep
-    b += align_up(sizeof(double) * (size_t)K + 1) * 2;             // tau
-    b += align_up(sizeof(double) * npan * pb * pb + 1) * 2;        // T factors
-    b += align_up(sizeof(double) * (size_t)K * K + 1) * 3;         // SU, RUc, T1
-    if (K > core_smem_kmax()) b += align_up(sizeof(double) * (size_t)K * K + 1);
-    if (t.Bv) b += align_up(sizeof(double) * (size_t)t.rb * t.ra + 1);
+    b += A((size_t)nb * K) * 3;                          // Us = [Cu | Wu], Vs = [Cv | -Y], Vk
+    b += A(ra) + A(K) + A(npa * pb * pb) + A(npk * pb * pb);  // tau, T factors of Wu and Vs
+    b += A((size_t)rc * ra) * 2;                         // Pu, Pu2
+    b += A((size_t)K * K) * 3;                           // RU, SU, T1
+    if (K > core_smem_kmax()) b += A((size_t)K * K);
+    if (t.Bv) b += A((size_t)t.rb * t.ra);
     return b + 1024;
 }
 
@@ -409,6 +413,16 @@ int run_core_buckets(hicma_tlr_ctx *c, std::vector<CoreTask> &cores, const CoreP
     return 0;
 }
 
+// Recompression of a batch of low-rank updates C = [Cu Au][Cv -Y]^T.
+// The old U is orthonormal, so on that side only the new columns need an
+// orthogonal factorisation: Au is projected twice against Cu (block classical
+// Gram-Schmidt, DMMA GEMMs) and the residual Wu (nb x ra) gets a Householder
+// QR, giving R_U = [[I, Pu], [0, R(Wu)]].  The old V = V Sigma is orthogonal
+// only up to the core solver's tolerance relative to its largest singular
+// value, which is not enough to project its weak columns, so [Cv, -Y] gets a
+// full Householder QR for R_V.  The core M = R_U R_V^T is decomposed and
+// truncated (core kernel), then new U = Cu U_top + Q(Wu) [U_bot; 0] and
+// new V = [Cv, -Y] (R_U^T U_r).
 int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, double acc, int maxrank,
                    int fixed_rank, int *d_rank_task_base, bool fp32) {
     if (tasks.empty()) return 0;
@@ -417,59 +431,77 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
     while (i0 < tasks.size()) {
         c->ar->off = mark;
         std::vector<CopyTask> copies, keeps;
-        std::vector<GemmTask> g1, g2, g3, g4;
+        std::vector<GemmTask> g1, g2, gU, g3, g4;
+        std::vector<ProjTask> projs;
         std::vector<QRTask> qrs;
+        std::vector<AssembleTask> asm_;
         std::vector<CoreTask> cores;
         std::vector<QApplyTask> apps;
         size_t i = i0;
         int *rank_task = d_rank_task_base;
         for (; i < tasks.size(); ++i) {
             const RecompTask &t = tasks[i];
-            const size_t need = recomp_ws_bytes(nb, t);
-            if (need > ws_free(c)) {
+            if (recomp_ws_bytes(nb, t) > ws_free(c)) {
                 if (i == i0) { set_err("workspace too small for one recompression (K=%d)", t.rc + t.ra); return HICMA_TLR_ERR_OOM; }
                 break;
             }
-            const int K = t.rc + t.ra;
+            const int rc = t.rc, ra = t.ra, K = rc + ra;
             CoreTask ct{};
             ct.rank_out = t.rank_dst;
             ct.rank_task = rank_task + (i - i0);
             ct.K = K;
             if (K == 0) { cores.push_back(ct); continue; }
-            const int pb = qr_panel_width(nb);
-            const size_t npan = (size_t)(K + pb - 1) / pb + 1;
+            const int pbw = qr_panel_width(nb);
+            const size_t npk = (size_t)(K + pbw - 1) / pbw + 1, npa = (size_t)(ra + pbw - 1) / pbw + 1;
             double *Us = ws_alloc<double>(c, (size_t)nb * K);
             double *Vs = ws_alloc<double>(c, (size_t)nb * K);
             double *Vk = ws_alloc<double>(c, (size_t)nb * K);
-            double *tauU = ws_alloc<double>(c, K), *tauV = ws_alloc<double>(c, K);
-            double *TU = ws_alloc<double>(c, npan * pb * pb), *TV = ws_alloc<double>(c, npan * pb * pb);
-            double *SU = ws_alloc<double>(c, (size_t)K * K), *RUc = ws_alloc<double>(c, (size_t)K * K);
-            double *T1 = ws_alloc<double>(c, (size_t)K * K);
+            double *tauU = ws_alloc<double>(c, ra), *tauV = ws_alloc<double>(c, K);
+            double *TU = ws_alloc<double>(c, npa * pbw * pbw), *TV = ws_alloc<double>(c, npk * pbw * pbw);
+            double *Pu = ws_alloc<double>(c, (size_t)rc * ra), *Pu2 = ws_alloc<double>(c, (size_t)rc * ra);
+            double *RU = ws_alloc<double>(c, (size_t)K * K);
+            double *SU = ws_alloc<double>(c, (size_t)K * K), *T1 = ws_alloc<double>(c, (size_t)K * K);
             double *work = K > core_smem_kmax() ? ws_alloc<double>(c, (size_t)K * K) : nullptr;
-            if (t.rc > 0) {
-                copies.push_back(make_copy(t.Cu, nb, Us, nb, nb, t.rc));
-                copies.push_back(make_copy(t.Cv, nb, Vs, nb, nb, t.rc));
+            double *Wu = Us + (size_t)nb * rc;
+            double *Yb = Vs + (size_t)nb * rc;
+            if (rc > 0) {
+                copies.push_back(make_copy(t.Cu, nb, Us, nb, nb, rc));
+                copies.push_back(make_copy(t.Cv, nb, Vs, nb, nb, rc));
             }
-            if (t.ra > 0) {
-                copies.push_back(make_copy(t.Au, nb, Us + (size_t)nb * t.rc, nb, nb, t.ra));
-                double *Y = Vs + (size_t)nb * t.rc;
+            if (ra > 0) {
+                copies.push_back(make_copy(t.Au, nb, Wu, nb, nb, ra));
                 if (t.Bv) {
-                    double *P = ws_alloc<double>(c, (size_t)t.rb * t.ra);
-                    g1.push_back(make_gemm(1, 0, t.rb, t.ra, nb, 1.0, t.Bv, nb, t.Av, nb, 0.0, P, t.rb));
-                    g2.push_back(make_gemm(0, 0, nb, t.ra, t.rb, -1.0, t.Bu, nb, P, t.rb, 0.0, Y, nb));
+                    double *P = ws_alloc<double>(c, (size_t)t.rb * ra);
+                    g1.push_back(make_gemm(1, 0, t.rb, ra, nb, 1.0, t.Bv, nb, t.Av, nb, 0.0, P, t.rb));
+                    g2.push_back(make_gemm(0, 0, nb, ra, t.rb, -1.0, t.Bu, nb, P, t.rb, 0.0, Yb, nb));
                 } else {
-                    g1.push_back(make_gemm(0, 0, nb, t.ra, nb, -1.0, t.Bu, nb, t.Av, nb, 0.0, Y, nb));
+                    g1.push_back(make_gemm(0, 0, nb, ra, nb, -1.0, t.Bu, nb, t.Av, nb, 0.0, Yb, nb));
                 }
+                // two rounds of projection of Au against the old orthonormal U
+                if (rc > 0) projs.push_back(ProjTask{Us, Wu, Pu, Pu2, nb, rc, ra});
+                qrs.push_back(QRTask{Wu, tauU, TU, nb, ra, nb});
             }
             keeps.push_back(make_copy(Vs, nb, Vk, nb, nb, K));
-            qrs.push_back(QRTask{Us, tauU, TU, nb, K, nb});
             qrs.push_back(QRTask{Vs, tauV, TV, nb, K, nb});
-            ct.RU = Us; ct.RV = Vs; ct.ldru = nb; ct.ldrv = nb;
-            ct.SU = SU; ct.RUc = RUc; ct.work = work;
+            asm_.push_back(AssembleTask{Pu, Wu, RU, rc, ra, nb});
+            ct.RU = RU; ct.RV = Vs; ct.ldru = K; ct.ldrv = nb;
+            ct.SU = SU; ct.RUc = nullptr; ct.work = work;
             cores.push_back(ct);
-            apps.push_back(QApplyTask{Us, TU, SU, t.outU, ct.rank_task, nb, K, nb, K, nb, maxrank});
-            // V Sigma = M^T U = R_V (R_U^T U): new V = Vs_orig (R_U^T U_r)
-            GemmTask a = make_gemm(1, 0, K, K, K, 1.0, RUc, K, SU, K, 0.0, T1, K);
+            // new U = Q(Wu) [U_bot; 0] + Cu U_top
+            if (ra > 0) {
+                apps.push_back(QApplyTask{Wu, TU, SU + rc, t.outU, ct.rank_task, nb, ra, nb, K, nb, maxrank});
+                if (rc > 0) {
+                    GemmTask u = make_gemm(0, 0, nb, maxrank, rc, 1.0, Us, nb, SU, K, 1.0, t.outU, nb);
+                    u.n_dev = ct.rank_task;
+                    gU.push_back(u);
+                }
+            } else {
+                GemmTask u = make_gemm(0, 0, nb, maxrank, rc, 1.0, Us, nb, SU, K, 0.0, t.outU, nb);
+                u.n_dev = ct.rank_task;
+                gU.push_back(u);
+            }
+            // V Sigma = M^T U = R_V (R_U^T U): new V = [Cv, -Y] (R_U^T U_r)
+            GemmTask a = make_gemm(1, 0, K, K, K, 1.0, RU, K, SU, K, 0.0, T1, K);
             a.n_dev = ct.rank_task;
             g3.push_back(a);
             GemmTask b = make_gemm(0, 0, nb, maxrank, K, 1.0, Vk, nb, T1, K, 0.0, t.outV, nb);
@@ -480,10 +512,29 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
         TRY(run_gemms(c, g1, fp32));
         TRY(run_gemms(c, g2, fp32));
         TRY(run_copies(c, keeps));
+        if (!projs.empty()) {
+            double fl = 0.0, by = 0.0;
+            for (auto &p : projs) {
+                fl += 8.0 * p.nb * p.rc * p.ra;             // two rounds of C^T W and C P
+                by += 8.0 * p.nb * (p.rc + 2.0 * p.ra);     // C and W read once, W written once
+            }
+            Prof pr(c, P_PROJ, fl, by);
+            ProjTask *d = stage(c, projs.data(), projs.size());
+            if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+            launch_bcgs2(d, (int)projs.size(), c->cur);
+            TRY(check_launch(c));
+        }
         TRY(run_qr(c, qrs, nb));
+        if (!asm_.empty()) {
+            AssembleTask *d = stage(c, asm_.data(), asm_.size());
+            if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+            launch_assemble_r(d, (int)asm_.size(), c->cur);
+            TRY(check_launch(c));
+        }
         CoreParams cp{0, acc, maxrank, fixed_rank, nb, c->d_flags + 1, c->d_flags + 2};
         TRY(run_core_buckets(c, cores, cp));
         TRY(run_qapply(c, apps, nb));
+        TRY(run_gemms(c, gU));
         TRY(run_gemms(c, g3));
         TRY(run_gemms(c, g4));
         i0 = i;
@@ -1332,7 +1383,16 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             if (verbose) fprintf(stderr, "dpotrf failed: info = %d (panel %d)\n", info, k);
             break;
         }
-        if (verbose > 1) fprintf(stderr, "panel %d done\n", k);
+        if (verbose > 1) {
+            static double t_last = 0.0;
+            const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+            if (k == 0) t_last = 0.0;
+            fprintf(stderr, "panel %3d wall %8.3f ms trsm %7.3f syrk %7.3f gemm %7.3f potrf(k+1) %7.3f tasks %zu\n", k,
+                    (now - t_last) * 1e3, elapsed(ev[T0], ev[T1]) * 1e3,
+                    k + 1 < NT ? elapsed(ev[S0], ev[S1]) * 1e3 : 0.0, k + 1 < NT ? elapsed(ev[G0], ev[G1]) * 1e3 : 0.0,
+                    k + 1 < NT ? elapsed(ev[P0], ev[P1]) * 1e3 : 0.0, rec.size());
+            t_last = now;
+        }
     }
     for (auto &e : ev) cudaEventDestroy(e);
     cudaEventDestroy(evP);

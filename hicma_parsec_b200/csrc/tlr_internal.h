@@ -73,10 +73,32 @@ struct CopyTask {
     int lds, ldd;
     int rows, cols;
     double alpha;
+    double beta;        // dst = alpha src + beta dst (beta = 0: plain copy)
 };
 void launch_copy_batched(const CopyTask *d_tasks, int ntasks, int max_cols, cudaStream_t st);
 void launch_zero_upper(double *A, int n, int lda, cudaStream_t st);
 void launch_set_identity(double *A, int n, int lda, cudaStream_t st);
+
+// ------------------------------------------------- recompression helpers ---
+// Explicit K x K upper triangular factor of [Cu, Au] (K = rc + ra) after the
+// projection of Au on the orthonormal Cu: RU = [[I, Pu], [0, R(Wu)]].
+struct AssembleTask {
+    const double *Pu;   // rc x ra (ld rc)
+    const double *Wu;   // QR'd residual, R in its top ra x ra (ld nb)
+    double *RU;         // K x K (ld K)
+    int rc, ra, nb;
+};
+void launch_assemble_r(const AssembleTask *d_tasks, int ntasks, cudaStream_t st);
+// Two rounds of block Gram-Schmidt of W (nb x ra, ld nb) against the
+// orthonormal C (nb x rc, ld nb): W -= C (C^T W) twice, P = sum of the two
+// coefficient blocks (rc x ra, ld rc); P2 is scratch of the same size.
+struct ProjTask {
+    const double *C;
+    double *W;
+    double *P, *P2;
+    int nb, rc, ra;
+};
+void launch_bcgs2(const ProjTask *d_tasks, int ntasks, cudaStream_t st);
 
 // ---------------------------------------------------------------- POTRF -----
 // Factor the jb x jb diagonal block at A (lda) in place (lower), write its

@@ -158,15 +158,16 @@ class Context:
     def stream(self) -> int:
         return self.lib.hicma_tlr_stream(self.h) or 0
 
-    PROF_CLASSES = ("gemm", "qr", "qapply", "core_svd", "potrf", "cov", "copy", "other")
+    PROF_CLASSES = ("gemm", "qr", "qapply", "core_svd", "potrf", "cov", "copy", "other", "proj")
 
     def prof_enable(self, on: bool = True) -> None:
         _check(self.lib.hicma_tlr_prof_enable(self.h, int(on)), "hicma_tlr_prof_enable")
 
     def prof_read(self) -> dict:
-        out = np.zeros(32)
-        _check(self.lib.hicma_tlr_prof_read(self.h, _p(out), 8), "hicma_tlr_prof_read")
-        o = out.reshape(8, 4)
+        nc = len(self.PROF_CLASSES)
+        out = np.zeros(4 * nc)
+        _check(self.lib.hicma_tlr_prof_read(self.h, _p(out), nc), "hicma_tlr_prof_read")
+        o = out.reshape(nc, 4)
         return {name: {"launches": int(o[k, 0]), "seconds": float(o[k, 1]), "flops": float(o[k, 2]),
                        "bytes": float(o[k, 3])} for k, name in enumerate(self.PROF_CLASSES)}
 

@@ -199,7 +199,8 @@ int hicma_tlr_check(hicma_tlr_ctx *ctx, hicma_tlr_desc *L, const hicma_tlr_probl
 
 /* Per-kernel-class device timing (CUDA events around launches on the context
  * stream).  Classes: 0 GEMM, 1 QR, 2 Q-apply, 3 core SVD, 4 tile POTRF,
- * 5 covariance generation, 6 copies.  out[4*k + j]: j = 0 launches,
+ * 5 covariance generation, 6 copies, 7 other, 8 Gram-Schmidt projections.
+ * out[4*k + j]: j = 0 launches,
  * 1 seconds, 2 algorithmic flops, 3 algorithmic bytes.  Enabling resets. */
 int hicma_tlr_prof_enable(hicma_tlr_ctx *ctx, int on);
 int hicma_tlr_prof_read(hicma_tlr_ctx *ctx, double *out, int nclass);
