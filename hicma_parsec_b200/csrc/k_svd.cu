@@ -5,13 +5,25 @@
 // hicma_parsec/HiCMA_dpotrf_L_2flow.jdf:830-903,985-1058) and the rank rule of
 // starsh_dense_dlrrsdd (STARSH_gen.jdf:162-171).
 //
-// One CTA per core.  M = R_U R_V^T is formed in shared memory (global
-// scratch when K is large) and a one-sided (Hestenes) Jacobi SVD
-// orthogonalises its columns, W = M J = U Sigma, with a round-robin
-// tournament ordering: each round rotates K/2 disjoint column pairs in
-// parallel, LP lanes per pair, the three dot products of a pair reduced with
-// warp shuffles.  The rotations are not accumulated: the caller recovers
-// V Sigma = M^T U = R_V (R_U^T U) with two GEMMs, so only W lives on chip.
+// One CTA per core, QR-preconditioned one-sided Jacobi (Drmac and Veselic,
+// "New fast and accurate Jacobi SVD algorithm", SIMAX 2008):
+//   1. T = M^T with M = R_U R_V^T is formed in shared memory (global scratch
+//      when K is large).
+//   2. Householder QR with column pivoting, T P = Q R, one warp choosing the
+//      pivot and building the reflector, all warps applying it (one column
+//      per warp, exact partial column norms recomputed in the same pass).  It
+//      stops at step k once the trailing block's Frobenius norm is below the
+//      truncation floor, so only the leading k rows of R survive; k is about
+//      the numerical rank, not K.
+//   3. R^T (K x k, in place) is orthogonalised by one-sided (Hestenes) Jacobi,
+//      X J = W Sigma, with a round-robin tournament ordering: each round
+//      rotates k/2 disjoint column pairs in parallel, LP lanes per pair, dot
+//      products reduced with warp shuffles.  The rows of a pivoted R are
+//      graded, so the columns of R^T are nearly orthogonal and few sweeps are
+//      needed.
+//   4. P^T M = R^T Q^T, so the left singular vectors of M are the rows of W
+//      permuted back: U[piv[q], :] = W[q, :] / sigma.  Neither Q nor J is
+//      formed; the caller recovers V Sigma = M^T U = R_V (R_U^T U) with GEMMs.
 // One-sided Jacobi resolves small singular values to high relative accuracy,
 // which the absolute truncation threshold needs; the decision is FP64.
 #include "tlr_internal.h"
@@ -36,8 +48,9 @@ __device__ __forceinline__ double group_sum(double v) {
 template <int LP, int CT>
 __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ tasks, CoreParams p) {
     extern __shared__ double sm[];
-    __shared__ int rotated;
-    __shared__ int rank_sh;
+    __shared__ int rotated, rank_sh, stop_sh;
+    __shared__ double tau_sh, tail_sh, tau2_sh;
+    constexpr int NW = CT / 32;
     const CoreTask t = tasks[blockIdx.x];
     const int K = t.K;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -50,66 +63,157 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
     }
     const bool in_smem = K <= KMAX_SMEM;
     double *W = in_smem ? sm : t.work;
-    double *sig = in_smem ? sm + (size_t)K * K : sm;
-    int *order = (int *)(sig + K);
+    double *sig = in_smem ? sm + (size_t)K * K : sm;   // partial norms^2, then sigma
+    double *hv = sig + K;                               // Householder vector
+    int *order = (int *)(hv + K);
+    int *piv = order + K;
 
-    // M = RU RV^T (RU, RV upper triangular; RU null: identity); clean copy of RU
+    // 1. T = M^T: T(i, c) = M(c, i) = sum_{l >= max(i, c)} RU(c, l) RV(i, l)
+    //    (RU null: M = RV^T, T = RV); clean copy of RU on request
     for (long long idx = tid; idx < (long long)K * K; idx += CT) {
-        const int i = (int)(idx % K), j = (int)(idx / K);
+        const int i = (int)(idx % K), c = (int)(idx / K);
         double s = 0.0;
         if (t.RU) {
-            const int l0 = i > j ? i : j;
+            const int l0 = i > c ? i : c;
             for (int l = l0; l < K; ++l)
-                s += t.RU[(size_t)i + (size_t)l * t.ldru] * t.RV[(size_t)j + (size_t)l * t.ldrv];
-            if (t.RUc) t.RUc[idx] = (i <= j) ? t.RU[(size_t)i + (size_t)j * t.ldru] : 0.0;
+                s += t.RU[(size_t)c + (size_t)l * t.ldru] * t.RV[(size_t)i + (size_t)l * t.ldrv];
+            if (t.RUc) t.RUc[idx] = (i <= c) ? t.RU[(size_t)i + (size_t)c * t.ldru] : 0.0;
         } else {
-            s = (j <= i) ? t.RV[(size_t)j + (size_t)i * t.ldrv] : 0.0;
+            s = (i <= c) ? t.RV[(size_t)i + (size_t)c * t.ldrv] : 0.0;
         }
         W[idx] = s;
     }
     __syncthreads();
-
-    // Columns whose norm is below tau can only move the result by O(tau) and
-    // are truncated anyway: pairs involving them are not rotated.  tau is
-    // 1e-3 of the absolute threshold (recompression) or of tol * ||M||_F
-    // (generation); fixed-rank mode keeps every rotation.
-    __shared__ double tau2_sh;
+    // column norms^2 and the identity pivot
+    for (int c = warp; c < K; c += NW) {
+        double s2 = 0.0;
+        for (int r = lane; r < K; r += 32) s2 += W[(size_t)c * K + r] * W[(size_t)c * K + r];
+        s2 = group_sum<32>(s2);
+        if (lane == 0) { sig[c] = s2; piv[c] = c; }
+    }
+    __syncthreads();
+    // Truncation floor tau2 on squared norms: 1e-3 of the absolute threshold
+    // (recompression) or of tol * ||M||_F (generation); zero in fixed-rank mode.
     if (tid == 0) {
         double tau = 0.0;
         if (p.mode == 0 && p.fixed_rank <= 0) tau = 1e-3 * p.tol;
-        tau2_sh = tau * tau;
-    }
-    if (p.mode == 1) {
-        double s2 = 0.0;
-        for (long long idx = tid; idx < (long long)K * K; idx += CT) s2 += W[idx] * W[idx];
-        s2 = group_sum<32>(s2);
-        __shared__ double red[CT / 32];
-        if (lane == 0) red[warp] = s2;
-        __syncthreads();
-        if (tid == 0) {
+        double tau2 = tau * tau;
+        if (p.mode == 1) {
             double tot = 0.0;
-            for (int w = 0; w < CT / 32; ++w) tot += red[w];
-            tau2_sh = 1e-6 * p.tol * p.tol * tot;
+            for (int c = 0; c < K; ++c) tot += sig[c];
+            tau2 = 1e-6 * p.tol * p.tol * tot;
         }
+        tau2_sh = tau2;
+        tail_sh = 0.0;
     }
     __syncthreads();
     const double tau2 = tau2_sh;
 
+    // 2. pivoted Householder QR of T, stopped when the trailing mass <= tau2
+    int k = K;
+    for (int j = 0; j < K; ++j) {
+        if (warp == 0) {
+            double tr = 0.0, best = -1.0;
+            int bi = j;
+            for (int c = j + lane; c < K; c += 32) {
+                const double v = sig[c];
+                tr += v;
+                if (v > best) { best = v; bi = c; }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                tr += __shfl_xor_sync(0xffffffffu, tr, o);
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            const bool stop = !(tr > tau2);
+            if (lane == 0) {
+                stop_sh = stop;
+                if (stop) tail_sh = tr;
+            }
+            if (!stop) {
+                double *cj = W + (size_t)j * K;
+                if (bi != j) {
+                    double *cb = W + (size_t)bi * K;
+                    for (int r = lane; r < K; r += 32) {
+                        const double x = cj[r];
+                        cj[r] = cb[r];
+                        cb[r] = x;
+                    }
+                    if (lane == 0) {
+                        const double sx = sig[j]; sig[j] = sig[bi]; sig[bi] = sx;
+                        const int px = piv[j]; piv[j] = piv[bi]; piv[bi] = px;
+                    }
+                    __syncwarp();
+                }
+                const double alpha = cj[j];
+                double s2 = 0.0;
+                for (int r = j + 1 + lane; r < K; r += 32) s2 += cj[r] * cj[r];
+                s2 = group_sum<32>(s2);
+                double th = 0.0, scl = 0.0, beta = alpha;
+                if (s2 > 0.0) {
+                    beta = -copysign(sqrt(alpha * alpha + s2), alpha);
+                    th = (beta - alpha) / beta;
+                    scl = 1.0 / (alpha - beta);
+                }
+                for (int r = j + 1 + lane; r < K; r += 32) {
+                    hv[r] = cj[r] * scl;
+                    cj[r] = 0.0;
+                }
+                if (lane == 0) {
+                    hv[j] = 1.0;
+                    cj[j] = beta;
+                    tau_sh = th;
+                }
+            }
+        }
+        __syncthreads();
+        if (stop_sh) { k = j; break; }
+        const double th = tau_sh;
+        for (int c = j + 1 + warp; c < K; c += NW) {
+            double *col = W + (size_t)c * K;
+            double w = 0.0;
+            for (int r = j + lane; r < K; r += 32) w += hv[r] * col[r];
+            w = group_sum<32>(w) * th;
+            double s2 = 0.0;
+            for (int r = j + lane; r < K; r += 32) {
+                const double x = col[r] - w * hv[r];
+                col[r] = x;
+                if (r > j) s2 += x * x;
+            }
+            s2 = group_sum<32>(s2);
+            if (lane == 0) sig[c] = s2;
+        }
+        __syncthreads();
+    }
+    // R^T in place: swap the upper and lower triangles of the rows that stay
+    for (long long idx = tid; idx < (long long)K * K; idx += CT) {
+        const int i = (int)(idx % K), c = (int)(idx / K);
+        if (i < c && i < k) {
+            const double x = W[(size_t)i + (size_t)c * K];
+            W[(size_t)i + (size_t)c * K] = W[(size_t)c + (size_t)i * K];
+            W[(size_t)c + (size_t)i * K] = x;
+        }
+    }
+    __syncthreads();
+
+    // 3. one-sided Jacobi on the k columns (length K) of R^T
     constexpr int GPW = 32 / LP;                 // pair groups per warp
-    const int groups = (CT / 32) * GPW;          // pair groups per CTA
+    const int groups = NW * GPW;                 // pair groups per CTA
     const int gsub = lane / LP, gl = lane % LP;
-    const int Kp = K + (K & 1);
+    const int kp = k + (k & 1);
     // A pair counts as orthogonal when |c| <= tolj sqrt(a b).  The computed dot
     // products of K-term columns carry a rounding error of about K eps, so a
     // tighter threshold would keep rotating noise and never converge.
     const double tolj = 4.4e-16 * (double)(K > 16 ? K : 16);
     int sweeps = 0;
-    if (K > 1) {
+    if (k > 1) {
         for (int sweep = 0; sweep < MAX_SWEEPS; ++sweep) {
             if (tid == 0) rotated = 0;
-            // exact squared column norms at the start of every sweep (sig is
-            // free until the sweeps end); rotations keep them up to date
-            for (int c = warp; c < K; c += CT / 32) {
+            // exact squared column norms at the start of every sweep; rotations
+            // keep them up to date
+            for (int c = warp; c < k; c += NW) {
                 double s2 = 0.0;
                 for (int r = lane; r < K; r += 32) s2 += W[(size_t)c * K + r] * W[(size_t)c * K + r];
                 s2 = group_sum<32>(s2);
@@ -117,17 +221,17 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
             }
             __syncthreads();
             ++sweeps;
-            for (int round = 0; round < Kp - 1; ++round) {
+            for (int round = 0; round < kp - 1; ++round) {
                 // uniform trip count per warp: every lane reaches the shuffles
-                for (int base = warp * GPW; base < Kp / 2; base += groups) {
+                for (int base = warp * GPW; base < kp / 2; base += groups) {
                     const int pr = base + gsub;
                     int a = 0, b = 0;
-                    bool valid = pr < Kp / 2;
+                    bool valid = pr < kp / 2;
                     if (valid) {
-                        a = tourney(pr, round, Kp);
-                        b = tourney(Kp - 1 - pr, round, Kp);
+                        a = tourney(pr, round, kp);
+                        b = tourney(kp - 1 - pr, round, kp);
                         if (a > b) { const int tmp = a; a = b; b = tmp; }
-                        valid = b < K && sig[a] > tau2 && sig[b] > tau2;
+                        valid = b < k && sig[a] > tau2 && sig[b] > tau2;
                     }
                     double aa = 0.0, bb = 0.0, cc = 0.0;
                     double *mp = W + (size_t)a * K, *mq = W + (size_t)b * K;
@@ -165,18 +269,18 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
         }
     }
 
-    // singular values and descending order
-    for (int c = warp; c < K; c += CT / 32) {
+    // 4. singular values and descending order
+    for (int c = warp; c < k; c += NW) {
         double s = 0.0;
         for (int r = lane; r < K; r += 32) s += W[(size_t)c * K + r] * W[(size_t)c * K + r];
         s = group_sum<32>(s);
         if (lane == 0) sig[c] = sqrt(s);
     }
     __syncthreads();
-    for (int c = tid; c < K; c += CT) {
+    for (int c = tid; c < k; c += CT) {
         const double sc = sig[c];
         int pos = 0;
-        for (int l = 0; l < K; ++l) {
+        for (int l = 0; l < k; ++l) {
             const double sl = sig[l];
             pos += (sl > sc) || (sl == sc && l < c);
         }
@@ -190,21 +294,23 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
                 r = p.fixed_rank < K ? p.fixed_rank : K;
             } else {
                 r = 0;
-                while (r < K && sig[order[r]] >= p.tol) ++r;
+                while (r < k && sig[order[r]] >= p.tol) ++r;
             }
             if (r > p.maxrank) {
                 r = p.maxrank;
                 if (p.overflow) atomicAdd(p.overflow, 1);
             }
         } else {
-            double total = 0.0;
-            for (int l = 0; l < K; ++l) total += sig[l] * sig[l];
+            // the truncated trailing mass belongs to the tail of the spectrum
+            const double dropped = tail_sh;
+            double total = dropped;
+            for (int l = 0; l < k; ++l) total += sig[l] * sig[l];
             if (total == 0.0) {
                 r = 0;
             } else {
                 const double thr = p.tol * p.tol * total;
-                double tail = 0.0;
-                r = K;
+                double tail = dropped;
+                r = k;
                 while (r > 0) {
                     const double s2 = sig[order[r - 1]] * sig[order[r - 1]];
                     if (tail + s2 > thr) break;
@@ -220,12 +326,17 @@ __global__ void __launch_bounds__(CT) k_core_svd(const CoreTask *__restrict__ ta
         if (p.sweeps) atomicAdd(p.sweeps, sweeps);
     }
     __syncthreads();
-    // left singular vectors, all K columns in decreasing sigma order
+    // left singular vectors of M in decreasing sigma order: U(piv[q], i) = W(q, order[i]) / sigma;
+    // columns past k (zero singular values) are zero
     for (long long idx = tid; idx < (long long)K * K; idx += CT) {
-        const int row = (int)(idx % K), i = (int)(idx / K);
-        const int c = order[i];
-        const double s = sig[c];
-        t.SU[idx] = s > 0.0 ? W[(size_t)c * K + row] / s : 0.0;
+        const int q = (int)(idx % K), i = (int)(idx / K);
+        if (i < k) {
+            const int c = order[i];
+            const double s = sig[c];
+            t.SU[(size_t)piv[q] + (size_t)i * K] = s > 0.0 ? W[(size_t)c * K + q] / s : 0.0;
+        } else {
+            t.SU[idx] = 0.0;
+        }
     }
 }
 
@@ -244,10 +355,12 @@ void launch_core_svd_batched(const CoreTask *d_tasks, int ntasks, int kmax, cons
     if (ntasks <= 0) return;
     if (kmax < 1) kmax = 1;
     size_t smem;
+    // W (K x K, on chip when small), partial norms / sigma, Householder vector,
+    // order and pivot
     if (kmax <= KMAX_SMEM)
-        smem = sizeof(double) * ((size_t)kmax * kmax + kmax) + sizeof(int) * kmax;
+        smem = sizeof(double) * ((size_t)kmax * kmax + 2 * (size_t)kmax) + 2 * sizeof(int) * kmax;
     else
-        smem = sizeof(double) * (size_t)kmax + sizeof(int) * kmax;
+        smem = 2 * sizeof(double) * (size_t)kmax + 2 * sizeof(int) * kmax;
     smem = (smem + 15) / 16 * 16;
     // lanes per pair ~ K/8 elements each; more pair groups per CTA for large K
     if (kmax <= 64) launch_lp<8, 256>(d_tasks, ntasks, smem, p, st);
