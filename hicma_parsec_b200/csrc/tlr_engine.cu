@@ -79,7 +79,8 @@ struct hicma_tlr_ctx_s {
     Arena *ar = nullptr;                // arena of `cur`
     char *h_stage = nullptr, *d_stage = nullptr;
     size_t stage_bytes = 0, stage_off = 0;
-    int *d_flags = nullptr;     // [0] info, [1] overflow count
+    int *d_flags = nullptr;     // [0] info, [1] overflow count, [2] Jacobi sweeps, [3] device wait timed out
+    int nsm = 148;              // SM count of the device
     double *d_scal = nullptr;   // device scalars
     int precision = HICMA_TLR_PREC_FP64;
     long long launches = 0;
@@ -137,6 +138,18 @@ int ctx_sync(hicma_tlr_ctx *c) {
 }
 
 void ws_reset(hicma_tlr_ctx *c) { c->ar->off = 0; }
+
+// After a synchronisation: report (and clear) a bounded device wait that gave up.
+int check_timeout(hicma_tlr_ctx *c) {
+    int f = 0;
+    CUDA_TRY(cudaMemcpy(&f, c->d_flags + 3, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f) {
+        CUDA_TRY(cudaMemset(c->d_flags + 3, 0, sizeof(int)));
+        set_err("a bounded device wait gave up (tile POTRF task queue)");
+        return HICMA_TLR_ERR_TIMEOUT;
+    }
+    return 0;
+}
 template <class T>
 T *ws_alloc(hicma_tlr_ctx *c, size_t n) {
     const size_t bytes = align_up(n * sizeof(T) + 1);
@@ -324,6 +337,23 @@ int potrf_tile(hicma_tlr_ctx *c, double *A, int n, int lda, double *Linv, int ld
     cudaStream_t st = c->cur;
     const size_t mark = c->ar->off;
     Prof pf(c, P_POTRF, (double)n * n * n / 3.0 * (Linv ? 2.0 : 1.0), 8.0 * n * (double)n * (Linv ? 3.0 : 2.0));
+    if (n <= potrf_tile_max_n()) {
+        // one persistent launch: block Cholesky and block inverse as a task queue
+        const int nblk = (n + DBK - 1) / DBK;
+        int *cnt = ws_alloc<int>(c, potrf_tile_scratch_ints(n));
+        double *D = Linv ? nullptr : ws_alloc<double>(c, (size_t)nblk * DBK * DBK);
+        if (!cnt || (!Linv && !D)) { set_err("workspace exhausted (potrf)"); return HICMA_TLR_ERR_OOM; }
+        if (Linv) CUDA_TRY(cudaMemset2DAsync(Linv, (size_t)ldl * sizeof(double), 0, sizeof(double) * n, n, st));
+        if (launch_potrf_tile(A, lda, n, Linv, ldl, D, cnt, d_info, info_base, c->d_flags + 3, c->nsm, st)) {
+            set_err("tile POTRF launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+            return HICMA_TLR_ERR_CUDA;
+        }
+        TRY(check_launch(c));
+        launch_zero_upper(A, n, lda, st);
+        TRY(check_launch(c));
+        c->ar->off = mark;
+        return 0;
+    }
     double *dscr = nullptr;
     if (!Linv) {
         dscr = ws_alloc<double>(c, DBK * DBK);
@@ -691,6 +721,7 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     CUDA_TRY(cudaMalloc(&c->d_flags, 64 * sizeof(int)));
     CUDA_TRY(cudaMalloc(&c->d_scal, 64 * sizeof(double)));
     CUDA_TRY(cudaMemset(c->d_flags, 0, 64 * sizeof(int)));
+    CUDA_TRY(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
     *out = c;
     return 0;
 }
@@ -1167,6 +1198,58 @@ static int run_syrk(hicma_tlr_ctx *c, hicma_tlr_desc *A, int k, const std::vecto
     return 0;
 }
 
+// All low-rank SYRK contributions to diagonal tile m at once, right before
+// its POTRF: A_mm -= sum_j U_mj (V_mj^T V_mj) U_mj^T over the off-band tiles
+// (m, j), j < m.  The factors of column j are final once panel j is done, so
+// deferring is exact; applying them as one K-concatenated DMMA GEMM
+// (K = sum of the ranks) reads and writes the dense tile once instead of once
+// per panel.  Chunked to the free workspace.
+static int run_syrk_lazy(hicma_tlr_ctx *c, hicma_tlr_desc *A, int m) {
+    const int NB = A->NB;
+    const size_t mark = c->ar->off;
+    std::vector<int> js;
+    for (int j = 0; j < m; ++j)
+        if (!A->is_dense(m, j) && A->rank(m, j) > 0) js.push_back(j);
+    size_t p = 0;
+    while (p < js.size()) {
+        c->ar->off = mark;
+        // columns that fit: per tile r^2 (W) + 2 NB r (Y and U, concatenated)
+        size_t q = p, sumr = 0, need = 4096;
+        const size_t avail = ws_free(c);
+        while (q < js.size()) {
+            const size_t r = (size_t)A->rank(m, js[q]);
+            const size_t add = align_up(sizeof(double) * r * r + 1) + 2 * sizeof(double) * NB * r;
+            if (q > p && need + add + 2 * 256 > avail) break;
+            need += add;
+            sumr += r;
+            ++q;
+        }
+        double *Yc = ws_alloc<double>(c, (size_t)NB * sumr);
+        double *Uc = ws_alloc<double>(c, (size_t)NB * sumr);
+        if (!Yc || !Uc) { set_err("workspace too small (syrk, K=%zu)", sumr); return HICMA_TLR_ERR_OOM; }
+        std::vector<GemmTask> g1, g2;
+        std::vector<CopyTask> cp;
+        size_t off = 0;
+        for (size_t t = p; t < q; ++t) {
+            const int j = js[t], r = A->rank(m, j);
+            double *W = ws_alloc<double>(c, (size_t)r * r);
+            if (!W) { set_err("workspace too small (syrk)"); return HICMA_TLR_ERR_OOM; }
+            g1.push_back(make_gemm(1, 0, r, r, NB, 1.0, A->V(m, j), NB, A->V(m, j), NB, 0.0, W, r));
+            g2.push_back(make_gemm(0, 0, NB, r, r, 1.0, A->U(m, j), NB, W, r, 0.0, Yc + off * NB, NB));
+            cp.push_back(make_copy(A->U(m, j), NB, Uc + off * NB, NB, NB, r));
+            off += r;
+        }
+        TRY(run_gemms(c, g1));
+        TRY(run_gemms(c, g2));
+        TRY(run_copies(c, cp));
+        std::vector<GemmTask> g3{make_gemm(0, 1, NB, NB, (int)sumr, -1.0, Yc, NB, Uc, NB, 1.0, A->dense(m, m), NB, 1)};
+        TRY(run_gemms(c, g3));
+        p = q;
+    }
+    c->ar->off = mark;
+    return 0;
+}
+
 static unsigned long syrk_ops(const hicma_tlr_desc *A, int k, int m) {
     const unsigned long NB = A->NB;
     if (A->is_dense(m, k)) return op_counts('m', NB, NB, NB, 0);
@@ -1193,7 +1276,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     c->ar = &c->main_ar;
     c->main_ar.off = 0;
     c->hi_ar.off = 0;
-    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 3 * sizeof(int), c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 4 * sizeof(int), c->stream));
     TRY(ctx_sync(c));
     int *d_info = c->d_flags;
     int *rtask = ws_alloc<int>(c, (size_t)NT * NT + 16);
@@ -1277,7 +1360,8 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                 if (!lookahead) c->cur = c->stream;
                 c->ar->off = 0;
                 CUDA_TRY(cudaStreamWaitEvent(c->cur, evT, 0));
-                TRY(run_syrk(c, A, k, std::vector<int>{k + 1}));
+                if (A->is_dense(k + 1, k)) TRY(run_syrk(c, A, k, std::vector<int>{k + 1}));
+                TRY(run_syrk_lazy(c, A, k + 1));
                 CUDA_TRY(cudaEventRecord(ev[P0], c->cur));
                 TRY(potrf_tile(c, A->dense(k + 1, k + 1), NB, NB, A->linv(k + 1), NB, d_info, (k + 1) * NB));
                 CUDA_TRY(cudaEventRecord(ev[P1], c->cur));
@@ -1288,7 +1372,8 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             c->ar->off = base_mark;
             std::vector<int> ms;
             for (int m = k + 2; m < NT; ++m) {
-                ms.push_back(m);
+                // low-rank contributions are applied lazily before POTRF(m)
+                if (A->is_dense(m, k)) ms.push_back(m);
                 log_op(syrk_ops(A, k, m), m, m);
             }
             TRY(run_syrk(c, A, k, ms));
@@ -1398,8 +1483,13 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     cudaEventDestroy(evP);
     cudaEventDestroy(evT);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-    int flags_h[3] = {0, 0, 0};
-    CUDA_TRY(cudaMemcpy(flags_h, c->d_flags, 3 * sizeof(int), cudaMemcpyDeviceToHost));
+    int flags_h[4] = {0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpy(flags_h, c->d_flags, 4 * sizeof(int), cudaMemcpyDeviceToHost));
+    if (flags_h[3]) {
+        cudaMemset(c->d_flags + 3, 0, sizeof(int));
+        set_err("a bounded device wait gave up (tile POTRF task queue)");
+        return HICMA_TLR_ERR_TIMEOUT;
+    }
     const int overflow = flags_h[1];
     A->stats[8] = flags_h[2];
     if (tileops)
@@ -1859,7 +1949,8 @@ int hicma_tlr_k_potrf(hicma_tlr_ctx *c, int n, double *d_A, int lda, double *d_l
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     ws_reset(c);
     TRY(potrf_tile(c, d_A, n, lda, d_linv, n, d_info, info_offset));
-    return ctx_sync(c);
+    TRY(ctx_sync(c));
+    return check_timeout(c);
 }
 
 int hicma_tlr_k_lr_update(hicma_tlr_ctx *c, int nb, const double *d_Au, const double *d_Av, int ra,

@@ -101,6 +101,14 @@ struct ProjTask {
 void launch_bcgs2(const ProjTask *d_tasks, int ntasks, cudaStream_t st);
 
 // ---------------------------------------------------------------- POTRF -----
+// Tile Cholesky (+ inverse when X is given, X zeroed by the caller) in one
+// persistent launch of `grid` CTAs; n <= potrf_tile_max_n().  cnt: scratch of
+// potrf_tile_scratch_ints(n) ints; D: (n/64 rounded up) * 4096 doubles when X
+// is null.  *timeout is set if a bounded device wait gave up.
+int potrf_tile_max_n();
+size_t potrf_tile_scratch_ints(int n);
+int launch_potrf_tile(double *A, int lda, int n, double *X, int ldx, double *D, int *cnt, int *info,
+                      int info_base, int *timeout, int grid, cudaStream_t st);
 // Factor the jb x jb diagonal block at A (lda) in place (lower), write its
 // inverse into Dinv (ldd); on failure set *info = info_base + j + 1 once.
 void launch_potrf_diag(double *A, int lda, int jb, double *Dinv, int ldd, int *info,
