@@ -266,7 +266,11 @@ def run_ours(args, cfg):
             for c in range(m):
                 tiles[(m, c)] = A0.tile(m, c)
 
-    W = tlr.TLRMatrix(ctx, n, nb, mr, A0.band_size)
+    # the working copy gets A0's layout: created at the generation band, then widened
+    W = tlr.TLRMatrix(ctx, n, nb, mr, cfg["band"])
+    if A0.band_size != cfg["band"]:
+        W.generate(prob, acc, mr)
+        W.band_regenerate(prob, A0.band_size)
     stream = torch.cuda.ExternalStream(ctx.stream)
 
     def step():
@@ -335,7 +339,10 @@ def run_ours(args, cfg):
         host = torch.empty(nbytes // 8, dtype=torch.float64, pin_memory=True)
         ranks = np.empty((n // nb) ** 2, dtype=np.int32)
         A0.store_get(host.data_ptr(), ranks)
-        out = torch.empty(nbytes // 8 + (n // nb) ** 2 * nb * 2 * mr, dtype=torch.float64, pin_memory=True)
+        # the factor's store: W holds a factor of the same matrix, so its size (plus the
+        # slack of one more panel of rank growth) bounds what store_get writes
+        out = torch.empty(int(W.store_bytes() * 1.25) // 8 + (n // nb) * nb * 2 * mr, dtype=torch.float64,
+                          pin_memory=True)
         torch.cuda.synchronize()
         ts = []
         d2h = 0
