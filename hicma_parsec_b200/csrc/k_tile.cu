@@ -172,10 +172,47 @@ __global__ void __launch_bounds__(256) k_assemble_r(const AssembleTask *__restri
     }
 }
 
+__global__ void __launch_bounds__(256) k_sumsq_batched(const NormTask *__restrict__ tasks) {
+    const NormTask t = tasks[blockIdx.x];
+    __shared__ double red[8];
+    double s = 0.0;
+    for (long long idx = threadIdx.x; idx < (long long)t.rows * t.cols; idx += blockDim.x) {
+        const int r = (int)(idx % t.rows), c = (int)(idx / t.rows);
+        const double x = t.X[(size_t)r + (size_t)c * t.ld];
+        s += x * x;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < 8; ++w) tot += red[w];
+        *t.out = tot;
+    }
+}
+
+__global__ void k_precision_select(const SelTask *__restrict__ tasks, int ntasks, double thr2, int *count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ntasks) return;
+    const SelTask t = tasks[i];
+    const bool low = (*t.na) * (*t.nb) <= thr2;
+    *t.sel32 = low ? t.n : 0;
+    *t.sel64 = low ? 0 : t.n;
+    if (low && count) atomicAdd(count, 1);
+}
+
 }  // namespace
 
 void launch_assemble_r(const AssembleTask *d_tasks, int ntasks, cudaStream_t st) {
     if (ntasks > 0) k_assemble_r<<<ntasks, 256, 0, st>>>(d_tasks);
+}
+
+void launch_sumsq_batched(const NormTask *d_tasks, int ntasks, cudaStream_t st) {
+    if (ntasks > 0) k_sumsq_batched<<<ntasks, 256, 0, st>>>(d_tasks);
+}
+void launch_precision_select(const SelTask *d_tasks, int ntasks, double thr2, int *count, cudaStream_t st) {
+    if (ntasks > 0) k_precision_select<<<(ntasks + 127) / 128, 128, 0, st>>>(d_tasks, ntasks, thr2, count);
 }
 
 void launch_sumsq(const double *X, const double *Y, int m, int n, long long ld, int sym_lower, double *partial,

@@ -79,7 +79,7 @@ struct hicma_tlr_ctx_s {
     Arena *ar = nullptr;                // arena of `cur`
     char *h_stage = nullptr, *d_stage = nullptr;
     size_t stage_bytes = 0, stage_off = 0;
-    int *d_flags = nullptr;     // [0] info, [1] overflow count, [2] Jacobi sweeps, [3] device wait timed out
+    int *d_flags = nullptr;     // [0] info, [1] overflow, [2] Jacobi sweeps, [3] wait timed out, [4] FP32 updates
     int nsm = 148;              // SM count of the device
     double *d_scal = nullptr;   // device scalars
     int precision = HICMA_TLR_PREC_FP64;
@@ -93,7 +93,7 @@ struct hicma_tlr_ctx_s {
     struct ProfRec { int cls; cudaEvent_t a, b; double flops, bytes; };
     std::vector<ProfRec> prof_recs;
     std::vector<cudaEvent_t> ev_pool;
-    double prof_acc[9][4] = {};
+    double prof_acc[14][4] = {};
 };
 
 struct hicma_tlr_desc_s {
@@ -186,7 +186,12 @@ T *stage(hicma_tlr_ctx *c, const T *src, size_t n) {
     return d;
 }
 
-enum { P_GEMM = 0, P_QR, P_QAPPLY, P_CORE, P_POTRF, P_COV, P_COPY, P_OTHER, P_PROJ, P_NCLASS };
+enum {
+    P_GEMM = 0, P_QR, P_QAPPLY, P_CORE, P_POTRF, P_COV, P_COPY, P_OTHER, P_PROJ,
+    // batched DMMA GEMMs by call site (P_GEMM: recompression outputs and the rest)
+    P_GEMM_Y, P_GEMM_TRSM, P_GEMM_SYRK, P_GEMM_DENSE, P_GEMM_GEN,
+    P_NCLASS
+};
 
 cudaEvent_t pool_event(hicma_tlr_ctx *c) {
     if (!c->ev_pool.empty()) {
@@ -284,7 +289,7 @@ int run_core(hicma_tlr_ctx *c, std::vector<CoreTask> &v, int kmax, const CorePar
     return check_launch(c);
 }
 
-int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false) {
+int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false, int cls = 0) {
     if (v.empty()) return 0;
     std::vector<int> off(v.size() + 1);
     off[0] = 0;
@@ -298,7 +303,7 @@ int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false) {
         fl += 2.0 * t.m * (double)t.n * t.k;
         by += 8.0 * ((double)t.m * t.k + (double)t.k * t.n + (t.beta != 0.0 ? 2.0 : 1.0) * t.m * (double)t.n);
     }
-    Prof pf(c, P_GEMM, fl, by);
+    Prof pf(c, cls, fl, by);
     launch_gemm_batched(dt, doff, (int)v.size(), off.back(), c->cur, fp32);
     v.clear();
     return check_launch(c);
@@ -409,6 +414,8 @@ struct RecompTask {
     int rb;
     double *outU, *outV;
     int *rank_dst;
+    // squared Frobenius norms of the A and B factor tiles (device); null: FP64
+    const double *na = nullptr, *nb = nullptr;
 };
 
 // Workspace of one low-rank update (K = rc + ra).
@@ -422,7 +429,7 @@ size_t recomp_ws_bytes(int nb, const RecompTask &t) {
     b += A(ra) + A(K) + A(npa * pb * pb) + A(npk * pb * pb);  // tau, T factors of Wu and Vs
     b += A((size_t)rc * ra) * 2;                         // Pu, Pu2
     b += A((size_t)K * K) * 3;                           // RU, SU, T1
-    if (K > core_smem_kmax()) b += A((size_t)K * K);
+    if (K > core_smem_kmax()) b += A(core_work_doubles(K));
     if (t.Bv) b += A((size_t)t.rb * t.ra);
     return b + 1024;
 }
@@ -453,16 +460,20 @@ int run_core_buckets(hicma_tlr_ctx *c, std::vector<CoreTask> &cores, const CoreP
 // full Householder QR for R_V.  The core M = R_U R_V^T is decomposed and
 // truncated (core kernel), then new U = Cu U_top + Q(Wu) [U_bot; 0] and
 // new V = [Cv, -Y] (R_U^T U_r).
+// thr2 > 0 enables the precision policy: the products forming Y run in FP32
+// for updates whose factor tiles satisfy ||A||_F^2 ||B||_F^2 <= thr2.
 int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, double acc, int maxrank,
-                   int fixed_rank, int *d_rank_task_base, bool fp32) {
+                   int fixed_rank, int *d_rank_task_base, double thr2) {
     if (tasks.empty()) return 0;
     const size_t mark = c->ar->off;
     size_t i0 = 0;
     while (i0 < tasks.size()) {
         c->ar->off = mark;
         std::vector<CopyTask> copies, keeps;
-        std::vector<GemmTask> g1, g2, gU, g3, g4;
+        std::vector<GemmTask> g1, g2, g1s, g2s, gU, g3, g4;
         std::vector<ProjTask> projs;
+        std::vector<SelTask> sels;
+        int *sel = thr2 > 0.0 ? ws_alloc<int>(c, 2 * (tasks.size() - i0) + 2) : nullptr;
         std::vector<QRTask> qrs;
         std::vector<AssembleTask> asm_;
         std::vector<CoreTask> cores;
@@ -491,7 +502,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             double *Pu = ws_alloc<double>(c, (size_t)rc * ra), *Pu2 = ws_alloc<double>(c, (size_t)rc * ra);
             double *RU = ws_alloc<double>(c, (size_t)K * K);
             double *SU = ws_alloc<double>(c, (size_t)K * K), *T1 = ws_alloc<double>(c, (size_t)K * K);
-            double *work = K > core_smem_kmax() ? ws_alloc<double>(c, (size_t)K * K) : nullptr;
+            double *work = K > core_smem_kmax() ? ws_alloc<double>(c, core_work_doubles(K)) : nullptr;
             double *Wu = Us + (size_t)nb * rc;
             double *Yb = Vs + (size_t)nb * rc;
             if (rc > 0) {
@@ -502,8 +513,19 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                 copies.push_back(make_copy(t.Au, nb, Wu, nb, nb, ra));
                 if (t.Bv) {
                     double *P = ws_alloc<double>(c, (size_t)t.rb * ra);
-                    g1.push_back(make_gemm(1, 0, t.rb, ra, nb, 1.0, t.Bv, nb, t.Av, nb, 0.0, P, t.rb));
-                    g2.push_back(make_gemm(0, 0, nb, ra, t.rb, -1.0, t.Bu, nb, P, t.rb, 0.0, Yb, nb));
+                    GemmTask a1 = make_gemm(1, 0, t.rb, ra, nb, 1.0, t.Bv, nb, t.Av, nb, 0.0, P, t.rb);
+                    GemmTask a2 = make_gemm(0, 0, nb, ra, t.rb, -1.0, t.Bu, nb, P, t.rb, 0.0, Yb, nb);
+                    if (sel && t.na && t.nb) {
+                        // both precisions are queued; the selector zeroes one column count
+                        int *s64 = sel + 2 * (i - i0), *s32 = s64 + 1;
+                        sels.push_back(SelTask{t.na, t.nb, s64, s32, ra});
+                        a1.n_dev = s64; a2.n_dev = s64;
+                        g1.push_back(a1); g2.push_back(a2);
+                        a1.n_dev = s32; a2.n_dev = s32;
+                        g1s.push_back(a1); g2s.push_back(a2);
+                    } else {
+                        g1.push_back(a1); g2.push_back(a2);
+                    }
                 } else {
                     g1.push_back(make_gemm(0, 0, nb, ra, nb, -1.0, t.Bu, nb, t.Av, nb, 0.0, Yb, nb));
                 }
@@ -539,8 +561,16 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             g4.push_back(b);
         }
         TRY(run_copies(c, copies));
-        TRY(run_gemms(c, g1, fp32));
-        TRY(run_gemms(c, g2, fp32));
+        if (!sels.empty()) {
+            SelTask *d = stage(c, sels.data(), sels.size());
+            if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+            launch_precision_select(d, (int)sels.size(), thr2, c->d_flags + 4, c->cur);
+            TRY(check_launch(c));
+        }
+        TRY(run_gemms(c, g1, false, P_GEMM_Y));
+        TRY(run_gemms(c, g1s, true, P_GEMM_Y));
+        TRY(run_gemms(c, g2, false, P_GEMM_Y));
+        TRY(run_gemms(c, g2s, true, P_GEMM_Y));
         TRY(run_copies(c, keeps));
         if (!projs.empty()) {
             double fl = 0.0, by = 0.0;
@@ -722,16 +752,47 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     CUDA_TRY(cudaMalloc(&c->d_scal, 64 * sizeof(double)));
     CUDA_TRY(cudaMemset(c->d_flags, 0, 64 * sizeof(int)));
     CUDA_TRY(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+    {
+        // keep freed matrix storage cached in this process's pool (no trimming at
+        // every synchronisation); hicma_tlr_fini returns it
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t thr = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        }
+    }
     *out = c;
     return 0;
 }
 
+// Matrix storage comes from the device's stream-ordered memory pool on the
+// context stream: a request that finishes in a serving process frees without
+// the device-wide synchronisation of cudaFree, and the next request reuses the
+// cached pages.  Both streams of the context are drained first, so the memory
+// is free of pending work on either.
+static cudaError_t dev_alloc(hicma_tlr_ctx *c, void **p, size_t bytes) {
+    cudaError_t e = cudaMallocAsync(p, bytes, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e;
+}
+static void dev_free(hicma_tlr_ctx *c, void *p) {
+    if (!p) return;
+    if (c) {
+        cudaStreamSynchronize(c->stream_hi);
+        cudaStreamSynchronize(c->stream);
+        cudaFreeAsync(p, c->stream);
+    } else {
+        cudaFree(p);
+    }
+}
+
 static void desc_free_device(hicma_tlr_desc *A) {
-    cudaFree(A->d_pts);
-    cudaFree(A->d_band);
-    cudaFree(A->d_lr);
-    cudaFree(A->d_rank);
-    cudaFree(A->d_linv);
+    hicma_tlr_ctx *c = A->ctx;
+    dev_free(c, A->d_pts);
+    dev_free(c, A->d_band);
+    dev_free(c, A->d_lr);
+    dev_free(c, A->d_rank);
+    dev_free(c, A->d_linv);
     A->d_pts = A->d_band = A->d_lr = A->d_linv = nullptr;
     A->d_rank = nullptr;
 }
@@ -752,8 +813,13 @@ int hicma_tlr_fini(hicma_tlr_ctx *c) {
     cudaFree(c->d_flags);
     cudaFree(c->d_scal);
     cudaStreamSynchronize(c->stream_hi);
+    cudaStreamSynchronize(c->stream);
     cudaStreamDestroy(c->stream_hi);
     cudaStreamDestroy(c->stream);
+    {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+    }
     delete c;
     return 0;
 }
@@ -788,12 +854,12 @@ int hicma_tlr_desc_create(hicma_tlr_ctx *c, int N, int NB, int maxrank, int band
     A->nslots = mm > 0 ? mm * (mm + 1) / 2 : 0;
     const size_t band_bytes = (size_t)NT * A->band_alloc * NB * (size_t)NB * sizeof(double);
     const size_t lr_bytes = (size_t)A->nslots * 2 * (size_t)NB * maxrank * sizeof(double);
-    if (cudaMalloc(&A->d_band, band_bytes) != cudaSuccess ||
-        (lr_bytes && cudaMalloc(&A->d_lr, lr_bytes) != cudaSuccess) ||
-        cudaMalloc(&A->d_rank, (size_t)NT * NT * sizeof(int)) != cudaSuccess) {
+    if (dev_alloc(c, (void **)&A->d_band, band_bytes) != cudaSuccess ||
+        (lr_bytes && dev_alloc(c, (void **)&A->d_lr, lr_bytes) != cudaSuccess) ||
+        dev_alloc(c, (void **)&A->d_rank, (size_t)NT * NT * sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         set_err("descriptor allocation failed (band %zu B, low-rank slots %zu B)", band_bytes, lr_bytes);
-        cudaFree(A->d_band); cudaFree(A->d_lr); cudaFree(A->d_rank);
+        dev_free(c, A->d_band); dev_free(c, A->d_lr); dev_free(c, A->d_rank);
         delete A;
         return HICMA_TLR_ERR_OOM;
     }
@@ -848,15 +914,15 @@ int hicma_tlr_desc_copy(hicma_tlr_ctx *c, const hicma_tlr_desc *src, hicma_tlr_d
     dst->factored = src->factored;
     if (src->d_pts) {
         if (!dst->d_pts || dst->ndim != src->ndim) {
-            cudaFree(dst->d_pts);
-            CUDA_TRY(cudaMalloc(&dst->d_pts, (size_t)src->ndim * src->N * sizeof(double)));
+            dev_free(c, dst->d_pts);
+            CUDA_TRY(dev_alloc(c, (void **)&dst->d_pts, (size_t)src->ndim * src->N * sizeof(double)));
         }
         dst->ndim = src->ndim;
         CUDA_TRY(cudaMemcpyAsync(dst->d_pts, src->d_pts, (size_t)src->ndim * src->N * sizeof(double),
                                  cudaMemcpyDeviceToDevice, c->stream));
     }
     if (src->factored && src->d_linv) {
-        if (!dst->d_linv) CUDA_TRY(cudaMalloc(&dst->d_linv, NT * NB * NB * sizeof(double)));
+        if (!dst->d_linv) CUDA_TRY(dev_alloc(c, (void **)&dst->d_linv, NT * NB * NB * sizeof(double)));
         CUDA_TRY(cudaMemcpyAsync(dst->d_linv, src->d_linv, NT * NB * NB * sizeof(double),
                                  cudaMemcpyDeviceToDevice, c->stream));
     }
@@ -873,9 +939,9 @@ static int set_points(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_probl
         points = h.data();
     }
     if (!A->d_pts || A->ndim != ndim) {
-        cudaFree(A->d_pts);
+        dev_free(c, A->d_pts);
         A->d_pts = nullptr;
-        CUDA_TRY(cudaMalloc(&A->d_pts, (size_t)ndim * A->N * sizeof(double)));
+        CUDA_TRY(dev_alloc(c, (void **)&A->d_pts, (size_t)ndim * A->N * sizeof(double)));
     }
     A->ndim = ndim;
     CUDA_TRY(cudaMemcpyAsync(A->d_pts, points, (size_t)ndim * A->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -919,7 +985,7 @@ static size_t compress_ws_bytes(int nb, int s) {
     b += align_up(sizeof(double) * (size_t)s + 1) * 2;
     b += align_up(sizeof(double) * npan * pb * pb + 1) * 2;
     b += align_up(sizeof(double) * (size_t)s * s + 1);
-    if (s > core_smem_kmax()) b += align_up(sizeof(double) * (size_t)s * s + 1);
+    if (s > core_smem_kmax()) b += align_up(sizeof(double) * core_work_doubles(s) + 1);
     return b + 1024;
 }
 
@@ -950,7 +1016,7 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
             double *tauY = ws_alloc<double>(c, s), *tauW = ws_alloc<double>(c, s);
             double *TY = ws_alloc<double>(c, npan * pb * pb), *TW = ws_alloc<double>(c, npan * pb * pb);
             double *SU = ws_alloc<double>(c, (size_t)s * s);
-            double *work = s > core_smem_kmax() ? ws_alloc<double>(c, (size_t)s * s) : nullptr;
+            double *work = s > core_smem_kmax() ? ws_alloc<double>(c, core_work_doubles(s)) : nullptr;
             int *rt = d_rank_task_base + (i - i0);
             gy.push_back(make_gemm(0, 0, nb, s, nb, 1.0, t.A, nb, Omega, nb, 0.0, Y, nb));
             qy.push_back(QRTask{Y, tauY, TY, nb, s, nb});
@@ -969,16 +1035,16 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
             g.n_dev = rt;
             gv.push_back(g);
         }
-        TRY(run_gemms(c, gy));
+        TRY(run_gemms(c, gy, false, P_GEMM_GEN));
         TRY(run_qr(c, qy, nb));
         TRY(run_qapply(c, aq, nb));
-        TRY(run_gemms(c, gw));
+        TRY(run_gemms(c, gw, false, P_GEMM_GEN));
         TRY(run_copies(c, keeps));
         TRY(run_qr(c, qw, nb));
         CoreParams cp{1, tol, maxrank, 0, nb, nullptr, nullptr};
         TRY(run_core_buckets(c, cores, cp));
         TRY(run_qapply(c, au, nb));
-        TRY(run_gemms(c, gv));
+        TRY(run_gemms(c, gv, false, P_GEMM_GEN));
         i0 = i;
     }
     c->ar->off = mark;
@@ -1142,10 +1208,10 @@ int hicma_tlr_band_regenerate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, con
     band_size = std::min(band_size, NT);
     TRY(ctx_sync(c));
     if (band_size > A->band_alloc) {
-        cudaFree(A->d_band);
+        dev_free(c, A->d_band);
         A->d_band = nullptr;
         const size_t bytes = (size_t)NT * band_size * NB * (size_t)NB * sizeof(double);
-        if (cudaMalloc(&A->d_band, bytes) != cudaSuccess) {
+        if (dev_alloc(c, (void **)&A->d_band, bytes) != cudaSuccess) {
             cudaGetLastError();
             set_err("band allocation of %zu bytes failed", bytes);
             return HICMA_TLR_ERR_OOM;
@@ -1181,7 +1247,7 @@ static int run_syrk(hicma_tlr_ctx *c, hicma_tlr_desc *A, int k, const std::vecto
         double *W = ws_alloc<double>(c, (size_t)r * r);
         double *X = ws_alloc<double>(c, (size_t)NB * r);
         if (!W || !X) {
-            TRY(run_gemms(c, g1)); TRY(run_gemms(c, g2)); TRY(run_gemms(c, g3));
+            TRY(run_gemms(c, g1, false, P_GEMM_SYRK)); TRY(run_gemms(c, g2, false, P_GEMM_SYRK)); TRY(run_gemms(c, g3, false, P_GEMM_SYRK));
             c->ar->off = mark;
             W = ws_alloc<double>(c, (size_t)r * r);
             X = ws_alloc<double>(c, (size_t)NB * r);
@@ -1191,9 +1257,9 @@ static int run_syrk(hicma_tlr_ctx *c, hicma_tlr_desc *A, int k, const std::vecto
         g2.push_back(make_gemm(0, 0, NB, r, r, 1.0, A->U(m, k), NB, W, r, 0.0, X, NB));
         g3.push_back(make_gemm(0, 1, NB, NB, r, -1.0, X, NB, A->U(m, k), NB, 1.0, A->dense(m, m), NB));
     }
-    TRY(run_gemms(c, g1));
-    TRY(run_gemms(c, g2));
-    TRY(run_gemms(c, g3));
+    TRY(run_gemms(c, g1, false, P_GEMM_SYRK));
+    TRY(run_gemms(c, g2, false, P_GEMM_SYRK));
+    TRY(run_gemms(c, g3, false, P_GEMM_SYRK));
     c->ar->off = mark;
     return 0;
 }
@@ -1239,11 +1305,11 @@ static int run_syrk_lazy(hicma_tlr_ctx *c, hicma_tlr_desc *A, int m) {
             cp.push_back(make_copy(A->U(m, j), NB, Uc + off * NB, NB, NB, r));
             off += r;
         }
-        TRY(run_gemms(c, g1));
-        TRY(run_gemms(c, g2));
+        TRY(run_gemms(c, g1, false, P_GEMM_SYRK));
+        TRY(run_gemms(c, g2, false, P_GEMM_SYRK));
         TRY(run_copies(c, cp));
         std::vector<GemmTask> g3{make_gemm(0, 1, NB, NB, (int)sumr, -1.0, Yc, NB, Uc, NB, 1.0, A->dense(m, m), NB, 1)};
-        TRY(run_gemms(c, g3));
+        TRY(run_gemms(c, g3, false, P_GEMM_SYRK));
         p = q;
     }
     c->ar->off = mark;
@@ -1266,7 +1332,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     const int NT = A->NT, NB = A->NB, band = A->band;
     const bool mixed = c->precision == HICMA_TLR_PREC_MIXED;
     if (!A->d_linv) {
-        if (cudaMalloc(&A->d_linv, (size_t)NT * NB * NB * sizeof(double)) != cudaSuccess) {
+        if (dev_alloc(c, (void **)&A->d_linv, (size_t)NT * NB * NB * sizeof(double)) != cudaSuccess) {
             cudaGetLastError();
             set_err("allocation of the diagonal inverses failed");
             return HICMA_TLR_ERR_OOM;
@@ -1276,11 +1342,18 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     c->ar = &c->main_ar;
     c->main_ar.off = 0;
     c->hi_ar.off = 0;
-    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 4 * sizeof(int), c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 5 * sizeof(int), c->stream));
     TRY(ctx_sync(c));
     int *d_info = c->d_flags;
     int *rtask = ws_alloc<int>(c, (size_t)NT * NT + 16);
     if (!rtask) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
+    // precision policy: squared Frobenius norms of the low-rank tiles of the
+    // current panel column, and the product-norm bound under which the FP32
+    // rounding of a product (about sqrt(NB) 2^-24 ||A|| ||B||) stays below acc/100
+    double *d_fro2 = mixed ? ws_alloc<double>(c, (size_t)NT + 16) : nullptr;
+    if (mixed && !d_fro2) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
+    const double thr = 0.01 * acc / (std::sqrt((double)NB) * 5.9604644775390625e-8);
+    const double thr2 = mixed ? thr * thr : 0.0;
     const size_t base_mark = c->ar->off;
     std::vector<unsigned long> tops((size_t)NT * NT, 0);
     unsigned long op_total = 0;
@@ -1330,7 +1403,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                 if (r == 0) continue;
                 double *tmp = ws_alloc<double>(c, (size_t)NB * r);
                 if (!tmp) {
-                    TRY(run_gemms(c, g)); TRY(run_copies(c, cp));
+                    TRY(run_gemms(c, g, false, P_GEMM_TRSM)); TRY(run_copies(c, cp));
                     c->ar->off = base_mark;
                     tmp = ws_alloc<double>(c, (size_t)NB * r);
                     if (!tmp) { set_err("workspace too small (trsm)"); return HICMA_TLR_ERR_OOM; }
@@ -1343,8 +1416,19 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                     cp.push_back(make_copy(tmp, NB, A->V(m, k), NB, NB, r));
                 }
             }
-            TRY(run_gemms(c, g));
+            TRY(run_gemms(c, g, false, P_GEMM_TRSM));
             TRY(run_copies(c, cp));
+            if (mixed) {
+                std::vector<NormTask> nt;
+                for (int m = k + 1; m < NT; ++m)
+                    if (!A->is_dense(m, k)) nt.push_back(NormTask{A->V(m, k), NB, A->rank(m, k), NB, d_fro2 + m});
+                if (!nt.empty()) {
+                    NormTask *d = stage(c, nt.data(), nt.size());
+                    if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+                    launch_sumsq_batched(d, (int)nt.size(), c->stream);
+                    TRY(check_launch(c));
+                }
+            }
         }
         CUDA_TRY(cudaEventRecord(ev[T1], c->stream));
         CUDA_TRY(cudaEventRecord(evT, c->stream));
@@ -1394,7 +1478,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                         if (ra == 0) continue;
                         double *tmp = ws_alloc<double>(c, (size_t)ra * NB);
                         if (!tmp) {
-                            TRY(run_gemms(c, g1)); TRY(run_gemms(c, g2)); TRY(run_gemms(c, g3));
+                            TRY(run_gemms(c, g1, false, P_GEMM_DENSE)); TRY(run_gemms(c, g2, false, P_GEMM_DENSE)); TRY(run_gemms(c, g3, false, P_GEMM_DENSE));
                             c->ar->off = base_mark;
                             tmp = ws_alloc<double>(c, (size_t)ra * NB);
                             if (!tmp) { set_err("workspace too small (gemm)"); return HICMA_TLR_ERR_OOM; }
@@ -1408,7 +1492,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                         double *rr = ws_alloc<double>(c, (size_t)ra * rb);
                         double *tmp = ws_alloc<double>(c, (size_t)NB * std::max(ra, rb));
                         if (!rr || !tmp) {
-                            TRY(run_gemms(c, g1)); TRY(run_gemms(c, g2)); TRY(run_gemms(c, g3));
+                            TRY(run_gemms(c, g1, false, P_GEMM_DENSE)); TRY(run_gemms(c, g2, false, P_GEMM_DENSE)); TRY(run_gemms(c, g3, false, P_GEMM_DENSE));
                             c->ar->off = base_mark;
                             rr = ws_alloc<double>(c, (size_t)ra * rb);
                             tmp = ws_alloc<double>(c, (size_t)NB * std::max(ra, rb));
@@ -1434,17 +1518,18 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                         if (ra == 0 || rb == 0) continue;
                         rec.push_back(RecompTask{A->U(m, n), A->V(m, n), rc, A->U(m, k), A->V(m, k), ra,
                                                  A->U(n, k), A->V(n, k), rb, A->U(m, n), A->V(m, n),
-                                                 A->d_rank + (size_t)n * NT + m});
+                                                 A->d_rank + (size_t)n * NT + m,
+                                                 mixed ? d_fro2 + m : nullptr, mixed ? d_fro2 + n : nullptr});
                         rec_meta.push_back({m, n, ra, rb, rc});
                         rec_case.push_back(0);
                     }
                 }
             }
-            TRY(run_gemms(c, g1));
-            TRY(run_gemms(c, g2));
-            TRY(run_gemms(c, g3));
+            TRY(run_gemms(c, g1, false, P_GEMM_DENSE));
+            TRY(run_gemms(c, g2, false, P_GEMM_DENSE));
+            TRY(run_gemms(c, g3, false, P_GEMM_DENSE));
             c->ar->off = base_mark;
-            TRY(run_recompress(c, NB, rec, acc, maxrank, fixed_rank, rtask, mixed));
+            TRY(run_recompress(c, NB, rec, acc, maxrank, fixed_rank, rtask, thr2));
             CUDA_TRY(cudaEventRecord(ev[G1], c->stream));
         }
         // ---- panel end: info, ranks, timings
@@ -1483,8 +1568,8 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     cudaEventDestroy(evP);
     cudaEventDestroy(evT);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-    int flags_h[4] = {0, 0, 0, 0};
-    CUDA_TRY(cudaMemcpy(flags_h, c->d_flags, 4 * sizeof(int), cudaMemcpyDeviceToHost));
+    int flags_h[5] = {0, 0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpy(flags_h, c->d_flags, 5 * sizeof(int), cudaMemcpyDeviceToHost));
     if (flags_h[3]) {
         cudaMemset(c->d_flags + 3, 0, sizeof(int));
         set_err("a bounded device wait gave up (tile POTRF task queue)");
@@ -1492,6 +1577,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     }
     const int overflow = flags_h[1];
     A->stats[8] = flags_h[2];
+    A->stats[9] = flags_h[4];
     if (tileops)
         for (size_t i = 0; i < tops.size(); ++i) tileops[i] += tops[i];
     if (opcounters) opcounters[0] += op_total;
@@ -1964,7 +2050,7 @@ int hicma_tlr_k_lr_update(hicma_tlr_ctx *c, int nb, const double *d_Au, const do
     if (!d_r) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
     std::vector<RecompTask> v{RecompTask{d_Cu, d_Cv, *rc, d_Au, d_Av, ra, d_Bu, d_Bv, rb, d_Cu, d_Cv, d_r}};
     CUDA_TRY(cudaMemsetAsync(c->d_flags + 1, 0, sizeof(int), c->stream));
-    TRY(run_recompress(c, nb, v, acc, maxrank, fixed_rank, d_r + 1, c->precision == HICMA_TLR_PREC_MIXED));
+    TRY(run_recompress(c, nb, v, acc, maxrank, fixed_rank, d_r + 1, 0.0));
     int r = 0;
     CUDA_TRY(cudaMemcpyAsync(&r, d_r, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     TRY(ctx_sync(c));

@@ -100,6 +100,24 @@ struct ProjTask {
 };
 void launch_bcgs2(const ProjTask *d_tasks, int ntasks, cudaStream_t st);
 
+// ------------------------------------------------------ precision policy ---
+// out = sum of squares of X (rows x cols, ld): one CTA per task.
+struct NormTask {
+    const double *X;
+    int rows, cols, ld;
+    double *out;
+};
+void launch_sumsq_batched(const NormTask *d_tasks, int ntasks, cudaStream_t st);
+// Per recompression: its products run in FP32 when na * nb <= thr2 (squared
+// Frobenius norms of the two factor tiles); sel32 / sel64 receive n or 0 and
+// serve as the device-side column counts of the two launches.
+struct SelTask {
+    const double *na, *nb;
+    int *sel64, *sel32;
+    int n;
+};
+void launch_precision_select(const SelTask *d_tasks, int ntasks, double thr2, int *count, cudaStream_t st);
+
 // ---------------------------------------------------------------- POTRF -----
 // Tile Cholesky (+ inverse when X is given, X zeroed by the caller) in one
 // persistent launch of `grid` CTAs; n <= potrf_tile_max_n().  cnt: scratch of
@@ -152,7 +170,7 @@ struct CoreTask {
     const double *RV;    // K x K upper (ld ldrv)
     double *SU;          // out: K x K, left singular vectors sorted by decreasing sigma
     double *RUc;         // out (if RU): clean copy of RU, K x K, zeros below the diagonal
-    double *work;        // K*K doubles when K > core_smem_kmax()
+    double *work;        // core_work_doubles(K) doubles when K > core_smem_kmax()
     int *rank_out;       // rank map entry (may be null)
     int *rank_task;      // per-task rank for the apply steps
     int K, ldru, ldrv;
@@ -167,6 +185,8 @@ struct CoreParams {
     int *sweeps;         // device counter of Jacobi sweeps (diagnostics, may be null)
 };
 int core_smem_kmax();
+// Global scratch (doubles) of one core with K > core_smem_kmax().
+size_t core_work_doubles(int K);
 // All tasks of one launch should have K <= kmax; shared memory is sized from kmax.
 void launch_core_svd_batched(const CoreTask *d_tasks, int ntasks, int kmax, const CoreParams &p,
                              cudaStream_t st);

@@ -184,7 +184,8 @@ int hicma_tlr_loglik(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, const double *y, dou
 /* Statistics of the last factorization on A: [0] seconds, [1] TLR flops
  * (op_counts model), [2] recompressions capped at maxrank, [3] number of
  * launches of library kernels, [4] POTRF s, [5] TRSM s, [6] SYRK s,
- * [7] GEMM/recompression s, [8] Jacobi sweeps summed over all cores.
+ * [7] GEMM/recompression s, [8] Jacobi sweeps summed over all cores, [9] recompressions
+ * whose products ran in FP32 under HICMA_TLR_PREC_MIXED.
  * nstats <= 12. */
 int hicma_tlr_last_stats(hicma_tlr_desc *A, double *stats, int nstats);
 
@@ -199,7 +200,9 @@ int hicma_tlr_check(hicma_tlr_ctx *ctx, hicma_tlr_desc *L, const hicma_tlr_probl
 
 /* Per-kernel-class device timing (CUDA events around launches on the context
  * stream).  Classes: 0 GEMM, 1 QR, 2 Q-apply, 3 core SVD, 4 tile POTRF,
- * 5 covariance generation, 6 copies, 7 other, 8 Gram-Schmidt projections.
+ * 5 covariance generation, 6 copies, 7 other, 8 Gram-Schmidt projections, then the batched
+ * GEMMs by call site: 0 recompression outputs and the rest, 9 recompression products (Y),
+ * 10 TRSM, 11 SYRK, 12 dense band cases, 13 generation.
  * out[4*k + j]: j = 0 launches,
  * 1 seconds, 2 algorithmic flops, 3 algorithmic bytes.  Enabling resets. */
 int hicma_tlr_prof_enable(hicma_tlr_ctx *ctx, int on);

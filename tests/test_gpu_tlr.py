@@ -140,3 +140,27 @@ def test_argument_errors(ctx):
     with pytest.raises(tlr.TLRError) as e:
         tlr.HiCMA_dpotrf_L(ctx, tlr.LOWER, A, TOL, 0, NB)     # maxrank > NB/2
     assert e.value.code == tlr.ERR_ARG
+
+
+def test_mixed_precision_policy(ctx):
+    """FP32 products for small-norm updates: same residual bound and a log
+    determinant within 1e-8 of the plain FP64 factorization; the products of
+    at least one update (far-apart tiles) ran in FP32."""
+    from hicma_parsec_b200 import tlr
+    A, _, prob = _gpu_run(ctx, dict(kind=2, noise=1e-4))
+    B = tlr.TLRMatrix(ctx, N, NB, MAXRANK, 1)
+    B.copy_from(A)
+    assert A.potrf(TOL, MAXRANK) == 0
+    ld64 = A.logdet()
+    ctx.set_precision(tlr.PREC_MIXED)
+    try:
+        assert B.potrf(TOL, MAXRANK) == 0
+    finally:
+        ctx.set_precision(tlr.PREC_FP64)
+    st = B.stats()
+    assert st[9] >= 1
+    ldm = B.logdet()
+    assert abs(ldm - ld64) <= 1e-8 * abs(ld64)
+    oprob = O.Problem(kind=2, noise=1e-4)
+    res = O.check_dpotrf2(B.uncompress(), O.dense_matrix(oprob, O.gen_points(N, 2)))
+    assert res <= 10 * TOL, res
