@@ -6,7 +6,8 @@
 // (hicma_parsec/HiCMA_dpotrf_L_2flow.jdf:704-708,717-728,745-778) and the
 // products inside HCORE (low-rank SYRK/GEMM, QR/SVD recompression).
 //
-// CTA tile 64 x 64 x 16, 4 warps (2 x 2, 32 x 32 each = 4 x 4 DMMA tiles),
+// CTA tile 64 x 64 x 16 (or 128 x 32 x 16 for outputs a rank wide), 4 warps
+// (2 x 2 or 4 x 1, 32 x 32 each = 4 x 4 DMMA tiles),
 // operands staged in shared memory by cp.async (2 stages, zero-filled at the
 // edges).  op(A)/op(B) transposes are handled by the load mapping so every
 // global load walks the contiguous dimension.  A batch is a list of tasks
@@ -35,19 +36,21 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+template <int BM_, int BN_>
 struct Smem {
-    double A[2][BK][BM + PAD];
-    double B[2][BK][BN + PAD];
+    double A[2][BK][BM_ + PAD];
+    double B[2][BK][BN_ + PAD];
 };
 
-__device__ __forceinline__ void load_stage(Smem &sm, int s, const GemmTask &t, int i0, int j0,
+template <int BM_, int BN_>
+__device__ __forceinline__ void load_stage(Smem<BM_, BN_> &sm, int s, const GemmTask &t, int i0, int j0,
                                            int k0) {
     const int tid = threadIdx.x;
 #pragma unroll
-    for (int q = 0; q < (BM * BK) / NT; ++q) {
+    for (int q = 0; q < (BM_ * BK) / NT; ++q) {
         const int e = tid + q * NT;
         int i, kk;
-        if (t.opA == 0) { i = e & (BM - 1); kk = e / BM; }
+        if (t.opA == 0) { i = e & (BM_ - 1); kk = e / BM_; }
         else            { kk = e & (BK - 1); i = e / BK; }
         const int gi = i0 + i, gk = k0 + kk;
         const bool p = gi < t.m && gk < t.k;
@@ -56,11 +59,11 @@ __device__ __forceinline__ void load_stage(Smem &sm, int s, const GemmTask &t, i
         cp_async8(&sm.A[s][kk][i], src, p);
     }
 #pragma unroll
-    for (int q = 0; q < (BN * BK) / NT; ++q) {
+    for (int q = 0; q < (BN_ * BK) / NT; ++q) {
         const int e = tid + q * NT;
         int j, kk;
         if (t.opB == 0) { kk = e & (BK - 1); j = e / BK; }
-        else            { j = e & (BN - 1); kk = e / BN; }
+        else            { j = e & (BN_ - 1); kk = e / BN_; }
         const int gj = j0 + j, gk = k0 + kk;
         const bool p = gj < t.n && gk < t.k;
         const double *src = t.B;
@@ -70,9 +73,13 @@ __device__ __forceinline__ void load_stage(Smem &sm, int s, const GemmTask &t, i
     cp_async_commit();
 }
 
-__device__ __forceinline__ void gemm_tile(Smem &sm, GemmTask t, int tm, int tn) {
-    const int i0 = tm * BM, j0 = tn * BN;
-    if (t.lower && j0 >= i0 + BM) return;
+// One BM_ x BN_ output tile; four warps of 32 x 32 (2 x 2 for 64 x 64,
+// 4 x 1 for the narrow 128 x 32 tile used when n is a rank).
+template <int BM_, int BN_>
+__device__ __forceinline__ void gemm_tile(Smem<BM_, BN_> &sm, GemmTask t, int tm, int tn) {
+    constexpr int WM = BM_ / 32;
+    const int i0 = tm * BM_, j0 = tn * BN_;
+    if (t.lower && j0 >= i0 + BM_) return;
     if (t.n_dev) {
         const int nd = *t.n_dev;
         t.n = nd < t.n ? nd : t.n;
@@ -80,7 +87,7 @@ __device__ __forceinline__ void gemm_tile(Smem &sm, GemmTask t, int tm, int tn) 
     if (j0 >= t.n) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, tig = lane & 3;
-    const int wm = warp & 1, wn = warp >> 1;
+    const int wm = warp % WM, wn = warp / WM;
 
     double acc[4][4][2];
 #pragma unroll
@@ -89,11 +96,11 @@ __device__ __forceinline__ void gemm_tile(Smem &sm, GemmTask t, int tm, int tn) 
         for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
 
     const int ktiles = (t.k + BK - 1) / BK;
-    if (ktiles > 0) load_stage(sm, 0, t, i0, j0, 0);
+    if (ktiles > 0) load_stage<BM_, BN_>(sm, 0, t, i0, j0, 0);
     for (int kt = 0; kt < ktiles; ++kt) {
         const int s = kt & 1;
         if (kt + 1 < ktiles) {
-            load_stage(sm, s ^ 1, t, i0, j0, (kt + 1) * BK);
+            load_stage<BM_, BN_>(sm, s ^ 1, t, i0, j0, (kt + 1) * BK);
             cp_async_wait<1>();
         } else {
             cp_async_wait<0>();
@@ -134,9 +141,10 @@ __device__ __forceinline__ void gemm_tile(Smem &sm, GemmTask t, int tm, int tn) 
     }
 }
 
-__global__ void __launch_bounds__(NT) k_gemm_batched(const GemmTask *__restrict__ tasks,
+template <int BM_, int BN_>
+__global__ void __launch_bounds__(NT, 3) k_gemm_batched(const GemmTask *__restrict__ tasks,
                                                      const int *__restrict__ tile_off, int ntasks) {
-    __shared__ __align__(16) Smem sm;
+    __shared__ __align__(16) Smem<BM_, BN_> sm;
     const int bid = blockIdx.x;
     int lo = 0, hi = ntasks - 1;
     while (lo < hi) {
@@ -145,12 +153,12 @@ __global__ void __launch_bounds__(NT) k_gemm_batched(const GemmTask *__restrict_
     }
     const GemmTask t = tasks[lo];
     const int local = bid - tile_off[lo];
-    gemm_tile(sm, t, local % t.tiles_m, local / t.tiles_m);
+    gemm_tile<BM_, BN_>(sm, t, local % t.tiles_m, local / t.tiles_m);
 }
 
 __global__ void __launch_bounds__(NT) k_gemm_single(GemmTask t) {
-    __shared__ __align__(16) Smem sm;
-    gemm_tile(sm, t, blockIdx.x, blockIdx.y);
+    __shared__ __align__(16) Smem<BM, BN> sm;
+    gemm_tile<BM, BN>(sm, t, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -233,7 +241,13 @@ void launch_gemm_batched(const GemmTask *d_tasks, const int *d_tile_off, int nta
     if (fp32)
         k_sgemm_batched<<<total_tiles, 256, 0, st>>>(d_tasks, d_tile_off, ntasks);
     else
-        k_gemm_batched<<<total_tiles, NT, 0, st>>>(d_tasks, d_tile_off, ntasks);
+        k_gemm_batched<BM, BN><<<total_tiles, NT, 0, st>>>(d_tasks, d_tile_off, ntasks);
+}
+
+void launch_gemm_batched_narrow(const GemmTask *d_tasks, const int *d_tile_off, int ntasks, int total_tiles,
+                                cudaStream_t st) {
+    if (ntasks <= 0 || total_tiles <= 0) return;
+    k_gemm_batched<GEMM_NARROW_M, GEMM_NARROW_N><<<total_tiles, NT, 0, st>>>(d_tasks, d_tile_off, ntasks);
 }
 
 void launch_gemm_single(const GemmTask &t, cudaStream_t st) {

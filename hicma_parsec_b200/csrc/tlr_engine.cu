@@ -289,8 +289,20 @@ int run_core(hicma_tlr_ctx *c, std::vector<CoreTask> &v, int kmax, const CorePar
     return check_launch(c);
 }
 
+int run_gemms_narrow(hicma_tlr_ctx *c, std::vector<GemmTask> &v, int cls);
+
 int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false, int cls = 0) {
     if (v.empty()) return 0;
+    if (!fp32) {
+        // outputs a rank wide go to the 128 x 32 tile variant
+        std::vector<GemmTask> narrow, wide;
+        for (auto &t : v) ((t.n <= GEMM_NARROW_N || t.n_dev) && !t.lower ? narrow : wide).push_back(t);
+        if (!narrow.empty()) {
+            TRY(run_gemms_narrow(c, narrow, cls));
+            if (wide.empty()) { v.clear(); return 0; }
+            v.swap(wide);
+        }
+    }
     std::vector<int> off(v.size() + 1);
     off[0] = 0;
     for (size_t i = 0; i < v.size(); ++i) off[i + 1] = off[i] + gemm_tiles(v[i]);
@@ -305,6 +317,29 @@ int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false, int
     }
     Prof pf(c, cls, fl, by);
     launch_gemm_batched(dt, doff, (int)v.size(), off.back(), c->cur, fp32);
+    v.clear();
+    return check_launch(c);
+}
+
+int run_gemms_narrow(hicma_tlr_ctx *c, std::vector<GemmTask> &v, int cls) {
+    std::vector<int> off(v.size() + 1);
+    off[0] = 0;
+    for (size_t i = 0; i < v.size(); ++i) {
+        GemmTask &t = v[i];
+        t.tiles_m = (t.m + GEMM_NARROW_M - 1) / GEMM_NARROW_M;
+        off[i + 1] = off[i] + t.tiles_m * ((t.n + GEMM_NARROW_N - 1) / GEMM_NARROW_N);
+    }
+    if (off.back() == 0) { v.clear(); return 0; }
+    GemmTask *dt = stage(c, v.data(), v.size());
+    int *doff = stage(c, off.data(), off.size());
+    if (!dt || !doff) { set_err("task staging failed"); return HICMA_TLR_ERR_CUDA; }
+    double fl = 0, by = 0;
+    for (auto &t : v) {
+        fl += 2.0 * t.m * (double)t.n * t.k;
+        by += 8.0 * ((double)t.m * t.k + (double)t.k * t.n + (t.beta != 0.0 ? 2.0 : 1.0) * t.m * (double)t.n);
+    }
+    Prof pf(c, cls, fl, by);
+    launch_gemm_batched_narrow(dt, doff, (int)v.size(), off.back(), c->cur);
     v.clear();
     return check_launch(c);
 }

@@ -31,6 +31,11 @@ struct GemmTask {
 void launch_gemm_batched(const GemmTask *d_tasks, const int *d_tile_off, int ntasks,
                          int total_tiles, cudaStream_t st, bool fp32 = false);
 void launch_gemm_single(const GemmTask &t, cudaStream_t st);
+// FP64 variant with 128 x 32 output tiles for outputs a rank wide (n <= 32, or
+// n capped on the device by n_dev); tiles_m of its tasks must be ceil(m / 128).
+constexpr int GEMM_NARROW_M = 128, GEMM_NARROW_N = 32;
+void launch_gemm_batched_narrow(const GemmTask *d_tasks, const int *d_tile_off, int ntasks, int total_tiles,
+                                cudaStream_t st);
 
 inline int gemm_tiles_m(int m) { return (m + 63) / 64; }
 inline int gemm_tiles(const GemmTask &t) { return gemm_tiles_m(t.m) * gemm_tiles_m(t.n); }
