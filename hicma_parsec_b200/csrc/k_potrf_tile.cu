@@ -4,7 +4,8 @@
 // :233-242) together with the inverse L^-1 that the panel solves of this
 // engine apply as a GEMM.  The tile is split into 64 x 64 blocks and the
 // blocked right-looking algorithm becomes a list of block tasks:
-//   DIAG(j)      Cholesky of A_jj and D_j = L_jj^-1 (one CTA, shared memory)
+//   DIAG(j)      Cholesky of A_jj and D_j = L_jj^-1 (one CTA, shared memory,
+//                8-column panels factored by one warp)
 //   PANEL(j,i)   L_ij = A_ij D_j^T
 //   UPD(j,i,k)   A_ik -= L_ij L_kj^T                       (j < k <= i)
 //   XDIAG(j,k)   X_jk = D_j B_jk                           (k < j)
@@ -156,31 +157,43 @@ __device__ bool diag_block(double *sm, double *Ajj, int lda, int jb, double *Dj,
         S[c * LDS + r] = __ldcg(Ajj + r + (size_t)c * lda);
     }
     __syncthreads();
-    // right-looking column Cholesky; the scaling of column c is deferred to
-    // step c + 1 so each step needs two barriers
-    for (int c = 0; c < jb; ++c) {
-        if (tid == 0) {
-            const double d = S[c * LDS + c];
-            if (!(d > 0.0)) {
-                fail = 1;
-                if (info) atomicCAS(info, 0, info_col0 + c + 1);
-            } else {
-                const double p = sqrt(d);
-                S[c * LDS + c] = p;
-                invd[c] = 1.0 / p;
+    // blocked right-looking Cholesky: warp 0 factors each 8-column panel with
+    // warp-level synchronisation only, then all threads apply the panel's
+    // rank-8 update to the trailing block (two CTA barriers per panel)
+    for (int p0 = 0; p0 < jb; p0 += 8) {
+        const int pe = min(jb, p0 + 8);
+        if (tid < 32) {
+            const int lane = tid;
+            for (int c = p0; c < pe; ++c) {
+                const double d = S[c * LDS + c];
+                if (!(d > 0.0)) {
+                    if (lane == 0) {
+                        fail = 1;
+                        if (info) atomicCAS(info, 0, info_col0 + c + 1);
+                    }
+                    break;
+                }
+                const double piv = sqrt(d), inv = 1.0 / piv;
+                __syncwarp();
+                if (lane == 0) { S[c * LDS + c] = piv; invd[c] = inv; }
+                for (int r = c + 1 + lane; r < jb; r += 32) S[c * LDS + r] *= inv;
+                __syncwarp();
+                for (int cc = c + 1; cc < pe; ++cc) {
+                    const double lc = S[c * LDS + cc];
+                    for (int r = cc + lane; r < jb; r += 32) S[cc * LDS + r] -= S[c * LDS + r] * lc;
+                }
+                __syncwarp();
             }
         }
         __syncthreads();
         if (fail) return false;
-        const double inv = invd[c], inv2 = inv * inv;
-        const int w = jb - c - 1;
+        const int w = jb - pe;
         for (int idx = tid; idx < w * w; idx += NTH) {
-            const int cc = c + 1 + idx / w, r = c + 1 + idx % w;
-            if (r >= cc) S[cc * LDS + r] -= S[c * LDS + r] * S[c * LDS + cc] * inv2;
-        }
-        if (c > 0) {
-            const double ip = invd[c - 1];
-            for (int r = c + tid; r < jb; r += NTH) S[(c - 1) * LDS + r] *= ip;
+            const int cc = pe + idx / w, r = pe + idx % w;
+            if (r < cc) continue;
+            double acc = S[cc * LDS + r];
+            for (int l = p0; l < pe; ++l) acc -= S[l * LDS + r] * S[l * LDS + cc];
+            S[cc * LDS + r] = acc;
         }
         __syncthreads();
     }

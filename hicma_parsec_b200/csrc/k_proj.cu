@@ -140,7 +140,27 @@ __global__ void __launch_bounds__(PT, 2) k_bcgs2(const ProjTask *__restrict__ ta
     for (int idx = threadIdx.x; idx < t.rc * t.ra; idx += PT) t.P[idx] += t.P2[idx];
 }
 
+// P = C^T W for a batch (the inner product B_V^T A_V of a recompression):
+// the split-K DMMA reduction of the projection, one CTA per product.
+__global__ void __launch_bounds__(PT, 2) k_gram_batched(const GramTask *__restrict__ tasks) {
+    extern __shared__ double red[];
+    const GramTask t = tasks[blockIdx.x];
+    if (t.rc <= 0 || t.ra <= 0) return;
+    proj_gram(t.C, t.W, t.P, t.nb, t.rc, t.ra, red);
+}
+
 }  // namespace
+
+void launch_gram_batched(const GramTask *d_tasks, int ntasks, cudaStream_t st) {
+    if (ntasks <= 0) return;
+    const int smem = PW * PB * PB * (int)sizeof(double);
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(k_gram_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        configured = true;
+    }
+    k_gram_batched<<<ntasks, PT, smem, st>>>(d_tasks);
+}
 
 void launch_bcgs2(const ProjTask *d_tasks, int ntasks, cudaStream_t st) {
     if (ntasks <= 0) return;

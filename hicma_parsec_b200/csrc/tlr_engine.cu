@@ -508,6 +508,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
         std::vector<GemmTask> g1, g2, g1s, g2s, gU, g3, g4;
         std::vector<ProjTask> projs;
         std::vector<SelTask> sels;
+        std::vector<GramTask> grams;
         int *sel = thr2 > 0.0 ? ws_alloc<int>(c, 2 * (tasks.size() - i0) + 2) : nullptr;
         std::vector<QRTask> qrs;
         std::vector<AssembleTask> asm_;
@@ -559,7 +560,8 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                         a1.n_dev = s32; a2.n_dev = s32;
                         g1s.push_back(a1); g2s.push_back(a2);
                     } else {
-                        g1.push_back(a1); g2.push_back(a2);
+                        grams.push_back(GramTask{t.Bv, t.Av, P, nb, t.rb, ra});
+                        g2.push_back(a2);
                     }
                 } else {
                     g1.push_back(make_gemm(0, 0, nb, ra, nb, -1.0, t.Bu, nb, t.Av, nb, 0.0, Yb, nb));
@@ -600,6 +602,18 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             SelTask *d = stage(c, sels.data(), sels.size());
             if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
             launch_precision_select(d, (int)sels.size(), thr2, c->d_flags + 4, c->cur);
+            TRY(check_launch(c));
+        }
+        if (!grams.empty()) {
+            double fl = 0.0, by = 0.0;
+            for (auto &g : grams) {
+                fl += 2.0 * g.nb * (double)g.rc * g.ra;
+                by += 8.0 * g.nb * (double)(g.rc + g.ra);
+            }
+            Prof pf(c, P_GEMM_Y, fl, by);
+            GramTask *d = stage(c, grams.data(), grams.size());
+            if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+            launch_gram_batched(d, (int)grams.size(), c->cur);
             TRY(check_launch(c));
         }
         TRY(run_gemms(c, g1, false, P_GEMM_Y));
@@ -787,26 +801,15 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     CUDA_TRY(cudaMalloc(&c->d_scal, 64 * sizeof(double)));
     CUDA_TRY(cudaMemset(c->d_flags, 0, 64 * sizeof(int)));
     CUDA_TRY(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
-    {
-        // keep freed matrix storage cached in this process's pool (no trimming at
-        // every synchronisation); hicma_tlr_fini returns it
-        cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-            uint64_t thr = UINT64_MAX;
-            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-        }
-    }
     *out = c;
     return 0;
 }
 
-// Matrix storage comes from the device's stream-ordered memory pool on the
-// context stream: a request that finishes in a serving process frees without
-// the device-wide synchronisation of cudaFree, and the next request reuses the
-// cached pages.  Both streams of the context are drained first, so the memory
-// is free of pending work on either.
+// Matrix storage: zero-filled cudaMalloc regions (a region per array), so no
+// result depends on what the memory held before.
 static cudaError_t dev_alloc(hicma_tlr_ctx *c, void **p, size_t bytes) {
-    cudaError_t e = cudaMallocAsync(p, bytes, c->stream);
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, bytes, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     return e;
 }
@@ -815,10 +818,8 @@ static void dev_free(hicma_tlr_ctx *c, void *p) {
     if (c) {
         cudaStreamSynchronize(c->stream_hi);
         cudaStreamSynchronize(c->stream);
-        cudaFreeAsync(p, c->stream);
-    } else {
-        cudaFree(p);
     }
+    cudaFree(p);
 }
 
 static void desc_free_device(hicma_tlr_desc *A) {
@@ -851,10 +852,6 @@ int hicma_tlr_fini(hicma_tlr_ctx *c) {
     cudaStreamSynchronize(c->stream);
     cudaStreamDestroy(c->stream_hi);
     cudaStreamDestroy(c->stream);
-    {
-        cudaMemPool_t pool;
-        if (cudaDeviceGetDefaultMemPool(&pool, c->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
-    }
     delete c;
     return 0;
 }

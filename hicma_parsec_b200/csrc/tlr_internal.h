@@ -104,6 +104,14 @@ struct ProjTask {
     int nb, rc, ra;
 };
 void launch_bcgs2(const ProjTask *d_tasks, int ntasks, cudaStream_t st);
+// P = C^T W (rc x ra, ld rc) with C nb x rc and W nb x ra (ld nb): one CTA per
+// product, split-K over its warps, fixed-order reduction.
+struct GramTask {
+    const double *C, *W;
+    double *P;
+    int nb, rc, ra;
+};
+void launch_gram_batched(const GramTask *d_tasks, int ntasks, cudaStream_t st);
 
 // ------------------------------------------------------ precision policy ---
 // out = sum of squares of X (rows x cols, ld): one CTA per task.

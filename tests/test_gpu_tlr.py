@@ -164,3 +164,4 @@ def test_mixed_precision_policy(ctx):
     oprob = O.Problem(kind=2, noise=1e-4)
     res = O.check_dpotrf2(B.uncompress(), O.dense_matrix(oprob, O.gen_points(N, 2)))
     assert res <= 10 * TOL, res
+
