@@ -390,6 +390,26 @@ def run_ours(args, cfg):
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs",
                     "avg_launch_ms": t_launch * 1e3, "launches": pd["launches"]}
 
+    # accuracy of the factor that was timed (untimed): matrix-free residual with
+    # Gaussian probes against the exact covariance; with --accuracy also the
+    # log-determinant against a factorization at e/100
+    accuracy = {"residual_probe": W.check_probe(prob, 16, 0), "nprobe": 16, "tolerance": 10 * acc}
+    ld = W.logdet()
+    accuracy["logdet"] = ld
+    if args.accuracy:
+        R = tlr.TLRMatrix(ctx, n, nb, mr, cfg["band"])
+        if R.generate(prob, acc / 100, mr) != 0:
+            accuracy["logdet_ref"] = None
+        else:
+            if A0.band_size != cfg["band"]:
+                R.band_regenerate(prob, A0.band_size)
+            if R.potrf(acc / 100, mr) == 0:
+                ld_ref = R.logdet()
+                accuracy.update({"logdet_ref_e_over_100": ld_ref,
+                                 "logdet_rel_err": abs(ld - ld_ref) / abs(ld_ref),
+                                 "residual_probe_e_over_100": R.check_probe(prob, 16, 0)})
+        R.close()
+
     # end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -444,7 +464,7 @@ def run_ours(args, cfg):
                 "phase_s": {"potrf": st[4], "trsm": st[5], "syrk": st[6], "gemm_recompress": st[7]},
                 "jacobi_sweeps_total": st[8],
                 "kernel_classes": prof, "gpu_launches": launches * args.steps,
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk}
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "accuracy": accuracy}
         print(json.dumps(line), flush=True)
     W.close()
     A0.close()
@@ -497,6 +517,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serving", action="store_true", help="run the MLE serving benchmark instead")
+    ap.add_argument("--accuracy", action="store_true",
+                    help="also compare the log-determinant with a factorization at e/100")
     ap.add_argument("--profile-run", action="store_true",
                     help="one generation + one factorization with per-class timing (for ncu captures)")
     ap.add_argument("--requests", type=int, default=16)

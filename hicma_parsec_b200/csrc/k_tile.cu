@@ -10,6 +10,8 @@
 // that they match the CPU restatement bit for bit; exp/sqrt are CUDA's.
 #include "tlr_internal.h"
 
+#include <algorithm>
+
 namespace tlr {
 namespace {
 
@@ -202,6 +204,15 @@ __global__ void k_precision_select(const SelTask *__restrict__ tasks, int ntasks
     if (low && count) atomicAdd(count, 1);
 }
 
+// out[i] += sum_k parts[k * len + i], k in increasing order (deterministic).
+__global__ void k_accumulate(double *out, const double *parts, int nparts, long long len) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len; i += (long long)gridDim.x * blockDim.x) {
+        double s = out[i];
+        for (int k = 0; k < nparts; ++k) s += parts[(size_t)k * len + i];
+        out[i] = s;
+    }
+}
+
 }  // namespace
 
 void launch_assemble_r(const AssembleTask *d_tasks, int ntasks, cudaStream_t st) {
@@ -213,6 +224,12 @@ void launch_sumsq_batched(const NormTask *d_tasks, int ntasks, cudaStream_t st) 
 }
 void launch_precision_select(const SelTask *d_tasks, int ntasks, double thr2, int *count, cudaStream_t st) {
     if (ntasks > 0) k_precision_select<<<(ntasks + 127) / 128, 128, 0, st>>>(d_tasks, ntasks, thr2, count);
+}
+
+void launch_accumulate(double *out, const double *parts, int nparts, long long len, cudaStream_t st) {
+    if (len <= 0 || nparts <= 0) return;
+    const long long blocks = std::min<long long>((len + 255) / 256, 4096);
+    k_accumulate<<<(int)blocks, 256, 0, st>>>(out, parts, nparts, len);
 }
 
 void launch_sumsq(const double *X, const double *Y, int m, int n, long long ld, int sym_lower, double *partial,

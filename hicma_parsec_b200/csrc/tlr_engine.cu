@@ -1974,6 +1974,136 @@ static int densify(hicma_tlr_ctx *c, hicma_tlr_desc *A, double *D) {
     return 0;
 }
 
+// Full-size counterpart of check_dpotrf2 (testing_dpotrf.c:111-180): with
+// Gaussian probes Z (N x p), ||(A - L L^T) Z||_F / ||A Z||_F estimates
+// ||A - L L^T||_F / ||A||_F without forming an N x N matrix.  A Z uses the
+// exact covariance, regenerated block-row by block-row in workspace chunks;
+// L (L^T Z) uses the TLR tiles.  Partial products are summed in a fixed order.
+int hicma_tlr_check_probe(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_problem *prob, int nprobe,
+                          unsigned long long seed, double *res_est) {
+    ARG_CHECK(c && L && prob && res_est && nprobe >= 1 && nprobe <= 64, "check_probe arguments");
+    if (!L->factored) { set_err("descriptor is not factored"); return HICMA_TLR_ERR_STATE; }
+    ARG_CHECK(L->d_pts, "no points");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    CUDA_TRY(cudaSetDevice(c->device));
+    c->cur = c->stream;
+    c->ar = &c->main_ar;
+    ws_reset(c);
+    const int NT = L->NT, NB = L->NB, p = nprobe;
+    const size_t N = L->N;
+    double *Z = ws_alloc<double>(c, N * p), *AZ = ws_alloc<double>(c, N * p);
+    double *W = ws_alloc<double>(c, N * p), *Y = ws_alloc<double>(c, N * p);
+    double *part = ws_alloc<double>(c, 1024), *sc = ws_alloc<double>(c, 8);
+    if (!Z || !AZ || !W || !Y || !part || !sc) { set_err("workspace too small (check_probe)"); return HICMA_TLR_ERR_OOM; }
+    launch_gaussian(Z, (int)N, p, (int)N, seed ^ 0x9E3779B97F4A7C15ull, c->stream);
+    CUDA_TRY(cudaMemsetAsync(AZ, 0, N * p * sizeof(double), c->stream));
+    CUDA_TRY(cudaMemsetAsync(W, 0, N * p * sizeof(double), c->stream));
+    CUDA_TRY(cudaMemsetAsync(Y, 0, N * p * sizeof(double), c->stream));
+    const size_t base = c->ar->off;
+    const CovParams cp = cov_params(L, prob);
+    // ---- A Z: tiles (m, n <= m) in chunks; P = A_mn Z_n, P' = A_mn^T Z_m
+    const size_t per_tile = align_up(sizeof(double) * (size_t)NB * NB + 1) + 2 * align_up(sizeof(double) * (size_t)NB * p + 1);
+    for (int m = 0; m < NT; ++m) {
+        int n0 = 0;
+        while (n0 <= m) {
+            c->ar->off = base;
+            const size_t reserve = align_up(sizeof(double) * (size_t)NB * p + 1) + 4096;
+            const size_t fit = ws_free(c) > reserve ? (ws_free(c) - reserve) / (per_tile + 1024) : 0;
+            if (fit < 1) { set_err("workspace too small (check_probe tile)"); return HICMA_TLR_ERR_OOM; }
+            const int n1 = std::min(m + 1, n0 + (int)std::min<size_t>(fit, 256));
+            const int cnt = n1 - n0;
+            double *R = ws_alloc<double>(c, (size_t)cnt * NB * NB);
+            double *P = ws_alloc<double>(c, (size_t)cnt * NB * p);
+            double *Pt = ws_alloc<double>(c, (size_t)cnt * NB * p);
+            std::vector<CovTask> ct;
+            std::vector<GemmTask> g;
+            std::vector<CopyTask> cpy;
+            for (int n = n0; n < n1; ++n) {
+                double *tile = R + (size_t)(n - n0) * NB * NB;
+                ct.push_back(CovTask{tile, NB, m * NB, n * NB, NB, NB});
+                g.push_back(make_gemm(0, 0, NB, p, NB, 1.0, tile, NB, Z + (size_t)n * NB, (int)N, 0.0,
+                                      P + (size_t)(n - n0) * NB * p, NB));
+                if (n < m) {
+                    double *pt = Pt + (size_t)(n - n0) * NB * p;
+                    g.push_back(make_gemm(1, 0, NB, p, NB, 1.0, tile, NB, Z + (size_t)m * NB, (int)N, 0.0, pt, NB));
+                    cpy.push_back(make_copy(pt, NB, AZ + (size_t)n * NB, (int)N, NB, p, 1.0, 1.0));
+                }
+            }
+            CovTask *dct = stage(c, ct.data(), ct.size());
+            if (!dct) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+            launch_cov_batched(cp, dct, (int)ct.size(), NB, NB, c->stream);
+            TRY(check_launch(c));
+            TRY(run_gemms(c, g));
+            // AZ_m += sum of the chunk's P in order (AZ_m is NB x p with ld N: one column at a time)
+            {
+                // gather column blocks: P is [tile](NB x p) contiguous, so accumulate into a packed
+                // NB x p buffer, then add it to the strided AZ_m with one copy
+                double *acc = ws_alloc<double>(c, (size_t)NB * p);
+                if (!acc) { set_err("workspace too small (check_probe acc)"); return HICMA_TLR_ERR_OOM; }
+                CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(double) * NB * p, c->stream));
+                launch_accumulate(acc, P, cnt, (long long)NB * p, c->stream);
+                TRY(check_launch(c));
+                std::vector<CopyTask> one{make_copy(acc, NB, AZ + (size_t)m * NB, (int)N, NB, p, 1.0, 1.0)};
+                TRY(run_copies(c, one));
+            }
+            TRY(run_copies(c, cpy));
+            n0 = n1;
+        }
+    }
+    c->ar->off = base;
+    // ---- W = L^T Z: block row m contributes L_mn^T Z_m to W_n (n <= m)
+    for (int m = 0; m < NT; ++m) {
+        c->ar->off = base;
+        std::vector<GemmTask> g1, g2;
+        const double *Zm = Z + (size_t)m * NB;
+        for (int n = 0; n <= m; ++n) {
+            double *Wn = W + (size_t)n * NB;
+            if (L->is_dense(m, n)) {
+                g2.push_back(make_gemm(1, 0, NB, p, NB, 1.0, L->dense(m, n), NB, Zm, (int)N, 1.0, Wn, (int)N));
+            } else {
+                const int r = L->rank(m, n);
+                if (r <= 0) continue;
+                double *t = ws_alloc<double>(c, (size_t)r * p);
+                if (!t) { set_err("workspace too small (check_probe)"); return HICMA_TLR_ERR_OOM; }
+                g1.push_back(make_gemm(1, 0, r, p, NB, 1.0, L->U(m, n), NB, Zm, (int)N, 0.0, t, r));
+                g2.push_back(make_gemm(0, 0, NB, p, r, 1.0, L->V(m, n), NB, t, r, 1.0, Wn, (int)N));
+            }
+        }
+        TRY(run_gemms(c, g1));
+        TRY(run_gemms(c, g2));
+    }
+    // ---- Y = L W: block column n contributes L_mn W_n to Y_m (m >= n)
+    for (int n = 0; n < NT; ++n) {
+        c->ar->off = base;
+        std::vector<GemmTask> g1, g2;
+        const double *Wn = W + (size_t)n * NB;
+        for (int m = n; m < NT; ++m) {
+            double *Ym = Y + (size_t)m * NB;
+            if (L->is_dense(m, n)) {
+                g2.push_back(make_gemm(0, 0, NB, p, NB, 1.0, L->dense(m, n), NB, Wn, (int)N, 1.0, Ym, (int)N));
+            } else {
+                const int r = L->rank(m, n);
+                if (r <= 0) continue;
+                double *t = ws_alloc<double>(c, (size_t)r * p);
+                if (!t) { set_err("workspace too small (check_probe)"); return HICMA_TLR_ERR_OOM; }
+                g1.push_back(make_gemm(1, 0, r, p, NB, 1.0, L->V(m, n), NB, Wn, (int)N, 0.0, t, r));
+                g2.push_back(make_gemm(0, 0, NB, p, r, 1.0, L->U(m, n), NB, t, r, 1.0, Ym, (int)N));
+            }
+        }
+        TRY(run_gemms(c, g1));
+        TRY(run_gemms(c, g2));
+    }
+    const int nblk = 1024;
+    launch_sumsq(AZ, Y, (int)N, p, (long long)N, 0, part, nblk, sc + 0, c->stream);
+    launch_sumsq(AZ, nullptr, (int)N, p, (long long)N, 0, part, nblk, sc + 1, c->stream);
+    double h[2] = {0, 0};
+    CUDA_TRY(cudaMemcpyAsync(h, sc, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    TRY(ctx_sync(c));
+    ws_reset(c);
+    *res_est = h[1] > 0.0 ? std::sqrt(h[0] / h[1]) : 0.0;
+    return 0;
+}
+
 int hicma_tlr_check(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_problem *prob, hicma_tlr_desc *A0,
                     double *res_llt, double *res_diff) {
     ARG_CHECK(c && L && prob, "null");

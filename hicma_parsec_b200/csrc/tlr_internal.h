@@ -121,6 +121,8 @@ struct NormTask {
     double *out;
 };
 void launch_sumsq_batched(const NormTask *d_tasks, int ntasks, cudaStream_t st);
+// out[i] += sum_k parts[k * len + i] for k = 0 .. nparts-1 in order.
+void launch_accumulate(double *out, const double *parts, int nparts, long long len, cudaStream_t st);
 // Per recompression: its products run in FP32 when na * nb <= thr2 (squared
 // Frobenius norms of the two factor tiles); sel32 / sel64 receive n or 0 and
 // serve as the device-side column counts of the two launches.

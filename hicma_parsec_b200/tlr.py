@@ -106,6 +106,7 @@ def load_library(path: str | None = None):
         "hicma_tlr_loglik": (i, [vp, vp, vp, dp, dp, vp]),
         "hicma_tlr_last_stats": (i, [vp, vp, i]),
         "hicma_tlr_check": (i, [vp, vp, C.POINTER(CProblem), vp, dp, dp]),
+        "hicma_tlr_check_probe": (i, [vp, vp, C.POINTER(CProblem), i, C.c_ulonglong, dp]),
         "hicma_tlr_prof_enable": (i, [vp, i]),
         "hicma_tlr_prof_read": (i, [vp, vp, i]),
         "hicma_tlr_k_cov": (i, [C.POINTER(CProblem), vp, i, i, i, i, i, vp, i, vp]),
@@ -327,6 +328,14 @@ class TLRMatrix:
         _check(self.lib.hicma_tlr_check(self.ctx.h, self.h, C.byref(cp), approx.h if approx else None,
                                         C.byref(r1), C.byref(r2)), "hicma_tlr_check")
         return r1.value, r2.value
+
+    def check_probe(self, prob: Problem, nprobe: int = 16, seed: int = 0) -> float:
+        """||(A - L L^T) Z||_F / ||A Z||_F with nprobe Gaussian probes (any N)."""
+        r = C.c_double()
+        cp = prob.c()
+        _check(self.lib.hicma_tlr_check_probe(self.ctx.h, self.h, C.byref(cp), nprobe, seed, C.byref(r)),
+               "hicma_tlr_check_probe")
+        return r.value
 
     def logdet(self) -> float:
         v = C.c_double()

@@ -198,6 +198,14 @@ int hicma_tlr_last_stats(hicma_tlr_desc *A, double *stats, int nstats);
 int hicma_tlr_check(hicma_tlr_ctx *ctx, hicma_tlr_desc *L, const hicma_tlr_problem *prob,
                     hicma_tlr_desc *A0, double *res_llt, double *res_diff);
 
+/* Full-size counterpart of check_dpotrf2 (hicma_parsec/testing_dpotrf.c:111-180)
+ * for N where no N x N matrix fits: with nprobe (1..64) seeded Gaussian probe
+ * vectors Z, res_est = ||(A - L L^T) Z||_F / ||A Z||_F, A the exact covariance
+ * (regenerated on the device tile by tile), L the TLR factor in L.  Uses the
+ * context workspace (4 N nprobe doubles plus tile chunks). */
+int hicma_tlr_check_probe(hicma_tlr_ctx *ctx, hicma_tlr_desc *L, const hicma_tlr_problem *prob, int nprobe,
+                          unsigned long long seed, double *res_est);
+
 /* Per-kernel-class device timing (CUDA events around launches on the context
  * stream).  Classes: 0 GEMM, 1 QR, 2 Q-apply, 3 core SVD, 4 tile POTRF,
  * 5 covariance generation, 6 copies, 7 other, 8 Gram-Schmidt projections, then the batched

@@ -165,3 +165,17 @@ def test_mixed_precision_policy(ctx):
     res = O.check_dpotrf2(B.uncompress(), O.dense_matrix(oprob, O.gen_points(N, 2)))
     assert res <= 10 * TOL, res
 
+
+
+def test_probe_residual_matches_dense_check(ctx):
+    """The matrix-free residual estimate (Gaussian probes, exact covariance
+    regenerated tile by tile) agrees with the dense check_dpotrf2 residual on the
+    reference's own test case, and is deterministic for a given seed."""
+    from hicma_parsec_b200 import tlr
+    A, _, prob = _gpu_run(ctx, dict(kind=2, noise=1e-4))
+    assert A.potrf(TOL, MAXRANK) == 0
+    exact, _ = A.check(prob)
+    est = A.check_probe(prob, 16, 7)
+    assert est == A.check_probe(prob, 16, 7)
+    assert est <= 10 * TOL
+    assert 0.5 * exact <= est <= 2.0 * exact, (est, exact)
