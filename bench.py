@@ -362,7 +362,7 @@ def run_ours(args, cfg):
     kernels = {"k_gemm_batched": (agg([n for n in prof if n.startswith("gemm")]), "tensor"),
                "k_qr": (prof["qr"], "fp64"), "k_qapply": (prof["qapply"], "fp64"),
                "k_core_svd": (prof["core_svd"], "fp64"), "k_bcgs2": (prof["proj"], "tensor"),
-               "k_copy_batched": (prof["copy"], "hbm")}
+               "k_copy_batched": (prof["copy"], "hbm"), "k_gram_batched": (prof["gram"], "tensor")}
     dom = max(kernels, key=lambda k: kernels[k][0]["seconds"])
     pd, kind = kernels[dom]
     launches = int(st[3])  # kernel launches of one factorization (engine counter)

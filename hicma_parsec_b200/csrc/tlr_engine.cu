@@ -93,7 +93,7 @@ struct hicma_tlr_ctx_s {
     struct ProfRec { int cls; cudaEvent_t a, b; double flops, bytes; };
     std::vector<ProfRec> prof_recs;
     std::vector<cudaEvent_t> ev_pool;
-    double prof_acc[14][4] = {};
+    double prof_acc[15][4] = {};
 };
 
 struct hicma_tlr_desc_s {
@@ -190,6 +190,7 @@ enum {
     P_GEMM = 0, P_QR, P_QAPPLY, P_CORE, P_POTRF, P_COV, P_COPY, P_OTHER, P_PROJ,
     // batched DMMA GEMMs by call site (P_GEMM: recompression outputs and the rest)
     P_GEMM_Y, P_GEMM_TRSM, P_GEMM_SYRK, P_GEMM_DENSE, P_GEMM_GEN,
+    P_GRAM,   // split-K inner products B_V^T A_V of the recompressions
     P_NCLASS
 };
 
@@ -610,7 +611,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                 fl += 2.0 * g.nb * (double)g.rc * g.ra;
                 by += 8.0 * g.nb * (double)(g.rc + g.ra);
             }
-            Prof pf(c, P_GEMM_Y, fl, by);
+            Prof pf(c, P_GRAM, fl, by);
             GramTask *d = stage(c, grams.data(), grams.size());
             if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
             launch_gram_batched(d, (int)grams.size(), c->cur);

@@ -210,7 +210,7 @@ int hicma_tlr_check_probe(hicma_tlr_ctx *ctx, hicma_tlr_desc *L, const hicma_tlr
  * stream).  Classes: 0 GEMM, 1 QR, 2 Q-apply, 3 core SVD, 4 tile POTRF,
  * 5 covariance generation, 6 copies, 7 other, 8 Gram-Schmidt projections, then the batched
  * GEMMs by call site: 0 recompression outputs and the rest, 9 recompression products (Y),
- * 10 TRSM, 11 SYRK, 12 dense band cases, 13 generation.
+ * 10 TRSM, 11 SYRK, 12 dense band cases, 13 generation; 14 split-K inner products (Gram kernel).
  * out[4*k + j]: j = 0 launches,
  * 1 seconds, 2 algorithmic flops, 3 algorithmic bytes.  Enabling resets. */
 int hicma_tlr_prof_enable(hicma_tlr_ctx *ctx, int on);
