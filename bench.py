@@ -46,6 +46,8 @@ CONFIGS = {
                 workload="2D sqexp N=27000 NB=2700 e=1e-8 maxrank=150 band=1 FP64 (scaled twin of N=270000)"),
     "c3": dict(kind=4, n=108000, nb=2700, maxrank=1350, acc=1e-8, noise=1e-4, band=1, autoband=True,
                workload="3D exp N=108000 NB=2700 e=1e-8 maxrank=1350 band auto FP64"),
+    "c3s": dict(kind=4, n=27000, nb=2700, maxrank=1350, acc=1e-8, noise=1e-4, band=1, autoband=True,
+                workload="3D exp N=27000 NB=2700 e=1e-8 maxrank=1350 band auto FP64 (scaled twin of N=108000)"),
     "c4": dict(kind=3, n=216000, nb=2700, maxrank=500, acc=1e-8, noise=1e-4, band=1, autoband=True,
                workload="3D sqexp N=216000 NB=2700 e=1e-8 maxrank=500 band auto FP64"),
 }
@@ -254,6 +256,10 @@ def run_profile(args, cfg):
     ctx.prof_enable(True)
     if A.generate(prob, acc, mr) != 0:
         raise SystemExit("generation rejected a tile")
+    if cfg["autoband"]:
+        band = tlr.parsec_band_size_auto_tuning(A.rank_map(), n // nb, nb)
+        if band != 1:
+            A.band_regenerate(prob, band)
     gen = ctx.prof_read()
     ctx.prof_enable(True)
     info = A.potrf(acc, mr)

@@ -1101,42 +1101,62 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
     ws_reset(c);
     const int NT = A->NT, NB = A->NB;
     TRY(gen_band_tiles(c, A, prob));
-    // off-band tiles: generate dense into the workspace, compress into slots
-    const int s = std::min(maxrank + 10, NB);    // STARSH_gen.jdf:262-266
-    double *Omega = ws_alloc<double>(c, (size_t)NB * s);
-    double *Ident = ws_alloc<double>(c, (size_t)s * s);
+    // off-band tiles: generate dense into the workspace, compress into slots.
+    // The reference samples min(maxrank + 10, NB) columns for every tile
+    // (STARSH_gen.jdf:262-266); the sampled singular values only matter up to
+    // the rank, so tiles start with s = min(160, s_full) samples (the on-chip
+    // core) and a tile whose rank comes within max(32, s/4) of s is generated
+    // again with twice the samples, up to s_full.  Rejected tiles (2r >= NB)
+    // stay rejected: more samples can only raise the rank.
+    const int s_full = std::min(maxrank + 10, NB);
+    double *Omega = ws_alloc<double>(c, (size_t)NB * s_full);
+    double *Ident = ws_alloc<double>(c, (size_t)s_full * s_full);
     int *rtask = ws_alloc<int>(c, (size_t)NT * NT + 1);
     if (!Omega || !Ident || !rtask) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
-    launch_gaussian(Omega, NB, s, NB, prob->seed ^ 0x5DEECE66Dull, c->stream);
+    launch_gaussian(Omega, NB, s_full, NB, prob->seed ^ 0x5DEECE66Dull, c->stream);
     TRY(check_launch(c));
-    launch_set_identity(Ident, s, s, c->stream);
-    TRY(check_launch(c));
-    std::vector<std::pair<int, int>> tiles;
+    std::vector<std::pair<int, int>> pending;
     for (int m = A->band; m < NT; ++m)
-        for (int n = 0; n <= m - A->band; ++n) tiles.push_back({m, n});
-    const size_t per_tile = align_up(sizeof(double) * (size_t)NB * NB + 1) + compress_ws_bytes(NB, s);
-    size_t chunk = std::max<size_t>(1, ws_free(c) / (per_tile + 4096));
+        for (int n = 0; n <= m - A->band; ++n) pending.push_back({m, n});
     const CovParams cp = cov_params(A, prob);
-    for (size_t t0 = 0; t0 < tiles.size(); t0 += chunk) {
-        const size_t t1 = std::min(tiles.size(), t0 + chunk);
-        const size_t mark = c->ar->off;
-        std::vector<CovTask> cov;
-        std::vector<CompressTask> comp;
-        for (size_t i = t0; i < t1; ++i) {
-            const int m = tiles[i].first, n = tiles[i].second;
-            double *D = ws_alloc<double>(c, (size_t)NB * NB);
-            cov.push_back(CovTask{D, NB, m * NB, n * NB, NB, NB});
-            comp.push_back(CompressTask{D, A->U(m, n), A->V(m, n), A->d_rank + (size_t)n * NT + m});
-        }
-        CovTask *dcov = stage(c, cov.data(), cov.size());
-        if (!dcov) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
-        {
-            Prof pf(c, P_COV, 0, 8.0 * cov.size() * (double)NB * NB);
-            launch_cov_batched(cp, dcov, (int)cov.size(), NB, NB, c->stream);
-        }
+    int s = std::min(160, s_full);
+    while (!pending.empty()) {
+        launch_set_identity(Ident, s, s, c->stream);
         TRY(check_launch(c));
-        TRY(run_compress(c, NB, maxrank, tol, Omega, s, comp, Ident, rtask));
-        c->ar->off = mark;
+        const size_t per_tile = align_up(sizeof(double) * (size_t)NB * NB + 1) + compress_ws_bytes(NB, s);
+        const size_t chunk = std::max<size_t>(1, ws_free(c) / (per_tile + 4096));
+        for (size_t t0 = 0; t0 < pending.size(); t0 += chunk) {
+            const size_t t1 = std::min(pending.size(), t0 + chunk);
+            const size_t mark = c->ar->off;
+            std::vector<CovTask> cov;
+            std::vector<CompressTask> comp;
+            for (size_t i = t0; i < t1; ++i) {
+                const int m = pending[i].first, n = pending[i].second;
+                double *D = ws_alloc<double>(c, (size_t)NB * NB);
+                cov.push_back(CovTask{D, NB, m * NB, n * NB, NB, NB});
+                comp.push_back(CompressTask{D, A->U(m, n), A->V(m, n), A->d_rank + (size_t)n * NT + m});
+            }
+            CovTask *dcov = stage(c, cov.data(), cov.size());
+            if (!dcov) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+            {
+                Prof pf(c, P_COV, 0, 8.0 * cov.size() * (double)NB * NB);
+                launch_cov_batched(cp, dcov, (int)cov.size(), NB, NB, c->stream);
+            }
+            TRY(check_launch(c));
+            TRY(run_compress(c, NB, maxrank, tol, Omega, s, comp, Ident, rtask));
+            c->ar->off = mark;
+        }
+        if (s >= s_full) break;
+        TRY(ctx_sync(c));
+        CUDA_TRY(cudaMemcpy(A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
+        std::vector<std::pair<int, int>> more;
+        const int margin = std::max(32, s / 4);
+        for (auto &t : pending) {
+            const int r = A->rank(t.first, t.second);
+            if (r >= 0 && r > s - margin) more.push_back(t);
+        }
+        pending.swap(more);
+        s = std::min(2 * s, s_full);
     }
     TRY(ctx_sync(c));
     CUDA_TRY(cudaMemcpy(A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
