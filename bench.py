@@ -481,7 +481,7 @@ def run_ours(args, cfg):
 
 
 def run_serving(args):
-    """MLE serving stream: the same seeded requests served
+    """MLE serving stream (N log-uniform requests of uneven sizes): the same seeded requests served
     sequentially on one slot and by the continuous-batching loop."""
     import torch
     from hicma_parsec_b200 import serving

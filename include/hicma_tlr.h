@@ -51,7 +51,7 @@ extern "C" {
 #define HICMA_TLR_KIND_SQEXP_3D 3
 #define HICMA_TLR_KIND_EXP_3D   4
 
-/* Precision policy of the factorization (north-star addition). */
+/* Precision policy of the factorization (no reference counterpart). */
 #define HICMA_TLR_PREC_FP64   0   /* everything in FP64                              */
 #define HICMA_TLR_PREC_MIXED  1   /* off-band low-rank products of small-norm tiles in
                                      FP32; band, diagonal and truncation stay FP64     */
@@ -172,7 +172,7 @@ int hicma_tlr_store_bytes(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, size_t *bytes_n
 int hicma_tlr_store_get(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, double *buf, int *Ar);
 int hicma_tlr_store_set(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, const double *buf, const int *Ar);
 
-/* North-star additions (no reference counterpart; testing_dpotrf.c stops at
+/* Additions beyond the reference (no reference counterpart; testing_dpotrf.c stops at
  * the factor).  Require a factored descriptor. */
 int hicma_tlr_logdet(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, double *logdet);
 /* Solve A X = B in place; B is host N x nrhs column-major (leading dim ldb). */

@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY.  Nothing in the shipped library imports this module:
 only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline legs of
-``bench.py`` use it, and only as the checker (or as the timed CPU restatement).
+``bench.py`` use it, and only to compare results against (or as the timed CPU restatement).
 
 PARITY UNPINNED.  The arithmetic of the reference lives in three git
 submodules that are empty in the reference tree (``dplasma``, ``hcore``,

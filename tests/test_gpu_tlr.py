@@ -4,7 +4,7 @@ The reference's CTest entries (hicma_parsec/CMakeLists.txt:59-62) run
 ``testing_dpotrf_tlr -N 2700 -t 270 -e 1e-8 -u 130 -D 2 --check``: 2D
 squared-exponential covariance, tile 270, accuracy 1e-8, maxrank 130.  Its
 pass criteria are ``check_dpotrf2`` and ``check_diff`` <= tol
-(testing_dpotrf.c:851-853,891-893).  The north star adds: residual <= 10 e,
+(testing_dpotrf.c:851-853,891-893).  The parity bar used here adds: residual <= 10 e,
 log-determinant relative error <= 1e-8, per-tile ranks within +/-2 of the
 oracle's TLR run.
 """
