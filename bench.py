@@ -155,6 +155,19 @@ def cpu_sample_tasks(tiles: dict, nb: int, S: int, acc: float, maxrank: int, thr
     return secs, ops
 
 
+def max_over_ranks(x: float, device=None) -> float:
+    """Job time of N replicas: the maximum over ranks of each rank's device
+    time (all ranks call it; one process or no process group: x itself).
+    NCCL needs a device tensor, gloo a host one (device=None)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() < 2:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def load_traffic_ratios() -> dict:
     """Measured DRAM bytes per algorithmic unit (flop, or byte for copy-like
     kernels) of each kernel, from an ncu capture summarised under profiles/:
@@ -347,9 +360,7 @@ def run_ours(args, cfg):
     clk = clocks.stop()
     secs = e0.elapsed_time(e1) * 1e-3
     if world > 1:
-        tt = torch.tensor([secs], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        secs = float(tt.item())
+        secs = max_over_ranks(secs, dev)
         dist.barrier()
     s_per_factor = secs / (args.steps * world)
     st = W.stats()
