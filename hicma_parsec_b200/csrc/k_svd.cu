@@ -354,7 +354,7 @@ constexpr int CL_CT = 256;
 __device__ __forceinline__ double ldg2(const double *p) { return __ldcg(p); }
 __device__ __forceinline__ int ldg2(const int *p) { return __ldcg(p); }
 
-__global__ void __launch_bounds__(CL_CT, 1) k_core_svd_cl(const CoreTask *__restrict__ tasks, CoreParams p) {
+__global__ void __launch_bounds__(CL_CT) k_core_svd_cl(const CoreTask *__restrict__ tasks, CoreParams p) {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     constexpr int NW = CL_CT / 32;
@@ -395,7 +395,6 @@ __global__ void __launch_bounds__(CL_CT, 1) k_core_svd_cl(const CoreTask *__rest
     cl.sync();
     for (int c = gw; c < K; c += GW) {
         double s2 = 0.0;
-        #pragma unroll 4
         for (int r = lane; r < K; r += 32) { const double x = ldg2(W + (size_t)c * K + r); s2 += x * x; }
         s2 = group_sum<32>(s2);
         if (lane == 0) { sig[c] = s2; piv[c] = c; }
@@ -444,7 +443,6 @@ __global__ void __launch_bounds__(CL_CT, 1) k_core_svd_cl(const CoreTask *__rest
                 double *cj = W + (size_t)j * K;
                 if (bi != j) {
                     double *cb = W + (size_t)bi * K;
-                    #pragma unroll 4
                     for (int r = lane; r < K; r += 32) {
                         const double x = ldg2(cj + r);
                         cj[r] = ldg2(cb + r);
@@ -458,7 +456,6 @@ __global__ void __launch_bounds__(CL_CT, 1) k_core_svd_cl(const CoreTask *__rest
                 }
                 const double alpha = ldg2(cj + j);
                 double s2 = 0.0;
-                #pragma unroll 4
                 for (int r = j + 1 + lane; r < K; r += 32) { const double x = ldg2(cj + r); s2 += x * x; }
                 s2 = group_sum<32>(s2);
                 double th = 0.0, scl = 0.0, beta = alpha;
@@ -467,7 +464,6 @@ __global__ void __launch_bounds__(CL_CT, 1) k_core_svd_cl(const CoreTask *__rest
                     th = (beta - alpha) / beta;
                     scl = 1.0 / (alpha - beta);
                 }
-                #pragma unroll 4
                 for (int r = j + 1 + lane; r < K; r += 32) {
                     hv[r] = ldg2(cj + r) * scl;
                     cj[r] = 0.0;
@@ -485,11 +481,9 @@ __global__ void __launch_bounds__(CL_CT, 1) k_core_svd_cl(const CoreTask *__rest
         for (int c = j + 1 + gw; c < K; c += GW) {
             double *col = W + (size_t)c * K;
             double w = 0.0;
-            #pragma unroll 4
             for (int r = j + lane; r < K; r += 32) w += ldg2(hv + r) * ldg2(col + r);
             w = group_sum<32>(w) * th;
             double s2 = 0.0;
-            #pragma unroll 4
             for (int r = j + lane; r < K; r += 32) {
                 const double x = ldg2(col + r) - w * ldg2(hv + r);
                 col[r] = x;
@@ -519,7 +513,6 @@ __global__ void __launch_bounds__(CL_CT, 1) k_core_svd_cl(const CoreTask *__rest
         for (int sweep = 0; sweep < MAX_SWEEPS; ++sweep) {
             for (int c = gw; c < k; c += GW) {
                 double s2 = 0.0;
-                #pragma unroll 4
                 for (int r = lane; r < K; r += 32) { const double x = ldg2(W + (size_t)c * K + r); s2 += x * x; }
                 s2 = group_sum<32>(s2);
                 if (lane == 0) sig[c] = s2;
@@ -536,7 +529,6 @@ __global__ void __launch_bounds__(CL_CT, 1) k_core_svd_cl(const CoreTask *__rest
                     if (!(sa > tau2 && sb > tau2)) continue;
                     double *mp = W + (size_t)a * K, *mq = W + (size_t)b * K;
                     double aa = 0.0, bb = 0.0, cc = 0.0;
-                    #pragma unroll 4
                     for (int r = lane; r < K; r += 32) {
                         const double x = ldg2(mp + r), y = ldg2(mq + r);
                         aa += x * x; bb += y * y; cc += x * y;
@@ -551,7 +543,6 @@ __global__ void __launch_bounds__(CL_CT, 1) k_core_svd_cl(const CoreTask *__rest
                     if (fabs(zeta) > 1e150) tt = 0.5 / zeta;
                     else tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
                     const double cs = 1.0 / sqrt(1.0 + tt * tt), sn = cs * tt;
-                    #pragma unroll 4
                     for (int r = lane; r < K; r += 32) {
                         const double x = ldg2(mp + r), y = ldg2(mq + r);
                         mp[r] = cs * x - sn * y;
@@ -572,7 +563,6 @@ __global__ void __launch_bounds__(CL_CT, 1) k_core_svd_cl(const CoreTask *__rest
     }
     for (int c = gw; c < k; c += GW) {
         double s = 0.0;
-        #pragma unroll 4
         for (int r = lane; r < K; r += 32) { const double x = ldg2(W + (size_t)c * K + r); s += x * x; }
         s = group_sum<32>(s);
         if (lane == 0) sig[c] = sqrt(s);
