@@ -75,12 +75,9 @@ __global__ void __launch_bounds__(256) k_potrf_diag(double *A, int lda, int jb, 
 
 void launch_potrf_diag(double *A, int lda, int jb, double *Dinv, int ldd, int *info, int info_base,
                        cudaStream_t st) {
-    static bool configured = false;
     const size_t smem = 2 * DB * LDS * sizeof(double);
-    if (!configured) {
-        cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = true;
-    }
+    // per device and thread-safe: set on every launch (a host-side call, no synchronisation)
+    cudaFuncSetAttribute(k_potrf_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_potrf_diag<<<1, 256, smem, st>>>(A, lda, jb, Dinv, ldd, info, info_base);
 }
 

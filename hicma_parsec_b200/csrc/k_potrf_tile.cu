@@ -398,11 +398,8 @@ int launch_potrf_tile(double *A, int lda, int n, double *X, int ldx, double *D, 
     if (cudaMemsetAsync(cnt, 0, potrf_tile_scratch_ints(n) * sizeof(int), st) != cudaSuccess) return -1;
     const int smem = (int)sizeof(double) * (2 * TB * TPITCH > 2 * TB * LDS + 32 * 32 + TB ? 2 * TB * TPITCH
                                                                                         : 2 * TB * LDS + 32 * 32 + TB);
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        configured = true;
-    }
+    // per device and thread-safe: set on every launch (a host-side call, no synchronisation)
+    cudaFuncSetAttribute(k_potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     PotrfParams P{A, lda, n, nblk, X, ldx, D, L->d, L->n, cnt, info, info_base, timeout};
     if (grid > L->n) grid = L->n;
     if (grid < 1) grid = 1;

@@ -154,22 +154,16 @@ __global__ void __launch_bounds__(PT, 2) k_gram_batched(const GramTask *__restri
 void launch_gram_batched(const GramTask *d_tasks, int ntasks, cudaStream_t st) {
     if (ntasks <= 0) return;
     const int smem = PW * PB * PB * (int)sizeof(double);
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_gram_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        configured = true;
-    }
+    // per device and thread-safe: set on every launch (a host-side call, no synchronisation)
+    cudaFuncSetAttribute(k_gram_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     k_gram_batched<<<ntasks, PT, smem, st>>>(d_tasks);
 }
 
 void launch_bcgs2(const ProjTask *d_tasks, int ntasks, cudaStream_t st) {
     if (ntasks <= 0) return;
     const int smem = PW * PB * PB * (int)sizeof(double);
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(k_bcgs2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        configured = true;
-    }
+    // per device and thread-safe: set on every launch (a host-side call, no synchronisation)
+    cudaFuncSetAttribute(k_bcgs2, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     k_bcgs2<<<ntasks, PT, smem, st>>>(d_tasks);
 }
 
