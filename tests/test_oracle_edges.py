@@ -1,0 +1,95 @@
+"""Edge cases of the CPU oracle (the restated reference algorithm) at sizes that
+finish in seconds: band > 1, one tile, rank-0 inputs, fixed rank, the maxrank
+cap, the generation rejection rule, and solve / log-likelihood against dense."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import tlr_oracle as O
+
+N, NB = 540, 54
+
+
+@pytest.fixture(scope="module")
+def setup():
+    prob = O.Problem(kind=2, beta=0.02, noise=1e-2)     # short length scale: tiles compress at N=540
+    pts = O.gen_points(N, 2)
+    return prob, pts, O.dense_matrix(prob, pts)
+
+
+@pytest.mark.parametrize("band", [1, 2, 3])
+def test_band_factorization_meets_checks(setup, band):
+    prob, pts, A = setup
+    T, info = O.generate(prob, N, NB, 1e-9, NB // 2 - 1, band, pts)
+    assert info == 0
+    assert all(T.is_dense(m, n) for (m, n) in T.dense)
+    st = O.tlr_potrf(T, 1e-9)
+    assert st.info == 0
+    L = O.uncompress(T)
+    assert O.check_dpotrf2(L, A) <= 10 * 1e-9
+    ld_dense = 2.0 * np.log(np.diag(np.linalg.cholesky(A))).sum()
+    assert abs(O.logdet(T) - ld_dense) <= 1e-8 * abs(ld_dense)
+
+
+def test_single_tile_is_dense_cholesky(setup):
+    prob, pts, _ = setup
+    T, info = O.generate(prob, NB, NB, 1e-9, 20, 1, pts[:NB])
+    assert info == 0 and list(T.dense) == [(0, 0)] and not T.U
+    A0 = T.dense[(0, 0)].copy()
+    assert O.tlr_potrf(T, 1e-9).info == 0
+    assert np.allclose(T.dense[(0, 0)], np.linalg.cholesky(A0))
+
+
+def test_solve_and_loglik_match_dense(setup):
+    prob, pts, A = setup
+    T, _ = O.generate(prob, N, NB, 1e-10, NB // 2 - 1, 1, pts)
+    assert O.tlr_potrf(T, 1e-10).info == 0
+    y = np.random.default_rng(5).standard_normal(N)
+    ll, ld, x = O.loglik(T, y)
+    xd = np.linalg.solve(A, y)
+    assert np.linalg.norm(x - xd) <= 1e-6 * np.linalg.norm(xd)
+    lld = -0.5 * (y @ xd + np.linalg.slogdet(A)[1] + N * math.log(2 * math.pi))
+    assert abs(ll - lld) <= 1e-8 * abs(lld)
+    Y = np.stack([y, 2 * y], axis=1)          # several right-hand sides at once
+    X = O.solve(T, Y)
+    assert np.allclose(X[:, 1], 2 * X[:, 0])
+
+
+def test_recompress_rank_zero_inputs():
+    rng = np.random.default_rng(0)
+    nb = 40
+    U, V, r, ov = O.recompress(np.zeros((nb, 0)), np.zeros((nb, 0)), np.zeros((nb, 0)), np.zeros((nb, 0)), 1e-8, 10)
+    assert r == 0 and U.shape == (nb, 0) and not ov
+    Au, _ = np.linalg.qr(rng.standard_normal((nb, 3)))
+    Y = rng.standard_normal((nb, 3))
+    U, V, r, _ = O.recompress(np.zeros((nb, 0)), np.zeros((nb, 0)), Au, Y, 1e-12, 10)
+    assert r == 3 and np.allclose(U @ V.T, -Au @ Y.T)
+
+
+def test_recompress_fixed_rank_and_cap():
+    rng = np.random.default_rng(1)
+    nb = 60
+    Cu, _ = np.linalg.qr(rng.standard_normal((nb, 8)))
+    Cv = rng.standard_normal((nb, 8))
+    Au, _ = np.linalg.qr(rng.standard_normal((nb, 8)))
+    Y = rng.standard_normal((nb, 8))
+    _, _, r, ov = O.recompress(Cu, Cv, Au, Y, 1e-12, 30, fixed_rank=5)
+    assert r == 5 and not ov
+    _, _, r, ov = O.recompress(Cu, Cv, Au, Y, 1e-12, 6)        # full rank 16 > maxrank 6
+    assert r == 6 and ov
+
+
+def test_generation_rejects_tiles_that_do_not_compress():
+    # at beta = 0.03 the first sub-diagonal tiles need rank >= NB/2 and are rejected
+    # (info -1, rank 0 stored); a band of 2 keeps them dense and generation succeeds
+    prob = O.Problem(kind=2, beta=0.03, noise=1e-2)
+    pts = O.gen_points(N, 2)
+    T, info = O.generate(prob, N, NB, 1e-9, NB // 2 - 1, 1, pts)
+    assert info == -1
+    assert any(T.rank(m, n) == 0 and m - n == 1 for (m, n) in T.U)
+    T2, info2 = O.generate(prob, N, NB, 1e-9, NB // 2 - 1, 2, pts)
+    assert info2 == 0 and T2.is_dense(1, 0)
+    O.band_regenerate(T, prob, pts, 2)
+    for key in T2.U:
+        assert np.allclose(T.U[key] @ T.V[key].T, T2.U[key] @ T2.V[key].T)
