@@ -35,7 +35,9 @@ static void usage(void) {
             " -G --genmaxrank   maxrank used in generation (default maxrank)\n"
             " -U --compmaxrank  maxrank of buffers (default maxrank)\n"
             " -f --fixedrank    fixed rank in recompression (0 = accuracy mode)\n"
-            " -D --kind_of_problem 2: st-2d-sqexp 3: st-3d-sqexp 4: st-3d-exp\n"
+            " -D --kind_of_problem 1: ed-2d-sin 2: st-2d-sqexp 3: st-3d-sqexp 4: st-3d-exp 5: ed-3d-sin\n"
+            " -w --wave_k       wave number of -D 1, 5 (default 50)\n"
+            " -j --add_diag     diagonal of -D 1, 5 (default N)\n"
             " -Z --band         band size (default 1)\n"
             " -E --auto-band    auto-tune band size (default 1)\n"
             " -Y --lookahead    lookahead (-1: band size)\n"
@@ -50,7 +52,7 @@ int main(int argc, char **argv) {
     int N = 0, NB = 0, maxrank = 0, genmaxrank = 0, compmaxrank = 0, fixedrk = 0, kind = 2, band_size = 1;
     int auto_band = 1, lookahead = -1, send_full_tile = 0, two_flow = 0, HNB = 300, check = 0, verbose = 0;
     int device = 0, precision = HICMA_TLR_PREC_FP64;
-    double tol = 1e-8, noise = 0.1, beta = 0.1, sigma = 1.0, ws_gib = 0.0;
+    double tol = 1e-8, noise = 0.1, beta = 0.1, sigma = 1.0, ws_gib = 0.0, wave_k = 50.0, add_diag = 0.0;
     unsigned long long seed = 0;
     static struct option opts[] = {
         {"N", required_argument, 0, 'N'},          {"NB", required_argument, 0, 't'},
@@ -72,6 +74,8 @@ int main(int argc, char **argv) {
         {"h", no_argument, 0, 'h'},                {"P", required_argument, 0, 'P'},
         {"Q", required_argument, 0, 'Q'},          {"c", required_argument, 0, 'c'},
         {"cores", required_argument, 0, 'c'},      {"g", required_argument, 0, 'g'},
+        {"wave_k", required_argument, 0, 'w'},     {"w", required_argument, 0, 'w'},
+        {"add_diag", required_argument, 0, 'j'},   {"j", required_argument, 0, 'j'},
         {"noise", required_argument, 0, 1001},     {"beta", required_argument, 0, 1002},
         {"sigma", required_argument, 0, 1003},     {"seed", required_argument, 0, 1004},
         {"precision", required_argument, 0, 1005}, {"ws", required_argument, 0, 1006},
@@ -97,6 +101,8 @@ int main(int argc, char **argv) {
             case 'v': verbose = optarg ? atoi(optarg) : 1; break;
             case 'h': usage(); return 0;
             case 'P': case 'Q': case 'c': case 'g': break;
+            case 'w': wave_k = atof(optarg); break;
+            case 'j': add_diag = atof(optarg); break;
             case 1001: noise = atof(optarg); break;
             case 1002: beta = atof(optarg); break;
             case 1003: sigma = atof(optarg); break;
@@ -111,14 +117,16 @@ int main(int argc, char **argv) {
     if (maxrank <= 0) { maxrank = NB / 2; fprintf(stderr, "Max rank has not been specified. Forced to the size of a tile %d\n", maxrank); }
     if (genmaxrank <= 0) genmaxrank = maxrank;
     if (compmaxrank <= 0) compmaxrank = maxrank;
-    if (kind < 2 || kind > 4) { fprintf(stderr, "Wrong value of \"kind_of_problem\" parameter (2, 3 or 4)\n"); return 1; }
+    if (add_diag <= 0.0) add_diag = (double)N;   /* hicma_parsec.c:289-291 */
+    if (kind < 1 || kind > 5) { fprintf(stderr, "Wrong value of \"kind_of_problem\" parameter (1 to 5)\n"); return 1; }
     if (N % NB != 0) { fprintf(stderr, "N must be a multiple of NB\n"); return 1; }
     const int NT = N / NB;
     const double flops = (N * (((1. / 6.) * N + 0.5) * N + (1. / 3.))) + (N * (((1. / 6.) * N) * N - (1. / 6.)));
     if (verbose) {
         printf("M:%d N:%d NB:%d NB:%d HNB:%d HNB:%d\n", N, N, NB, NB, HNB, HNB);
         printf("kind_of_problem:%d %s\n", kind, str_problem[kind]);
-        printf("tol:%.1e noise:%g fixed_rk:%d\n", tol, noise, fixedrk);
+        printf("tol:%.1e add_diag:%g fixed_rk:%d wave_k:%g\n", tol, add_diag, fixedrk, wave_k);
+        printf("noise:%g beta:%g sigma:%g seed:%llu\n", noise, beta, sigma, seed);
         printf("send_full_tile:%d lookahead: %d band_size:%d max_rank:%d gen:%d comp:%d\n", send_full_tile,
                lookahead, band_size, maxrank, genmaxrank, compmaxrank);
     }
@@ -128,7 +136,7 @@ int main(int argc, char **argv) {
     int rc = hicma_tlr_init(device, (size_t)(ws_gib * (1ull << 30)), &ctx);
     if (rc) { fprintf(stderr, "init failed: %s\n", hicma_tlr_last_error()); return 1; }
     hicma_tlr_set_precision(ctx, precision);
-    hicma_tlr_problem prob = {kind, beta, 0.5, noise, sigma, seed};
+    hicma_tlr_problem prob = {kind, beta, 0.5, noise, sigma, seed, wave_k, add_diag};
     hicma_tlr_desc *A = NULL;
     rc = hicma_tlr_desc_create(ctx, N, NB, maxrank > genmaxrank ? maxrank : genmaxrank, band_size, &A);
     if (rc) { fprintf(stderr, "descriptor: %s\n", hicma_tlr_last_error()); return 1; }
@@ -231,7 +239,7 @@ int main(int argc, char **argv) {
            offband_ops ? (double)band_ops / offband_ops : 0.0);
     printf("R-LO %d %d %d %d   %d %d   %d %d %d %d   %d %s %.1e %g %d %g   %d %d %d %d %d %d %d %d   "
            "%g %d %d   %g %d %d   %g %d %d   %lf %lf   %lf %lf %lf %lf    %lf %lf %lf %lf %lf    %le %le %le %d \"",
-           N, N, NB, NB, HNB, HNB, 1, 1, 1, 1, kind, str_problem[kind], tol, noise, fixedrk, 0.0, send_full_tile,
+           N, N, NB, NB, HNB, HNB, 1, 1, 1, 1, kind, str_problem[kind], tol, add_diag, fixedrk, wave_k, send_full_tile,
            band_size, lookahead, 0, auto_band, maxrank, genmaxrank, compmaxrank, iavg_before, imin_before,
            imax_before, iavgrk, iminrk, imaxrk, favgrk, fminrk, fmaxrk, mem, mem_max, cpt[0] + cpt[1] + cpt[2],
            cpt[0], cpt[1], cpt[2], time_starsh, time_hicma, time_opt_band, time_regenerate, 0.0, (double)total,

@@ -5,9 +5,12 @@
 // sqrexp_kernel_3d,exp_kernel_3d} (kernel pointers chosen at
 // hicma_parsec/testing_dpotrf.c:338,346,354; call shape of
 // hicma_parsec/STARSH_gen.jdf:70-72): A_ij = sigma * k(|x_i - x_j|) with the
-// nugget added where the global row and column indices coincide.  Distances
-// are accumulated with explicitly rounded operations (no FMA contraction) so
-// that they match the CPU restatement bit for bit; exp/sqrt are CUDA's.
+// nugget added where the global row and column indices coincide.  The
+// electrodynamics kinds restate starsh_eddata_block_sin_kernel_{2d,3d}
+// (hicma_parsec/testing_dpotrf.c:330,361): A_ij = sin(k r) / r, and add_diag
+// where r == 0.  Distances are accumulated with explicitly rounded operations
+// (no FMA contraction) so that they match the CPU restatement bit for bit;
+// exp/sin/sqrt are CUDA's.
 #include "tlr_internal.h"
 
 #include <algorithm>
@@ -40,11 +43,16 @@ __global__ void __launch_bounds__(COV_ROWS) k_cov_batched(CovParams p, const Cov
             }
         }
         double v;
-        if (p.kind == HICMA_TLR_KIND_EXP_3D)
-            v = __dmul_rn(p.sigma, exp(-__ddiv_rn(__dsqrt_rn(r2), p.beta)));
-        else
-            v = __dmul_rn(p.sigma, exp(-__ddiv_rn(r2, den)));
-        if (gr == gc) v = __dadd_rn(v, p.noise);
+        if (p.kind == HICMA_TLR_KIND_ED_SIN_2D || p.kind == HICMA_TLR_KIND_ED_SIN_3D) {
+            const double rr = __dsqrt_rn(r2);
+            v = r2 == 0.0 ? p.add_diag : __ddiv_rn(sin(__dmul_rn(p.wave_k, rr)), rr);
+        } else {
+            if (p.kind == HICMA_TLR_KIND_EXP_3D)
+                v = __dmul_rn(p.sigma, exp(-__ddiv_rn(__dsqrt_rn(r2), p.beta)));
+            else
+                v = __dmul_rn(p.sigma, exp(-__ddiv_rn(r2, den)));
+            if (gr == gc) v = __dadd_rn(v, p.noise);
+        }
         t.out[(size_t)r + (size_t)c * t.ld] = v;
     }
 }

@@ -706,9 +706,11 @@ uint64_t mix64h(uint64_t x) {
 
 int kind_ndim(int kind) {
     switch (kind) {
+        case HICMA_TLR_KIND_ED_SIN_2D: return 2;
         case HICMA_TLR_KIND_SQEXP_2D: return 2;
         case HICMA_TLR_KIND_SQEXP_3D: return 3;
         case HICMA_TLR_KIND_EXP_3D: return 3;
+        case HICMA_TLR_KIND_ED_SIN_3D: return 3;
         default: return 0;
     }
 }
@@ -964,7 +966,7 @@ int hicma_tlr_desc_copy(hicma_tlr_ctx *c, const hicma_tlr_desc *src, hicma_tlr_d
 
 static int set_points(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_problem *prob, const double *points) {
     const int ndim = kind_ndim(prob->kind);
-    ARG_CHECK(ndim > 0, "unsupported problem kind (-D 2, 3 or 4)");
+    ARG_CHECK(ndim > 0, "unsupported problem kind (-D 1, 2, 3, 4 or 5)");
     std::vector<double> h;
     if (!points) {
         h.resize((size_t)ndim * A->N);
@@ -981,11 +983,20 @@ static int set_points(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_probl
     return ctx_sync(c);
 }
 
-static CovParams cov_params(const hicma_tlr_desc *A, const hicma_tlr_problem *prob) {
+// Kernel parameters of a problem over N points.  A non-positive add_diag of
+// the electrodynamics kinds means N, the reference's default
+// (hicma_parsec/hicma_parsec.c:289-291).
+static CovParams make_cov_params(const hicma_tlr_problem *prob, const double *d_points, int N, int ndim) {
     CovParams p;
-    p.pts = A->d_pts; p.N = A->N; p.ndim = A->ndim; p.kind = prob->kind;
+    p.pts = d_points; p.N = N; p.ndim = ndim; p.kind = prob->kind;
     p.beta = prob->beta; p.sigma = prob->sigma; p.noise = prob->noise;
+    p.wave_k = prob->wave_k;
+    p.add_diag = prob->add_diag > 0.0 ? prob->add_diag : (double)N;
     return p;
+}
+
+static CovParams cov_params(const hicma_tlr_desc *A, const hicma_tlr_problem *prob) {
+    return make_cov_params(prob, A->d_pts, A->N, A->ndim);
 }
 
 static int gen_band_tiles(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_problem *prob) {
@@ -2188,9 +2199,7 @@ int hicma_tlr_k_cov(const hicma_tlr_problem *prob, const double *d_points, int N
     ARG_CHECK(r0 >= 0 && c0 >= 0 && r0 + nr <= N && c0 + nc <= N, "k_cov range");
     const int ndim = kind_ndim(prob->kind);
     ARG_CHECK(ndim > 0, "kind");
-    CovParams p;
-    p.pts = d_points; p.N = N; p.ndim = ndim; p.kind = prob->kind;
-    p.beta = prob->beta; p.sigma = prob->sigma; p.noise = prob->noise;
+    const CovParams p = make_cov_params(prob, d_points, N, ndim);
     CovTask t{d_out, ld, r0, c0, nr, nc};
     CovTask *dt = nullptr;
     cudaStream_t st = (cudaStream_t)stream;

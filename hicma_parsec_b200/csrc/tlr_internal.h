@@ -64,6 +64,7 @@ struct CovParams {
     const double *pts;  // [ndim][N]
     int N, ndim, kind;
     double beta, sigma, noise;
+    double wave_k, add_diag;   // electrodynamics kinds
 };
 void launch_cov_batched(const CovParams &p, const CovTask *d_tasks, int ntasks, int max_nr,
                         int max_nc, cudaStream_t st);

@@ -24,8 +24,8 @@ LIB_PATH = os.path.join(HERE, "lib", "libhicma_tlr.so")
 
 LOWER = 122
 UPPER = 121
-KIND_SQEXP_2D, KIND_SQEXP_3D, KIND_EXP_3D = 2, 3, 4
-KIND_NDIM = {2: 2, 3: 3, 4: 3}
+KIND_ED_SIN_2D, KIND_SQEXP_2D, KIND_SQEXP_3D, KIND_EXP_3D, KIND_ED_SIN_3D = 1, 2, 3, 4, 5
+KIND_NDIM = {1: 2, 2: 2, 3: 3, 4: 3, 5: 3}
 PREC_FP64, PREC_MIXED = 0, 1
 ERR_ARG, ERR_CUDA, ERR_OOM, ERR_RANK_OVERFLOW, ERR_TIMEOUT, ERR_STATE, ERR_NOT_SUPPORTED = -1, -2, -3, -4, -5, -6, -7
 
@@ -40,26 +40,32 @@ class TLRError(RuntimeError):
 
 class CProblem(C.Structure):
     _fields_ = [("kind", C.c_int), ("beta", C.c_double), ("nu", C.c_double), ("noise", C.c_double),
-                ("sigma", C.c_double), ("seed", C.c_ulonglong)]
+                ("sigma", C.c_double), ("seed", C.c_ulonglong), ("wave_k", C.c_double),
+                ("add_diag", C.c_double)]
 
 
 @dataclass
 class Problem:
-    """STARS-H spatial-statistics problem (``starsh_ssdata_generate`` arguments,
-    hicma_parsec/testing_dpotrf.c:300-358; defaults of the reference)."""
+    """STARS-H problem (``starsh_ssdata_generate`` / ``starsh_eddata_generate``
+    arguments, hicma_parsec/testing_dpotrf.c:300-365; defaults of the reference).
+    ``wave_k`` and ``add_diag`` apply to the electrodynamics kinds 1 and 5 only;
+    ``add_diag <= 0`` means N (hicma_parsec/hicma_parsec.c:289-291)."""
     kind: int = KIND_SQEXP_2D
     beta: float = 0.1
     nu: float = 0.5
     noise: float = 0.1
     sigma: float = 1.0
     seed: int = 0
+    wave_k: float = 50.0
+    add_diag: float = 0.0
 
     @property
     def ndim(self) -> int:
         return KIND_NDIM[self.kind]
 
     def c(self) -> CProblem:
-        return CProblem(self.kind, self.beta, self.nu, self.noise, self.sigma, self.seed)
+        return CProblem(self.kind, self.beta, self.nu, self.noise, self.sigma, self.seed, self.wave_k,
+                        self.add_diag)
 
 
 def _p(a):

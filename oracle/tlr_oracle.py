@@ -23,7 +23,8 @@ and restates from their published mathematics the absent third-party pieces:
 
 * STARS-H point placement (jittered grid + Morton order) and the squared
   exponential / exponential covariance kernels (call sites
-  ``testing_dpotrf.c:336-358``);
+  ``testing_dpotrf.c:336-358``) and the electrodynamics ``sin(k r) / r``
+  kernels in 2D and 3D (call sites ``testing_dpotrf.c:325-334,359-365``);
 * STARS-H ``starsh_dense_dlrrsdd`` rank rule: the smallest rank whose
   discarded singular values have Frobenius norm <= tol * (Frobenius norm of the
   sampled spectrum); a tile is rejected (rank -1, ``STARSH_gen.jdf:169-171``)
@@ -47,12 +48,14 @@ import numpy as np
 import scipy.linalg as sla
 
 # Problem kinds (``-D``), numbering of ``testing_dpotrf.c:12``.
+KIND_ED_SIN_2D = 1
 KIND_SQEXP_2D = 2
 KIND_SQEXP_3D = 3
 KIND_EXP_3D = 4
-KIND_NAMES = {KIND_SQEXP_2D: "st-2d-sqexp", KIND_SQEXP_3D: "st-3d-sqexp",
-              KIND_EXP_3D: "st-3d-exp"}
-KIND_NDIM = {KIND_SQEXP_2D: 2, KIND_SQEXP_3D: 3, KIND_EXP_3D: 3}
+KIND_ED_SIN_3D = 5
+KIND_NAMES = {KIND_ED_SIN_2D: "ed-2d-sin", KIND_SQEXP_2D: "st-2d-sqexp", KIND_SQEXP_3D: "st-3d-sqexp",
+              KIND_EXP_3D: "st-3d-exp", KIND_ED_SIN_3D: "ed-3d-sin"}
+KIND_NDIM = {KIND_ED_SIN_2D: 2, KIND_SQEXP_2D: 2, KIND_SQEXP_3D: 3, KIND_EXP_3D: 3, KIND_ED_SIN_3D: 3}
 
 FLUCTUATION = 0.66666667          # hicma_parsec_internal.h:107
 MORTON_BITS = 21
@@ -137,6 +140,8 @@ class Problem:
     noise: float = 0.1         # testing_dpotrf.c:305 (the reference's nugget)
     sigma: float = 1.0         # testing_dpotrf.c:306
     seed: int = 0
+    wave_k: float = 50.0       # electrodynamics wave number (hicma_parsec.c:188, flag -w)
+    add_diag: float = 0.0      # electrodynamics diagonal; <= 0 means N (hicma_parsec.c:289-291, flag -j)
 
     @property
     def ndim(self) -> int:
@@ -147,13 +152,24 @@ def cov_block(prob: Problem, pts: np.ndarray, r0: int, nr: int, c0: int, nc: int
     """Column-major covariance block A[r0:r0+nr, c0:c0+nc]; the nugget is
     added where the global row and column indices coincide.  Same call shape
     as ``kernel(nrows, ncols, irow, icol, data, data, out, ld)``
-    (``STARSH_gen.jdf:70-72``)."""
+    (``STARSH_gen.jdf:70-72``).
+
+    Electrodynamics kinds (``-D 1``, ``-D 5``): ``sin(k r) / r`` with ``k`` the
+    wave number, and ``add_diag`` (N when not positive) where ``r == 0``; no
+    nugget, no variance."""
     X = pts[r0:r0 + nr]
     Y = pts[c0:c0 + nc]
     r2 = np.zeros((nr, nc))
     for a in range(pts.shape[1]):
         d = X[:, a][:, None] - Y[:, a][None, :]
         r2 = r2 + d * d
+    if prob.kind in (KIND_ED_SIN_2D, KIND_ED_SIN_3D):
+        r = np.sqrt(r2)
+        diag = prob.add_diag if prob.add_diag > 0.0 else float(pts.shape[0])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            A = np.sin(prob.wave_k * r) / r
+        A[r2 == 0.0] = diag
+        return A
     if prob.kind == KIND_EXP_3D:
         A = prob.sigma * np.exp(-np.sqrt(r2) / prob.beta)
     else:

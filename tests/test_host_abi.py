@@ -40,7 +40,7 @@ def test_library_is_sm100a(lib):
     assert os.path.exists(build.LIB)
 
 
-@pytest.mark.parametrize("kind,n", [(2, 2700), (2, 10000), (3, 1000), (4, 4913), (3, 999)])
+@pytest.mark.parametrize("kind,n", [(2, 2700), (2, 10000), (3, 1000), (4, 4913), (3, 999), (1, 2700), (5, 1000)])
 def test_points_bit_identical(kind, n):
     from hicma_parsec_b200 import tlr
     P = tlr.points(tlr.Problem(kind=kind, seed=0), n)
@@ -73,3 +73,14 @@ def test_argument_errors_without_gpu(lib):
         tlr.points(tlr.Problem(kind=9), 10)
     G = np.zeros(4, np.int32)
     assert lib.hicma_tlr_band_autotune(None, 2, 10, 0) == tlr.ERR_ARG
+
+
+@pytest.mark.parametrize("kind", [0, 6, 7])
+def test_unbuilt_problem_kinds_are_argument_errors(lib, kind):
+    """randtlr (-D 0) and the RBF mesh problems (-D 6, 7) are not built: the C
+    library answers with an argument error, not with some other kernel."""
+    import ctypes as C
+    from hicma_parsec_b200 import tlr
+    buf = np.zeros(30)
+    prob = tlr.CProblem(kind, 0.1, 0.5, 0.1, 1.0, 0, 50.0, 0.0)
+    assert lib.hicma_tlr_points(C.byref(prob), 10, buf.ctypes.data_as(C.c_void_p)) == tlr.ERR_ARG

@@ -93,3 +93,24 @@ def test_generation_rejects_tiles_that_do_not_compress():
     O.band_regenerate(T, prob, pts, 2)
     for key in T2.U:
         assert np.allclose(T.U[key] @ T.V[key].T, T2.U[key] @ T2.V[key].T)
+
+
+@pytest.mark.parametrize("kind,k", [(1, 50.0), (5, 5.0)])
+def test_electrodynamics_kinds(kind, k):
+    """-D 1 / -D 5: sin(k r)/r with add_diag (default N) on the diagonal.  The
+    kernel is positive semi-definite in 2D and 3D, so the matrix is SPD with
+    smallest eigenvalue about N - k; the TLR factor meets the reference check."""
+    n, nb = 2700, 270
+    prob = O.Problem(kind=kind, wave_k=k)
+    pts = O.gen_points(n, O.KIND_NDIM[kind])
+    A = O.dense_matrix(prob, pts)
+    assert np.all(np.diag(A) == n) and np.allclose(A, A.T)
+    off = A[1, 0]
+    r = float(np.sqrt(np.sum((pts[1] - pts[0]) ** 2)))
+    assert off == np.sin(k * r) / r
+    assert np.linalg.eigvalsh(A)[0] >= n - k - 1e-6 * n
+    T, info = O.generate(prob, n, nb, 1e-8, 130, 1, pts)
+    assert info == 0
+    assert O.tlr_potrf(T, 1e-8).info == 0
+    assert O.check_dpotrf2(O.uncompress(T), A) <= 1e-8
+    assert O.dense_matrix(O.Problem(kind=kind, wave_k=k, add_diag=7.0), pts)[3, 3] == 7.0

@@ -1,0 +1,65 @@
+"""Electrodynamics problem kinds on the GPU (``-D 1`` ed-2d-sin, ``-D 5``
+ed-3d-sin; hicma_parsec/testing_dpotrf.c:325-334,359-365) against the oracle.
+
+A_ij = sin(k r)/r with r = |x_i - x_j| and add_diag (default N) where r == 0.
+Bars: tile entries within 1e-12 absolute of the oracle (CUDA's sin against the
+host libm; entries are at most k in size off the diagonal); generation ranks
+within +/-3 of the oracle's exact-SVD ranks; residual ||A - L L^T||_F / ||A||_F
+<= 10 e and log-determinant within 1e-8 relative of a dense FP64 Cholesky.
+"""
+import numpy as np
+import pytest
+
+from oracle import tlr_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+N, NB, TOL, MAXRANK = 2700, 270, 1e-8, 130
+CASES = [(1, 50.0), (5, 5.0)]       # (kind, wave number): ranks 50-104 and 40-49 at e = 1e-8
+
+
+@pytest.mark.parametrize("kind,k", CASES)
+def test_cov_tiles_match_oracle(kind, k):
+    from hicma_parsec_b200 import tlr
+    prob = tlr.Problem(kind=kind, wave_k=k)
+    P = tlr.points(prob, N)
+    dP = torch.from_numpy(P).cuda()
+    pts = P.T.copy()
+    oprob = O.Problem(kind=kind, wave_k=k)
+    st = torch.cuda.current_stream().cuda_stream
+    for (m, c) in [(0, 0), (3, 1), (9, 0), (5, 5)]:
+        out = torch.zeros((NB, NB), dtype=torch.float64, device="cuda")
+        rc = tlr.load_library().hicma_tlr_k_cov(prob.c(), dP.data_ptr(), N, m * NB, NB, c * NB, NB,
+                                               out.data_ptr(), NB, st)
+        assert rc == 0, tlr.last_error()
+        got = out.cpu().numpy().T
+        ref = O.cov_block(oprob, pts, m * NB, NB, c * NB, NB)
+        assert np.max(np.abs(got - ref)) <= 1e-12
+        if m == c:
+            assert np.all(np.diag(got) == float(N))
+
+
+@pytest.mark.parametrize("kind,k", CASES)
+def test_factorization_matches_oracle(ctx, kind, k):
+    from hicma_parsec_b200 import tlr
+    prob = tlr.Problem(kind=kind, wave_k=k)
+    A = tlr.TLRMatrix(ctx, N, NB, MAXRANK, 1)
+    try:
+        assert A.generate(prob, TOL, MAXRANK) == 0
+        oprob = O.Problem(kind=kind, wave_k=k)
+        pts = O.gen_points(N, O.KIND_NDIM[kind])
+        T, info = O.generate(oprob, N, NB, TOL, MAXRANK, 1, pts)
+        assert info == 0
+        G0, Gref = A.rank_map(), T.rank_array()
+        off = Gref >= 0
+        assert np.max(np.abs(G0[off] - Gref[off])) <= 3
+        assert A.potrf(TOL) == 0
+        Aexact = O.dense_matrix(oprob, pts)
+        res = O.check_dpotrf2(A.uncompress(), Aexact)
+        assert res <= 10 * TOL, res
+        ld_exact = 2.0 * np.sum(np.log(np.diag(np.linalg.cholesky(Aexact))))
+        assert abs(A.logdet() - ld_exact) / abs(ld_exact) <= 1e-8
+    finally:
+        A.close()
