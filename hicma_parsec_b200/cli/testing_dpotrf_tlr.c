@@ -35,9 +35,9 @@ static void usage(void) {
             " -G --genmaxrank   maxrank used in generation (default maxrank)\n"
             " -U --compmaxrank  maxrank of buffers (default maxrank)\n"
             " -f --fixedrank    fixed rank in recompression (0 = accuracy mode)\n"
-            " -D --kind_of_problem 1: ed-2d-sin 2: st-2d-sqexp 3: st-3d-sqexp 4: st-3d-exp 5: ed-3d-sin\n"
+            " -D --kind_of_problem 0: randtlr 1: ed-2d-sin 2: st-2d-sqexp 3: st-3d-sqexp 4: st-3d-exp 5: ed-3d-sin\n"
             " -w --wave_k       wave number of -D 1, 5 (default 50)\n"
-            " -j --add_diag     diagonal of -D 1, 5 (default N)\n"
+            " -j --add_diag     diagonal of -D 0, 1, 5 (default N)\n"
             " -Z --band         band size (default 1)\n"
             " -E --auto-band    auto-tune band size (default 1)\n"
             " -Y --lookahead    lookahead (-1: band size)\n"
@@ -118,7 +118,7 @@ int main(int argc, char **argv) {
     if (genmaxrank <= 0) genmaxrank = maxrank;
     if (compmaxrank <= 0) compmaxrank = maxrank;
     if (add_diag <= 0.0) add_diag = (double)N;   /* hicma_parsec.c:289-291 */
-    if (kind < 1 || kind > 5) { fprintf(stderr, "Wrong value of \"kind_of_problem\" parameter (1 to 5)\n"); return 1; }
+    if (kind < 0 || kind > 5) { fprintf(stderr, "Wrong value of \"kind_of_problem\" parameter (0 to 5)\n"); return 1; }
     if (N % NB != 0) { fprintf(stderr, "N must be a multiple of NB\n"); return 1; }
     const int NT = N / NB;
     const double flops = (N * (((1. / 6.) * N + 0.5) * N + (1. / 3.))) + (N * (((1. / 6.) * N) * N - (1. / 6.)));

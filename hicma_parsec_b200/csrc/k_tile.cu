@@ -8,7 +8,10 @@
 // nugget added where the global row and column indices coincide.  The
 // electrodynamics kinds restate starsh_eddata_block_sin_kernel_{2d,3d}
 // (hicma_parsec/testing_dpotrf.c:330,361): A_ij = sin(k r) / r, and add_diag
-// where r == 0.  Distances are accumulated with explicitly rounded operations
+// where r == 0.  randtlr (hicma_parsec/testing_dpotrf.c:315-321) reads a
+// basis instead of points: pts holds [Q | Q diag(S)] (N x 2K, column-major)
+// and A_ij = sum_k Q[i][k] (Q S)[j][k], plus add_diag where i == j.
+// Distances are accumulated with explicitly rounded operations
 // (no FMA contraction) so that they match the CPU restatement bit for bit;
 // exp/sin/sqrt are CUDA's.
 #include "tlr_internal.h"
@@ -27,6 +30,19 @@ __global__ void __launch_bounds__(COV_ROWS) k_cov_batched(CovParams p, const Cov
     const int c0 = blockIdx.y * COV_COLS;
     if (r >= t.nr || c0 >= t.nc) return;
     const int gr = t.r0 + r;
+    if (p.kind == HICMA_TLR_KIND_RANDTLR) {
+        const int K = p.ndim / 2;
+        const int cend = min(c0 + COV_COLS, t.nc);
+        for (int c = c0; c < cend; ++c) {
+            const int gc = t.c0 + c;
+            double acc = 0.0;
+            for (int k = 0; k < K; ++k)
+                acc = fma(p.pts[(size_t)k * p.N + gr], p.pts[(size_t)(K + k) * p.N + gc], acc);
+            if (gr == gc) acc += p.add_diag;
+            t.out[(size_t)r + (size_t)c * t.ld] = acc;
+        }
+        return;
+    }
     double xr[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) xr[a] = a < p.ndim ? p.pts[(size_t)a * p.N + gr] : 0.0;
@@ -78,6 +94,26 @@ __global__ void k_gaussian(double *out, int rows, int cols, int ld, unsigned lon
         const int r = (int)(i % rows), c = (int)(i / rows);
         out[(size_t)r + (size_t)c * ld] = g;
     }
+}
+
+// randtlr bases: block b of a chunk was factored in place (R on and above
+// the diagonal of Xr_b, NB x K, ld NB) and Q_b (NB x K) formed from its
+// reflectors.  Column j is flipped where R_jj < 0 (the unique thin QR with a
+// positive diagonal) and written to pts column j, and times decay^j to pts
+// column K + j, at global row (m0 + b) * NB + i.
+__global__ void k_randtlr_finish(const double *__restrict__ Xr, const double *__restrict__ Q, int nb, int K,
+                                 int m0, double *__restrict__ pts, int N, double decay) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y, b = blockIdx.z;
+    if (i >= nb || j >= K) return;
+    const size_t blk = (size_t)b * nb * K;
+    const double sg = Xr[blk + (size_t)j + (size_t)j * nb] < 0.0 ? -1.0 : 1.0;
+    double sj = 1.0;
+    for (int t = 0; t < j; ++t) sj *= decay;
+    const double q = Q[blk + (size_t)i + (size_t)j * nb] * sg;
+    const size_t row = (size_t)(m0 + b) * nb + i;
+    pts[(size_t)j * N + row] = q;
+    pts[(size_t)(K + j) * N + row] = q * sj;
 }
 
 constexpr int CP_COLS = 4;
@@ -259,6 +295,13 @@ void launch_gaussian(double *out, int rows, int cols, int ld, unsigned long long
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
     k_gaussian<<<blocks, 256, 0, st>>>(out, rows, cols, ld, seed);
+}
+
+void launch_randtlr_finish(const double *Xr, const double *Q, int nb, int K, int nblk, int m0, double *pts, int N,
+                           double decay, cudaStream_t st) {
+    if (nb <= 0 || K <= 0 || nblk <= 0) return;
+    dim3 grid((nb + 255) / 256, K, nblk);
+    k_randtlr_finish<<<grid, 256, 0, st>>>(Xr, Q, nb, K, m0, pts, N, decay);
 }
 
 void launch_copy_batched(const CopyTask *d_tasks, int ntasks, int max_cols, cudaStream_t st) {

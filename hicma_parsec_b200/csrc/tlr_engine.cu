@@ -715,6 +715,13 @@ int kind_ndim(int kind) {
     }
 }
 
+// Columns of the per-row data a problem's kernel reads: the point coordinates,
+// or for randtlr the basis [Q | Q diag(S)] of K = min(NB, RANDTLR_KMAX) columns.
+int data_ndim(int kind, int NB) {
+    if (kind == HICMA_TLR_KIND_RANDTLR) return 2 * std::min(NB, RANDTLR_KMAX);
+    return kind_ndim(kind);
+}
+
 int grid_side(long long n, int ndim) {
     long long s = std::max(1LL, (long long)llround(std::pow((double)n, 1.0 / ndim)));
     auto pw = [&](long long x) { long long r = 1; for (int i = 0; i < ndim; ++i) r *= x; return r; };
@@ -964,11 +971,61 @@ int hicma_tlr_desc_copy(hicma_tlr_ctx *c, const hicma_tlr_desc *src, hicma_tlr_d
     return ctx_sync(c);
 }
 
+// randtlr bases on the device (restated starsh_randtlr_generate,
+// hicma_parsec/testing_dpotrf.c:315-321): per block row m a Gaussian NB x K
+// matrix (counter generator, seed (seed ^ RANDTLR_SEED_XOR) + m), its
+// Householder QR, Q formed from the reflectors, column signs fixed by R's
+// diagonal, and Q diag(S) beside it.  Chunked over block rows to the arena.
+static int build_randtlr_basis(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_problem *prob) {
+    const int NB = A->NB, NT = A->NT, N = A->N;
+    const int K = std::min(NB, RANDTLR_KMAX);
+    const int pb = qr_panel_width(NB);
+    const size_t npan = (size_t)(K + pb - 1) / pb + 1;
+    const size_t mark = c->ar->off;
+    double *ident = ws_alloc<double>(c, (size_t)K * K);
+    if (!ident) { set_err("workspace too small for the randtlr bases"); return HICMA_TLR_ERR_OOM; }
+    launch_set_identity(ident, K, K, c->stream);
+    TRY(check_launch(c));
+    const size_t per_block = 2 * align_up(sizeof(double) * (size_t)NB * K + 1) + align_up(sizeof(double) * K + 1) +
+                             align_up(sizeof(double) * npan * pb * pb + 1) + 4096;
+    const int chunk = (int)std::min<size_t>((size_t)NT, ws_free(c) / per_block);
+    if (chunk < 1) { c->ar->off = mark; set_err("workspace too small for the randtlr bases"); return HICMA_TLR_ERR_OOM; }
+    const size_t inner = c->ar->off;
+    for (int m0 = 0; m0 < NT; m0 += chunk) {
+        c->ar->off = inner;
+        const int nblk = std::min(chunk, NT - m0);
+        double *G = ws_alloc<double>(c, (size_t)nblk * NB * K);
+        double *Q = ws_alloc<double>(c, (size_t)nblk * NB * K);
+        double *tau = ws_alloc<double>(c, (size_t)nblk * K);
+        double *T = ws_alloc<double>(c, (size_t)nblk * npan * pb * pb);
+        if (!G || !Q || !tau || !T) { c->ar->off = mark; set_err("workspace too small for the randtlr bases"); return HICMA_TLR_ERR_OOM; }
+        std::vector<QRTask> qr;
+        std::vector<QApplyTask> ap;
+        for (int b = 0; b < nblk; ++b) {
+            double *Gb = G + (size_t)b * NB * K;
+            double *Tb = T + (size_t)b * npan * pb * pb;
+            const unsigned long long sd = ((unsigned long long)prob->seed ^ RANDTLR_SEED_XOR) + (unsigned long long)(m0 + b);
+            launch_gaussian(Gb, NB, K, NB, sd, c->stream);
+            qr.push_back(QRTask{Gb, tau + (size_t)b * K, Tb, NB, K, NB});
+            ap.push_back(QApplyTask{Gb, Tb, ident, Q + (size_t)b * NB * K, nullptr, NB, K, NB, K, NB, K});
+        }
+        TRY(check_launch(c));
+        TRY(run_qr(c, qr, NB));
+        TRY(run_qapply(c, ap, NB));
+        launch_randtlr_finish(G, Q, NB, K, nblk, m0, A->d_pts, N, RANDTLR_DECAY, c->stream);
+        TRY(check_launch(c));
+    }
+    c->ar->off = mark;
+    return 0;
+}
+
 static int set_points(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_problem *prob, const double *points) {
-    const int ndim = kind_ndim(prob->kind);
-    ARG_CHECK(ndim > 0, "unsupported problem kind (-D 1, 2, 3, 4 or 5)");
+    const int ndim = data_ndim(prob->kind, A->NB);
+    ARG_CHECK(ndim > 0, "unsupported problem kind (-D 0, 1, 2, 3, 4 or 5)");
+    const bool randtlr = prob->kind == HICMA_TLR_KIND_RANDTLR;
+    ARG_CHECK(!(randtlr && points), "randtlr takes no points (its bases are built on the device)");
     std::vector<double> h;
-    if (!points) {
+    if (!points && !randtlr) {
         h.resize((size_t)ndim * A->N);
         TRY(hicma_tlr_points(prob, A->N, h.data()));
         points = h.data();
@@ -979,8 +1036,21 @@ static int set_points(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_probl
         CUDA_TRY(dev_alloc(c, (void **)&A->d_pts, (size_t)ndim * A->N * sizeof(double)));
     }
     A->ndim = ndim;
-    CUDA_TRY(cudaMemcpyAsync(A->d_pts, points, (size_t)ndim * A->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (randtlr) {
+        TRY(build_randtlr_basis(c, A, prob));
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(A->d_pts, points, (size_t)ndim * A->N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
     return ctx_sync(c);
+}
+
+// The descriptor's per-row data must be that of prob's kind (band
+// regeneration and the checks regenerate tiles from it).
+static int check_problem_data(const hicma_tlr_desc *A, const hicma_tlr_problem *prob) {
+    ARG_CHECK(A->d_pts, "no points: generate first");
+    ARG_CHECK(data_ndim(prob->kind, A->NB) == A->ndim && A->ndim > 0,
+              "problem kind differs from the one the descriptor was generated with");
+    return 0;
 }
 
 // Kernel parameters of a problem over N points.  A non-positive add_diag of
@@ -1108,6 +1178,9 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     CUDA_TRY(cudaSetDevice(c->device));
     if (info) *info = 0;
+    c->cur = c->stream;
+    c->ar = &c->main_ar;
+    ws_reset(c);
     TRY(set_points(c, A, prob, points));
     ws_reset(c);
     const int NT = A->NT, NB = A->NB;
@@ -1266,7 +1339,7 @@ int hicma_tlr_band_regenerate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, con
     ARG_CHECK(c && A && prob, "null");
     if (uplo != HICMA_TLR_LOWER) { set_err("only uplo = Lower is supported"); return HICMA_TLR_ERR_NOT_SUPPORTED; }
     ARG_CHECK(band_size >= A->slot_band, "band_size cannot shrink below the slot band");
-    ARG_CHECK(A->d_pts, "no points: generate first");
+    TRY(check_problem_data(A, prob));
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     const int NT = A->NT, NB = A->NB;
     band_size = std::min(band_size, NT);
@@ -2015,7 +2088,7 @@ int hicma_tlr_check_probe(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_p
                           unsigned long long seed, double *res_est) {
     ARG_CHECK(c && L && prob && res_est && nprobe >= 1 && nprobe <= 64, "check_probe arguments");
     if (!L->factored) { set_err("descriptor is not factored"); return HICMA_TLR_ERR_STATE; }
-    ARG_CHECK(L->d_pts, "no points");
+    TRY(check_problem_data(L, prob));
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     CUDA_TRY(cudaSetDevice(c->device));
     c->cur = c->stream;
@@ -2140,7 +2213,7 @@ int hicma_tlr_check(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_problem
                     double *res_llt, double *res_diff) {
     ARG_CHECK(c && L && prob, "null");
     if (!L->factored) { set_err("descriptor is not factored"); return HICMA_TLR_ERR_STATE; }
-    ARG_CHECK(L->d_pts, "no points");
+    TRY(check_problem_data(L, prob));
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     CUDA_TRY(cudaSetDevice(c->device));
     const size_t N = L->N;
@@ -2198,7 +2271,7 @@ int hicma_tlr_k_cov(const hicma_tlr_problem *prob, const double *d_points, int N
     ARG_CHECK(prob && d_points && d_out && N > 0 && nr >= 0 && nc >= 0 && ld >= nr, "k_cov arguments");
     ARG_CHECK(r0 >= 0 && c0 >= 0 && r0 + nr <= N && c0 + nc <= N, "k_cov range");
     const int ndim = kind_ndim(prob->kind);
-    ARG_CHECK(ndim > 0, "kind");
+    ARG_CHECK(ndim > 0, "kind (randtlr tiles come from hicma_tlr_generate: no points)");
     const CovParams p = make_cov_params(prob, d_points, N, ndim);
     CovTask t{d_out, ld, r0, c0, nr, nc};
     CovTask *dt = nullptr;

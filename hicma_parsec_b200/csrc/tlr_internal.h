@@ -71,6 +71,14 @@ void launch_cov_batched(const CovParams &p, const CovTask *d_tasks, int ntasks, 
 // Gaussian N(0,1) matrix (counter based, seeded), column-major rows x cols.
 void launch_gaussian(double *out, int rows, int cols, int ld, unsigned long long seed,
                      cudaStream_t st);
+// randtlr bases of nblk block rows from their in-place QRs Xr and formed Q
+// factors (each NB x K, ld NB, consecutive): pts[:, j] = sign(R_jj) Q[:, j],
+// pts[:, K + j] = decay^j pts[:, j] at rows (m0 + b) * NB + i.  pts is N x 2K.
+void launch_randtlr_finish(const double *Xr, const double *Q, int nb, int K, int nblk, int m0, double *pts, int N,
+                           double decay, cudaStream_t st);
+constexpr int RANDTLR_KMAX = 64;            // singular directions kept (0.5^64 is below FP64 resolution)
+constexpr double RANDTLR_DECAY = 0.5;       // hicma_parsec/testing_dpotrf.c:318
+constexpr unsigned long long RANDTLR_SEED_XOR = 0x52414E44544C5200ull;
 
 // --------------------------------------------------------------- copies -----
 struct CopyTask {

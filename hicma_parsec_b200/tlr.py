@@ -24,8 +24,8 @@ LIB_PATH = os.path.join(HERE, "lib", "libhicma_tlr.so")
 
 LOWER = 122
 UPPER = 121
-KIND_ED_SIN_2D, KIND_SQEXP_2D, KIND_SQEXP_3D, KIND_EXP_3D, KIND_ED_SIN_3D = 1, 2, 3, 4, 5
-KIND_NDIM = {1: 2, 2: 2, 3: 3, 4: 3, 5: 3}
+KIND_RANDTLR, KIND_ED_SIN_2D, KIND_SQEXP_2D, KIND_SQEXP_3D, KIND_EXP_3D, KIND_ED_SIN_3D = 0, 1, 2, 3, 4, 5
+KIND_NDIM = {1: 2, 2: 2, 3: 3, 4: 3, 5: 3}     # point kinds; randtlr has no points
 PREC_FP64, PREC_MIXED = 0, 1
 ERR_ARG, ERR_CUDA, ERR_OOM, ERR_RANK_OVERFLOW, ERR_TIMEOUT, ERR_STATE, ERR_NOT_SUPPORTED = -1, -2, -3, -4, -5, -6, -7
 
@@ -48,8 +48,9 @@ class CProblem(C.Structure):
 class Problem:
     """STARS-H problem (``starsh_ssdata_generate`` / ``starsh_eddata_generate``
     arguments, hicma_parsec/testing_dpotrf.c:300-365; defaults of the reference).
-    ``wave_k`` and ``add_diag`` apply to the electrodynamics kinds 1 and 5 only;
-    ``add_diag <= 0`` means N (hicma_parsec/hicma_parsec.c:289-291)."""
+    ``wave_k`` applies to the electrodynamics kinds 1 and 5, ``add_diag`` to them
+    and to randtlr (kind 0); ``add_diag <= 0`` means N
+    (hicma_parsec/hicma_parsec.c:289-291)."""
     kind: int = KIND_SQEXP_2D
     beta: float = 0.1
     nu: float = 0.5

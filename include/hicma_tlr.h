@@ -46,8 +46,9 @@ extern "C" {
 #define HICMA_TLR_UPPER 121
 #define HICMA_TLR_LOWER 122
 
-/* -D problem kinds (hicma_parsec/testing_dpotrf.c:12, :325-365).  Kinds 0
- * (randtlr) and 6, 7 (RBF meshes) are rejected with HICMA_TLR_ERR_ARG. */
+/* -D problem kinds (hicma_parsec/testing_dpotrf.c:12, :315-365).  Kinds 6, 7
+ * (RBF meshes) are rejected with HICMA_TLR_ERR_ARG. */
+#define HICMA_TLR_KIND_RANDTLR   0   /* random TLR, equal ranks (testing_dpotrf.c:315-321) */
 #define HICMA_TLR_KIND_ED_SIN_2D 1   /* sin(k r)/r, 2D (testing_dpotrf.c:325-334) */
 #define HICMA_TLR_KIND_SQEXP_2D  2
 #define HICMA_TLR_KIND_SQEXP_3D  3
@@ -62,10 +63,15 @@ extern "C" {
 typedef struct hicma_tlr_ctx_s  hicma_tlr_ctx;   /* device, stream, workspace      */
 typedef struct hicma_tlr_desc_s hicma_tlr_desc;  /* device tile store of a matrix */
 
-/* STARS-H problem (starsh_ssdata_generate / starsh_eddata_generate arguments,
- * hicma_parsec/testing_dpotrf.c:300-365).  Spatial statistics (kinds 2-4):
- * A_ij = sigma * k(|x_i - x_j|) + noise * [i == j].  Electrodynamics (kinds 1, 5):
- * A_ij = sin(wave_k * r) / r with r = |x_i - x_j|, and add_diag where r == 0. */
+/* STARS-H problem (starsh_ssdata_generate / starsh_eddata_generate /
+ * starsh_randtlr_generate arguments, hicma_parsec/testing_dpotrf.c:300-365).
+ * Spatial statistics (kinds 2-4): A_ij = sigma * k(|x_i - x_j|) + noise * [i == j].
+ * Electrodynamics (kinds 1, 5): A_ij = sin(wave_k * r) / r with r = |x_i - x_j|,
+ * and add_diag where r == 0.  randtlr (kind 0): tile (m, n) = Q_m diag(S) Q_n^T
+ * + add_diag * [m == n] I, Q_m a random orthonormal basis of block row m
+ * (first min(NB, 64) columns; seeded by seed), S_k = 0.5^k (decay of
+ * testing_dpotrf.c:318).  randtlr has no points: hicma_tlr_points rejects it
+ * and hicma_tlr_generate builds the bases on the device (points must be NULL). */
 typedef struct {
     int    kind;      /* HICMA_TLR_KIND_*                                   */
     double beta;      /* length scale (reference default 0.1)               */
@@ -73,8 +79,8 @@ typedef struct {
     double noise;     /* nugget added on the diagonal (reference 0.1)       */
     double sigma;     /* variance (default 1.0)                             */
     unsigned long long seed;  /* point placement seed (reference srand(0)) */
-    double wave_k;    /* wave number of kinds 1, 5 (default 50, hicma_parsec.c:188)     */
-    double add_diag;  /* diagonal of kinds 1, 5; <= 0 means N (hicma_parsec.c:289-291) */
+    double wave_k;    /* wave number of kinds 1, 5 (default 50, hicma_parsec.c:188)        */
+    double add_diag;  /* diagonal of kinds 0, 1, 5; <= 0 means N (hicma_parsec.c:289-291) */
 } hicma_tlr_problem;
 
 /* ---------------------------------------------------------------- setup -- */

@@ -21,6 +21,10 @@ dense factorization at run time).  This module therefore restates:
 
 and restates from their published mathematics the absent third-party pieces:
 
+* STARS-H ``randtlr`` (``-D 0``, ``testing_dpotrf.c:315-321``): per tile row a
+  random orthonormal basis Q_m, singular values S_k = 0.5**k, tiles
+  Q_m diag(S) Q_n^T plus ``add_diag`` on the diagonal (see
+  :func:`randtlr_basis`);
 * STARS-H point placement (jittered grid + Morton order) and the squared
   exponential / exponential covariance kernels (call sites
   ``testing_dpotrf.c:336-358``) and the electrodynamics ``sin(k r) / r``
@@ -48,15 +52,19 @@ import numpy as np
 import scipy.linalg as sla
 
 # Problem kinds (``-D``), numbering of ``testing_dpotrf.c:12``.
+KIND_RANDTLR = 0
 KIND_ED_SIN_2D = 1
 KIND_SQEXP_2D = 2
 KIND_SQEXP_3D = 3
 KIND_EXP_3D = 4
 KIND_ED_SIN_3D = 5
-KIND_NAMES = {KIND_ED_SIN_2D: "ed-2d-sin", KIND_SQEXP_2D: "st-2d-sqexp", KIND_SQEXP_3D: "st-3d-sqexp",
+KIND_NAMES = {KIND_RANDTLR: "randtlr", KIND_ED_SIN_2D: "ed-2d-sin", KIND_SQEXP_2D: "st-2d-sqexp", KIND_SQEXP_3D: "st-3d-sqexp",
               KIND_EXP_3D: "st-3d-exp", KIND_ED_SIN_3D: "ed-3d-sin"}
 KIND_NDIM = {KIND_ED_SIN_2D: 2, KIND_SQEXP_2D: 2, KIND_SQEXP_3D: 3, KIND_EXP_3D: 3, KIND_ED_SIN_3D: 3}
 
+RANDTLR_DECAY = 0.5               # testing_dpotrf.c:318
+RANDTLR_KMAX = 64                 # singular directions kept: 0.5**64 is below FP64 resolution
+RANDTLR_SEED_XOR = 0x52414E44544C5200
 FLUCTUATION = 0.66666667          # hicma_parsec_internal.h:107
 MORTON_BITS = 21
 
@@ -148,6 +156,58 @@ class Problem:
         return KIND_NDIM[self.kind]
 
 
+def gaussian_counter(seed: int, rows: int, cols: int) -> np.ndarray:
+    """rows x cols standard normals, column-major counter i = r + c * rows:
+    Box-Muller on u1 = (53 high bits of mix64(mix64(seed) + 2i) + 1) 2**-53 and
+    u2 = (53 high bits of mix64(mix64(seed) + 2i + 1)) 2**-53, g = sqrt(-2 ln u1)
+    cos(2 pi u2).  The same generator fills the device's sketch matrices."""
+    i = np.arange(rows * cols, dtype=np.uint64)
+    base = _mix64(np.array([seed], dtype=np.uint64))[0]
+    with np.errstate(over="ignore"):
+        z1 = _mix64(base + np.uint64(2) * i)
+        z2 = _mix64(base + np.uint64(2) * i + np.uint64(1))
+    u1 = ((z1 >> np.uint64(11)).astype(np.float64) + 1.0) * (2.0 ** -53)
+    u2 = (z2 >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
+    g = np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+    return g.reshape(cols, rows).T
+
+
+def randtlr_basis(n: int, nb: int, seed: int = 0) -> np.ndarray:
+    """STARS-H ``starsh_randtlr_generate(data, N, NB, decay=0.5, add_diag)``
+    (``testing_dpotrf.c:315-321``), restated: every block row m gets an
+    orthonormal NB x NB basis Q_m from the QR of a Gaussian matrix, and the
+    singular values are S_0 = 1, S_k = S_{k-1} * decay, so every off-diagonal
+    tile Q_m diag(S) Q_n^T has the same spectrum (the "equal ranks" problem).
+
+    Only the first K = min(NB, 64) columns of each Q_m are formed (the first K
+    columns of a QR depend only on the first K columns of its input, and
+    0.5**64 is far below the FP64 resolution of the tile entries).  The
+    Gaussian input of block m comes from :func:`gaussian_counter` with seed
+    ``(seed ^ RANDTLR_SEED_XOR) + m``; column signs are fixed so that R has a
+    positive diagonal (the unique thin QR).  Returns the (n, 2K) array
+    [Q | Q diag(S)], which plays the part of the points array."""
+    if n % nb != 0:
+        raise ValueError("N must be a multiple of NB")
+    K = min(nb, RANDTLR_KMAX)
+    S = RANDTLR_DECAY ** np.arange(K, dtype=np.float64)
+    out = np.empty((n, 2 * K))
+    for m in range(n // nb):
+        sd = ((seed ^ RANDTLR_SEED_XOR) + m) & 0xFFFFFFFFFFFFFFFF
+        Q, R = np.linalg.qr(gaussian_counter(sd, nb, K))
+        Q = Q * np.where(np.diag(R) < 0.0, -1.0, 1.0)
+        out[m * nb:(m + 1) * nb, :K] = Q
+        out[m * nb:(m + 1) * nb, K:] = Q * S
+    return out
+
+
+def problem_points(prob: "Problem", n: int, nb: int) -> np.ndarray:
+    """The per-row data a problem's kernel reads: points (n, ndim) for the
+    point kernels, the (n, 2K) basis for randtlr."""
+    if prob.kind == KIND_RANDTLR:
+        return randtlr_basis(n, nb, prob.seed)
+    return gen_points(n, prob.ndim, prob.seed)
+
+
 def cov_block(prob: Problem, pts: np.ndarray, r0: int, nr: int, c0: int, nc: int) -> np.ndarray:
     """Column-major covariance block A[r0:r0+nr, c0:c0+nc]; the nugget is
     added where the global row and column indices coincide.  Same call shape
@@ -156,9 +216,19 @@ def cov_block(prob: Problem, pts: np.ndarray, r0: int, nr: int, c0: int, nc: int
 
     Electrodynamics kinds (``-D 1``, ``-D 5``): ``sin(k r) / r`` with ``k`` the
     wave number, and ``add_diag`` (N when not positive) where ``r == 0``; no
-    nugget, no variance."""
+    nugget, no variance.  randtlr (``-D 0``): ``pts`` is the basis of
+    :func:`randtlr_basis` and the block is Q[rows] (Q diag(S))[cols]^T with
+    ``add_diag`` where the global indices coincide."""
     X = pts[r0:r0 + nr]
     Y = pts[c0:c0 + nc]
+    if prob.kind == KIND_RANDTLR:
+        K = pts.shape[1] // 2
+        A = X[:, :K] @ Y[:, K:].T
+        lo, hi = max(r0, c0), min(r0 + nr, c0 + nc)
+        if lo < hi:
+            i = np.arange(lo, hi)
+            A[i - r0, i - c0] += prob.add_diag if prob.add_diag > 0.0 else float(pts.shape[0])
+        return A
     r2 = np.zeros((nr, nc))
     for a in range(pts.shape[1]):
         d = X[:, a][:, None] - Y[:, a][None, :]
@@ -347,7 +417,7 @@ def generate(prob: Problem, n: int, nb: int, tol: float, maxrank: int, band: int
     if n % nb != 0:
         raise ValueError("N must be a multiple of NB")
     if pts is None:
-        pts = gen_points(n, prob.ndim, prob.seed)
+        pts = problem_points(prob, n, nb)
     T = TLRMatrix(n, nb, band, maxrank)
     nt = n // nb
     info = 0

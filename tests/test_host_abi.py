@@ -76,9 +76,10 @@ def test_argument_errors_without_gpu(lib):
 
 
 @pytest.mark.parametrize("kind", [0, 6, 7])
-def test_unbuilt_problem_kinds_are_argument_errors(lib, kind):
-    """randtlr (-D 0) and the RBF mesh problems (-D 6, 7) are not built: the C
-    library answers with an argument error, not with some other kernel."""
+def test_kinds_without_points_are_argument_errors(lib, kind):
+    """randtlr (-D 0) has no points (its bases are built on the device by the
+    generator); the RBF mesh problems (-D 6, 7) are not built.  The C library
+    answers hicma_tlr_points with an argument error for all three."""
     import ctypes as C
     from hicma_parsec_b200 import tlr
     buf = np.zeros(30)

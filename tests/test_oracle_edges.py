@@ -114,3 +114,41 @@ def test_electrodynamics_kinds(kind, k):
     assert O.tlr_potrf(T, 1e-8).info == 0
     assert O.check_dpotrf2(O.uncompress(T), A) <= 1e-8
     assert O.dense_matrix(O.Problem(kind=kind, wave_k=k, add_diag=7.0), pts)[3, 3] == 7.0
+
+
+def test_gaussian_counter_generator():
+    """The counter generator shared with the device sketches: u2 of entry i is
+    the uniform of counter 2i + 1, and the sample moments are those of N(0, 1)."""
+    g = O.gaussian_counter(123, 300, 200)
+    assert g.shape == (300, 200)
+    assert abs(g.mean()) < 0.01 and abs(g.var() - 1.0) < 0.02
+    u = O.uniform01(123, np.array([1, 3]))
+    assert np.all((u >= 0.0) & (u < 1.0))
+    assert np.array_equal(O.gaussian_counter(123, 300, 200), g)
+    assert not np.array_equal(O.gaussian_counter(124, 300, 200), g)
+
+
+def test_randtlr_equal_ranks_and_factor():
+    """-D 0: orthonormal per-block bases, every off-band tile with spectrum
+    0.5^k, hence one rank everywhere (27 at e = 1e-8), and a factor that meets
+    the reference check."""
+    n, nb = 2700, 270
+    prob = O.Problem(kind=O.KIND_RANDTLR)
+    B = O.problem_points(prob, n, nb)
+    K = 64
+    assert B.shape == (n, 2 * K)
+    for m in (0, 7):
+        Q = B[m * nb:(m + 1) * nb, :K]
+        assert np.allclose(Q.T @ Q, np.eye(K), atol=1e-13)
+        assert np.allclose(B[m * nb:(m + 1) * nb, K:], Q * 0.5 ** np.arange(K))
+    s = np.linalg.svd(O.cov_block(prob, B, 5 * nb, nb, 2 * nb, nb), compute_uv=False)
+    assert np.allclose(s[:30], 0.5 ** np.arange(30), rtol=1e-12, atol=1e-15)
+    A = O.dense_matrix(prob, B)
+    assert np.all((np.diag(A) > n) & (np.diag(A) < n + 1.0))       # add_diag defaults to N
+    T, info = O.generate(prob, n, nb, 1e-8, 130, 1, B)
+    assert info == 0
+    assert {T.rank(m, c) for (m, c) in T.U} == {27}
+    assert O.tlr_potrf(T, 1e-8).info == 0
+    assert O.check_dpotrf2(O.uncompress(T), A) <= 1e-8
+    small = O.problem_points(prob, 120, 40)                         # K = min(NB, 64) = 40
+    assert small.shape == (120, 80)

@@ -1,8 +1,9 @@
-"""Electrodynamics problem kinds on the GPU (``-D 1`` ed-2d-sin, ``-D 5``
-ed-3d-sin; hicma_parsec/testing_dpotrf.c:325-334,359-365) against the oracle.
+"""Problem kinds beyond the statistics kernels on the GPU, against the oracle:
+electrodynamics (``-D 1`` ed-2d-sin, ``-D 5`` ed-3d-sin;
+hicma_parsec/testing_dpotrf.c:325-334,359-365) and randtlr (``-D 0``, :315-321).
 
-A_ij = sin(k r)/r with r = |x_i - x_j| and add_diag (default N) where r == 0.
-Bars: tile entries within 1e-12 absolute of the oracle (CUDA's sin against the
+Electrodynamics: A_ij = sin(k r)/r with r = |x_i - x_j| and add_diag (default N)
+where r == 0.  Bars: tile entries within 1e-12 absolute of the oracle (CUDA's sin against the
 host libm; entries are at most k in size off the diagonal); generation ranks
 within +/-3 of the oracle's exact-SVD ranks; residual ||A - L L^T||_F / ||A||_F
 <= 10 e and log-determinant within 1e-8 relative of a dense FP64 Cholesky.
@@ -59,6 +60,37 @@ def test_factorization_matches_oracle(ctx, kind, k):
         Aexact = O.dense_matrix(oprob, pts)
         res = O.check_dpotrf2(A.uncompress(), Aexact)
         assert res <= 10 * TOL, res
+        ld_exact = 2.0 * np.sum(np.log(np.diag(np.linalg.cholesky(Aexact))))
+        assert abs(A.logdet() - ld_exact) / abs(ld_exact) <= 1e-8
+    finally:
+        A.close()
+
+
+def test_randtlr_matches_oracle(ctx):
+    """-D 0 randtlr (testing_dpotrf.c:315-321): the device builds the per-block
+    bases (Gaussian -> Householder QR -> Q with R's diagonal made positive);
+    band tiles within 1e-14 absolute of the oracle off the diagonal (entries
+    are about 1/NB) and 1e-11 on it (add_diag = N); every off-band tile has the
+    spectrum 0.5^k, so every rank is 27 at e = 1e-8; the factor meets the
+    residual and log-determinant bars."""
+    from hicma_parsec_b200 import tlr
+    prob = tlr.Problem(kind=tlr.KIND_RANDTLR)
+    oprob = O.Problem(kind=O.KIND_RANDTLR)
+    B = O.problem_points(oprob, N, NB)
+    A = tlr.TLRMatrix(ctx, N, NB, MAXRANK, 2)
+    try:
+        assert A.generate(prob, TOL, MAXRANK) == 0
+        for (m, n) in [(0, 0), (4, 3), (9, 8), (9, 9)]:
+            ref = O.cov_block(oprob, B, m * NB, NB, n * NB, NB)
+            got = A.tile(m, n)
+            bar = 1e-11 if m == n else 1e-14
+            assert np.max(np.abs(got - ref)) <= bar, (m, n)
+        G = A.rank_map()
+        ranks = {int(G[n * (N // NB) + m]) for m in range(2, N // NB) for n in range(0, m - 1)}
+        assert ranks == {27}
+        assert A.potrf(TOL) == 0
+        Aexact = O.dense_matrix(oprob, B)
+        assert O.check_dpotrf2(A.uncompress(), Aexact) <= 10 * TOL
         ld_exact = 2.0 * np.sum(np.log(np.diag(np.linalg.cholesky(Aexact))))
         assert abs(A.logdet() - ld_exact) / abs(ld_exact) <= 1e-8
     finally:
