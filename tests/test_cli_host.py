@@ -1,0 +1,46 @@
+"""The testing_dpotrf_tlr driver's argument handling, which runs before any
+GPU call (options of hicma_parsec/hicma_parsec.c:89-309): usage text, problem
+kind range, required sizes.  CPU only."""
+import os
+import subprocess
+
+import pytest
+
+
+@pytest.fixture(scope="module")
+def cli():
+    from hicma_parsec_b200 import build
+    if not os.path.exists(build.CLI):
+        pytest.skip("driver not built")
+    return build.CLI
+
+
+def run(cli, *args):
+    return subprocess.run([cli, *args], capture_output=True, text=True, timeout=60)
+
+
+def test_usage_lists_problem_kinds(cli):
+    r = run(cli, "-h")
+    assert r.returncode == 0
+    for name in ("randtlr", "ed-2d-sin", "st-2d-sqexp", "st-3d-sqexp", "st-3d-exp", "ed-3d-sin"):
+        assert name in r.stderr
+    assert "--wave_k" in r.stderr and "--add_diag" in r.stderr
+
+
+@pytest.mark.parametrize("kind", ["6", "7", "-1"])
+def test_unsupported_kind_is_rejected_before_gpu_use(cli, kind):
+    r = run(cli, "-N", "2700", "-t", "270", "-D", kind)
+    assert r.returncode == 1
+    assert "kind_of_problem" in r.stderr
+
+
+def test_sizes_are_required(cli):
+    r = run(cli, "-e", "1e-8")
+    assert r.returncode == 1
+    assert "NB" in r.stderr
+
+
+def test_n_must_be_a_multiple_of_nb(cli):
+    r = run(cli, "-N", "2701", "-t", "270", "-D", "2")
+    assert r.returncode == 1
+    assert "multiple" in r.stderr
