@@ -1,4 +1,5 @@
-"""Continuous-batching maximum-likelihood serving on one GPU.
+"""Continuous-batching maximum-likelihood serving on one GPU, and a replica
+router over the GPUs of a node.
 
 No counterpart in the reference (its driver stops at the factor,
 hicma_parsec/testing_dpotrf.c:830-903).  Each request is one Gaussian
@@ -69,6 +70,7 @@ class MLEResult:
     t_admit: float = 0.0
     t_done: float = 0.0
     latency: float = 0.0
+    device: int = -1
     gpu_s: dict = field(default_factory=dict)
 
 
@@ -151,70 +153,160 @@ def solve_request(ctx: tlr.Context, req: MLERequest) -> MLEResult:
     return res
 
 
-class MLEServer:
-    """Admission-controlled concurrent request loop on one GPU."""
+class ReplicaRouter:
+    """Routes a request stream over the GPUs of one node as replicas: every
+    request runs whole on one GPU and no data crosses between GPUs.
 
-    def __init__(self, device: int = 0, slots: int = 4, hbm_budget: int | None = None,
-                 workspace_bytes: int = 2 << 30):
-        self.device = device
+    Each GPU has `slots` contexts and an HBM budget.  A request is admitted to
+    the healthy GPU that has a free slot and the most budget left after taking
+    the request's footprint (ties go to the lower device index).  A request
+    larger than a GPU's whole budget is admitted only to an idle GPU and runs
+    there alone.  A solve that fails at the CUDA level (status ERR_CUDA, or an
+    exception out of the solve) marks its GPU failed: the GPU takes no further
+    requests, its contexts are not reused, and the request is routed once more
+    to another healthy GPU.  When no healthy GPU is left, the remaining
+    requests complete with status ERR_CUDA.
+
+    `make_context(device)`, `solve(ctx, req)` and `footprint(req)` default to
+    the library's context, :func:`solve_request` and :func:`footprint_bytes`.
+    """
+
+    def __init__(self, devices=(0,), slots: int = 4, hbm_budgets=None, workspace_bytes: int = 2 << 30,
+                 make_context=None, solve=None, footprint=None):
+        self.devices = list(devices)
         self.slots = slots
         self.workspace_bytes = workspace_bytes
-        if hbm_budget is None:
+        self._solve = solve or solve_request
+        self._footprint = footprint or footprint_bytes
+        make_context = make_context or (lambda d: tlr.Context(d, workspace_bytes))
+        if hbm_budgets is None:
             import torch
-            free, _ = torch.cuda.mem_get_info(device)
-            hbm_budget = int(0.8 * free) - slots * workspace_bytes
-        self.hbm_budget = hbm_budget
-        self._ctxs = [tlr.Context(device, workspace_bytes) for _ in range(slots)]
+            hbm_budgets = []
+            for d in self.devices:
+                free, _ = torch.cuda.mem_get_info(d)
+                hbm_budgets.append(int(0.8 * free) - slots * workspace_bytes)
+        self.hbm_budgets = [int(b) for b in hbm_budgets]
+        if len(self.hbm_budgets) != len(self.devices):
+            raise ValueError("one HBM budget per device")
+        self._ctxs = {i: [make_context(d) for _ in range(slots)] for i, d in enumerate(self.devices)}
+        self.failed: set = set()        # indices into devices
 
     def close(self):
-        for c in self._ctxs:
-            c.close()
-        self._ctxs = []
+        for ctxs in self._ctxs.values():
+            for c in ctxs:
+                try:
+                    c.close()
+                except Exception:       # a failed GPU may refuse; the others still close
+                    pass
+        self._ctxs = {}
+
+    def _choose(self, fp: int, free, budget, exclude) -> int | None:
+        best = None
+        for i in range(len(self.devices)):
+            if i in self.failed or i in exclude or not free[i]:
+                continue
+            full = self.hbm_budgets[i]
+            if fp > budget[i] and budget[i] < full:
+                continue
+            room = budget[i] - fp
+            if best is None or room > best[0]:
+                best = (room, i)
+        return None if best is None else best[1]
 
     def run(self, requests: list[MLERequest], realtime: bool = True) -> list[MLEResult]:
         """Serve `requests` (sorted by arrival).  With realtime=False all
         requests are available at t=0 (saturation).  Returns results in
-        request order with admission, completion and latency times."""
+        request order with admission and completion times, latency and the
+        device each ran on."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         results: dict[int, MLEResult] = {}
-        free_ctx: "queue.Queue[tlr.Context]" = queue.Queue()
-        for c in self._ctxs:
-            free_ctx.put(c)
-        budget = [self.hbm_budget]
+        free = {i: list(self._ctxs.get(i, [])) for i in range(len(self.devices))}
+        budget = list(self.hbm_budgets)
         cv = threading.Condition()
         t0 = time.perf_counter()
+        admit_time: dict[int, float] = {}
+        threads: list[threading.Thread] = []
 
-        def worker(req, ctx, fp):
-            r = solve_request(ctx, req)
+        def no_device_result(req):
+            r = MLEResult(rid=req.rid, n=req.n, status=tlr.ERR_CUDA, error="no healthy GPU left")
+            r.t_done = time.perf_counter() - t0
+            r.latency = r.t_done - (req.arrival if realtime else 0.0)
+            return r
+
+        def admit(req, exclude):
+            """Block until a GPU takes `req`; returns (device index, ctx, fp) or None."""
+            fp = self._footprint(req)
+            with cv:
+                while True:
+                    healthy = [i for i in range(len(self.devices)) if i not in self.failed and i not in exclude]
+                    if not healthy:
+                        return None
+                    i = self._choose(fp, free, budget, exclude)
+                    if i is not None:
+                        budget[i] -= fp
+                        return i, free[i].pop(), fp
+                    cv.wait()
+
+        def worker(req, i, ctx, fp, tried):
+            try:
+                r = self._solve(ctx, req)
+                device_fault = r.status == tlr.ERR_CUDA
+            except Exception as e:          # a failing solve must not take the router down
+                r = MLEResult(rid=req.rid, n=req.n, status=tlr.ERR_CUDA, error=f"{type(e).__name__}: {e}")
+                device_fault = True
+            with cv:
+                budget[i] += fp
+                if device_fault:
+                    self.failed.add(i)
+                    free[i] = []
+                else:
+                    free[i].append(ctx)
+                cv.notify_all()
+            if device_fault and len(tried) < 2:
+                nxt = admit(req, exclude=set(tried))
+                if nxt is not None:
+                    j, ctx2, fp2 = nxt
+                    worker(req, j, ctx2, fp2, tried + [j])
+                    return
+                r.error += "; no other healthy GPU to retry on"
+            r.device = self.devices[i]
             r.t_admit = admit_time[req.rid]
             r.t_done = time.perf_counter() - t0
             r.latency = r.t_done - (req.arrival if realtime else 0.0)
             with cv:
                 results[req.rid] = r
-                budget[0] += fp
-                free_ctx.put(ctx)
                 cv.notify_all()
 
-        admit_time = {}
-        threads = []
         for req in reqs:
             if realtime:
                 wait = req.arrival - (time.perf_counter() - t0)
                 if wait > 0:
                     time.sleep(wait)
-            fp = footprint_bytes(req)
-            with cv:
-                while free_ctx.empty() or (fp > budget[0] and budget[0] < self.hbm_budget):
-                    cv.wait()
-                budget[0] -= fp
-                ctx = free_ctx.get()
+            got = admit(req, exclude=set())
+            if got is None:
+                with cv:
+                    results[req.rid] = no_device_result(req)
+                continue
+            i, ctx, fp = got
             admit_time[req.rid] = time.perf_counter() - t0
-            th = threading.Thread(target=worker, args=(req, ctx, fp), daemon=True)
+            th = threading.Thread(target=worker, args=(req, i, ctx, fp, [i]), daemon=True)
             th.start()
             threads.append(th)
         for th in threads:
             th.join()
         return [results[r.rid] for r in requests]
+
+
+class MLEServer(ReplicaRouter):
+    """Admission-controlled concurrent request loop on one GPU."""
+
+    def __init__(self, device: int = 0, slots: int = 4, hbm_budget: int | None = None,
+                 workspace_bytes: int = 2 << 30, **kw):
+        super().__init__(devices=[device], slots=slots,
+                         hbm_budgets=None if hbm_budget is None else [hbm_budget],
+                         workspace_bytes=workspace_bytes, **kw)
+        self.device = device
+        self.hbm_budget = self.hbm_budgets[0]
 
 
 def summarize(results: list[MLEResult], makespan: float) -> dict:
