@@ -111,6 +111,7 @@ def load_library(path: str | None = None):
         "hicma_tlr_logdet": (i, [vp, vp, dp]),
         "hicma_tlr_solve": (i, [vp, vp, i, vp, C.c_long]),
         "hicma_tlr_loglik": (i, [vp, vp, vp, dp, dp, vp]),
+        "hicma_tlr_serve_loglik": (i, [vp, C.POINTER(CProblem), i, i, d, i, i, vp, dp, dp, vp, ip]),
         "hicma_tlr_last_stats": (i, [vp, vp, i]),
         "hicma_tlr_check": (i, [vp, vp, C.POINTER(CProblem), vp, dp, dp]),
         "hicma_tlr_check_probe": (i, [vp, vp, C.POINTER(CProblem), i, C.c_ulonglong, dp]),
@@ -390,6 +391,23 @@ def HiCMA_dpotrf_L(ctx: Context, uplo: int, A: TLRMatrix, acc: float, fixed_rank
                                          compmaxrank or maxrank, send_full_tile, C.byref(two), _p(tiles), _p(ops),
                                          _p(cpt), verbose), "HiCMA_dpotrf_L")
     return info, tiles.reshape(A.nt, A.nt), int(ops[0]), cpt
+
+
+def serve_loglik(ctx: Context, prob: Problem, n: int, nb: int, acc: float, y: np.ndarray, maxrank: int = 0,
+                 autoband: bool = True):
+    """One serving request in one library call (hicma_tlr_serve_loglik):
+    returns (status, loglik, logdet, x, band); status is 0 or the positive
+    factorization info; errors raise."""
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    if y.shape != (n,):
+        raise TLRError(ERR_ARG, "hicma_tlr_serve_loglik", "y must have N entries")
+    ll, ld, band = C.c_double(float("nan")), C.c_double(float("nan")), C.c_int(0)
+    x = np.empty(n)
+    cp = prob.c()
+    st = _check(ctx.lib.hicma_tlr_serve_loglik(ctx.h, C.byref(cp), n, nb, acc, maxrank, int(autoband), _p(y),
+                                               C.byref(ll), C.byref(ld), _p(x), C.byref(band)),
+                "hicma_tlr_serve_loglik")
+    return st, ll.value, ld.value, x, band.value
 
 
 def parsec_band_size_auto_tuning(rank_array: np.ndarray, nt: int, nb: int, verbose: int = 0) -> int:

@@ -194,6 +194,20 @@ int hicma_tlr_solve(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, int nrhs, double *B, 
 int hicma_tlr_loglik(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, const double *y, double *loglik,
                      double *logdet, double *x);
 
+/* One serving request (no reference counterpart): generate prob on a new
+ * N x N descriptor with tile NB (STARSH_gen), widen the band over tiles the rank
+ * rule rejected, else auto-tune it when autoband != 0
+ * (parsec_band_size_auto_tuning, band_size_auto_tuning.jdf:201-318), regenerate
+ * the band (parsec_band_regenerate), factor (HiCMA_dpotrf_L) and evaluate the
+ * log-likelihood of y (host, N).  maxrank <= 0 means min(NB/2 - 1, 200).
+ * Returns 0 with loglik, logdet, x (host N, may be NULL) and band (may be
+ * NULL) set; a positive return is the factorization's info (not positive
+ * definite); negative returns are errors.  The descriptor is released before
+ * returning; the context's workspace is reused. */
+int hicma_tlr_serve_loglik(hicma_tlr_ctx *ctx, const hicma_tlr_problem *prob, int N, int NB, double acc,
+                           int maxrank, int autoband, const double *y, double *loglik, double *logdet,
+                           double *x, int *band);
+
 /* Statistics of the last factorization on A: [0] seconds, [1] TLR flops
  * (op_counts model), [2] recompressions capped at maxrank, [3] number of
  * launches of library kernels, [4] POTRF s, [5] TRSM s, [6] SYRK s,

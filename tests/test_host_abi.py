@@ -73,6 +73,13 @@ def test_argument_errors_without_gpu(lib):
         tlr.points(tlr.Problem(kind=9), 10)
     G = np.zeros(4, np.int32)
     assert lib.hicma_tlr_band_autotune(None, 2, 10, 0) == tlr.ERR_ARG
+    # serve_loglik validates its arguments before any device work
+    y = np.zeros(10)
+    d = ctypes.c_double()
+    prob = tlr.Problem().c()
+    assert lib.hicma_tlr_serve_loglik(None, ctypes.byref(prob), 10, 5, 1e-8, 0, 1,
+                                      y.ctypes.data_as(ctypes.c_void_p), ctypes.byref(d), ctypes.byref(d),
+                                      None, None) == tlr.ERR_ARG
 
 
 @pytest.mark.parametrize("kind", [0, 6, 7])
