@@ -27,6 +27,39 @@ static double wtime(void) {
 static const char *str_problem[8] = {"randtlr", "ed-2d-sin", "st-2d-sqexp", "st-3d-sqexp",
                                      "st-3d-exp", "ed-3d-sin", "md-3d-virus", "md-3d-cube"};
 
+/* Rank map block of tlr_rank_stat under PRINT_RANK (testing_dpotrf.c:91-106). */
+static void print_rank_tile(const char *strid, const int *G, int NT, int band_size) {
+    printf("%s %d %d\n", strid, NT, NT);
+    for (int i = 0; i < NT; ++i) {
+        for (int j = 0; j < NT; ++j) printf("%3d ", i - j >= band_size ? G[(size_t)j * NT + i] : -1);
+        printf("\n");
+    }
+}
+
+/* The five maps of parsec_rank_print (rank_print.jdf:128-183); tiles outside
+ * the low-rank part print 0, as the reference's zero-initialised buffers do. */
+static void print_rank_history(hicma_tlr_desc *A, int NT) {
+    const size_t n2 = (size_t)NT * NT;
+    int *h = malloc(sizeof(int) * n2 * 4);
+    if (!h || hicma_tlr_rank_history(A, h, h + n2, h + 2 * n2, h + 3 * n2) != 0) { free(h); return; }
+    static const char *title[5] = {"Initial Rank", "Minimum Rank", "Maximum Rank", "Final Rank",
+                                   "Difference Rank, max - min"};
+    for (int t = 0; t < 5; ++t) {
+        printf("\n%s\n", title[t]);
+        for (int i = 0; i < NT; ++i) {
+            for (int j = 0; j < NT; ++j) {
+                const size_t k = (size_t)j * NT + i;
+                int v = t < 4 ? h[t * n2 + k] : h[2 * n2 + k] - h[n2 + k];
+                if (h[k] < 0) v = 0;
+                printf("%3d ", v);
+            }
+            printf("\n");
+        }
+        printf("\n\n");
+    }
+    free(h);
+}
+
 static void usage(void) {
     fprintf(stderr,
             "Mandatory: -N <n> -t <nb>\n"
@@ -45,13 +78,14 @@ static void usage(void) {
             " -x --check        check against dense factorization\n"
             " -v --verbose\n"
             " --noise <nugget> (default 0.1, testing_dpotrf.c:305)  --beta <len> (0.1)\n"
-            " --sigma <var> (1.0) --seed <s> (0) --precision fp64|mixed --ws <GiB> --device <id>\n");
+            " --sigma <var> (1.0) --seed <s> (0) --precision fp64|mixed --ws <GiB> --device <id>\n"
+            " --print-rank      print the rank maps (the reference's PRINT_RANK output)\n");
 }
 
 int main(int argc, char **argv) {
     int N = 0, NB = 0, maxrank = 0, genmaxrank = 0, compmaxrank = 0, fixedrk = 0, kind = 2, band_size = 1;
     int auto_band = 1, lookahead = -1, send_full_tile = 0, two_flow = 0, HNB = 300, check = 0, verbose = 0;
-    int device = 0, precision = HICMA_TLR_PREC_FP64;
+    int device = 0, precision = HICMA_TLR_PREC_FP64, print_rank = 0;
     double tol = 1e-8, noise = 0.1, beta = 0.1, sigma = 1.0, ws_gib = 0.0, wave_k = 50.0, add_diag = 0.0;
     unsigned long long seed = 0;
     static struct option opts[] = {
@@ -79,7 +113,8 @@ int main(int argc, char **argv) {
         {"noise", required_argument, 0, 1001},     {"beta", required_argument, 0, 1002},
         {"sigma", required_argument, 0, 1003},     {"seed", required_argument, 0, 1004},
         {"precision", required_argument, 0, 1005}, {"ws", required_argument, 0, 1006},
-        {"device", required_argument, 0, 1007},    {0, 0, 0, 0}};
+        {"device", required_argument, 0, 1007},    {"print-rank", no_argument, 0, 1008},
+        {0, 0, 0, 0}};
     int c, oi;
     while ((c = getopt_long_only(argc, argv, "", opts, &oi)) != -1) {
         switch (c) {
@@ -110,6 +145,7 @@ int main(int argc, char **argv) {
             case 1005: precision = strcmp(optarg, "mixed") == 0 ? HICMA_TLR_PREC_MIXED : HICMA_TLR_PREC_FP64; break;
             case 1006: ws_gib = atof(optarg); break;
             case 1007: device = atoi(optarg); break;
+            case 1008: print_rank = 1; break;
             default: usage(); return 1;
         }
     }
@@ -157,6 +193,7 @@ int main(int argc, char **argv) {
     hicma_tlr_rank_stat(rank_array, NT, band_size, &iminrk, &imaxrk, &iavgrk);
     printf("[****] TIME(s) %12.5f : Gather rank\tband_size= %d  NT= %4d avg= %lf min= %d max= %d\n", 0.0, band_size,
            NT, iavgrk, iminrk, imaxrk);
+    if (print_rank) print_rank_tile("init_rank_tile", rank_array, NT, band_size);
     const int imin_before = iminrk, imax_before = imaxrk;
     const double iavg_before = iavgrk;
     double time_opt_band = 0.0, time_regenerate = 0.0;
@@ -177,6 +214,7 @@ int main(int argc, char **argv) {
                band_size);
         hicma_tlr_rank_gather(ctx, A, rank_array, band_size);
         hicma_tlr_rank_stat(rank_array, NT, band_size, &iminrk, &imaxrk, &iavgrk);
+        if (print_rank) print_rank_tile("init_rank_tile", rank_array, NT, band_size);
     }
     /* memory estimate (testing_dpotrf.c:598-599) */
     const double mem = ((double)(NT - band_size) * (NT - band_size + 1) * NB * iavgrk + (double)band_size * NT * NB * NB) * 8 / 1073741824.0;
@@ -203,6 +241,7 @@ int main(int argc, char **argv) {
            time_hicma, send_full_tile, band_size, lookahead, kind, HNB, NB, N, two_flow, flops / 1e9 / time_hicma);
     if (info < 0) { fprintf(stderr, "HiCMA_dpotrf_L error %d: %s\n", info, hicma_tlr_last_error()); return 1; }
     if (info != 0) { printf("-- Factorization is suspicious (info = %d) ! \n", info); ret |= 1; }
+    if (print_rank) print_rank_history(A, NT);
 
     if (check && info == 0) {
         double res = 0, diff = 0;
@@ -227,6 +266,7 @@ int main(int argc, char **argv) {
     double favgrk;
     hicma_tlr_rank_gather(ctx, A, rank_array, band_size);
     hicma_tlr_rank_stat(rank_array, NT, band_size, &fminrk, &fmaxrk, &favgrk);
+    if (print_rank) print_rank_tile("rank_tile", rank_array, NT, band_size);
     unsigned long total = 0, band_ops = 0, offband_ops = 0;
     for (int i = 0; i < NT; ++i)
         for (int j = 0; j <= i; ++j) {
@@ -234,16 +274,22 @@ int main(int argc, char **argv) {
             if (i - j < band_size) band_ops += tileops[(size_t)i * NT + j];
             else offband_ops += tileops[(size_t)i * NT + j];
         }
-    printf("[****] TIME(s) %12.5f : Operation_counts : band_size= %d total= %le op_band= %le op_offband= %le ratio_band= %lf\n",
+    double st[12] = {0};
+    hicma_tlr_last_stats(A, st, 12);
+    const double path_ops = st[10], offpath_ops = (double)total - st[10];
+    printf("[****] TIME(s) %12.5f : Operation_counts : band_size= %d total= %le op_band= %le op_offband= %le "
+           "ratio_band= %lf op_critical_path= %le op_off_critical_path= %le ratio_critical_path= %lf\n",
            0.0, band_size, (double)total, (double)band_ops, (double)offband_ops,
-           offband_ops ? (double)band_ops / offband_ops : 0.0);
+           (double)band_ops / (double)offband_ops, path_ops, offpath_ops, path_ops / offpath_ops);
     printf("R-LO %d %d %d %d   %d %d   %d %d %d %d   %d %s %.1e %g %d %g   %d %d %d %d %d %d %d %d   "
-           "%g %d %d   %g %d %d   %g %d %d   %lf %lf   %lf %lf %lf %lf    %lf %lf %lf %lf %lf    %le %le %le %d \"",
+           "%g %d %d   %g %d %d   %g %d %d   %lf %lf   %lf %lf %lf %lf    %lf %lf %lf %lf %lf    "
+           "%le %le %le %le %le %lf %lf %d  GITHASH:N/A    \"",
            N, N, NB, NB, HNB, HNB, 1, 1, 1, 1, kind, str_problem[kind], tol, add_diag, fixedrk, wave_k, send_full_tile,
            band_size, lookahead, 0, auto_band, maxrank, genmaxrank, compmaxrank, iavg_before, imin_before,
            imax_before, iavgrk, iminrk, imaxrk, favgrk, fminrk, fmaxrk, mem, mem_max, cpt[0] + cpt[1] + cpt[2],
            cpt[0], cpt[1], cpt[2], time_starsh, time_hicma, time_opt_band, time_regenerate, 0.0, (double)total,
-           (double)band_ops, (double)offband_ops, two_flow);
+           (double)band_ops, (double)offband_ops, path_ops, offpath_ops, (double)band_ops / (double)offband_ops,
+           path_ops / offpath_ops, two_flow);
     for (int i = 0; i < argc; ++i) printf("%s ", argv[i]);
     printf("\"\n");
     free(tileops);

@@ -106,6 +106,10 @@ struct hicma_tlr_desc_s {
     long long nslots = 0;
     int *d_rank = nullptr;
     std::vector<int> h_rank;
+    // rank history of the last factorization (the reference's dcRank record,
+    // HiCMA_dpotrf_L_2flow.jdf:353-361,683-691,1101-1106): per off-band tile the
+    // rank it entered with and the smallest / largest rank it held; -1 elsewhere
+    std::vector<int> rk_init, rk_min, rk_max;
     double *d_linv = nullptr;
     bool factored = false;
     double stats[12] = {0};
@@ -1275,6 +1279,18 @@ int hicma_tlr_rank_gather(hicma_tlr_ctx *c, hicma_tlr_desc *A, int *rank_array, 
     return 0;
 }
 
+int hicma_tlr_rank_history(hicma_tlr_desc *A, int *initial, int *minimum, int *maximum, int *final_rank) {
+    ARG_CHECK(A, "null");
+    const size_t n2 = (size_t)A->NT * A->NT;
+    if (A->rk_init.size() != n2) { set_err("no factorization has run on this descriptor"); return HICMA_TLR_ERR_STATE; }
+    if (initial) std::memcpy(initial, A->rk_init.data(), n2 * sizeof(int));
+    if (minimum) std::memcpy(minimum, A->rk_min.data(), n2 * sizeof(int));
+    if (maximum) std::memcpy(maximum, A->rk_max.data(), n2 * sizeof(int));
+    if (final_rank)
+        for (size_t i = 0; i < n2; ++i) final_rank[i] = A->rk_init[i] < 0 ? -1 : A->h_rank[i];
+    return 0;
+}
+
 int hicma_tlr_rank_stat(const int *G, int NT, int band_size, int *minrk, int *maxrk, double *avgrk) {
     ARG_CHECK(G && NT > 0 && band_size >= 1, "rank_stat");
     int mn = 2147483647, mx = 0;
@@ -1479,6 +1495,11 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     c->ar = &c->main_ar;
     c->main_ar.off = 0;
     c->hi_ar.off = 0;
+    A->rk_init.assign((size_t)NT * NT, -1);
+    for (int n = 0; n < NT; ++n)
+        for (int m = n + band; m < NT; ++m) A->rk_init[(size_t)n * NT + m] = A->rank(m, n);
+    A->rk_min = A->rk_init;
+    A->rk_max = A->rk_init;
     CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 5 * sizeof(int), c->stream));
     TRY(ctx_sync(c));
     int *d_info = c->d_flags;
@@ -1503,9 +1524,13 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     const auto t_start = std::chrono::steady_clock::now();
     const long long launches0 = c->launches;
     int info = 0;
-    auto log_op = [&](unsigned long cnt, int i, int j) {
+    // ops of the critical path POTRF(k) -> TRSM(k+1,k) -> SYRK(k,k+1) (the
+    // reference's op_path, HiCMA_dpotrf_L_2flow.jdf:201,303-313,443-462)
+    unsigned long op_path = 0;
+    auto log_op = [&](unsigned long cnt, int i, int j, bool path = false) {
         tops[(size_t)i * NT + j] += cnt;
         op_total += cnt;
+        if (path) op_path += cnt;
     };
     auto elapsed = [&](cudaEvent_t a, cudaEvent_t b) {
         float ms = 0.f;
@@ -1521,7 +1546,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         CUDA_TRY(cudaEventRecord(ev[P1], c->cur));
         CUDA_TRY(cudaEventRecord(evP, c->cur));
     }
-    log_op(op_counts('c', NB, 0, 0, 0), 0, 0);
+    log_op(op_counts('c', NB, 0, 0, 0), 0, 0, true);
     CUDA_TRY(cudaEventSynchronize(ev[P1]));
     t_phase[0] += elapsed(ev[P0], ev[P1]);
     for (int k = 0; k < NT; ++k) {
@@ -1536,7 +1561,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             for (int m = k + 1; m < NT; ++m) {
                 const bool dense = A->is_dense(m, k);
                 const int r = dense ? NB : A->rank(m, k);
-                log_op(op_counts('t', NB, r, 1, 0), m, k);
+                log_op(op_counts('t', NB, r, 1, 0), m, k, m == k + 1);
                 if (r == 0) continue;
                 double *tmp = ws_alloc<double>(c, (size_t)NB * r);
                 if (!tmp) {
@@ -1574,8 +1599,8 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         std::vector<std::array<int, 5>> rec_meta;
         if (k + 1 < NT) {
             // ---- critical chain: SYRK(k, k+1) + POTRF(k+1)
-            log_op(syrk_ops(A, k, k + 1), k + 1, k + 1);
-            log_op(op_counts('c', NB, 0, 0, 0), k + 1, k + 1);
+            log_op(syrk_ops(A, k, k + 1), k + 1, k + 1, true);
+            log_op(op_counts('c', NB, 0, 0, 0), k + 1, k + 1, true);
             {
                 OnHi h(c);
                 if (!lookahead) c->cur = c->stream;
@@ -1673,8 +1698,16 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         TRY(ctx_sync(c));
         int hinfo = 0;
         CUDA_TRY(cudaMemcpy(&hinfo, d_info, sizeof(int), cudaMemcpyDeviceToHost));
-        if (!rec.empty())
+        if (!rec.empty()) {
             CUDA_TRY(cudaMemcpy(A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
+            // each tile takes at most one update per panel, so per-panel minima
+            // and maxima are the per-update ones of the reference
+            for (const auto &mt : rec_meta) {
+                const size_t i = (size_t)mt[1] * NT + mt[0];
+                A->rk_min[i] = std::min(A->rk_min[i], A->h_rank[i]);
+                A->rk_max[i] = std::max(A->rk_max[i], A->h_rank[i]);
+            }
+        }
         for (size_t i = 0; i < rec.size(); ++i) {
             const auto &mt = rec_meta[i];
             log_op(gemm_lr_ops(NB, mt[2], mt[3], mt[4], A->rank(mt[0], mt[1]), rec_case[i] == 1), mt[0], mt[1]);
@@ -1727,6 +1760,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     A->stats[2] = overflow;
     A->stats[3] = (double)(c->launches - launches0);
     A->stats[4] = t_phase[0]; A->stats[5] = t_phase[1]; A->stats[6] = t_phase[2]; A->stats[7] = t_phase[3];
+    A->stats[10] = (double)op_path;
     A->factored = (info == 0);
     c->main_ar.off = 0;
     c->hi_ar.off = 0;

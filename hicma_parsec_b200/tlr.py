@@ -111,6 +111,7 @@ def load_library(path: str | None = None):
         "hicma_tlr_logdet": (i, [vp, vp, dp]),
         "hicma_tlr_solve": (i, [vp, vp, i, vp, C.c_long]),
         "hicma_tlr_loglik": (i, [vp, vp, vp, dp, dp, vp]),
+        "hicma_tlr_rank_history": (i, [vp, vp, vp, vp, vp]),
         "hicma_tlr_serve_loglik": (i, [vp, C.POINTER(CProblem), i, i, d, i, i, vp, dp, dp, vp, ip]),
         "hicma_tlr_last_stats": (i, [vp, vp, i]),
         "hicma_tlr_check": (i, [vp, vp, C.POINTER(CProblem), vp, dp, dp]),
@@ -255,6 +256,15 @@ class TLRMatrix:
             return []
         b = self.band_size
         return [(m, n) for m in range(b, self.nt) for n in range(0, m - b + 1) if G[n * self.nt + m] < 0]
+
+    def rank_history(self) -> dict:
+        """Rank history of the last factorization: NT x NT arrays [m, n]
+        'initial', 'minimum', 'maximum', 'final' (-1 off the low-rank part)."""
+        nt = self.nt
+        out = {k: np.empty(nt * nt, dtype=np.int32) for k in ("initial", "minimum", "maximum", "final")}
+        _check(self.lib.hicma_tlr_rank_history(self.h, _p(out["initial"]), _p(out["minimum"]), _p(out["maximum"]),
+                                                _p(out["final"])), "hicma_tlr_rank_history")
+        return {k: v.reshape(nt, nt).T.copy() for k, v in out.items()}
 
     def rank_map(self) -> np.ndarray:
         G = np.empty(self.nt * self.nt, dtype=np.int32)

@@ -123,6 +123,15 @@ int hicma_tlr_generate(hicma_tlr_ctx *ctx, int uplo, hicma_tlr_desc *A, int *Ar,
 /* parsec_rank_gather (hicma_parsec.h:124-127): device rank map -> host. */
 int hicma_tlr_rank_gather(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, int *rank_array, int band_size);
 
+/* Rank history of the last factorization on A (the dcRank record gathered by
+ * parsec_rank_print, hicma_parsec/rank_print.jdf:62-69, filled at
+ * HiCMA_dpotrf_L_2flow.jdf:353-361,683-691,1101-1106): per off-band tile
+ * (m, n) at [n*NT + m] the rank it entered the factorization with, the
+ * smallest and largest rank it held, and its final rank; -1 for band and
+ * upper tiles.  Any pointer may be NULL.  HICMA_TLR_ERR_STATE before the
+ * first factorization of A. */
+int hicma_tlr_rank_history(hicma_tlr_desc *A, int *initial, int *minimum, int *maximum, int *final_rank);
+
 /* HICMA_get_stat2 (hicma_parsec/hicma_internal.c:52-71). */
 int hicma_tlr_rank_stat(const int *rank_array, int NT, int band_size, int *minrk, int *maxrk,
                         double *avgrk);
@@ -212,7 +221,9 @@ int hicma_tlr_serve_loglik(hicma_tlr_ctx *ctx, const hicma_tlr_problem *prob, in
  * (op_counts model), [2] recompressions capped at maxrank, [3] number of
  * launches of library kernels, [4] POTRF s, [5] TRSM s, [6] SYRK s,
  * [7] GEMM/recompression s, [8] Jacobi sweeps summed over all cores, [9] recompressions
- * whose products ran in FP32 under HICMA_TLR_PREC_MIXED.
+ * whose products ran in FP32 under HICMA_TLR_PREC_MIXED, [10] op count of the
+ * critical path POTRF(k) -> TRSM(k+1,k) -> SYRK(k,k+1) (the reference's op_path;
+ * the rest of [1] is its op_offpath).
  * nstats <= 12. */
 int hicma_tlr_last_stats(hicma_tlr_desc *A, double *stats, int nstats);
 

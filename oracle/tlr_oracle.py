@@ -545,6 +545,12 @@ class FactorStats:
     op_offband: int = 0
     op_path: int = 0
     op_offpath: int = 0
+    # rank history (the reference's dcRank record, HiCMA_dpotrf_L_2flow.jdf:353-361,
+    # 683-691,1101-1106): per off-band tile [m, n] the rank it entered with and the
+    # smallest / largest rank it held; -1 outside the low-rank part
+    rank_init: np.ndarray | None = None
+    rank_min: np.ndarray | None = None
+    rank_max: np.ndarray | None = None
 
     @property
     def total(self) -> int:
@@ -574,6 +580,15 @@ def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool
     nt, nb, band = T.nt, T.nb, T.band
     st = FactorStats(tileopcounters=np.zeros((nt, nt), dtype=np.uint64))
     tile_ops = st.tileopcounters
+    st.rank_init = np.full((nt, nt), -1, dtype=np.int64)
+    for (m, n) in T.U:
+        st.rank_init[m, n] = T.rank(m, n)
+    st.rank_min = st.rank_init.copy()
+    st.rank_max = st.rank_init.copy()
+
+    def track(m, n, r):
+        st.rank_min[m, n] = min(st.rank_min[m, n], r)
+        st.rank_max[m, n] = max(st.rank_max[m, n], r)
 
     def log(cnt, i, j, region, path):
         tile_ops[i, j] += np.uint64(cnt & _U64)
@@ -653,6 +668,7 @@ def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool
                     U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank)
                     st.overflow += int(ov)
                     T.U[(m, n)], T.V[(m, n)] = U, V
+                    track(m, n, r)
                     log(gemm_lr_opcount(nb, ra, 0, rc_old, r, True), m, n, "offband", False)
                 else:                                              # (v) :929-1097
                     Au, Av = T.U[(m, k)], T.V[(m, k)]
@@ -665,6 +681,7 @@ def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool
                     U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank)
                     st.overflow += int(ov)
                     T.U[(m, n)], T.V[(m, n)] = U, V
+                    track(m, n, r)
                     log(gemm_lr_opcount(nb, ra, rb, rc_old, r, False), m, n, "offband", False)
     return st
 
