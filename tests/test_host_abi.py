@@ -92,3 +92,27 @@ def test_kinds_without_points_are_argument_errors(lib, kind):
     buf = np.zeros(30)
     prob = tlr.CProblem(kind, 0.1, 0.5, 0.1, 1.0, 0, 50.0, 0.0)
     assert lib.hicma_tlr_points(C.byref(prob), 10, buf.ctypes.data_as(C.c_void_p)) == tlr.ERR_ARG
+
+
+def test_problem_struct_layout_matches_header(tmp_path):
+    """The ctypes mirror of hicma_tlr_problem has the C header's size and field
+    offsets (checked with the host C compiler)."""
+    import shutil
+    import subprocess
+    from hicma_parsec_b200 import tlr
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    fields = [name for name, _ in tlr.CProblem._fields_]
+    src = tmp_path / "layout.c"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    body = "".join(f'    printf("{f} %zu\\n", offsetof(hicma_tlr_problem, {f}));\n' for f in fields)
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "hicma_tlr.h"\nint main(void) {\n'
+                   '    printf("size %zu\\n", sizeof(hicma_tlr_problem));\n' + body + "    return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", inc, str(src), "-o", str(exe)], check=True, capture_output=True)
+    out = dict(line.split() for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                                                        text=True).stdout.splitlines())
+    assert int(out["size"]) == ctypes.sizeof(tlr.CProblem)
+    for f in fields:
+        assert int(out[f]) == getattr(tlr.CProblem, f).offset, f
