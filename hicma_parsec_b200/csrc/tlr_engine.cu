@@ -1527,6 +1527,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     // ops of the critical path POTRF(k) -> TRSM(k+1,k) -> SYRK(k,k+1) (the
     // reference's op_path, HiCMA_dpotrf_L_2flow.jdf:201,303-313,443-462)
     unsigned long op_path = 0;
+    double t_last = 0.0;   // wall time of the previous panel's end (verbose > 1)
     auto log_op = [&](unsigned long cnt, int i, int j, bool path = false) {
         tops[(size_t)i * NT + j] += cnt;
         op_total += cnt;
@@ -1724,9 +1725,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             break;
         }
         if (verbose > 1) {
-            static double t_last = 0.0;
             const double now = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-            if (k == 0) t_last = 0.0;
             fprintf(stderr, "panel %3d wall %8.3f ms trsm %7.3f syrk %7.3f gemm %7.3f potrf(k+1) %7.3f tasks %zu\n", k,
                     (now - t_last) * 1e3, elapsed(ev[T0], ev[T1]) * 1e3,
                     k + 1 < NT ? elapsed(ev[S0], ev[S1]) * 1e3 : 0.0, k + 1 < NT ? elapsed(ev[G0], ev[G1]) * 1e3 : 0.0,
