@@ -776,29 +776,58 @@ int hicma_tlr_points(const hicma_tlr_problem *prob, int N, double *points) {
     return 0;
 }
 
+// Releases whatever a context holds (also a partly built one from init).
+static void ctx_release(hicma_tlr_ctx *c) {
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->stream_hi) cudaStreamSynchronize(c->stream_hi);
+    for (auto &r : c->prof_recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    if (c->d_ws) cudaFree(c->d_ws);
+    if (c->d_stage) cudaFree(c->d_stage);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
+    if (c->d_flags) cudaFree(c->d_flags);
+    if (c->d_scal) cudaFree(c->d_scal);
+    if (c->stream_hi) cudaStreamDestroy(c->stream_hi);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
 int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     ARG_CHECK(out, "ctx pointer");
     *out = nullptr;
     CUDA_TRY(cudaSetDevice(device));
     auto *c = new hicma_tlr_ctx_s();
     c->device = device;
-    CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    auto fail = [&](cudaError_t e, const char *what) {
+        set_err("%s: %s", what, cudaGetErrorString(e));
+        cudaGetLastError();
+        ctx_release(c);
+        return e == cudaErrorMemoryAllocation ? HICMA_TLR_ERR_OOM : HICMA_TLR_ERR_CUDA;
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(e, "stream");
     int prio_lo = 0, prio_hi = 0;
-    CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-    CUDA_TRY(cudaStreamCreateWithPriority(&c->stream_hi, cudaStreamNonBlocking, prio_hi));
+    e = cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->stream_hi, cudaStreamNonBlocking, prio_hi);
+    if (e != cudaSuccess) return fail(e, "priority stream");
     c->cur = c->stream;
     size_t free_b = 0, total_b = 0;
-    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    e = cudaMemGetInfo(&free_b, &total_b);
+    if (e != cudaSuccess) return fail(e, "memory info");
     if (workspace_bytes == 0) {
         workspace_bytes = std::min<size_t>(free_b / 8, (size_t)8 << 30);
         workspace_bytes = std::max<size_t>(workspace_bytes, (size_t)256 << 20);
     }
     c->ws_bytes = workspace_bytes;
-    if (cudaMalloc(&c->d_ws, c->ws_bytes) != cudaSuccess) {
-        set_err("cudaMalloc workspace of %zu bytes failed", c->ws_bytes);
-        cudaStreamDestroy(c->stream);
-        delete c;
-        return HICMA_TLR_ERR_OOM;
+    e = cudaMalloc(&c->d_ws, c->ws_bytes);
+    if (e != cudaSuccess) {
+        c->d_ws = nullptr;
+        char what[96];
+        snprintf(what, sizeof what, "cudaMalloc workspace of %zu bytes", c->ws_bytes);
+        return fail(e, what);
     }
     {
         const size_t hi = std::min<size_t>(c->ws_bytes / 8, (size_t)512 << 20);
@@ -809,12 +838,13 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
         c->ar = &c->main_ar;
     }
     c->stage_bytes = (size_t)64 << 20;
-    CUDA_TRY(cudaMallocHost(&c->h_stage, c->stage_bytes));
-    CUDA_TRY(cudaMalloc(&c->d_stage, c->stage_bytes));
-    CUDA_TRY(cudaMalloc(&c->d_flags, 64 * sizeof(int)));
-    CUDA_TRY(cudaMalloc(&c->d_scal, 64 * sizeof(double)));
-    CUDA_TRY(cudaMemset(c->d_flags, 0, 64 * sizeof(int)));
-    CUDA_TRY(cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device));
+    if ((e = cudaMallocHost(&c->h_stage, c->stage_bytes)) != cudaSuccess) { c->h_stage = nullptr; return fail(e, "pinned staging"); }
+    if ((e = cudaMalloc(&c->d_stage, c->stage_bytes)) != cudaSuccess) { c->d_stage = nullptr; return fail(e, "device staging"); }
+    if ((e = cudaMalloc(&c->d_flags, 64 * sizeof(int))) != cudaSuccess) { c->d_flags = nullptr; return fail(e, "flags"); }
+    if ((e = cudaMalloc(&c->d_scal, 64 * sizeof(double))) != cudaSuccess) { c->d_scal = nullptr; return fail(e, "scalars"); }
+    if ((e = cudaMemset(c->d_flags, 0, 64 * sizeof(int))) != cudaSuccess) return fail(e, "flags reset");
+    if ((e = cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
+        return fail(e, "SM count");
     *out = c;
     return 0;
 }
@@ -857,16 +887,7 @@ int hicma_tlr_fini(hicma_tlr_ctx *c) {
         A->ctx = nullptr;
     }
     c->descs.clear();
-    cudaFree(c->d_ws);
-    cudaFree(c->d_stage);
-    cudaFreeHost(c->h_stage);
-    cudaFree(c->d_flags);
-    cudaFree(c->d_scal);
-    cudaStreamSynchronize(c->stream_hi);
-    cudaStreamSynchronize(c->stream);
-    cudaStreamDestroy(c->stream_hi);
-    cudaStreamDestroy(c->stream);
-    delete c;
+    ctx_release(c);
     return 0;
 }
 
