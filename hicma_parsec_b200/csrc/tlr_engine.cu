@@ -933,7 +933,13 @@ int hicma_tlr_desc_create(hicma_tlr_ctx *c, int N, int NB, int maxrank, int band
     A->h_rank.assign((size_t)NT * NT, -1);
     for (int m = 0; m < NT; ++m)
         for (int n = 0; n <= m - A->band; ++n) A->h_rank[(size_t)n * NT + m] = 0;
-    CUDA_TRY(cudaMemcpy(A->d_rank, A->h_rank.data(), (size_t)NT * NT * sizeof(int), cudaMemcpyHostToDevice));
+    const cudaError_t e = cudaMemcpy(A->d_rank, A->h_rank.data(), (size_t)NT * NT * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        set_err("rank map upload: %s", cudaGetErrorString(e));
+        dev_free(c, A->d_band); dev_free(c, A->d_lr); dev_free(c, A->d_rank);
+        delete A;
+        return HICMA_TLR_ERR_CUDA;
+    }
     c->descs.insert(A);
     *out = A;
     return 0;
