@@ -1811,7 +1811,12 @@ int hicma_tlr_dpotrf_L(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, d
         ARG_CHECK(*lookahead >= -1, "lookahead >= -1");
         if (*lookahead == -1) *lookahead = band_size;   // hicma_parsec.c:489-495
     }
-    if (two_flow) *two_flow = 1;
+    // The reference runs its 3-flow graph when band_size == 1 and 2-flow is not
+    // forced, leaving *two_flow at 0, and sets it to 1 otherwise
+    // (hicma_parsec.c:517-573).  At band 1 the 3-flow graph computes the same
+    // updates, so both are served by this path; *two_flow reports which one
+    // the reference would have run.
+    if (two_flow && (band_size != 1 || *two_flow)) *two_flow = 1;
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     CUDA_TRY(cudaSetDevice(c->device));
     const bool la = !(lookahead && *lookahead == 0);

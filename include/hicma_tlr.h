@@ -155,6 +155,10 @@ int hicma_tlr_band_regenerate(hicma_tlr_ctx *ctx, int uplo, hicma_tlr_desc *A,
  * panel critical path, then total factorization, TRSM+SYRK+GEMM of all
  * panels and the recompression share.  hmb is accepted and ignored (the
  * recursive sub-tiling of the reference is replaced by multi-CTA kernels).
+ * *two_flow (may be NULL): 0 on entry with band_size 1 selects the
+ * reference's 3-flow variant, which computes the same updates and is served
+ * by the same path; it is left 0 then and set to 1 otherwise
+ * (hicma_parsec.c:517-573).
  * Returns the reference's info (0, k*NB+i) or a negative error code. */
 int hicma_tlr_dpotrf_L(hicma_tlr_ctx *ctx, int uplo, hicma_tlr_desc *A, int *Ar,
                        double acc, int fixed_rank, int maxrank, int *lookahead,
