@@ -53,6 +53,7 @@ struct PotrfParams {
     int *info;
     int info_base;
     int *timeout;
+    long long spin_limit;   // polls before a wait gives up (SPIN_LIMIT in production)
 };
 
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
@@ -65,7 +66,7 @@ __device__ __forceinline__ int ld_volatile(const int *p) { return *(const volati
 
 // thread 0 only: wait until *p >= v
 __device__ bool wait_ge(const int *p, int v, const PotrfParams &P) {
-    for (long long it = 0; it < SPIN_LIMIT; ++it) {
+    for (long long it = 0; it < P.spin_limit; ++it) {
         if (ld_volatile(p) >= v) {
             __threadfence();
             return true;
@@ -379,6 +380,16 @@ const ItemList *get_items(int nblk, bool inv) {
     return &(g_items[key] = L);
 }
 
+// Exercise of the bounded wait above, for tests: thread 0 of CTA b waits
+// with wait_ge on the counter cnt[2 + b], which nothing sets, with limit
+// limit0 (CTA 0) or limit1 (the others).  The first wait to run out sets the
+// timeout and abort flags; the others then leave at their next poll.
+__global__ void k_wait_probe(PotrfParams P, long long limit0, long long limit1) {
+    if (threadIdx.x != 0) return;
+    P.spin_limit = blockIdx.x == 0 ? limit0 : limit1;
+    wait_ge(P.cnt + 2 + blockIdx.x, 1, P);
+}
+
 }  // namespace
 
 int potrf_tile_max_n() { return 128 * TB; }
@@ -400,10 +411,20 @@ int launch_potrf_tile(double *A, int lda, int n, double *X, int ldx, double *D, 
                                                                                         : 2 * TB * LDS + 32 * 32 + TB);
     // per device and thread-safe: set on every launch (a host-side call, no synchronisation)
     cudaFuncSetAttribute(k_potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    PotrfParams P{A, lda, n, nblk, X, ldx, D, L->d, L->n, cnt, info, info_base, timeout};
+    PotrfParams P{A, lda, n, nblk, X, ldx, D, L->d, L->n, cnt, info, info_base, timeout, SPIN_LIMIT};
     if (grid > L->n) grid = L->n;
     if (grid < 1) grid = 1;
     k_potrf_tile<<<grid, NTH, smem, st>>>(P);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// cnt: 2 + nblocks zeroed ints (abort flag at [1]); timeout: one zeroed int.
+int launch_wait_probe(int *cnt, int *timeout, int nblocks, long long limit0, long long limit1, cudaStream_t st) {
+    if (nblocks < 1 || nblocks > 64 || limit0 < 1 || limit1 < 1) return -1;
+    PotrfParams P{};
+    P.cnt = cnt;
+    P.timeout = timeout;
+    k_wait_probe<<<nblocks, 32, 0, st>>>(P, limit0, limit1);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -2350,6 +2350,40 @@ int hicma_tlr_k_cov(const hicma_tlr_problem *prob, const double *d_points, int N
     return 0;
 }
 
+int hicma_tlr_k_wait_probe(long long polls0, long long polls1, int nblocks, double *elapsed_ms, void *stream) {
+    ARG_CHECK(nblocks >= 1 && nblocks <= 64, "wait probe: 1..64 blocks");
+    ARG_CHECK(polls0 >= 1 && polls1 >= 1 && polls0 <= (1LL << 26) && polls1 <= (1LL << 26),
+              "wait probe: 1..2^26 polls");
+    cudaStream_t st = (cudaStream_t)stream;
+    int *buf = nullptr;   // [0] timeout flag, then cnt: [1] ticket, [2] abort, [3..] counters
+    CUDA_TRY(cudaMalloc(&buf, (3 + 64) * sizeof(int)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int flags[3] = {0, 0, 0};
+    float ms = 0.f;
+    cudaError_t e = cudaMemsetAsync(buf, 0, (3 + 64) * sizeof(int), st);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+    if (e == cudaSuccess && launch_wait_probe(buf + 1, buf, nblocks, polls0, polls1, st) != 0) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess) e = cudaMemcpy(flags, buf, 3 * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(buf);
+    if (e != cudaSuccess) {
+        set_err("wait probe: %s", cudaGetErrorString(e));
+        return HICMA_TLR_ERR_CUDA;
+    }
+    if (elapsed_ms) *elapsed_ms = ms;
+    if (flags[0]) {
+        set_err("a bounded device wait gave up (wait probe; abort flag %d)", flags[2]);
+        return HICMA_TLR_ERR_TIMEOUT;
+    }
+    return 0;
+}
+
 int hicma_tlr_k_dgemm(int transA, int transB, int m, int n, int k, double alpha, const double *A, int lda,
                       const double *B, int ldb, double beta, double *C, int ldc, void *stream) {
     ARG_CHECK(m >= 0 && n >= 0 && k >= 0 && A && B && C, "k_dgemm arguments");

@@ -148,6 +148,10 @@ void launch_precision_select(const SelTask *d_tasks, int ntasks, double thr2, in
 // potrf_tile_scratch_ints(n) ints; D: (n/64 rounded up) * 4096 doubles when X
 // is null.  *timeout is set if a bounded device wait gave up.
 int potrf_tile_max_n();
+// Test of the bounded dependency wait of the tile POTRF: nblocks CTAs wait on
+// counters nothing sets (CTA 0 with limit0 polls, the others limit1); cnt has
+// 2 + nblocks zeroed ints, timeout one zeroed int.
+int launch_wait_probe(int *cnt, int *timeout, int nblocks, long long limit0, long long limit1, cudaStream_t st);
 size_t potrf_tile_scratch_ints(int n);
 int launch_potrf_tile(double *A, int lda, int n, double *X, int ldx, double *D, int *cnt, int *info,
                       int info_base, int *timeout, int grid, cudaStream_t st);

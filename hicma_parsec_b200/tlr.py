@@ -112,6 +112,7 @@ def load_library(path: str | None = None):
         "hicma_tlr_solve": (i, [vp, vp, i, vp, C.c_long]),
         "hicma_tlr_loglik": (i, [vp, vp, vp, dp, dp, vp]),
         "hicma_tlr_rank_history": (i, [vp, vp, vp, vp, vp]),
+        "hicma_tlr_k_wait_probe": (i, [C.c_longlong, C.c_longlong, i, dp, vp]),
         "hicma_tlr_serve_loglik": (i, [vp, C.POINTER(CProblem), i, i, d, i, i, vp, dp, dp, vp, ip]),
         "hicma_tlr_last_stats": (i, [vp, vp, i]),
         "hicma_tlr_check": (i, [vp, vp, C.POINTER(CProblem), vp, dp, dp]),

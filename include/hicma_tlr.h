@@ -316,6 +316,15 @@ int hicma_tlr_k_compress(hicma_tlr_ctx *ctx, int nb, const double *d_A, double *
 int hicma_tlr_k_potrf_noalloc(int n, double *d_A, int lda, double *d_linv, int *d_info,
                               int info_offset, void *stream);
 
+/* Test of the bounded dependency wait of the tile POTRF task queue (no
+ * reference counterpart): nblocks (1..64) CTAs each wait, with the queue's own
+ * wait routine, on a counter that nothing sets; CTA 0 gives up after polls0
+ * polls, the others after polls1 (1..2^26; a poll is about 0.25 us).  The
+ * first wait to give up raises the abort flag, on which the others leave.
+ * Returns HICMA_TLR_ERR_TIMEOUT (the status a factorization reports when a
+ * wait gives up) with the kernel's duration in *elapsed_ms (may be NULL). */
+int hicma_tlr_k_wait_probe(long long polls0, long long polls1, int nblocks, double *elapsed_ms, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
