@@ -41,6 +41,45 @@ static void set_err(const char *fmt, ...) {
 extern "C" const char *hicma_tlr_last_error(void) { return g_err.c_str(); }
 void tlr::tlr_set_error(const char *msg) { g_err = msg ? msg : ""; }
 
+#ifdef TLR_BOUNDS_CHECK
+// ------------------------------------------------------ bounds registry ----
+// Live device regions, process-wide (contexts on several devices share it).
+static std::mutex g_bc_mu;
+static std::vector<std::pair<uintptr_t, size_t>> g_bc_regions;
+void tlr::bc_add(const void *p, size_t bytes) {
+    if (!p || !bytes) return;
+    std::lock_guard<std::mutex> lk(g_bc_mu);
+    g_bc_regions.push_back({(uintptr_t)p, bytes});
+}
+void tlr::bc_remove(const void *p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_bc_mu);
+    for (size_t i = g_bc_regions.size(); i-- > 0;)
+        if (g_bc_regions[i].first == (uintptr_t)p) {
+            g_bc_regions.erase(g_bc_regions.begin() + (long)i);
+            return;
+        }
+}
+bool tlr::bc_inside(const void *p, size_t bytes) {
+    if (!bytes) return true;
+    const uintptr_t a = (uintptr_t)p;
+    if (a + bytes < a) return false;
+    std::lock_guard<std::mutex> lk(g_bc_mu);
+    for (const auto &r : g_bc_regions)
+        if (a >= r.first && a + bytes <= r.first + r.second) return true;
+    return false;
+}
+#endif
+
+// Registers caller buffers for the length of a kernel-level call (bounds-checked builds).
+struct BcScope {
+    std::vector<const void *> ps;
+    void add(const void *p, size_t bytes) {
+        if (p && bytes) { bc_add(p, bytes); ps.push_back(p); }
+    }
+    ~BcScope() { for (const void *p : ps) bc_remove(p); }
+};
+
 #define CUDA_TRY(x)                                                                         \
     do {                                                                                    \
         cudaError_t e__ = (x);                                                              \
@@ -251,8 +290,173 @@ int check_launch(hicma_tlr_ctx *c) {
     return 0;
 }
 
+// Operand extents of every task of a launch (bounds-checked builds; no-ops
+// otherwise).  Device-side counts (rank read at run time) are bounded by the
+// host-side capacities checked here.
+#ifdef TLR_BOUNDS_CHECK
+#define BC(ptr, bytes, what, idx)                                                                      \
+    do {                                                                                               \
+        if (!bc_inside((ptr), (bytes))) {                                                              \
+            set_err("bounds check: %s of task %zu: [%p, +%zu B) lies outside every live allocation", \
+                    (what), (size_t)(idx), (const void *)(ptr), (size_t)(bytes));                      \
+            return HICMA_TLR_ERR_ARG;                                                                  \
+        }                                                                                              \
+    } while (0)
+#endif
+
+static int bc_gemms(const std::vector<GemmTask> &v) {
+#ifdef TLR_BOUNDS_CHECK
+    for (size_t i = 0; i < v.size(); ++i) {
+        const GemmTask &t = v[i];
+        // a device-side column count is a rank (or 0): never above the inner dimension
+        const int n = t.n_dev ? std::min(t.n, std::max(t.k, 0)) : t.n;
+        if (t.m <= 0 || n <= 0) continue;
+        BC(t.A, t.opA ? bc_span(t.k, t.m, t.lda) : bc_span(t.m, t.k, t.lda), "gemm A", i);
+        BC(t.B, t.opB ? bc_span(n, t.k, t.ldb) : bc_span(t.k, n, t.ldb), "gemm B", i);
+        BC(t.C, bc_span(t.m, n, t.ldc), "gemm C", i);
+        if (t.n_dev) BC(t.n_dev, sizeof(int), "gemm device count", i);
+    }
+#else
+    (void)v;
+#endif
+    return 0;
+}
+
+static int bc_copies(const std::vector<CopyTask> &v) {
+#ifdef TLR_BOUNDS_CHECK
+    for (size_t i = 0; i < v.size(); ++i) {
+        const CopyTask &t = v[i];
+        BC(t.src, bc_span(t.rows, t.cols, t.lds), "copy source", i);
+        BC(t.dst, bc_span(t.rows, t.cols, t.ldd), "copy destination", i);
+    }
+#else
+    (void)v;
+#endif
+    return 0;
+}
+
+static int bc_qr(const std::vector<QRTask> &v, int m_max) {
+#ifdef TLR_BOUNDS_CHECK
+    const int pb = qr_panel_width(m_max);
+    for (size_t i = 0; i < v.size(); ++i) {
+        const QRTask &t = v[i];
+        if (t.K <= 0) continue;
+        BC(t.X, bc_span(t.m, t.K, t.ld), "qr X", i);
+        BC(t.tau, bc_span(t.K, 1, t.K), "qr tau", i);
+        BC(t.T, (size_t)((t.K + pb - 1) / pb) * pb * pb * sizeof(double), "qr T", i);
+    }
+#else
+    (void)v; (void)m_max;
+#endif
+    return 0;
+}
+
+static int bc_qapply(const std::vector<QApplyTask> &v, int m_max) {
+#ifdef TLR_BOUNDS_CHECK
+    const int pb = qr_panel_width(m_max);
+    for (size_t i = 0; i < v.size(); ++i) {
+        const QApplyTask &t = v[i];
+        // columns read and written: up to the device rank, checked up to min(r_cap, K)
+        const int r = std::min(t.r_cap, t.K);
+        if (r <= 0) continue;
+        BC(t.X, bc_span(t.m, t.K, t.ld), "qapply X", i);
+        BC(t.T, (size_t)((t.K + pb - 1) / pb) * pb * pb * sizeof(double), "qapply T", i);
+        BC(t.S, bc_span(t.K, r, t.lds), "qapply S", i);
+        BC(t.out, bc_span(t.m, r, t.ldo), "qapply out", i);
+        if (t.r_dev) BC(t.r_dev, sizeof(int), "qapply rank", i);
+    }
+#else
+    (void)v; (void)m_max;
+#endif
+    return 0;
+}
+
+static int bc_cores(const std::vector<CoreTask> &v) {
+#ifdef TLR_BOUNDS_CHECK
+    for (size_t i = 0; i < v.size(); ++i) {
+        const CoreTask &t = v[i];
+        if (t.K <= 0) continue;
+        if (t.RU) BC(t.RU, bc_span(t.K, t.K, t.ldru), "core RU", i);
+        BC(t.RV, bc_span(t.K, t.K, t.ldrv), "core RV", i);
+        BC(t.SU, bc_span(t.K, t.K, t.K), "core SU", i);
+        if (t.RUc) BC(t.RUc, bc_span(t.K, t.K, t.K), "core RU copy", i);
+        if (t.work) BC(t.work, core_work_doubles(t.K) * sizeof(double), "core scratch", i);
+        if (t.rank_out) BC(t.rank_out, sizeof(int), "core rank", i);
+        if (t.rank_task) BC(t.rank_task, sizeof(int), "core task rank", i);
+    }
+#else
+    (void)v;
+#endif
+    return 0;
+}
+
+static int bc_cov(const CovParams &p, const std::vector<CovTask> &v) {
+#ifdef TLR_BOUNDS_CHECK
+    BC(p.pts, bc_span(p.N, p.ndim, p.N), "points", 0);
+    for (size_t i = 0; i < v.size(); ++i) {
+        const CovTask &t = v[i];
+        BC(t.out, bc_span(t.nr, t.nc, t.ld), "covariance tile", i);
+        if (t.r0 < 0 || t.c0 < 0 || t.r0 + t.nr > p.N || t.c0 + t.nc > p.N) {
+            set_err("bounds check: covariance tile %zu reads rows/cols outside 0..%d", i, p.N);
+            return HICMA_TLR_ERR_ARG;
+        }
+    }
+#else
+    (void)p; (void)v;
+#endif
+    return 0;
+}
+
+static int bc_recompress_parts(const std::vector<SelTask> &sels, const std::vector<GramTask> &grams,
+                               const std::vector<ProjTask> &projs, const std::vector<AssembleTask> &asm_) {
+#ifdef TLR_BOUNDS_CHECK
+    for (size_t i = 0; i < sels.size(); ++i) {
+        BC(sels[i].na, sizeof(double), "precision norm a", i);
+        BC(sels[i].nb, sizeof(double), "precision norm b", i);
+        BC(sels[i].sel64, sizeof(int), "precision count 64", i);
+        BC(sels[i].sel32, sizeof(int), "precision count 32", i);
+    }
+    for (size_t i = 0; i < grams.size(); ++i) {
+        const GramTask &t = grams[i];
+        BC(t.C, bc_span(t.nb, t.rc, t.nb), "gram C", i);
+        BC(t.W, bc_span(t.nb, t.ra, t.nb), "gram W", i);
+        BC(t.P, bc_span(t.rc, t.ra, t.rc), "gram P", i);
+    }
+    for (size_t i = 0; i < projs.size(); ++i) {
+        const ProjTask &t = projs[i];
+        BC(t.C, bc_span(t.nb, t.rc, t.nb), "projection C", i);
+        BC(t.W, bc_span(t.nb, t.ra, t.nb), "projection W", i);
+        BC(t.P, bc_span(t.rc, t.ra, t.rc), "projection P", i);
+        BC(t.P2, bc_span(t.rc, t.ra, t.rc), "projection P2", i);
+    }
+    for (size_t i = 0; i < asm_.size(); ++i) {
+        const AssembleTask &t = asm_[i];
+        const int K = t.rc + t.ra;
+        BC(t.Pu, bc_span(t.rc, t.ra, t.rc), "assemble Pu", i);
+        BC(t.Wu, bc_span(t.ra, t.ra, t.nb), "assemble Wu", i);
+        BC(t.RU, bc_span(K, K, K), "assemble RU", i);
+    }
+#else
+    (void)sels; (void)grams; (void)projs; (void)asm_;
+#endif
+    return 0;
+}
+
+static int bc_norms(const std::vector<NormTask> &v) {
+#ifdef TLR_BOUNDS_CHECK
+    for (size_t i = 0; i < v.size(); ++i) {
+        BC(v[i].X, bc_span(v[i].rows, v[i].cols, v[i].ld), "norm X", i);
+        BC(v[i].out, sizeof(double), "norm out", i);
+    }
+#else
+    (void)v;
+#endif
+    return 0;
+}
+
 int run_qr(hicma_tlr_ctx *c, std::vector<QRTask> &v, int m_max) {
     if (v.empty()) return 0;
+    TRY(bc_qr(v, m_max));
     QRTask *d = stage(c, v.data(), v.size());
     if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
     double fl = 0, by = 0;
@@ -270,6 +474,7 @@ int run_qr(hicma_tlr_ctx *c, std::vector<QRTask> &v, int m_max) {
 
 int run_qapply(hicma_tlr_ctx *c, std::vector<QApplyTask> &v, int m_max) {
     if (v.empty()) return 0;
+    TRY(bc_qapply(v, m_max));
     QApplyTask *d = stage(c, v.data(), v.size());
     if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
     double by = 0;
@@ -284,6 +489,7 @@ int run_qapply(hicma_tlr_ctx *c, std::vector<QApplyTask> &v, int m_max) {
 
 int run_core(hicma_tlr_ctx *c, std::vector<CoreTask> &v, int kmax, const CoreParams &cp) {
     if (v.empty()) return 0;
+    TRY(bc_cores(v));
     CoreTask *d = stage(c, v.data(), v.size());
     if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
     {
@@ -298,6 +504,7 @@ int run_gemms_narrow(hicma_tlr_ctx *c, std::vector<GemmTask> &v, int cls);
 
 int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false, int cls = 0) {
     if (v.empty()) return 0;
+    TRY(bc_gemms(v));
     if (!fp32) {
         // outputs a rank wide go to the 128 x 32 tile variant
         std::vector<GemmTask> narrow, wide;
@@ -351,6 +558,7 @@ int run_gemms_narrow(hicma_tlr_ctx *c, std::vector<GemmTask> &v, int cls) {
 
 int run_copies(hicma_tlr_ctx *c, std::vector<CopyTask> &v) {
     if (v.empty()) return 0;
+    TRY(bc_copies(v));
     int maxc = 0;
     for (auto &t : v) maxc = std::max(maxc, t.cols);
     CopyTask *dt = stage(c, v.data(), v.size());
@@ -378,6 +586,11 @@ CopyTask make_copy(const double *src, int lds, double *dst, int ldd, int rows, i
 // SYRK.  With Linv, L^-1 is then assembled block row by block row.
 int potrf_tile(hicma_tlr_ctx *c, double *A, int n, int lda, double *Linv, int ldl, int *d_info,
                int info_base) {
+#ifdef TLR_BOUNDS_CHECK
+    BC(A, bc_span(n, n, lda), "potrf tile", 0);
+    if (Linv) BC(Linv, bc_span(n, n, ldl), "potrf inverse", 0);
+    BC(d_info, sizeof(int), "potrf info", 0);
+#endif
     const int DBK = 64;
     cudaStream_t st = c->cur;
     const size_t mark = c->ar->off;
@@ -602,6 +815,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             b.n_dev = ct.rank_task;
             g4.push_back(b);
         }
+        TRY(bc_recompress_parts(sels, grams, projs, asm_));
         TRY(run_copies(c, copies));
         if (!sels.empty()) {
             SelTask *d = stage(c, sels.data(), sels.size());
@@ -785,6 +999,10 @@ static void ctx_release(hicma_tlr_ctx *c) {
         cudaEventDestroy(r.b);
     }
     for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+    bc_remove(c->d_ws);
+    bc_remove(c->d_stage);
+    bc_remove(c->d_flags);
+    bc_remove(c->d_scal);
     if (c->d_ws) cudaFree(c->d_ws);
     if (c->d_stage) cudaFree(c->d_stage);
     if (c->h_stage) cudaFreeHost(c->h_stage);
@@ -842,6 +1060,10 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     if ((e = cudaMalloc(&c->d_stage, c->stage_bytes)) != cudaSuccess) { c->d_stage = nullptr; return fail(e, "device staging"); }
     if ((e = cudaMalloc(&c->d_flags, 64 * sizeof(int))) != cudaSuccess) { c->d_flags = nullptr; return fail(e, "flags"); }
     if ((e = cudaMalloc(&c->d_scal, 64 * sizeof(double))) != cudaSuccess) { c->d_scal = nullptr; return fail(e, "scalars"); }
+    bc_add(c->d_ws, c->ws_bytes);
+    bc_add(c->d_stage, c->stage_bytes);
+    bc_add(c->d_flags, 64 * sizeof(int));
+    bc_add(c->d_scal, 64 * sizeof(double));
     if ((e = cudaMemset(c->d_flags, 0, 64 * sizeof(int))) != cudaSuccess) return fail(e, "flags reset");
     if ((e = cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
         return fail(e, "SM count");
@@ -853,7 +1075,12 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
 // result depends on what the memory held before.
 static cudaError_t dev_alloc(hicma_tlr_ctx *c, void **p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
-    if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, bytes, c->stream);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return e;
+    }
+    bc_add(*p, bytes);
+    e = cudaMemsetAsync(*p, 0, bytes, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     return e;
 }
@@ -863,6 +1090,7 @@ static void dev_free(hicma_tlr_ctx *c, void *p) {
         cudaStreamSynchronize(c->stream_hi);
         cudaStreamSynchronize(c->stream);
     }
+    bc_remove(p);
     cudaFree(p);
 }
 
@@ -1105,6 +1333,7 @@ static int gen_band_tiles(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_p
     for (int m = 0; m < A->NT; ++m)
         for (int n = std::max(m - A->band + 1, 0); n <= m; ++n)
             tasks.push_back(CovTask{A->dense(m, n), A->NB, m * A->NB, n * A->NB, A->NB, A->NB});
+    TRY(bc_cov(cov_params(A, prob), tasks));
     CovTask *dt = stage(c, tasks.data(), tasks.size());
     if (!dt) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
     Prof pf(c, P_COV, 0, 8.0 * tasks.size() * (double)A->NB * A->NB);
@@ -1251,6 +1480,7 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
                 cov.push_back(CovTask{D, NB, m * NB, n * NB, NB, NB});
                 comp.push_back(CompressTask{D, A->U(m, n), A->V(m, n), A->d_rank + (size_t)n * NT + m});
             }
+            TRY(bc_cov(cp, cov));
             CovTask *dcov = stage(c, cov.data(), cov.size());
             if (!dcov) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
             {
@@ -1613,6 +1843,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                 for (int m = k + 1; m < NT; ++m)
                     if (!A->is_dense(m, k)) nt.push_back(NormTask{A->V(m, k), NB, A->rank(m, k), NB, d_fro2 + m});
                 if (!nt.empty()) {
+                    TRY(bc_norms(nt));
                     NormTask *d = stage(c, nt.data(), nt.size());
                     if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
                     launch_sumsq_batched(d, (int)nt.size(), c->stream);
@@ -2199,6 +2430,7 @@ int hicma_tlr_check_probe(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_p
                     cpy.push_back(make_copy(pt, NB, AZ + (size_t)n * NB, (int)N, NB, p, 1.0, 1.0));
                 }
             }
+            TRY(bc_cov(cp, ct));
             CovTask *dct = stage(c, ct.data(), ct.size());
             if (!dct) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
             launch_cov_batched(cp, dct, (int)ct.size(), NB, NB, c->stream);
@@ -2284,7 +2516,12 @@ int hicma_tlr_check(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_problem
     const size_t N = L->N;
     double *DL = nullptr, *DA = nullptr, *D0 = nullptr, *part = nullptr, *sc = nullptr;
     int *dinfo = nullptr;
-    auto cleanup = [&]() { cudaFree(DL); cudaFree(DA); cudaFree(D0); cudaFree(part); cudaFree(sc); cudaFree(dinfo); };
+    auto cleanup = [&]() {
+        for (void *p : {(void *)DL, (void *)DA, (void *)D0, (void *)part, (void *)sc, (void *)dinfo}) {
+            bc_remove(p);
+            cudaFree(p);
+        }
+    };
     const int nblk = 1024;
     if (cudaMalloc(&DL, N * N * sizeof(double)) != cudaSuccess || cudaMalloc(&DA, N * N * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&part, nblk * sizeof(double)) != cudaSuccess || cudaMalloc(&sc, 8 * sizeof(double)) != cudaSuccess ||
@@ -2294,6 +2531,11 @@ int hicma_tlr_check(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_problem
         set_err("check: allocation of dense N x N buffers failed (N = %zu)", N);
         return HICMA_TLR_ERR_OOM;
     }
+    bc_add(DL, N * N * sizeof(double));
+    bc_add(DA, N * N * sizeof(double));
+    bc_add(part, nblk * sizeof(double));
+    bc_add(sc, 8 * sizeof(double));
+    bc_add(dinfo, sizeof(int));
     int rc = densify(c, L, DL);
     if (rc) { cleanup(); return rc; }
     // exact A (check_dpotrf2 uses the unapproximated matrix, testing_dpotrf.c:856-893)
@@ -2308,10 +2550,12 @@ int hicma_tlr_check(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_problem
     if (A0 && res_diff) {
         if (cudaMalloc(&D0, N * N * sizeof(double)) != cudaSuccess) {
             cudaGetLastError();
+            D0 = nullptr;
             cleanup();
             set_err("check: allocation failed");
             return HICMA_TLR_ERR_OOM;
         }
+        bc_add(D0, N * N * sizeof(double));
         rc = densify(c, A0, D0);
         if (rc) { cleanup(); return rc; }
         cudaMemsetAsync(dinfo, 0, sizeof(int), c->stream);
@@ -2348,6 +2592,47 @@ int hicma_tlr_k_cov(const hicma_tlr_problem *prob, const double *d_points, int N
     CUDA_TRY(cudaFreeAsync(dt, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     return 0;
+}
+
+int hicma_tlr_bounds_checked(void) {
+#ifdef TLR_BOUNDS_CHECK
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+int hicma_tlr_bounds_register(const void *p, size_t bytes) {
+#ifdef TLR_BOUNDS_CHECK
+    ARG_CHECK(p && bytes, "bounds_register arguments");
+    bc_add(p, bytes);
+    return 0;
+#else
+    (void)p; (void)bytes;
+    set_err("this library was built without TLR_BOUNDS_CHECK");
+    return HICMA_TLR_ERR_NOT_SUPPORTED;
+#endif
+}
+
+int hicma_tlr_bounds_unregister(const void *p) {
+#ifdef TLR_BOUNDS_CHECK
+    bc_remove(p);
+    return 0;
+#else
+    (void)p;
+    set_err("this library was built without TLR_BOUNDS_CHECK");
+    return HICMA_TLR_ERR_NOT_SUPPORTED;
+#endif
+}
+
+int hicma_tlr_bounds_inside(const void *p, size_t bytes) {
+#ifdef TLR_BOUNDS_CHECK
+    return bc_inside(p, bytes) ? 1 : 0;
+#else
+    (void)p; (void)bytes;
+    set_err("this library was built without TLR_BOUNDS_CHECK");
+    return HICMA_TLR_ERR_NOT_SUPPORTED;
+#endif
 }
 
 int hicma_tlr_k_wait_probe(long long polls0, long long polls1, int nblocks, double *elapsed_ms, void *stream) {
@@ -2397,6 +2682,10 @@ int hicma_tlr_k_dgemm(int transA, int transB, int m, int n, int k, double alpha,
 int hicma_tlr_k_potrf(hicma_tlr_ctx *c, int n, double *d_A, int lda, double *d_linv, int *d_info, int info_offset) {
     ARG_CHECK(c && d_A && n > 0 && lda >= n && d_info, "k_potrf arguments");
     std::lock_guard<std::recursive_mutex> lk(c->mu);
+    BcScope bc;
+    bc.add(d_A, bc_span(n, n, lda));
+    if (d_linv) bc.add(d_linv, bc_span(n, n, n));
+    bc.add(d_info, sizeof(int));
     ws_reset(c);
     TRY(potrf_tile(c, d_A, n, lda, d_linv, n, d_info, info_offset));
     TRY(ctx_sync(c));
@@ -2409,6 +2698,13 @@ int hicma_tlr_k_lr_update(hicma_tlr_ctx *c, int nb, const double *d_Au, const do
     ARG_CHECK(c && rc && d_Cu && d_Cv && nb > 0, "k_lr_update arguments");
     ARG_CHECK(ra >= 0 && rb >= 0 && *rc >= 0 && maxrank >= 1, "ranks");
     std::lock_guard<std::recursive_mutex> lk(c->mu);
+    BcScope bc;
+    bc.add(d_Au, bc_span(nb, ra, nb));
+    bc.add(d_Av, bc_span(nb, ra, nb));
+    bc.add(d_Bu, bc_span(nb, rb, nb));
+    bc.add(d_Bv, bc_span(nb, rb, nb));
+    bc.add(d_Cu, bc_span(nb, maxrank, nb));
+    bc.add(d_Cv, bc_span(nb, maxrank, nb));
     ws_reset(c);
     int *d_r = ws_alloc<int>(c, 2);
     if (!d_r) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
@@ -2427,6 +2723,10 @@ int hicma_tlr_k_compress(hicma_tlr_ctx *c, int nb, const double *d_A, double *d_
                          double tol, int *rank) {
     ARG_CHECK(c && d_A && d_U && d_V && rank && nb > 0 && maxrank >= 1 && tol > 0, "k_compress arguments");
     std::lock_guard<std::recursive_mutex> lk(c->mu);
+    BcScope bc;
+    bc.add(d_A, bc_span(nb, nb, nb));
+    bc.add(d_U, bc_span(nb, maxrank, nb));
+    bc.add(d_V, bc_span(nb, maxrank, nb));
     ws_reset(c);
     const int s = std::min(maxrank + 10, nb);
     double *Omega = ws_alloc<double>(c, (size_t)nb * s);

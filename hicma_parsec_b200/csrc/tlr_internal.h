@@ -9,6 +9,27 @@
 
 namespace tlr {
 
+// ------------------------------------------------------- bounds checking ----
+// Builds with TLR_BOUNDS_CHECK check on the host, before every batched launch,
+// that each task's operand extents lie inside one live device region (library
+// allocations, the workspace, or caller buffers registered for the length of
+// a kernel-level call); a launch that would leave them is refused with
+// HICMA_TLR_ERR_ARG and the offending task in the error message.  Other
+// builds compile the checks away.
+#ifdef TLR_BOUNDS_CHECK
+void bc_add(const void *p, size_t bytes);
+void bc_remove(const void *p);
+bool bc_inside(const void *p, size_t bytes);
+#else
+inline void bc_add(const void *, size_t) {}
+inline void bc_remove(const void *) {}
+inline bool bc_inside(const void *, size_t) { return true; }
+#endif
+// Bytes spanned by a rows x cols column-major block with leading dimension ld.
+inline size_t bc_span(long long rows, long long cols, long long ld, size_t elt = sizeof(double)) {
+    return rows <= 0 || cols <= 0 ? 0 : (size_t)((cols - 1) * ld + rows) * elt;
+}
+
 // ----------------------------------------------------------- batched DGEMM --
 // One problem of a batched C = alpha op(A) op(B) + beta C.  Tiles of 64x64
 // outputs are flattened over the batch with tile_off (prefix sums).

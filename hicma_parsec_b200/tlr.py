@@ -21,6 +21,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libhicma_tlr.so")
+# HICMA_TLR_LIB=checked selects the bounds-checked build (every batched launch
+# validated on the host first); a path selects that file.
+LIB_PATH_CHECKED = os.path.join(HERE, "lib", "libhicma_tlr_checked.so")
 
 LOWER = 122
 UPPER = 121
@@ -78,7 +81,8 @@ def load_library(path: str | None = None):
     global _lib
     if _lib is not None:
         return _lib
-    path = path or LIB_PATH
+    env = os.environ.get("HICMA_TLR_LIB", "")
+    path = path or (LIB_PATH_CHECKED if env == "checked" else (env or LIB_PATH))
     if not os.path.exists(path):
         raise RuntimeError(f"CUDA library not built: {path} (run python -m hicma_parsec_b200.build)")
     lib = C.CDLL(path)
@@ -113,6 +117,10 @@ def load_library(path: str | None = None):
         "hicma_tlr_loglik": (i, [vp, vp, vp, dp, dp, vp]),
         "hicma_tlr_rank_history": (i, [vp, vp, vp, vp, vp]),
         "hicma_tlr_k_wait_probe": (i, [C.c_longlong, C.c_longlong, i, dp, vp]),
+        "hicma_tlr_bounds_checked": (i, []),
+        "hicma_tlr_bounds_register": (i, [vp, C.c_size_t]),
+        "hicma_tlr_bounds_unregister": (i, [vp]),
+        "hicma_tlr_bounds_inside": (i, [vp, C.c_size_t]),
         "hicma_tlr_serve_loglik": (i, [vp, C.POINTER(CProblem), i, i, d, i, i, vp, dp, dp, vp, ip]),
         "hicma_tlr_last_stats": (i, [vp, vp, i]),
         "hicma_tlr_check": (i, [vp, vp, C.POINTER(CProblem), vp, dp, dp]),

@@ -316,6 +316,21 @@ int hicma_tlr_k_compress(hicma_tlr_ctx *ctx, int nb, const double *d_A, double *
 int hicma_tlr_k_potrf_noalloc(int n, double *d_A, int lda, double *d_linv, int *d_info,
                               int info_offset, void *stream);
 
+/* Bounds-checked builds (libhicma_tlr_checked.so, compiled with
+ * TLR_BOUNDS_CHECK; no reference counterpart): before every batched launch
+ * the host checks that each task's operand extents lie inside one live device
+ * region and refuses the launch with HICMA_TLR_ERR_ARG otherwise.  Regions are
+ * the library's own allocations, the context workspace, and caller buffers
+ * passed to the kernel-level entries (registered for the length of the call).
+ * _checked returns 1 in such a build, 0 otherwise; the other three manage and
+ * query the region list directly (HICMA_TLR_ERR_NOT_SUPPORTED in a build
+ * without the checks); _inside returns 1 when [p, p + bytes) lies in one
+ * region. */
+int hicma_tlr_bounds_checked(void);
+int hicma_tlr_bounds_register(const void *p, size_t bytes);
+int hicma_tlr_bounds_unregister(const void *p);
+int hicma_tlr_bounds_inside(const void *p, size_t bytes);
+
 /* Test of the bounded dependency wait of the tile POTRF task queue (no
  * reference counterpart): nblocks (1..64) CTAs each wait, with the queue's own
  * wait routine, on a counter that nothing sets; CTA 0 gives up after polls0
