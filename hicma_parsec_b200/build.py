@@ -62,7 +62,7 @@ def _compile(nvcc: str, src: str, force: bool, checked: bool = False) -> tuple[s
 
 def _link(nvcc: str, out: str, objs: list[str], force: bool) -> None:
     if force or not _newer(out, objs):
-        cmd = [nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", out, *objs, "-lpthread"]
+        cmd = [nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", out, *objs, "-lpthread", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -13,6 +13,8 @@
 // panel's tasks depend on the ranks the recompressions produced).
 #include "tlr_internal.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <array>
 #include <chrono>
@@ -70,6 +72,20 @@ bool tlr::bc_inside(const void *p, size_t bytes) {
     return false;
 }
 #endif
+
+// Named host range of a phase in profiler timelines (NVTX; a no-op unless a
+// tool is attached).  end() closes it early; the destructor closes it otherwise.
+struct NvtxRange {
+    bool open = true;
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    void end() {
+        if (open) {
+            nvtxRangePop();
+            open = false;
+        }
+    }
+    ~NvtxRange() { end(); }
+};
 
 // Registers caller buffers for the length of a kernel-level call (bounds-checked builds).
 struct BcScope {
@@ -1436,6 +1452,7 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
     ARG_CHECK(maxrank >= 1 && maxrank <= A->maxrank, "maxrank must be in [1, descriptor maxrank]");
     ARG_CHECK(tol > 0.0, "tol > 0");
     std::lock_guard<std::recursive_mutex> lk(c->mu);
+    NvtxRange nv("STARSH_gen");
     CUDA_TRY(cudaSetDevice(c->device));
     if (info) *info = 0;
     c->cur = c->stream;
@@ -1614,6 +1631,7 @@ int hicma_tlr_band_regenerate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, con
     ARG_CHECK(band_size >= A->slot_band, "band_size cannot shrink below the slot band");
     TRY(check_problem_data(A, prob));
     std::lock_guard<std::recursive_mutex> lk(c->mu);
+    NvtxRange nv("band_regenerate");
     const int NT = A->NT, NB = A->NB;
     band_size = std::min(band_size, NT);
     TRY(ctx_sync(c));
@@ -1808,11 +1826,13 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     CUDA_TRY(cudaEventSynchronize(ev[P1]));
     t_phase[0] += elapsed(ev[P0], ev[P1]);
     for (int k = 0; k < NT; ++k) {
+        NvtxRange nv_panel("panel");
         const double *Li = A->linv(k);
         CUDA_TRY(cudaStreamWaitEvent(c->stream, evP, 0));
         // ---- TRSM(m, k): dense C <- C L^-T ; low rank V <- L^-1 V (:366-401)
         CUDA_TRY(cudaEventRecord(ev[T0], c->stream));
         {
+            NvtxRange nv("TRSM");
             c->ar->off = base_mark;
             std::vector<GemmTask> g;
             std::vector<CopyTask> cp;
@@ -1862,6 +1882,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             log_op(op_counts('c', NB, 0, 0, 0), k + 1, k + 1, true);
             {
                 OnHi h(c);
+                NvtxRange nv("SYRK+POTRF(k+1)");
                 if (!lookahead) c->cur = c->stream;
                 c->ar->off = 0;
                 CUDA_TRY(cudaStreamWaitEvent(c->cur, evT, 0));
@@ -1873,6 +1894,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                 CUDA_TRY(cudaEventRecord(evP, c->cur));
             }
             // ---- SYRK(k, m), m > k+1
+            NvtxRange nv_syrk("SYRK");
             CUDA_TRY(cudaEventRecord(ev[S0], c->stream));
             c->ar->off = base_mark;
             std::vector<int> ms;
@@ -1883,7 +1905,9 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             }
             TRY(run_syrk(c, A, k, ms));
             CUDA_TRY(cudaEventRecord(ev[S1], c->stream));
+            nv_syrk.end();
             // ---- GEMM(m, n, k) (:699-1097)
+            NvtxRange nv_gemm("GEMM");
             CUDA_TRY(cudaEventRecord(ev[G0], c->stream));
             c->ar->off = base_mark;
             std::vector<GemmTask> g1, g2, g3;
@@ -2049,6 +2073,7 @@ int hicma_tlr_dpotrf_L(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, d
     // the reference would have run.
     if (two_flow && (band_size != 1 || *two_flow)) *two_flow = 1;
     std::lock_guard<std::recursive_mutex> lk(c->mu);
+    NvtxRange nv("HiCMA_dpotrf_L");
     CUDA_TRY(cudaSetDevice(c->device));
     const bool la = !(lookahead && *lookahead == 0);
     const int info = factorize(c, A, acc, fixed_rank, maxrank, tileopcounters, opcounters, critical_path_time, verbose, la);
@@ -2299,6 +2324,7 @@ int hicma_tlr_solve(hicma_tlr_ctx *c, hicma_tlr_desc *A, int nrhs, double *B, lo
     ARG_CHECK(c && A && B && nrhs > 0 && ldb >= A->N, "solve arguments");
     if (!A->factored) { set_err("descriptor is not factored"); return HICMA_TLR_ERR_STATE; }
     std::lock_guard<std::recursive_mutex> lk(c->mu);
+    NvtxRange nv("solve");
     CUDA_TRY(cudaSetDevice(c->device));
     ws_reset(c);
     const size_t N = A->N;
@@ -2386,6 +2412,7 @@ int hicma_tlr_check_probe(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_p
     if (!L->factored) { set_err("descriptor is not factored"); return HICMA_TLR_ERR_STATE; }
     TRY(check_problem_data(L, prob));
     std::lock_guard<std::recursive_mutex> lk(c->mu);
+    NvtxRange nv("check_probe");
     CUDA_TRY(cudaSetDevice(c->device));
     c->cur = c->stream;
     c->ar = &c->main_ar;
@@ -2512,6 +2539,7 @@ int hicma_tlr_check(hicma_tlr_ctx *c, hicma_tlr_desc *L, const hicma_tlr_problem
     if (!L->factored) { set_err("descriptor is not factored"); return HICMA_TLR_ERR_STATE; }
     TRY(check_problem_data(L, prob));
     std::lock_guard<std::recursive_mutex> lk(c->mu);
+    NvtxRange nv("check");
     CUDA_TRY(cudaSetDevice(c->device));
     const size_t N = L->N;
     double *DL = nullptr, *DA = nullptr, *D0 = nullptr, *part = nullptr, *sc = nullptr;
