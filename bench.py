@@ -306,6 +306,7 @@ def run_ours(args, cfg):
     ctx.set_precision(tlr.PREC_MIXED if args.precision == "mixed" else tlr.PREC_FP64)
     prob = tlr.Problem(kind=cfg["kind"], noise=cfg["noise"], beta=0.1, sigma=1.0, seed=0)
     n, nb, mr, acc = cfg["n"], cfg["nb"], cfg["maxrank"], cfg["acc"]
+    tuned = ctx.autotune(nb, mr) if getattr(args, "autotune", False) else None
     A0 = tlr.TLRMatrix(ctx, n, nb, mr, cfg["band"])
     t0 = time.perf_counter()
     info = A0.generate(prob, acc, mr)
@@ -482,6 +483,8 @@ def run_ours(args, cfg):
                            "l2": "inputs larger than L2 (compressed matrix ~%.1f GB resident)" % (A0.store_bytes() / 1e9),
                            "step": "device copy of the pristine compressed matrix + full TLR factorization",
                            "generation_s": t_gen, "autoband_s": t_band, "loglik_s": t_loglik,
+                           "kernel_choices": {"gemm_narrow_n": ctx.tuning()[0], "potrf_grid": ctx.tuning()[1],
+                                              "autotuned": tuned is not None},
                            "rank_min_max_avg": [rmin, rmax, ravg],
                            "final_rank_min_max_avg": list(tlr.HICMA_get_stat2(W.rank_map(), n // nb, W.band_size))},
                 "tlr_tflops": total_ops / s_per_factor / world / 1e12 if world else None,
@@ -542,6 +545,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--autotune", action="store_true",
+                    help="measure the kernel choices (hicma_tlr_autotune) before generation and use them")
     ap.add_argument("--serving", action="store_true", help="run the MLE serving benchmark instead")
     ap.add_argument("--accuracy", action="store_true",
                     help="also compare the log-determinant with a factorization at e/100")

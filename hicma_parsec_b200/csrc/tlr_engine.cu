@@ -22,6 +22,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <set>
 #include <string>
@@ -136,6 +137,9 @@ struct hicma_tlr_ctx_s {
     size_t stage_bytes = 0, stage_off = 0;
     int *d_flags = nullptr;     // [0] info, [1] overflow, [2] Jacobi sweeps, [3] wait timed out, [4] FP32 updates
     int nsm = 148;              // SM count of the device
+    // choices the autotuner measures (defaults: the hand-picked values)
+    int gemm_narrow_n = GEMM_NARROW_N;   // rank-wide outputs up to this width use 128 x 32 tiles
+    int potrf_grid = 0;                  // CTAs of the persistent tile POTRF (0: one per SM)
     double *d_scal = nullptr;   // device scalars
     int precision = HICMA_TLR_PREC_FP64;
     long long launches = 0;
@@ -524,7 +528,7 @@ int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false, int
     if (!fp32) {
         // outputs a rank wide go to the 128 x 32 tile variant
         std::vector<GemmTask> narrow, wide;
-        for (auto &t : v) ((t.n <= GEMM_NARROW_N || t.n_dev) && !t.lower ? narrow : wide).push_back(t);
+        for (auto &t : v) ((t.n <= c->gemm_narrow_n || t.n_dev) && !t.lower ? narrow : wide).push_back(t);
         if (!narrow.empty()) {
             TRY(run_gemms_narrow(c, narrow, cls));
             if (wide.empty()) { v.clear(); return 0; }
@@ -618,7 +622,8 @@ int potrf_tile(hicma_tlr_ctx *c, double *A, int n, int lda, double *Linv, int ld
         double *D = Linv ? nullptr : ws_alloc<double>(c, (size_t)nblk * DBK * DBK);
         if (!cnt || (!Linv && !D)) { set_err("workspace exhausted (potrf)"); return HICMA_TLR_ERR_OOM; }
         if (Linv) CUDA_TRY(cudaMemset2DAsync(Linv, (size_t)ldl * sizeof(double), 0, sizeof(double) * n, n, st));
-        if (launch_potrf_tile(A, lda, n, Linv, ldl, D, cnt, d_info, info_base, c->d_flags + 3, c->nsm, st)) {
+        const int grid = c->potrf_grid > 0 ? c->potrf_grid : c->nsm;
+        if (launch_potrf_tile(A, lda, n, Linv, ldl, D, cnt, d_info, info_base, c->d_flags + 3, grid, st)) {
             set_err("tile POTRF launch failed: %s", cudaGetErrorString(cudaGetLastError()));
             return HICMA_TLR_ERR_CUDA;
         }
@@ -1140,6 +1145,141 @@ void *hicma_tlr_stream(hicma_tlr_ctx *c) { return c ? (void *)c->stream : nullpt
 int hicma_tlr_set_precision(hicma_tlr_ctx *c, int precision) {
     ARG_CHECK(c && (precision == HICMA_TLR_PREC_FP64 || precision == HICMA_TLR_PREC_MIXED), "precision");
     c->precision = precision;
+    return 0;
+}
+
+// ------------------------------------------------------------- autotuner ----
+// Median device time (ms) of `reps` runs of `body` between events on the
+// context stream.
+static int time_median(hicma_tlr_ctx *c, int reps, const std::function<int()> &body, double *ms) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    std::vector<double> t;
+    int rc = 0;
+    for (int r = 0; r < reps && !rc; ++r) {
+        cudaEventRecord(e0, c->stream);
+        rc = body();
+        cudaEventRecord(e1, c->stream);
+        float v = 0.f;
+        if (!rc && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&v, e0, e1) == cudaSuccess)
+            t.push_back(v);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (t.empty()) { set_err("autotune: timing failed"); return HICMA_TLR_ERR_CUDA; }
+    std::sort(t.begin(), t.end());
+    *ms = t[t.size() / 2];
+    return 0;
+}
+
+int hicma_tlr_autotune(hicma_tlr_ctx *c, int NB, int maxrank, int reps, int *tuning, double *ms_out) {
+    ARG_CHECK(c && NB >= 64 && maxrank >= 1 && maxrank <= NB && reps >= 1 && reps <= 50, "autotune arguments");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    CUDA_TRY(cudaSetDevice(c->device));
+    c->cur = c->stream;
+    c->ar = &c->main_ar;
+    ws_reset(c);
+    const int keep_n = c->gemm_narrow_n, keep_g = c->potrf_grid;
+    auto restore = [&]() { c->gemm_narrow_n = keep_n; c->potrf_grid = keep_g; ws_reset(c); };
+    double times[12];
+    for (double &v : times) v = NAN;
+
+    // ---- tile POTRF grid: an SPD tile A0 = G G^T / NB + I, factored with each grid
+    double *G = ws_alloc<double>(c, (size_t)NB * NB), *A0 = ws_alloc<double>(c, (size_t)NB * NB);
+    double *At = ws_alloc<double>(c, (size_t)NB * NB), *Li = ws_alloc<double>(c, (size_t)NB * NB);
+    int *dinfo = ws_alloc<int>(c, 4);
+    if (!G || !A0 || !At || !Li || !dinfo) { restore(); set_err("autotune: workspace too small"); return HICMA_TLR_ERR_OOM; }
+    const size_t after_potrf_bufs = c->ar->off;
+    launch_gaussian(G, NB, NB, NB, 0x4155544FULL, c->stream);
+    launch_set_identity(A0, NB, NB, c->stream);
+    {
+        std::vector<GemmTask> g{make_gemm(0, 1, NB, NB, NB, 1.0 / NB, G, NB, G, NB, 1.0, A0, NB)};
+        int rc = run_gemms(c, g);
+        if (rc) { restore(); return rc; }
+    }
+    CUDA_TRY(cudaMemsetAsync(dinfo, 0, sizeof(int), c->stream));
+    const int grids[3] = {std::max(1, c->nsm / 2), c->nsm, 2 * c->nsm};
+    int best_g = c->nsm;
+    double best_t = INFINITY;
+    for (int gi = 0; gi < 3; ++gi) {
+        c->potrf_grid = grids[gi];
+        double ms = 0;
+        int rc = time_median(c, reps, [&]() {
+            std::vector<CopyTask> cp{make_copy(A0, NB, At, NB, NB, NB)};
+            TRY(run_copies(c, cp));
+            c->ar->off = after_potrf_bufs;
+            return potrf_tile(c, At, NB, NB, Li, NB, dinfo, 0);
+        }, &ms);
+        if (rc) { restore(); return rc; }
+        times[gi] = ms;
+        if (ms < best_t) { best_t = ms; best_g = grids[gi]; }
+    }
+    int hinfo = 0;
+    CUDA_TRY(cudaMemcpy(&hinfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost));
+    if (hinfo != 0) { restore(); set_err("autotune: test tile not positive definite (info %d)", hinfo); return HICMA_TLR_ERR_STATE; }
+    TRY(check_timeout(c));
+
+    // ---- rank-wide GEMM outputs: 128 x 32 tiles against 64 x 64 tiles for
+    // widths above the default, on batches shaped like the recompression
+    // products (m = NB rows, inner dimension 2n, distinct outputs)
+    c->ar->off = 0;
+    const int widths[4] = {48, 64, 96, 128};
+    const int kmax = 256;
+    double *Aop = ws_alloc<double>(c, (size_t)NB * kmax), *Bop = ws_alloc<double>(c, (size_t)kmax * 128);
+    if (!Aop || !Bop) { restore(); set_err("autotune: workspace too small"); return HICMA_TLR_ERR_OOM; }
+    const size_t per_out = ((size_t)NB * 128 * sizeof(double) + 1023) & ~(size_t)1023;
+    const int ntask = (int)std::min<size_t>(64, ws_free(c) / (per_out + 1024));
+    if (ntask < 4) { restore(); set_err("autotune: workspace too small"); return HICMA_TLR_ERR_OOM; }
+    std::vector<double *> outs(ntask);
+    for (int i = 0; i < ntask; ++i) outs[i] = ws_alloc<double>(c, (size_t)NB * 128);
+    launch_gaussian(Aop, NB, kmax, NB, 0x41555450ULL, c->stream);
+    launch_gaussian(Bop, kmax, 128, kmax, 0x41555451ULL, c->stream);
+    TRY(check_launch(c));
+    int narrow_n = GEMM_NARROW_N;
+    bool narrow_wins = true;
+    for (int wi = 0; wi < 4 && widths[wi] <= maxrank; ++wi) {   // outputs are at most maxrank wide
+        const int n = widths[wi], k = 2 * n;
+        double tn = 0, tw = 0;
+        for (int variant = 0; variant < 2; ++variant) {
+            c->gemm_narrow_n = variant == 0 ? n : 0;
+            double ms = 0;
+            int rc = time_median(c, reps, [&]() {
+                std::vector<GemmTask> g;
+                for (int i = 0; i < ntask; ++i) g.push_back(make_gemm(0, 0, NB, n, k, 1.0, Aop, NB, Bop, kmax, 0.0, outs[i], NB));
+                return run_gemms(c, g);
+            }, &ms);
+            if (rc) { restore(); return rc; }
+            (variant == 0 ? tn : tw) = ms;
+        }
+        times[3 + 2 * wi] = tn;
+        times[4 + 2 * wi] = tw;
+        if (narrow_wins && tn <= tw) narrow_n = n;
+        else narrow_wins = false;
+    }
+    c->gemm_narrow_n = narrow_n;
+    c->potrf_grid = best_g;
+    ws_reset(c);
+    if (tuning) { tuning[0] = c->gemm_narrow_n; tuning[1] = c->potrf_grid; }
+    if (ms_out) std::memcpy(ms_out, times, 11 * sizeof(double));
+    return 0;
+}
+
+int hicma_tlr_tuning_get(hicma_tlr_ctx *c, int *tuning) {
+    ARG_CHECK(c && tuning, "tuning_get arguments");
+    tuning[0] = c->gemm_narrow_n;
+    tuning[1] = c->potrf_grid;
+    return 0;
+}
+
+int hicma_tlr_tuning_set(hicma_tlr_ctx *c, const int *tuning) {
+    ARG_CHECK(c && tuning, "tuning_set arguments");
+    ARG_CHECK(tuning[0] >= 0 && tuning[0] <= 4096, "gemm_narrow_n in [0, 4096]");
+    ARG_CHECK(tuning[1] >= 0 && tuning[1] <= 16 * c->nsm, "potrf_grid in [0, 16 x SMs]");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    c->gemm_narrow_n = tuning[0];
+    c->potrf_grid = tuning[1];
     return 0;
 }
 

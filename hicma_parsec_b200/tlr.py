@@ -118,6 +118,9 @@ def load_library(path: str | None = None):
         "hicma_tlr_rank_history": (i, [vp, vp, vp, vp, vp]),
         "hicma_tlr_k_wait_probe": (i, [C.c_longlong, C.c_longlong, i, dp, vp]),
         "hicma_tlr_bounds_checked": (i, []),
+        "hicma_tlr_autotune": (i, [vp, i, i, i, vp, vp]),
+        "hicma_tlr_tuning_get": (i, [vp, vp]),
+        "hicma_tlr_tuning_set": (i, [vp, vp]),
         "hicma_tlr_bounds_register": (i, [vp, C.c_size_t]),
         "hicma_tlr_bounds_unregister": (i, [vp]),
         "hicma_tlr_bounds_inside": (i, [vp, C.c_size_t]),
@@ -193,6 +196,27 @@ class Context:
 
     def set_precision(self, prec: int) -> None:
         _check(self.lib.hicma_tlr_set_precision(self.h, prec), "hicma_tlr_set_precision")
+
+    def autotune(self, nb: int, maxrank: int, reps: int = 3) -> dict:
+        """hicma_tlr_autotune: measure the kernel choices for tile size nb and keep
+        the fastest; returns the table and the measured medians (ms)."""
+        t = np.zeros(2, dtype=np.int32)
+        ms = np.full(11, np.nan)
+        _check(self.lib.hicma_tlr_autotune(self.h, nb, maxrank, reps, _p(t), _p(ms)), "hicma_tlr_autotune")
+        widths = (48, 64, 96, 128)
+        return {"gemm_narrow_n": int(t[0]), "potrf_grid": int(t[1]),
+                "potrf_ms": [float(v) for v in ms[:3]],
+                "gemm_ms": {w: {"128x32": float(ms[3 + 2 * i]), "64x64": float(ms[4 + 2 * i])}
+                            for i, w in enumerate(widths)}}
+
+    def tuning(self) -> tuple:
+        t = np.zeros(2, dtype=np.int32)
+        _check(self.lib.hicma_tlr_tuning_get(self.h, _p(t)), "hicma_tlr_tuning_get")
+        return int(t[0]), int(t[1])
+
+    def set_tuning(self, gemm_narrow_n: int, potrf_grid: int) -> None:
+        t = np.array([gemm_narrow_n, potrf_grid], dtype=np.int32)
+        _check(self.lib.hicma_tlr_tuning_set(self.h, _p(t)), "hicma_tlr_tuning_set")
 
     def close(self) -> None:
         if self.h:

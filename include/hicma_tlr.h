@@ -169,6 +169,23 @@ int hicma_tlr_dpotrf_L(hicma_tlr_ctx *ctx, int uplo, hicma_tlr_desc *A, int *Ar,
 /* Precision policy for later hicma_tlr_dpotrf_L calls on this context. */
 int hicma_tlr_set_precision(hicma_tlr_ctx *ctx, int precision);
 
+/* Autotuner (no reference counterpart): measures on this device, for tile size
+ * NB, the choices that have several valid kernels and keeps the fastest in the
+ * context for later calls:
+ *   tuning[0]  widest rank-wide GEMM output sent to the 128 x 32 tile variant
+ *              instead of 64 x 64 tiles (candidates 32, 48, 64, 96, 128, up to
+ *              maxrank; default 32), timed on batches shaped like the
+ *              recompression products;
+ *   tuning[1]  CTAs of the persistent tile POTRF (candidates SMs/2, SMs, 2 SMs;
+ *              0 = one per SM, the default), timed on an SPD NB x NB tile.
+ * Each candidate runs reps (1..50) times; medians in ms_out[11] (may be NULL):
+ * [0..2] POTRF per grid, then for widths 48, 64, 96, 128 the 128 x 32 and the
+ * 64 x 64 variant (NaN where not measured).  Uses the context workspace.
+ * _get / _set read or restore a table (e.g. one cached from an earlier run). */
+int hicma_tlr_autotune(hicma_tlr_ctx *ctx, int NB, int maxrank, int reps, int *tuning, double *ms_out);
+int hicma_tlr_tuning_get(hicma_tlr_ctx *ctx, int *tuning);
+int hicma_tlr_tuning_set(hicma_tlr_ctx *ctx, const int *tuning);
+
 /* Asynchronous form (HiCMA_dpotrf_L_2flow_New / _Destruct,
  * hicma_parsec/hicma_parsec_internal.h:295-315): _start enqueues, _wait
  * completes and returns the info. */

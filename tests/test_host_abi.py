@@ -80,6 +80,11 @@ def test_argument_errors_without_gpu(lib):
     assert lib.hicma_tlr_serve_loglik(None, ctypes.byref(prob), 10, 5, 1e-8, 0, 1,
                                       y.ctypes.data_as(ctypes.c_void_p), ctypes.byref(d), ctypes.byref(d),
                                       None, None) == tlr.ERR_ARG
+    # the autotuner and its table need a context
+    t = np.zeros(2, np.int32)
+    assert lib.hicma_tlr_autotune(None, 270, 130, 3, t.ctypes.data_as(ctypes.c_void_p), None) == tlr.ERR_ARG
+    assert lib.hicma_tlr_tuning_get(None, t.ctypes.data_as(ctypes.c_void_p)) == tlr.ERR_ARG
+    assert lib.hicma_tlr_tuning_set(None, t.ctypes.data_as(ctypes.c_void_p)) == tlr.ERR_ARG
     # the wait probe refuses out-of-range limits before touching the device
     assert lib.hicma_tlr_k_wait_probe(0, 1, 1, None, None) == tlr.ERR_ARG
     assert lib.hicma_tlr_k_wait_probe(1, 1, 65, None, None) == tlr.ERR_ARG
