@@ -33,7 +33,7 @@ from . import tlr
 @dataclass
 class MLERequest:
     rid: int
-    kind: int            # tlr.KIND_* (2D/3D sqexp, 3D exp)
+    kind: int            # tlr.KIND_* of a point kernel (statistics or electrodynamics)
     n: int
     nb: int
     beta: float          # length scale
