@@ -146,6 +146,7 @@ struct hicma_tlr_ctx_s {
     std::recursive_mutex mu;
     std::thread async_thread;
     int async_ret = 0;
+    std::string async_err;   // error message of the background factorization (its own thread's)
     std::set<hicma_tlr_desc_s *> descs;   // live descriptors, orphaned by fini
     // per-kernel-class profiling (CUDA events around launches on `stream`)
     bool prof = false;
@@ -2228,6 +2229,7 @@ int hicma_tlr_dpotrf_L_start(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, in
         int la = -1, tf = 0;
         c->async_ret = hicma_tlr_dpotrf_L(c, HICMA_TLR_LOWER, A, nullptr, acc, fixed_rank, maxrank, &la, A->band, A->NB,
                                           maxrank, 0, &tf, nullptr, nullptr, nullptr, 0);
+        c->async_err = c->async_ret < 0 ? hicma_tlr_last_error() : "";
     });
     return 0;
 }
@@ -2236,6 +2238,10 @@ int hicma_tlr_dpotrf_L_wait(hicma_tlr_ctx *c, hicma_tlr_desc *A, int *Ar) {
     ARG_CHECK(c && A, "null");
     if (!c->async_thread.joinable()) { set_err("no factorization in flight"); return HICMA_TLR_ERR_STATE; }
     c->async_thread.join();
+    if (c->async_ret < 0) {
+        set_err("%s", c->async_err.c_str());   // the message was set on the background thread
+        return c->async_ret;
+    }
     if (Ar) std::memcpy(Ar, A->h_rank.data(), (size_t)A->NT * A->NT * sizeof(int));
     return c->async_ret;
 }

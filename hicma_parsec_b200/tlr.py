@@ -290,6 +290,16 @@ class TLRMatrix:
         b = self.band_size
         return [(m, n) for m in range(b, self.nt) for n in range(0, m - b + 1) if G[n * self.nt + m] < 0]
 
+    def potrf_start(self, acc: float, maxrank: int | None = None, fixed_rank: int = 0) -> None:
+        """HiCMA_dpotrf_L_2flow_New: enqueue the factorization on a background
+        thread and return; potrf_wait() completes it."""
+        _check(self.lib.hicma_tlr_dpotrf_L_start(self.ctx.h, self.h, acc, fixed_rank, maxrank or self.maxrank),
+               "hicma_tlr_dpotrf_L_start")
+
+    def potrf_wait(self) -> int:
+        """Wait for potrf_start; returns info (errors raise)."""
+        return _check(self.lib.hicma_tlr_dpotrf_L_wait(self.ctx.h, self.h, None), "hicma_tlr_dpotrf_L_wait")
+
     def rank_history(self) -> dict:
         """Rank history of the last factorization: NT x NT arrays [m, n]
         'initial', 'minimum', 'maximum', 'final' (-1 off the low-rank part)."""
