@@ -907,7 +907,7 @@ unsigned long op_counts(char op, unsigned long a, unsigned long b, unsigned long
         res = (unsigned long)((double)(n * n * n / 3) - (double)(n * n) / 2.0 + (double)(n / 6));
     } else if (op == 't') {
         const unsigned long m = a, n = b;
-        res = (cc == 1) ? n * m * m : m * n * n;
+        res = (cc == 1) ? n * m * m : (cc == 2 ? m * n * n : 0);   // other sides: 0 (and a message there)
     } else if (op == 'm') {
         res = a * b * cc * 2;
     } else if (op == 's') {
@@ -915,10 +915,10 @@ unsigned long op_counts(char op, unsigned long a, unsigned long b, unsigned long
     } else if (op == 'o') {
         const unsigned long m = a, n = b, k = cc;
         if (d == 1) res = 4 * n * m * k - 2 * n * k * k + 3 * n * k;
-        else res = 4 * n * m * k - 2 * m * k * k + 2 * m * k + n * k - k * k / 2 + k / 2;
+        else if (d == 2) res = 4 * n * m * k - 2 * m * k * k + 2 * m * k + n * k - k * k / 2 + k / 2;
     } else if (op == 'r') {
         const unsigned long m = a, n = b;
-        res = (cc == 1) ? m * m * n : m * n * n;
+        res = (cc == 1) ? m * m * n : (cc == 2 ? m * n * n : 0);
     }
     return res;
 }
@@ -2766,6 +2766,10 @@ int hicma_tlr_k_cov(const hicma_tlr_problem *prob, const double *d_points, int N
     CUDA_TRY(cudaFreeAsync(dt, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     return 0;
+}
+
+unsigned long hicma_tlr_op_counts(char op, unsigned long a, unsigned long b, unsigned long c, unsigned long d) {
+    return op_counts(op, a, b, c, d);
 }
 
 int hicma_tlr_bounds_checked(void) {

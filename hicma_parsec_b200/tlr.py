@@ -118,6 +118,7 @@ def load_library(path: str | None = None):
         "hicma_tlr_rank_history": (i, [vp, vp, vp, vp, vp]),
         "hicma_tlr_k_wait_probe": (i, [C.c_longlong, C.c_longlong, i, dp, vp]),
         "hicma_tlr_bounds_checked": (i, []),
+        "hicma_tlr_op_counts": (C.c_ulong, [C.c_char, C.c_ulong, C.c_ulong, C.c_ulong, C.c_ulong]),
         "hicma_tlr_autotune": (i, [vp, i, i, i, vp, vp]),
         "hicma_tlr_tuning_get": (i, [vp, vp]),
         "hicma_tlr_tuning_set": (i, [vp, vp]),

@@ -132,6 +132,13 @@ int hicma_tlr_rank_gather(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, int *rank_array
  * first factorization of A. */
 int hicma_tlr_rank_history(hicma_tlr_desc *A, int *initial, int *minimum, int *maximum, int *final_rank);
 
+/* op_counts (hicma_parsec/op_counts.h:10-72): the reference's flop model of one
+ * kernel call ('q' geqrf m=a n=b, 'c' potrf n=a, 't' trsm m=a n=b side=c,
+ * 'm' gemm a*b*c, 's' svd n=a, 'o' ormqr m=a n=b k=c side=d, 'r' trmm m=a n=b
+ * side=c), with its unsigned wrap-around and float32 casts; the counters of
+ * hicma_tlr_dpotrf_L and the band auto-tuning use it. */
+unsigned long hicma_tlr_op_counts(char op, unsigned long a, unsigned long b, unsigned long c, unsigned long d);
+
 /* HICMA_get_stat2 (hicma_parsec/hicma_internal.c:52-71). */
 int hicma_tlr_rank_stat(const int *rank_array, int NT, int band_size, int *minrk, int *maxrk,
                         double *avgrk);

@@ -16,7 +16,9 @@ dense factorization at run time).  This module therefore restates:
 * the generation graph of ``hicma_parsec/STARSH_gen.jdf`` (band tiles dense,
   off-band tiles compressed to a packed ``[U, V]`` pair plus a rank);
 * the band auto-tuning rule of ``hicma_parsec/band_size_auto_tuning.jdf``;
-* the flop model of ``hicma_parsec/op_counts.h`` (including its float32 casts);
+* the flop model of ``hicma_parsec/op_counts.h`` (including its float32 casts;
+  pinned bit for bit against that header compiled unchanged, the golden vectors
+  in ``tests/golden/op_counts.json``);
 * the checks of ``hicma_parsec/testing_dpotrf.c:111-230``;
 
 and restates from their published mathematics the absent third-party pieces:
@@ -278,7 +280,7 @@ def op_counts(op: str, a: int, b: int, c: int, d: int) -> int:
         return (t1 - t2 + t3 + t4) & _U64
     if op == "c":
         n = a
-        v = float((n * n * n) // 3) - float(n * n) / 2.0 + float(n // 6)
+        v = float(((n * n * n) & _U64) // 3) - float((n * n) & _U64) / 2.0 + float(n // 6)
         return int(v) & _U64
     if op == "t":
         m, n, side = a, b, c
