@@ -1,12 +1,14 @@
 /*
  * Golden vectors of the reference's flop model: includes hicma_parsec/op_counts.h
- * from the reference tree unchanged (build recipe: oracle/Makefile, output in
- * oracle/_ref/) and prints op_counts(op, a, b, c, d) for a fixed grid of
- * arguments, one JSON object per line.  Test infrastructure only: the output is
- * committed as tests/golden/op_counts.json and nothing in the library runs this.
+ * and hicma_parsec/flops.h from the reference tree unchanged (build recipe:
+ * oracle/Makefile, output in oracle/_ref/) and prints op_counts(op, a, b, c, d)
+ * for a fixed grid of arguments and FLOPS_DPOTRF(n) for a list of sizes, one
+ * JSON object per line.  Test infrastructure only: the output is committed as
+ * tests/golden/op_counts.json and nothing in the library runs this.
  */
 #include <stdio.h>
 
+#include "flops.h"
 #include "op_counts.h"
 
 static void emit(char op, unsigned long a, unsigned long b, unsigned long c, unsigned long d) {
@@ -37,5 +39,9 @@ int main(void) {
                 emit('m', w[i], w[j], w[k], 0);
                 for (unsigned long side = 1; side <= 2; ++side) emit('o', w[i], w[j], w[k], side);
             }
+    /* dense-equivalent flops of the driver's GFLOP/s column (testing_dpotrf.c) */
+    static const long sizes[] = {1, 2, 3, 54, 270, 2700, 27000, 108000, 216000, 270000, 1000000};
+    for (int i = 0; i < (int)(sizeof sizes / sizeof sizes[0]); ++i)
+        printf("{\"flops_dpotrf\": %ld, \"r\": %.17g}\n", sizes[i], (double)FLOPS_DPOTRF(sizes[i]));
     return 0;
 }

@@ -1,6 +1,7 @@
 """Regenerates tests/golden/op_counts.json from the reference's own
-hicma_parsec/op_counts.h: builds oracle/_ref/op_counts_golden with
-oracle/Makefile (the reference tree must be present) and stores its output.
+hicma_parsec/op_counts.h and hicma_parsec/flops.h: builds
+oracle/_ref/op_counts_golden with oracle/Makefile (the reference tree must be
+present) and stores its output.
 
     python tests/golden/make_op_counts.py [reference root]
 """
@@ -18,12 +19,15 @@ def main(ref: str) -> None:
     subprocess.run(["make", "-s", "-C", oracle, f"REF={ref}"], check=True)
     out = subprocess.run([os.path.join(oracle, "_ref", "op_counts_golden")], check=True, capture_output=True,
                          text=True).stdout
-    rows = [json.loads(line) for line in out.splitlines() if line.strip()]
+    recs = [json.loads(line) for line in out.splitlines() if line.strip()]
+    rows = [r for r in recs if "op" in r]
+    flops = [[r["flops_dpotrf"], r["r"]] for r in recs if "flops_dpotrf" in r]
     with open(os.path.join(HERE, "op_counts.json"), "w") as f:
-        json.dump({"source": "hicma_parsec/op_counts.h (reference tree, compiled unchanged)",
+        json.dump({"source": "hicma_parsec/op_counts.h and flops.h (reference tree, compiled unchanged)",
                    "fields": ["op", "a", "b", "c", "d", "r"],
-                   "rows": [[r["op"], r["a"], r["b"], r["c"], r["d"], r["r"]] for r in rows]}, f, separators=(",", ":"))
-    print(f"{len(rows)} rows")
+                   "rows": [[r["op"], r["a"], r["b"], r["c"], r["d"], r["r"]] for r in rows],
+                   "flops_dpotrf": flops}, f, separators=(",", ":"))
+    print(f"{len(rows)} op_counts rows, {len(flops)} FLOPS_DPOTRF sizes")
 
 
 if __name__ == "__main__":

@@ -38,3 +38,13 @@ def test_library_matches_reference_op_counts(rows):
 def test_fixture_covers_every_operation_and_wraparound(rows):
     assert {r[0] for r in rows} == set("qctmsor")
     assert any(r[0] == "q" and r[2] == 1 << 21 for r in rows)    # 2 n^3 wraps to 0
+
+
+def test_dense_equivalent_flops_match_reference():
+    """FLOPS_DPOTRF of hicma_parsec/flops.h (the driver's dense-equivalent
+    GFLOP/s column) against the oracle's restatement, bit for bit."""
+    with open(GOLDEN) as f:
+        g = json.load(f)
+    assert len(g["flops_dpotrf"]) >= 10
+    for n, ref in g["flops_dpotrf"]:
+        assert O.flops_dpotrf(n) == ref, n
