@@ -24,15 +24,22 @@ namespace {
 constexpr int COV_ROWS = 256;   // threads per block = rows per block
 constexpr int COV_COLS = 8;     // columns per block
 
+// Kernel families: the point kernels of the statistics problems, the
+// electrodynamics sin(k r)/r kernels, and the randtlr basis products.  One
+// instantiation each, so the families that need sin or the K-term loop do not
+// add registers or stack to the others.
+enum CovFamily { COV_STATS = 0, COV_ED = 1, COV_RANDTLR = 2 };
+
+template <int FAM>
 __global__ void __launch_bounds__(COV_ROWS) k_cov_batched(CovParams p, const CovTask *__restrict__ tasks) {
     const CovTask t = tasks[blockIdx.z];
     const int r = blockIdx.x * COV_ROWS + threadIdx.x;
     const int c0 = blockIdx.y * COV_COLS;
     if (r >= t.nr || c0 >= t.nc) return;
     const int gr = t.r0 + r;
-    if (p.kind == HICMA_TLR_KIND_RANDTLR) {
+    const int cend = min(c0 + COV_COLS, t.nc);
+    if (FAM == COV_RANDTLR) {
         const int K = p.ndim / 2;
-        const int cend = min(c0 + COV_COLS, t.nc);
         for (int c = c0; c < cend; ++c) {
             const int gc = t.c0 + c;
             double acc = 0.0;
@@ -47,7 +54,6 @@ __global__ void __launch_bounds__(COV_ROWS) k_cov_batched(CovParams p, const Cov
 #pragma unroll
     for (int a = 0; a < 3; ++a) xr[a] = a < p.ndim ? p.pts[(size_t)a * p.N + gr] : 0.0;
     const double den = __dmul_rn(__dmul_rn(2.0, p.beta), p.beta);
-    const int cend = min(c0 + COV_COLS, t.nc);
     for (int c = c0; c < cend; ++c) {
         const int gc = t.c0 + c;
         double r2 = 0.0;
@@ -59,7 +65,7 @@ __global__ void __launch_bounds__(COV_ROWS) k_cov_batched(CovParams p, const Cov
             }
         }
         double v;
-        if (p.kind == HICMA_TLR_KIND_ED_SIN_2D || p.kind == HICMA_TLR_KIND_ED_SIN_3D) {
+        if (FAM == COV_ED) {
             const double rr = __dsqrt_rn(r2);
             v = r2 == 0.0 ? p.add_diag : __ddiv_rn(sin(__dmul_rn(p.wave_k, rr)), rr);
         } else {
@@ -286,7 +292,12 @@ void launch_cov_batched(const CovParams &p, const CovTask *d_tasks, int ntasks, 
                         cudaStream_t st) {
     if (ntasks <= 0) return;
     dim3 grid((max_nr + COV_ROWS - 1) / COV_ROWS, (max_nc + COV_COLS - 1) / COV_COLS, ntasks);
-    k_cov_batched<<<grid, COV_ROWS, 0, st>>>(p, d_tasks);
+    if (p.kind == HICMA_TLR_KIND_RANDTLR)
+        k_cov_batched<COV_RANDTLR><<<grid, COV_ROWS, 0, st>>>(p, d_tasks);
+    else if (p.kind == HICMA_TLR_KIND_ED_SIN_2D || p.kind == HICMA_TLR_KIND_ED_SIN_3D)
+        k_cov_batched<COV_ED><<<grid, COV_ROWS, 0, st>>>(p, d_tasks);
+    else
+        k_cov_batched<COV_STATS><<<grid, COV_ROWS, 0, st>>>(p, d_tasks);
 }
 
 void launch_gaussian(double *out, int rows, int cols, int ld, unsigned long long seed, cudaStream_t st) {
