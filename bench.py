@@ -86,20 +86,36 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        rows = []
         with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
+            lines = f.readlines()
         os.unlink(self.path)
+        return self.parse(lines)
+
+    @staticmethod
+    def parse(lines) -> dict:
+        """Summary of nvidia-smi samples (FIELDS, csv, no header, no units):
+        median SM clock over the samples under load (above half the maximum),
+        the maximum clock, and the throttle reasons seen active."""
+        rows = []
+        for line in lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [v for v in (num(r[1]) for r in rows) if v is not None]
+        mxs = [v for v in (num(r[2]) for r in rows) if v is not None]
+        mx = max(mxs) if mxs else None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
-        load = [s for s in sm if s > 0.5 * mx] or sm
+        load = ([s for s in sm if s > 0.5 * mx] if mx else []) or sm
         return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx, "reasons": reasons,
                 "samples": len(rows)}
 
