@@ -515,18 +515,50 @@ def band_autotune(G: np.ndarray, nt: int, nb: int, verbose: bool = False) -> int
 # --------------------------------------------------------------------------
 # Tile kernels (HCORE / CORE_d* restated)
 # --------------------------------------------------------------------------
-def recompress(Cu, Cv, Au, Y, acc, maxrank, fixed_rank=0):
+def r_factor_scholqr3(V: np.ndarray) -> np.ndarray:
+    """R of V = Q R (Q not formed) by shifted CholeskyQR3 (Fukaya, Kannan,
+    Nakatsukasa, Yamamoto and Yanagisawa, SIAM J. Sci. Comput. 42(1), 2020):
+    columns scaled to unit norm, then three passes of G = X^T X, R_p = chol(G)
+    and X <- X R_p^-1, the first with the shift 11 (m K + K (K + 1)) u ||X||^2
+    (||X||_F^2 bounds ||X||_2^2), later ones shifted the same way only if the
+    plain Cholesky breaks down; R = R_3 R_2 R_1 D.  A candidate for the V side
+    of the recompression built from Gram products and triangular multiplies
+    (tensor-core friendly) instead of Householder reflections."""
+    m, K = V.shape
+    d = np.linalg.norm(V, axis=0)
+    d[d == 0.0] = 1.0
+    X = V / d
+    R = np.eye(K)
+    u = np.finfo(np.float64).eps / 2
+    for p in range(3):
+        G = X.T @ X
+        shift = 11.0 * (m * K + K * (K + 1)) * u * float(np.trace(G))
+        try:
+            Rp = np.linalg.cholesky(G + (shift if p == 0 else 0.0) * np.eye(K)).T
+        except np.linalg.LinAlgError:
+            Rp = np.linalg.cholesky(G + shift * np.eye(K)).T
+        X = sla.solve_triangular(Rp, X.T, trans="T", lower=False).T
+        R = Rp @ R
+    return R * d
+
+
+def recompress(Cu, Cv, Au, Y, acc, maxrank, fixed_rank=0, v_side="householder"):
     """C_new = [Cu, Au] [Cv, -Y]^T recompressed (restated
     ``HCORE_dgemm_qr_svd`` + ``HCORE_dgemm_ormqr``, call sites
     ``HiCMA_dpotrf_L_2flow.jdf:830-903,985-1058``).  Returns
-    (U, V, rank, overflow)."""
+    (U, V, rank, overflow).  ``v_side="scholqr3"`` takes R_V from
+    :func:`r_factor_scholqr3` and forms the new V as [Cv, -Y] R_U^T U_r (no
+    Q_V needed), the form the device uses."""
     Us = np.hstack([Cu, Au])
     Vs = np.hstack([Cv, -Y])
     nb, K = Us.shape
     if K == 0:
         return np.zeros((nb, 0)), np.zeros((nb, 0)), 0, False
     Qu, Ru = np.linalg.qr(Us)
-    Qv, Rv = np.linalg.qr(Vs)
+    if v_side == "scholqr3":
+        Rv = r_factor_scholqr3(Vs)
+    else:
+        Qv, Rv = np.linalg.qr(Vs)
     u, s, vt = np.linalg.svd(Ru @ Rv.T)
     if fixed_rank > 0:
         r = min(fixed_rank, K)
@@ -534,6 +566,8 @@ def recompress(Cu, Cv, Au, Y, acc, maxrank, fixed_rank=0):
         r = int(np.count_nonzero(s >= acc))
     overflow = r > maxrank
     r = min(r, maxrank)
+    if v_side == "scholqr3":
+        return (np.ascontiguousarray(Qu @ u[:, :r]), np.ascontiguousarray(Vs @ (Ru.T @ u[:, :r])), r, overflow)
     return (np.ascontiguousarray(Qu @ u[:, :r]),
             np.ascontiguousarray(Qv @ (vt[:r].T * s[:r])), r, overflow)
 
@@ -576,7 +610,8 @@ def potrf_tile(A: np.ndarray):
         return L, 0
 
 
-def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool = True) -> FactorStats:
+def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool = True,
+              v_side: str = "householder") -> FactorStats:
     """In-place 2-flow TLR Cholesky (``HiCMA_dpotrf_L_2flow.jdf:175-1113``)
     run in a sequential order compatible with its data flow."""
     nt, nb, band = T.nt, T.nb, T.band
@@ -667,7 +702,7 @@ def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool
                     ra = Au.shape[1]
                     rc_old = T.U[(m, n)].shape[1]
                     Y = T.dense[(n, k)] @ Av
-                    U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank)
+                    U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank, v_side)
                     st.overflow += int(ov)
                     T.U[(m, n)], T.V[(m, n)] = U, V
                     track(m, n, r)
@@ -680,7 +715,7 @@ def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool
                         continue
                     rc_old = T.U[(m, n)].shape[1]
                     Y = Bu @ (Bv.T @ Av)
-                    U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank)
+                    U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank, v_side)
                     st.overflow += int(ov)
                     T.U[(m, n)], T.V[(m, n)] = U, V
                     track(m, n, r)

@@ -152,3 +152,29 @@ def test_randtlr_equal_ranks_and_factor():
     assert O.check_dpotrf2(O.uncompress(T), A) <= 1e-8
     small = O.problem_points(prob, 120, 40)                         # K = min(NB, 64) = 40
     assert small.shape == (120, 80)
+
+
+def test_scholqr3_v_side_keeps_ranks_and_accuracy():
+    """Shifted CholeskyQR3 for R_V (Gram products and triangular multiplies, the
+    tensor-core-friendly candidate for the device's V-side QR) gives the same
+    final ranks, residual and log det as Householder on the reference's case."""
+    prob = O.Problem(kind=2, noise=1e-4)
+    pts = O.gen_points(2700, 2)
+    T0, info = O.generate(prob, 2700, 270, 1e-8, 130, 1, pts)
+    assert info == 0
+    Th, Tc = T0.copy(), T0.copy()
+    assert O.tlr_potrf(Th, 1e-8).info == 0
+    assert O.tlr_potrf(Tc, 1e-8, v_side="scholqr3").info == 0
+    Gh, Gc = Th.rank_array(), Tc.rank_array()
+    assert np.array_equal(Gh, Gc)
+    A = O.dense_matrix(prob, pts)
+    rh, rc = O.check_dpotrf2(O.uncompress(Th), A), O.check_dpotrf2(O.uncompress(Tc), A)
+    assert rc <= 10 * 1e-8 and abs(rc - rh) <= 0.01 * rh
+    assert abs(O.logdet(Tc) - O.logdet(Th)) <= 1e-12 * abs(O.logdet(Th))
+    # R factor itself: R^T R = V^T V and upper triangular, also for dependent columns
+    rng = np.random.default_rng(2)
+    V = rng.standard_normal((300, 40)) @ np.diag(10.0 ** -np.arange(40) * 0.25)
+    V[:, 39] = V[:, 3]                                      # an exactly dependent column
+    R = O.r_factor_scholqr3(V)
+    assert np.allclose(np.tril(R, -1), 0.0)
+    assert np.linalg.norm(R.T @ R - V.T @ V) <= 1e-12 * np.linalg.norm(V.T @ V)
