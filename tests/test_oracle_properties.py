@@ -10,7 +10,7 @@ library's host-side generators, over random shapes, ranks and seeds:
 * band auto-tuning: the library equals the oracle on random rank maps."""
 import numpy as np
 import pytest
-from hypothesis import HealthCheck, given, settings
+from hypothesis import HealthCheck, assume, given, settings
 from hypothesis import strategies as st
 
 from oracle import tlr_oracle as O
@@ -75,3 +75,24 @@ def test_band_autotune_and_stats_library_equal_oracle(nt, nb, seed, band):
         mn, mx, av = tlr.HICMA_get_stat2(G, nt, band)
         omn, omx, oav = O.rank_stat(G, nt, band)
         assert (mn, mx) == (omn, omx) and av == pytest.approx(oav, rel=1e-15)
+
+
+@settings(max_examples=12, deadline=None, suppress_health_check=[HealthCheck.too_slow, HealthCheck.filter_too_much])
+@given(kind=st.sampled_from([2, 3, 4]), nt=st.integers(2, 6), nb=st.sampled_from([48, 64, 96]),
+       beta=st.floats(0.01, 0.1), noise_exp=st.integers(-4, -1), band=st.integers(1, 3),
+       tol_exp=st.integers(-10, -6), seed=st.integers(0, 1000))
+def test_tlr_factorization_meets_the_check(kind, nt, nb, beta, noise_exp, band, tol_exp, seed):
+    """Whenever generation accepts every tile, the oracle's TLR Cholesky meets
+    the reference's check at 10 e and its log det matches the dense one."""
+    n, tol = nt * nb, 10.0 ** tol_exp
+    band = min(band, nt)
+    prob = O.Problem(kind=kind, beta=beta, noise=10.0 ** noise_exp, seed=seed)
+    pts = O.gen_points(n, O.KIND_NDIM[kind], seed)
+    T, info = O.generate(prob, n, nb, tol, nb // 2 - 1, band, pts)
+    assume(info == 0)                            # else a tile needs rank >= NB/2: rejected by the rule
+    st_ = O.tlr_potrf(T, tol)
+    assert st_.info == 0
+    A = O.dense_matrix(prob, pts)
+    assert O.check_dpotrf2(O.uncompress(T), A) <= 10 * tol
+    ld = 2.0 * np.sum(np.log(np.diag(np.linalg.cholesky(A))))
+    assert abs(O.logdet(T) - ld) <= 1e-6 * abs(ld)
