@@ -174,6 +174,7 @@ int main(int argc, char **argv) {
     hicma_tlr_set_precision(ctx, precision);
     hicma_tlr_problem prob = {kind, beta, 0.5, noise, sigma, seed, wave_k, add_diag};
     hicma_tlr_desc *A = NULL;
+    const int band_created = band_size;   /* slots of the off-band tiles are laid out for this band */
     rc = hicma_tlr_desc_create(ctx, N, NB, maxrank > genmaxrank ? maxrank : genmaxrank, band_size, &A);
     if (rc) { fprintf(stderr, "descriptor: %s\n", hicma_tlr_last_error()); return 1; }
 
@@ -222,12 +223,12 @@ int main(int argc, char **argv) {
     printf("[****] TIME(s) %12.5f : Memory_count\tNB= %4d N= %7d maxrank= %d band_size= %d memory_per_node= %lf GB memory_per_node_max= %lf GB\n",
            0.0, NB, N, maxrank, band_size, mem, mem_max);
 
+    /* the matrix before factorization, for check_diff (testing_dpotrf.c:642-660) */
     hicma_tlr_desc *A0 = NULL;
     if (check) {
-        if (hicma_tlr_desc_create(ctx, N, NB, maxrank > genmaxrank ? maxrank : genmaxrank, 1, &A0) == 0) {
-            if (band_size > 1) hicma_tlr_band_regenerate(ctx, HICMA_TLR_LOWER, A0, &prob, band_size);
-            hicma_tlr_desc_copy(ctx, A, A0);
-        }
+        rc = hicma_tlr_desc_create(ctx, N, NB, maxrank > genmaxrank ? maxrank : genmaxrank, band_created, &A0);
+        if (rc == 0) rc = hicma_tlr_desc_copy(ctx, A, A0);
+        if (rc) { fprintf(stderr, "copy for the check: %s\n", hicma_tlr_last_error()); return 1; }
     }
     unsigned long *tileops = calloc((size_t)NT * NT, sizeof(unsigned long));
     unsigned long opcounters[1] = {0};

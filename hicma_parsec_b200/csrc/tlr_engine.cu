@@ -1357,10 +1357,22 @@ int hicma_tlr_desc_info(const hicma_tlr_desc *A, int *N, int *NB, int *NT, int *
 int hicma_tlr_desc_copy(hicma_tlr_ctx *c, const hicma_tlr_desc *src, hicma_tlr_desc *dst) {
     ARG_CHECK(c && src && dst, "null");
     ARG_CHECK(src->N == dst->N && src->NB == dst->NB && src->maxrank == dst->maxrank &&
-                  src->band_alloc == dst->band_alloc && src->slot_band == dst->slot_band,
-              "descriptor shapes differ");
+                  src->slot_band == dst->slot_band,
+              "descriptor shapes differ (N, NB, maxrank and the band it was created with must match)");
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     const size_t NB = src->NB, NT = src->NT;
+    if (dst->band_alloc != src->band_alloc) {
+        // the source's band was widened (band regeneration): the copy adopts it
+        dev_free(c, dst->d_band);
+        dst->d_band = nullptr;
+        const size_t bytes = NT * src->band_alloc * NB * NB * sizeof(double);
+        if (dev_alloc(c, (void **)&dst->d_band, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            set_err("band allocation of %zu bytes failed", bytes);
+            return HICMA_TLR_ERR_OOM;
+        }
+        dst->band_alloc = src->band_alloc;
+    }
     CUDA_TRY(cudaMemcpyAsync(dst->d_band, src->d_band, NT * src->band_alloc * NB * NB * sizeof(double),
                              cudaMemcpyDeviceToDevice, c->stream));
     if (src->nslots)

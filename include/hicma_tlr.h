@@ -101,7 +101,9 @@ int hicma_tlr_desc_create(hicma_tlr_ctx *ctx, int N, int NB, int maxrank, int ba
 int hicma_tlr_desc_destroy(hicma_tlr_desc *A);
 int hicma_tlr_desc_info(const hicma_tlr_desc *A, int *N, int *NB, int *NT, int *maxrank,
                         int *band_size);
-/* Device-to-device copy of all tiles and ranks (same shape required). */
+/* Device-to-device copy of all tiles, ranks and points.  N, NB, maxrank and the
+ * band size dst was created with must equal src's; a band src has since widened
+ * (hicma_tlr_band_regenerate) is adopted by dst. */
 int hicma_tlr_desc_copy(hicma_tlr_ctx *ctx, const hicma_tlr_desc *src, hicma_tlr_desc *dst);
 
 /* ----------------------------------------------------------- generation -- */

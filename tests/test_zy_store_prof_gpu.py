@@ -65,3 +65,30 @@ def test_store_layout_round_trip_and_profiling(ctx):
     finally:
         A.close()
         B.close()
+
+
+def test_copy_adopts_a_widened_band(ctx):
+    """hicma_tlr_desc_copy onto a descriptor created like the source: a band the
+    source widened after generation is adopted (the driver's copy for
+    check_diff after band auto-tuning); a different creation band is refused."""
+    from hicma_parsec_b200 import tlr
+    prob = tlr.Problem(kind=2, noise=0.1)
+    A = tlr.TLRMatrix(ctx, N, NB, MAXRANK, 1)
+    B = tlr.TLRMatrix(ctx, N, NB, MAXRANK, 1)
+    C = tlr.TLRMatrix(ctx, N, NB, MAXRANK, 2)
+    try:
+        assert A.generate(prob, TOL, MAXRANK) == 0
+        A.band_regenerate(prob, 3)
+        B.copy_from(A)
+        assert B.band_size == 3
+        assert np.array_equal(B.rank_map(), A.rank_map())
+        assert np.array_equal(B.tile(5, 3), A.tile(5, 3))
+        with pytest.raises(tlr.TLRError) as e:
+            C.copy_from(A)
+        assert e.value.code == tlr.ERR_ARG
+        assert A.potrf(TOL) == 0 and B.potrf(TOL) == 0
+        assert abs(A.logdet() - B.logdet()) <= 1e-12 * abs(A.logdet())
+    finally:
+        A.close()
+        B.close()
+        C.close()
