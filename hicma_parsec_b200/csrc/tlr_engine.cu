@@ -2293,6 +2293,7 @@ int hicma_tlr_tile_set(hicma_tlr_ctx *c, hicma_tlr_desc *A, int m, int n, const 
     TRY(ctx_sync(c));
     if (A->is_dense(m, n)) {
         CUDA_TRY(cudaMemcpy(A->dense(m, n), buf, NB * NB * sizeof(double), cudaMemcpyHostToDevice));
+        A->factored = false;   // the held factor no longer belongs to this matrix
         return 0;
     }
     ARG_CHECK(rank >= 0 && rank <= A->maxrank, "rank in [0, maxrank]");
