@@ -93,3 +93,18 @@ def test_not_positive_definite_and_library_errors(fake):
     fake.script = {"raise": True}
     r = serving.solve_request(None, req())
     assert r.status == tlr.ERR_OOM and "out of memory" in r.error
+
+
+def test_mle_evaluator_decisions(monkeypatch):
+    """mle.device_loglik: the same band rules, -inf for a factorization that is
+    not positive definite, and the matrix released every time."""
+    from hicma_parsec_b200 import mle
+    monkeypatch.setattr(mle.tlr, "TLRMatrix", FakeMatrix)
+    FakeMatrix.calls = []
+    y = np.zeros(8000)
+    ev = mle.device_loglik(None, 2, 8000, 1000, y, 1e-8, 499, seed=3, autoband=False)
+    FakeMatrix.script = {"rejected": [(7, 1)]}
+    assert ev(0.1, 1.0, 1e-3) == -1.0 and ("band", 7) in FakeMatrix.calls
+    FakeMatrix.script = {"info": 5}
+    assert ev(0.1, 1.0, 1e-3) == -np.inf
+    assert sum(1 for c in FakeMatrix.calls if c == ("close",)) == 2
