@@ -124,3 +124,19 @@ def test_problem_struct_layout_matches_header(tmp_path):
     assert int(out["size"]) == ctypes.sizeof(tlr.CProblem)
     for f in fields:
         assert int(out[f]) == getattr(tlr.CProblem, f).offset, f
+
+
+def test_rank_stat_and_autotune_edges():
+    """Empty low-rank parts (band >= NT) and the smallest grids, against the
+    oracle: the reference's INT_MAX / 0 / NaN statistics and its band loop,
+    which returns NT when no band beats the TLR cost."""
+    from hicma_parsec_b200 import tlr
+    G = np.full(9, 5, dtype=np.int32)
+    mn, mx, av = tlr.HICMA_get_stat2(G, 3, 3)
+    omn, omx, oav = O.rank_stat(G, 3, 3)
+    assert (mn, mx) == (omn, omx) == (2**31 - 1, 0) and np.isnan(av) and np.isnan(oav)
+    for nt in (1, 2, 3):
+        for nb in (2, 270, 2700):
+            for r in (0, 1, nb // 2):
+                G = np.full(nt * nt, r, dtype=np.int32)
+                assert tlr.parsec_band_size_auto_tuning(G, nt, nb) == O.band_autotune(G, nt, nb), (nt, nb, r)
