@@ -50,6 +50,12 @@ CONFIGS = {
                 workload="3D exp N=27000 NB=2700 e=1e-8 maxrank=1350 band auto FP64 (scaled twin of N=108000)"),
     "c4": dict(kind=3, n=216000, nb=2700, maxrank=500, acc=1e-8, noise=1e-4, band=1, autoband=True,
                workload="3D sqexp N=216000 NB=2700 e=1e-8 maxrank=500 band auto FP64"),
+    # the other STARS-H problem kinds of the reference driver (-D 0, -D 1)
+    "rt": dict(kind=0, n=270000, nb=2700, maxrank=150, acc=1e-8, noise=0.0, band=1, autoband=False,
+               workload="randtlr (-D 0) N=270000 NB=2700 decay 0.5 e=1e-8 maxrank=150 band=1 FP64"),
+    "ed2s": dict(kind=1, n=27000, nb=2700, maxrank=1350, acc=1e-8, noise=0.0, band=1, autoband=True,
+                 workload="electrodynamics 2D sin(kr)/r k=50 (-D 1) N=27000 NB=2700 e=1e-8 maxrank=1350 "
+                          "band auto FP64"),
 }
 METRIC = "TLR Cholesky s/factor at e=1e-8"
 UNIT = "s/factor"
@@ -222,7 +228,7 @@ def run_reference(args, cfg):
     threads = os.cpu_count() or 1
     nb, S = cfg["nb"], min(CPU_SAMPLE_ROWS, cfg["n"] // cfg["nb"])
     prob = O.Problem(kind=cfg["kind"], noise=cfg["noise"])
-    pts = O.gen_points(cfg["n"], prob.ndim, 0)
+    pts = O.problem_points(prob, cfg["n"], nb)
     tiles = {}
     for m in range(S):
         tiles[(m, m)] = O.cov_block(prob, pts, m * nb, nb, m * nb, nb)
