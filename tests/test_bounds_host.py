@@ -59,3 +59,15 @@ def test_loader_selects_the_checked_build(monkeypatch):
                            env={**os.environ, "HICMA_TLR_LIB": env})
         assert r.returncode == 0, r.stderr
         assert r.stdout.strip() == want
+
+
+def test_missing_library_fails_loudly():
+    """No CPU fallback: without the CUDA library the binding refuses to load."""
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("from hicma_parsec_b200 import tlr\n"
+            "try:\n    tlr.load_library()\nexcept RuntimeError as e:\n    print('refused:', e)\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=120,
+                       env={**os.environ, "HICMA_TLR_LIB": os.path.join(root, "no_such_lib.so")})
+    assert r.returncode == 0 and r.stdout.startswith("refused:") and "not built" in r.stdout
