@@ -49,7 +49,7 @@ print(json.dumps(out))
 
 
 def run(env):
-    r = subprocess.run([sys.executable, "-c", SCRIPT], cwd=ROOT, capture_output=True, text=True, timeout=900,
+    r = subprocess.run([sys.executable, "-c", SCRIPT], cwd=ROOT, capture_output=True, text=True, timeout=600,
                        env={**os.environ, "HICMA_TLR_LIB": env})
     assert r.returncode == 0, r.stderr[-3000:]
     return json.loads(r.stdout.strip().splitlines()[-1])

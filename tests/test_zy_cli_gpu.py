@@ -19,7 +19,7 @@ ARGS = ["-N", "2700", "-t", "270", "-e", "1e-8", "-u", "130", "-D", "2", "-v", "
 
 def run_cli(*extra):
     from hicma_parsec_b200 import build
-    r = subprocess.run([build.CLI, *ARGS, *extra], capture_output=True, text=True, timeout=900)
+    r = subprocess.run([build.CLI, *ARGS, *extra], capture_output=True, text=True, timeout=300)
     return r
 
 
