@@ -108,3 +108,27 @@ def test_compare_logs_command(tmp_path, oracle_run):
     assert ranklog.main([str(pa), str(pb), "--tol", "3"]) == 1
     res = ranklog.compare_logs(ranklog.parse_log(a), ranklog.parse_log(b))
     assert res["same_problem"] and res["maps"]["final"].max_abs == 4
+
+
+from hypothesis import given, settings  # noqa: E402
+from hypothesis import strategies as st  # noqa: E402
+
+
+@settings(max_examples=30, deadline=None)
+@given(nt=st.integers(1, 14), band=st.integers(1, 4), seed=st.integers(0, 10**6))
+def test_rank_map_blocks_round_trip(nt, band, seed):
+    """Any rank map printed in the driver's formats parses back to itself."""
+    rng = np.random.default_rng(seed)
+    G = np.where(np.tril(np.ones((nt, nt), bool), -band), rng.integers(0, 999, (nt, nt)), -1)
+    mn = np.where(G >= 0, np.maximum(G - rng.integers(0, 5, (nt, nt)), 0), -1)
+    mx = np.where(G >= 0, G + rng.integers(0, 5, (nt, nt)), -1)
+    text = (ranklog.format_rank_tile("init_rank_tile", G, band) + ranklog.format_rank_history(G, mn, mx, G) +
+            ranklog.format_rank_tile("rank_tile", G, band))
+    log = ranklog.parse_log(text)
+    low = G >= 0
+    assert np.array_equal(log.map("initial"), np.where(low, G, -1))
+    assert np.array_equal(log.map("final"), np.where(low, G, -1))
+    assert np.array_equal(log.map("Maximum Rank"), np.where(low, mx, 0))
+    assert np.array_equal(log.map("Difference Rank, max - min"), np.where(low, mx - mn, 0))
+    d = ranklog.diff_maps(log.map("final"), G, 0, band)
+    assert d.differing == 0
