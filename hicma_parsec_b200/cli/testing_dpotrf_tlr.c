@@ -69,8 +69,8 @@ static void usage(void) {
             " -U --compmaxrank  maxrank of buffers (default maxrank)\n"
             " -f --fixedrank    fixed rank in recompression (0 = accuracy mode)\n"
             " -D --kind_of_problem 0: randtlr 1: ed-2d-sin 2: st-2d-sqexp 3: st-3d-sqexp 4: st-3d-exp 5: ed-3d-sin\n"
-            " -w --wave_k       wave number of -D 1, 5 (default 50)\n"
-            " -j --add_diag     diagonal of -D 0, 1, 5 (default N)\n"
+            " -w --wavek        wave number of -D 1, 5 (default 50)\n"
+            " -j --adddiag      diagonal of -D 0, 1, 5 (default N)\n"
             " -Z --band         band size (default 1)\n"
             " -E --auto-band    auto-tune band size (default 1)\n"
             " -Y --lookahead    lookahead (-1: band size)\n"
@@ -109,7 +109,16 @@ int main(int argc, char **argv) {
         {"Q", required_argument, 0, 'Q'},          {"c", required_argument, 0, 'c'},
         {"cores", required_argument, 0, 'c'},      {"g", required_argument, 0, 'g'},
         {"wave_k", required_argument, 0, 'w'},     {"w", required_argument, 0, 'w'},
+        {"wavek", required_argument, 0, 'w'},      {"adddiag", required_argument, 0, 'j'},
         {"add_diag", required_argument, 0, 'j'},   {"j", required_argument, 0, 'j'},
+        {"grid-rows", required_argument, 0, 'P'},  {"grid-cols", required_argument, 0, 'Q'},
+        /* RBF mesh problems (-D 6, 7; not built): accepted so reference command lines parse */
+        {"rbf_kernel", required_argument, 0, 'B'}, {"B", required_argument, 0, 'B'},
+        {"numobj", required_argument, 0, 'K'},     {"K", required_argument, 0, 'K'},
+        {"mesh_file", required_argument, 0, 'M'},  {"M", required_argument, 0, 'M'},
+        {"order", required_argument, 0, 'O'},      {"O", required_argument, 0, 'O'},
+        {"radius", required_argument, 0, 'R'},     {"R", required_argument, 0, 'R'},
+        {"density", required_argument, 0, 'S'},    {"S", required_argument, 0, 'S'},
         {"noise", required_argument, 0, 1001},     {"beta", required_argument, 0, 1002},
         {"sigma", required_argument, 0, 1003},     {"seed", required_argument, 0, 1004},
         {"precision", required_argument, 0, 1005}, {"ws", required_argument, 0, 1006},
@@ -136,6 +145,7 @@ int main(int argc, char **argv) {
             case 'v': verbose = optarg ? atoi(optarg) : 1; break;
             case 'h': usage(); return 0;
             case 'P': case 'Q': case 'c': case 'g': break;
+            case 'B': case 'K': case 'M': case 'O': case 'R': case 'S': break;
             case 'w': wave_k = atof(optarg); break;
             case 'j': add_diag = atof(optarg); break;
             case 1001: noise = atof(optarg); break;

@@ -24,7 +24,7 @@ def test_usage_lists_problem_kinds(cli):
     assert r.returncode == 0
     for name in ("randtlr", "ed-2d-sin", "st-2d-sqexp", "st-3d-sqexp", "st-3d-exp", "ed-3d-sin"):
         assert name in r.stderr
-    assert "--wave_k" in r.stderr and "--add_diag" in r.stderr
+    assert "--wavek" in r.stderr and "--adddiag" in r.stderr
 
 
 @pytest.mark.parametrize("kind", ["6", "7", "-1"])
@@ -44,3 +44,14 @@ def test_n_must_be_a_multiple_of_nb(cli):
     r = run(cli, "-N", "2701", "-t", "270", "-D", "2")
     assert r.returncode == 1
     assert "multiple" in r.stderr
+
+
+def test_reference_option_spellings_parse(cli):
+    """The reference driver's long options (hicma_parsec/hicma_parsec.c:89-161),
+    including the RBF mesh flags of the problems that are not built, parse; the
+    run then stops at the unsupported kind before any GPU use."""
+    r = run(cli, "--N", "2700", "--NB", "270", "--fixedacc", "1e-8", "--maxrank", "130", "--wavek", "25",
+            "--adddiag", "3000", "--grid-rows", "1", "--grid-cols", "1", "--rbf_kernel", "0", "--numobj", "1",
+            "--mesh_file", "x", "--order", "1", "--radius", "0.5", "--density", "0.1", "--kind_of_problem", "7")
+    assert r.returncode == 1
+    assert "kind_of_problem" in r.stderr and "unrecognized" not in r.stderr
