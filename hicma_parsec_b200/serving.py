@@ -165,7 +165,9 @@ class ReplicaRouter:
     exception out of the solve) marks its GPU failed: the GPU takes no further
     requests, its contexts are not reused, and the request is routed once more
     to another healthy GPU.  When no healthy GPU is left, the remaining
-    requests complete with status ERR_CUDA.
+    requests complete with status ERR_CUDA.  A GPU whose contexts cannot be
+    created at start-up is marked failed the same way (the reason is kept in
+    ``init_errors``); the router starts if at least one GPU does.
 
     `make_context(device)`, `solve(ctx, req)` and `footprint(req)` default to
     the library's context, :func:`solve_request` and :func:`footprint_bytes`.
@@ -188,8 +190,26 @@ class ReplicaRouter:
         self.hbm_budgets = [int(b) for b in hbm_budgets]
         if len(self.hbm_budgets) != len(self.devices):
             raise ValueError("one HBM budget per device")
-        self._ctxs = {i: [make_context(d) for _ in range(slots)] for i, d in enumerate(self.devices)}
         self.failed: set = set()        # indices into devices
+        self.init_errors: dict = {}     # device index -> why its contexts could not be created
+        self._ctxs = {}
+        for i, d in enumerate(self.devices):
+            made = []
+            try:
+                for _ in range(slots):
+                    made.append(make_context(d))
+            except Exception as e:      # a GPU that cannot start serves nothing; the others go on
+                for ctx in made:
+                    try:
+                        ctx.close()
+                    except Exception:
+                        pass
+                made = []
+                self.failed.add(i)
+                self.init_errors[i] = f"{type(e).__name__}: {e}"
+            self._ctxs[i] = made
+        if len(self.failed) == len(self.devices):
+            raise RuntimeError(f"no GPU could be initialised: {self.init_errors}")
 
     def close(self):
         for ctxs in self._ctxs.values():

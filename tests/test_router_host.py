@@ -150,3 +150,21 @@ def test_realtime_arrivals_and_single_gpu_server():
         assert r.t_admit >= q.arrival - 1e-3 and r.latency > 0
     assert srv.hbm_budget == 100
     srv.close()
+
+
+def test_a_gpu_that_cannot_start_is_left_out():
+    budgets = [1000, 1000]
+    g = FakeGPUs(budgets)
+
+    def make(device):
+        if device == 0:
+            raise RuntimeError("out of memory")
+        return FakeCtx(device)
+
+    rt = serving.ReplicaRouter(devices=[0, 1], slots=2, hbm_budgets=budgets, make_context=make, solve=g.solve,
+                               footprint=g.footprint)
+    assert rt.failed == {0} and "out of memory" in rt.init_errors[0]
+    res = run_bounded(rt, reqs([10] * 5))
+    assert all(r.status == 0 and r.device == 1 for r in res)
+    with pytest.raises(RuntimeError):
+        serving.ReplicaRouter(devices=[0], slots=1, hbm_budgets=[10], make_context=make, solve=g.solve)
