@@ -23,7 +23,7 @@ LIB = os.path.join(LIBDIR, "libhicma_tlr.so")
 LIB_CHECKED = os.path.join(LIBDIR, "libhicma_tlr_checked.so")
 OBJ_CHECKED = os.path.join(OBJ, "checked")
 # sources whose host code carries the launch checks of the checked build
-CHECKED_SOURCES = ["tlr_engine.cu", "serve.cu"]
+CHECKED_SOURCES = ["tlr_engine.cu", "serve.cu", "k_potrf.cu"]
 CLI_SRC = os.path.join(HERE, "cli", "testing_dpotrf_tlr.c")
 CLI = os.path.join(LIBDIR, "testing_dpotrf_tlr")
 SOURCES = ["k_gemm.cu", "k_tile.cu", "k_potrf.cu", "k_potrf_tile.cu", "k_qr.cu", "k_proj.cu", "k_svd.cu", "tlr_engine.cu", "serve.cu"]

@@ -9,7 +9,7 @@
 #include "tlr_internal.h"
 
 #include <cstdio>
-#include <mutex>
+#include <vector>
 
 namespace tlr {
 namespace {
@@ -100,9 +100,31 @@ constexpr int NOALLOC_MAX_N = 4096;
 constexpr size_t NOALLOC_SCRATCH = 64 * 64 + (size_t)64 * NOALLOC_MAX_N;
 __device__ __align__(256) double g_potrf_scratch[NOALLOC_SCRATCH];
 
-constexpr int MAX_DEVICES = 64;
-std::mutex g_scratch_mu;
-double *g_scratch_ptr[MAX_DEVICES] = {nullptr};
+int noalloc_fail(const char *what, cudaError_t e) {
+    char msg[320];
+    snprintf(msg, sizeof msg, "hicma_tlr_k_potrf_noalloc: %s: %s", what, cudaGetErrorString(e));
+    tlr_set_error(msg);
+    return HICMA_TLR_ERR_CUDA;
+}
+
+#ifdef TLR_BOUNDS_CHECK
+// Extent checks of the bounds-checked build: every operand of every launch
+// must lie inside one registered region (the caller's A, L^-1 and info are
+// registered for the length of the call, the scratch array for the life of
+// the process).
+bool noalloc_inside(const void *p, size_t bytes, const char *what) {
+    if (bc_inside(p, bytes)) return true;
+    char msg[320];
+    snprintf(msg, sizeof msg, "bounds check: %s [%p, +%zu B) lies outside every live allocation", what, p, bytes);
+    tlr_set_error(msg);
+    return false;
+}
+bool noalloc_gemm_inside(const GemmTask &t) {
+    return noalloc_inside(t.A, t.opA ? bc_span(t.k, t.m, t.lda) : bc_span(t.m, t.k, t.lda), "noalloc gemm A") &&
+           noalloc_inside(t.B, t.opB ? bc_span(t.n, t.k, t.ldb) : bc_span(t.k, t.n, t.ldb), "noalloc gemm B") &&
+           noalloc_inside(t.C, bc_span(t.m, t.n, t.ldc), "noalloc gemm C");
+}
+#endif
 
 }  // namespace
 }  // namespace tlr
@@ -118,63 +140,84 @@ extern "C" int hicma_tlr_k_potrf_noalloc(int n, double *d_A, int lda, double *d_
         tlr_set_error(msg);
         return HICMA_TLR_ERR_ARG;
     }
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) {
-        tlr_set_error("hicma_tlr_k_potrf_noalloc: no current CUDA device");
-        return HICMA_TLR_ERR_CUDA;
-    }
+    // an error left by the caller's earlier work is reported as such, not
+    // blamed on (or cleared by) this call
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) return noalloc_fail("an earlier CUDA error is pending", pending);
+    // The host-side name of the array is not a device address: ask the runtime
+    // for it on every call (a host-side lookup once the module is loaded; the
+    // first call on a device loads it, so that call belongs before any stream
+    // capture).  Looking it up each time keeps the address right after a
+    // device reset or under another driver context of the same device.
     double *scratch = nullptr;
     {
-        // once per device, with that device current: the host-side name of the
-        // array is not a device address, so ask the runtime for it
-        std::lock_guard<std::mutex> lk(g_scratch_mu);
-        if (!g_scratch_ptr[dev]) {
-            void *p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_potrf_scratch);
-            if (e != cudaSuccess || !p) {
-                tlr_set_error("hicma_tlr_k_potrf_noalloc: cudaGetSymbolAddress of the scratch array failed");
-                return HICMA_TLR_ERR_CUDA;
-            }
-            g_scratch_ptr[dev] = (double *)p;
-        }
-        scratch = g_scratch_ptr[dev];
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_potrf_scratch);
+        if (e != cudaSuccess || !p) return noalloc_fail("cudaGetSymbolAddress of the scratch array failed", e);
+        scratch = (double *)p;
     }
     cudaStream_t st = (cudaStream_t)stream;
     double *dscr = scratch;              // 64 x 64 diagonal-block inverse
     double *tmp = scratch + 64 * 64;     // 64 x n row panel
     const int DBK = 64;
-    if (d_linv && cudaMemset2DAsync(d_linv, (size_t)n * sizeof(double), 0, sizeof(double) * n, n, st) != cudaSuccess) {
-        tlr_set_error("hicma_tlr_k_potrf_noalloc: clearing the inverse failed");
-        return HICMA_TLR_ERR_CUDA;
+#ifdef TLR_BOUNDS_CHECK
+    if (!bc_inside(scratch, NOALLOC_SCRATCH * sizeof(double))) bc_add(scratch, NOALLOC_SCRATCH * sizeof(double));
+    struct Scope {
+        std::vector<const void *> ps;
+        void add(const void *p, size_t b) { if (p && b) { bc_add(p, b); ps.push_back(p); } }
+        ~Scope() { for (const void *p : ps) bc_remove(p); }
+    } reg;
+    reg.add(d_A, bc_span(n, n, lda));
+    if (d_linv) reg.add(d_linv, bc_span(n, n, n));
+    reg.add(d_info, sizeof(int));
+#define NOALLOC_GEMM(task)                                                     \
+    do {                                                                       \
+        const GemmTask t__ = (task);                                           \
+        if (!noalloc_gemm_inside(t__)) return HICMA_TLR_ERR_ARG;               \
+        launch_gemm_single(t__, st);                                           \
+        const cudaError_t e__ = cudaGetLastError();                            \
+        if (e__ != cudaSuccess) return noalloc_fail("GEMM launch failed", e__); \
+    } while (0)
+#else
+#define NOALLOC_GEMM(task)                                                     \
+    do {                                                                       \
+        launch_gemm_single((task), st);                                        \
+        const cudaError_t e__ = cudaGetLastError();                            \
+        if (e__ != cudaSuccess) return noalloc_fail("GEMM launch failed", e__); \
+    } while (0)
+#endif
+    if (d_linv) {
+        const cudaError_t e = cudaMemset2DAsync(d_linv, (size_t)n * sizeof(double), 0, sizeof(double) * n, n, st);
+        if (e != cudaSuccess) return noalloc_fail("clearing the inverse failed", e);
     }
     for (int j = 0; j < n; j += DBK) {
         const int jb = n - j < DBK ? n - j : DBK;
         double *Dinv = d_linv ? d_linv + j + (size_t)j * n : dscr;
         const int ldd = d_linv ? n : DBK;
         launch_potrf_diag(d_A + j + (size_t)j * lda, lda, jb, Dinv, ldd, d_info, info_offset + j, st);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return noalloc_fail("diagonal-block launch failed", e);
         if (j + jb < n) {
             const int rows = n - j - jb;
             double *Pn = d_A + (j + jb) + (size_t)j * lda;
-            launch_gemm_single(make_gemm(0, 1, rows, jb, jb, 1.0, Pn, lda, Dinv, ldd, 0.0, Pn, lda), st);
-            launch_gemm_single(make_gemm(0, 1, rows, rows, jb, -1.0, Pn, lda, Pn, lda, 1.0,
-                                         d_A + (j + jb) + (size_t)(j + jb) * lda, lda, 1),
-                               st);
+            NOALLOC_GEMM(make_gemm(0, 1, rows, jb, jb, 1.0, Pn, lda, Dinv, ldd, 0.0, Pn, lda));
+            NOALLOC_GEMM(make_gemm(0, 1, rows, rows, jb, -1.0, Pn, lda, Pn, lda, 1.0,
+                                   d_A + (j + jb) + (size_t)(j + jb) * lda, lda, 1));
         }
     }
     launch_zero_upper(d_A, n, lda, st);
+    {
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return noalloc_fail("clearing the upper triangle failed", e);
+    }
     if (d_linv) {
         for (int i0 = DBK; i0 < n; i0 += DBK) {
             const int ib = n - i0 < DBK ? n - i0 : DBK;
-            launch_gemm_single(make_gemm(0, 0, ib, i0, i0, 1.0, d_A + i0, lda, d_linv, n, 0.0, tmp, ib), st);
-            launch_gemm_single(make_gemm(0, 0, ib, i0, ib, -1.0, d_linv + i0 + (size_t)i0 * n, n, tmp, ib, 0.0,
-                                         d_linv + i0, n),
-                               st);
+            NOALLOC_GEMM(make_gemm(0, 0, ib, i0, i0, 1.0, d_A + i0, lda, d_linv, n, 0.0, tmp, ib));
+            NOALLOC_GEMM(make_gemm(0, 0, ib, i0, ib, -1.0, d_linv + i0 + (size_t)i0 * n, n, tmp, ib, 0.0,
+                                   d_linv + i0, n));
         }
     }
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        tlr_set_error(cudaGetErrorString(e));
-        return HICMA_TLR_ERR_CUDA;
-    }
+#undef NOALLOC_GEMM
     return 0;
 }

@@ -332,13 +332,16 @@ int hicma_tlr_k_compress(hicma_tlr_ctx *ctx, int nb, const double *d_A, double *
  * context, no allocation, no freeing: its scratch is a fixed array inside the
  * library (2.1 MB of device memory on every GPU that loads the library, held
  * until the process exits), which limits n to 1..4096; larger n returns
- * HICMA_TLR_ERR_ARG with a message in hicma_tlr_last_error().  The first call
- * on a device looks up the device address of that array, so make that first
- * call before capturing the stream into a CUDA graph.  The work is enqueued on
- * `stream` (NULL = legacy default stream) and the call returns without
- * waiting.  All calls share the one array: calls whose work overlaps on the
- * GPU (other streams, other host threads) race on it and must be ordered by
- * the caller. */
+ * HICMA_TLR_ERR_ARG with a message in hicma_tlr_last_error().  Every call
+ * looks up the device address of that array for the current device and
+ * context (a host-side lookup once the library's module is loaded); the first
+ * call on a device loads the module, so make that first call before capturing
+ * the stream into a CUDA graph.  A CUDA error already pending when the call
+ * starts is reported (HICMA_TLR_ERR_CUDA) and left in place; a failed launch
+ * stops the call at once.  The work is enqueued on `stream` (NULL = legacy
+ * default stream) and the call returns without waiting.  All calls share the
+ * one array: calls whose work overlaps on the GPU (other streams, other host
+ * threads) race on it and must be ordered by the caller. */
 int hicma_tlr_k_potrf_noalloc(int n, double *d_A, int lda, double *d_linv, int *d_info,
                               int info_offset, void *stream);
 

@@ -64,6 +64,43 @@ def test_noalloc_potrf_matches_allocating_entry(ctx):
         assert np.linalg.norm(Li2 @ L2 - np.eye(n)) < 1e-9 * n
 
 
+def test_noalloc_potrf_without_inverse_and_not_spd(ctx):
+    """With no L^-1 buffer the scratch array holds each diagonal-block inverse
+    that the panel product reads; a tile that is not positive definite reports
+    the same info (info_offset + first failing column) as the allocating entry."""
+    from hicma_parsec_b200 import tlr
+    lib = tlr.load_library()
+    stream = torch.cuda.current_stream().cuda_stream
+    n = 1500
+    A = _spd(n, 5)
+    dA1, dA2 = _dev(A), _dev(A)
+    info1 = torch.zeros(1, dtype=torch.int32, device="cuda")
+    info2 = torch.zeros(1, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    assert lib.hicma_tlr_k_potrf(ctx.h, n, dA1.data_ptr(), n, None, info1.data_ptr(), 0) == 0, tlr.last_error()
+    assert lib.hicma_tlr_k_potrf_noalloc(n, dA2.data_ptr(), n, None, info2.data_ptr(), 0, stream) == 0, \
+        tlr.last_error()
+    torch.cuda.synchronize()
+    assert int(info1.item()) == 0 and int(info2.item()) == 0
+    L1, L2 = np.tril(_host(dA1)), np.tril(_host(dA2))
+    np.testing.assert_allclose(L2, L1, rtol=0, atol=1e-8 * np.max(np.abs(L1)))
+    assert np.linalg.norm(L2 @ L2.T - A) / np.linalg.norm(A) < 1e-13
+    # not positive definite from column 700 on (its diagonal entry made negative)
+    B = A.copy()
+    B[700, 700] = -1.0
+    offset = 5 * 2700
+    dB1, dB2 = _dev(B), _dev(B)
+    info1.zero_()
+    info2.zero_()
+    torch.cuda.synchronize()
+    assert lib.hicma_tlr_k_potrf(ctx.h, n, dB1.data_ptr(), n, None, info1.data_ptr(), offset) == 0, tlr.last_error()
+    assert lib.hicma_tlr_k_potrf_noalloc(n, dB2.data_ptr(), n, None, info2.data_ptr(), offset, stream) == 0, \
+        tlr.last_error()
+    torch.cuda.synchronize()
+    assert int(info1.item()) == offset + 701
+    assert int(info2.item()) == int(info1.item())
+
+
 def test_noalloc_potrf_rejects_oversize():
     from hicma_parsec_b200 import tlr
     if not torch.cuda.is_available():
