@@ -11,12 +11,15 @@ Printed JSON line (rank 0): metric/value (s/factor, lower is better), the
 end-to-end number through the C ABI with host buffers (pinned host copy of
 the compressed matrix in, factor out), the roofline of the dominant kernel
 class (measured with CUDA events on the library's stream), the CPU
-restatement timed on a bounded sample, and the SM clocks seen during the
-timed region.
+restatement timed on whole factorizations (the workload's N = 27,000 twin,
+scaled by op counts, and the reference's own 2700 case), and the SM clocks
+seen during the timed region.
 
 ``--impl reference`` times the CPU restatement of the reference algorithm
-(the oracle port; the reference itself cannot be built here) on a bounded
-sample of the same workload and extrapolates to seconds per factorization.
+(the oracle port run as a task graph on the host cores; the reference itself
+cannot be built here): every step is one whole factorization of the
+workload's N = 27,000 twin, extrapolated to seconds per factorization of the
+workload by op counts.
 Multi-GPU (torchrun): independent replicas, no collectives.
 """
 from __future__ import annotations
@@ -59,7 +62,6 @@ CONFIGS = {
 }
 METRIC = "TLR Cholesky s/factor at e=1e-8"
 UNIT = "s/factor"
-CPU_SAMPLE_ROWS = 12      # panel-0 sample: tiles (m, n) with n < m < 12
 WORK_FIXTURE = os.path.join(ROOT, "oracle", "workload_ops.json")
 
 
@@ -126,55 +128,64 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-# ------------------------------------------------------------- CPU sample --
-def cpu_sample_tasks(tiles: dict, nb: int, S: int, acc: float, maxrank: int, threads: int):
-    """Time the panel-0 tasks of the TLR Cholesky restricted to tiles (m, n)
-    with n < m < S on the host cores (oracle restatement, one BLAS thread per
-    task, tasks of a class in parallel as the reference's PaRSEC workers
-    would run them).  Returns (seconds, algorithmic ops of the sample)."""
+# ------------------------------------------------------------- CPU runs ----
+TWIN_N = 27000            # full CPU runs: the workload's scaled twin (10 x 10 tiles of 2700)
+
+
+def cpu_twin_matrix(cfg, threads: int):
+    """The scaled twin of a workload (same kernel, tile size, accuracy,
+    maxrank and nugget at N = 27,000, or the workload itself when smaller),
+    generated on the host cores by the oracle's randomized compression (one
+    BLAS thread per tile, tiles in parallel).  Returns (matrix, seconds)."""
     from concurrent.futures import ThreadPoolExecutor
-    import scipy.linalg as sla
     from threadpoolctl import threadpool_limits
     from oracle import tlr_oracle as O
-    ops = 0
-    with threadpool_limits(limits=1):
-        t0 = time.perf_counter()
-        L, _ = O.potrf_tile(tiles[(0, 0)])
-        ops += O.op_counts("c", nb, 0, 0, 0)
+    nb, mr, acc = cfg["nb"], cfg["maxrank"], cfg["acc"]
+    n = min(cfg["n"], TWIN_N)
+    prob = O.Problem(kind=cfg["kind"], noise=cfg["noise"])
+    pts = O.problem_points(prob, n, nb)
+    nt = n // nb
+    T = O.TLRMatrix(n, nb, 1, mr)
 
-        def trsm(m):
-            U, V = tiles[(m, 0)]
-            return m, (U, sla.solve_triangular(L, V, lower=True))
+    def gen(mc):
+        m, c = mc
+        with threadpool_limits(limits=1):
+            A = O.cov_block(prob, pts, m * nb, nb, c * nb, nb)
+            if m == c:
+                return mc, A
+            U, V, r = O.compress_tile_rsvd(A, acc, mr)
+            if r < 0:
+                raise SystemExit(f"CPU twin: generation rejected tile {mc}")
+            return mc, (U, V)
 
-        with ThreadPoolExecutor(threads) as ex:
-            res = dict(ex.map(trsm, range(1, S)))
-            for m in range(1, S):
-                ops += O.op_counts("t", nb, res[m][0].shape[1], 1, 0)
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        for (m, c), v in ex.map(gen, [(m, c) for m in range(nt) for c in range(m + 1)]):
+            if m == c:
+                T.dense[(m, c)] = v
+            else:
+                T.U[(m, c)], T.V[(m, c)] = v
+    return T, time.perf_counter() - t0
 
-            def syrk(m):
-                U, V = res[m]
-                D = tiles[(m, m)] - U @ ((V.T @ V) @ U.T)
-                return D.shape[0]
 
-            list(ex.map(syrk, range(1, S)))
-            for m in range(1, S):
-                r = res[m][0].shape[1]
-                ops += O.op_counts("m", r, r, nb, 0) + O.op_counts("m", nb, r, r, 0) + O.op_counts("m", nb, nb, r, 0)
+def cpu_full_run(T, acc: float, threads: int):
+    """One whole TLR factorization of T (a copy) by the oracle's task-graph
+    run on the host cores.  Returns (seconds, op_counts flops)."""
+    from oracle import tlr_oracle as O
+    W = T.copy()
+    t0 = time.perf_counter()
+    st = O.tlr_potrf_dag(W, acc, threads)
+    secs = time.perf_counter() - t0
+    if st.info != 0:
+        raise SystemExit(f"CPU twin factorization failed, info={st.info}")
+    return secs, float(st.total)
 
-            def gemm(mn):
-                m, n = mn
-                Au, Av = res[m]
-                Bu, Bv = res[n]
-                Cu, Cv = tiles[(m, n)]
-                if Au.shape[1] == 0 or Bu.shape[1] == 0:
-                    return 0
-                Y = Bu @ (Bv.T @ Av)
-                U, V, r, _ = O.recompress(Cu, Cv, Au, Y, acc, maxrank)
-                return O.gemm_lr_opcount(nb, Au.shape[1], Bu.shape[1], Cu.shape[1], r, False)
 
-            ops += sum(ex.map(gemm, [(m, n) for m in range(2, S) for n in range(1, m)]))
-        secs = time.perf_counter() - t0
-    return secs, ops
+def cpu_twin_supported(cfg) -> bool:
+    """Full CPU runs are bounded to a few seconds for the 2D workloads; the
+    3D twins (stacked ranks up to a few thousand, dense SVDs of that size per
+    update) would take minutes per run."""
+    return cfg["kind"] == 2
 
 
 def max_over_ranks(x: float, device=None) -> float:
@@ -220,42 +231,42 @@ def load_work_fixture(cfg_name: str):
 
 # ------------------------------------------------------------------ arms ----
 def run_reference(args, cfg):
-    """CPU restatement on a bounded sample; rank 0 only."""
+    """The CPU restatement of the reference algorithm (the oracle's task-graph
+    run; the reference itself cannot be built here) on the host cores, rank 0
+    only: every step is one whole factorization of the workload's scaled twin,
+    extrapolated to the workload by op_counts flops."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle import tlr_oracle as O
     threads = os.cpu_count() or 1
-    nb, S = cfg["nb"], min(CPU_SAMPLE_ROWS, cfg["n"] // cfg["nb"])
-    prob = O.Problem(kind=cfg["kind"], noise=cfg["noise"])
-    pts = O.problem_points(prob, cfg["n"], nb)
-    tiles = {}
-    for m in range(S):
-        tiles[(m, m)] = O.cov_block(prob, pts, m * nb, nb, m * nb, nb)
-        for n in range(m):
-            U, V, r = O.compress_tile_rsvd(O.cov_block(prob, pts, m * nb, nb, n * nb, nb), cfg["acc"], cfg["maxrank"])
-            tiles[(m, n)] = (U, V)
+    if not cpu_twin_supported(cfg):
+        print(json.dumps({"impl": "reference", "unavailable": "no bounded CPU run for this workload "
+                          "(3D twins take minutes per factorization on the host)"}), flush=True)
+        return
+    T, t_gen = cpu_twin_matrix(cfg, threads)
     fx = load_work_fixture(args.config)
     times = []
-    sample_ops = 0
+    ops = 0.0
     for i in range(args.warmup + args.steps):
-        secs, sample_ops = cpu_sample_tasks(tiles, nb, S, cfg["acc"], cfg["maxrank"], threads)
+        secs, ops = cpu_full_run(T, cfg["acc"], threads)
         if i >= args.warmup:
             times.append(secs)
     t = statistics.median(times)
-    if fx and fx.get("total_ops"):
-        scale = fx["total_ops"] / sample_ops
-        value = t * scale
-        how = (f"panel-0 tasks on tiles (m,n), n<m<{S} ({sample_ops:.3e} op_counts flops, {t:.2f} s); "
+    n_twin = T.n
+    if n_twin == cfg["n"]:
+        value, how = t, f"whole factorization of the workload itself ({ops:.3e} op_counts flops)"
+    elif fx and fx.get("total_ops"):
+        value = t * fx["total_ops"] / ops
+        how = (f"whole factorization of the N={n_twin} twin ({ops:.3e} op_counts flops, median {t:.2f} s); "
                f"scaled by the workload's {fx['total_ops']:.3e} op_counts flops")
     else:
-        value = None
-        how = "panel-0 sample; workload op total unknown (no fixture)"
+        value, how = None, "twin run; workload op total unknown (no fixture)"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": cfg["workload"], "sample": how},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": how},
+            "config": {"workload": cfg["workload"], "sample": how, "twin_generation_s": t_gen},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": how,
+                             "full_run_s": t, "full_run_ops": ops, "full_run_n": n_twin},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -345,15 +356,7 @@ def run_ours(args, cfg):
     t_band = time.perf_counter() - t0
     rmin, rmax, ravg = tlr.HICMA_get_stat2(A0.rank_map(), n // nb, A0.band_size)
 
-    # CPU sample tiles come from the generated matrix before any factorization
     cpu = None
-    S = min(CPU_SAMPLE_ROWS, n // nb)
-    tiles = {}
-    if rank == 0 and world == 1 and not args.no_cpu and A0.band_size == 1:
-        for m in range(S):
-            tiles[(m, m)] = A0.tile(m, m)
-            for c in range(m):
-                tiles[(m, c)] = A0.tile(m, c)
 
     # the working copy gets A0's layout: created at the generation band, then widened
     W = tlr.TLRMatrix(ctx, n, nb, mr, cfg["band"])
@@ -488,12 +491,25 @@ def run_ours(args, cfg):
                "path": "hicma_tlr_store_set (pinned host -> HBM) + hicma_tlr_dpotrf_L + hicma_tlr_store_get"}
         del host, out
 
-    if tiles:
+    if rank == 0 and world == 1 and not args.no_cpu and cpu_twin_supported(cfg):
+        # whole factorizations on the host cores: the N=27000 twin (scaled to this
+        # run's op count) and the reference's own 2700 case
         threads = os.cpu_count() or 1
-        csecs, cops = cpu_sample_tasks(tiles, nb, S, acc, mr, threads)
-        cpu = {"value": csecs * total_ops / cops, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"panel-0 tasks on tiles (m,n), n<m<{S}: {cops:.3e} op_counts flops in {csecs:.2f} s, "
-                         f"scaled to this run's {total_ops:.3e} op_counts flops"}
+        T, t_gen_cpu = cpu_twin_matrix(cfg, threads)
+        csecs, cops = cpu_full_run(T, acc, threads)
+        del T
+        c1 = CONFIGS["c1"]
+        T1, _ = cpu_twin_matrix(c1, threads)
+        c1secs, c1ops = cpu_full_run(T1, c1["acc"], threads)
+        del T1
+        T_n = min(n, TWIN_N)
+        cpu = {"value": csecs * total_ops / cops if T_n < n else csecs, "unit": UNIT, "cores": threads,
+               "kind": "port",
+               "sample": (f"whole TLR factorization of the N={T_n} twin on the host cores (oracle task graph, "
+                          f"one BLAS thread per task): {csecs:.2f} s for {cops:.3e} op_counts flops"
+                          + (f", scaled to this run's {total_ops:.3e} op_counts flops" if T_n < n else "")),
+               "full_run_s": csecs, "full_run_ops": cops, "full_run_n": T_n,
+               "c1_full_run_s": c1secs, "c1_full_run_ops": c1ops}
 
     if rank == 0:
         line = {"metric": METRIC, "value": s_per_factor, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -565,7 +581,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--workspace-gb", type=float, default=16.0)
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--autotune", action="store_true",
                     help="measure the kernel choices (hicma_tlr_autotune) before generation and use them")

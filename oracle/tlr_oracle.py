@@ -723,6 +723,176 @@ def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool
     return st
 
 
+def tlr_potrf_dag(T: TLRMatrix, acc: float, threads: int, fixed_rank: int = 0) -> FactorStats:
+    """The same 2-flow TLR Cholesky as :func:`tlr_potrf` (same task bodies),
+    run as a task graph on ``threads`` host threads the way the reference's
+    PaRSEC runtime runs it: a task starts as soon as the tiles it reads are
+    final and the tile it writes has received every earlier update
+    (``HiCMA_dpotrf_L_2flow.jdf`` flows), ready tasks are taken critical path
+    first (lower panel index, then POTRF > TRSM > SYRK > GEMM, the order of the
+    priorities at ``:50-61,189,290,429,611``), and every task calls BLAS and
+    LAPACK on one thread (the reference links MKL sequential,
+    ``hicma_parsec/CMakeLists.txt:47-54``).  The timed CPU baseline; results
+    equal :func:`tlr_potrf`'s up to the rounding of single- versus
+    multi-threaded BLAS.  Returns the op counts of the run."""
+    import heapq
+    import threading
+    from threadpoolctl import threadpool_limits
+
+    nt, nb, band = T.nt, T.nb, T.band
+    st = FactorStats(tileopcounters=np.zeros((nt, nt), dtype=np.uint64))
+    st.rank_init = np.full((nt, nt), -1, dtype=np.int64)
+    for (m, n) in T.U:
+        st.rank_init[m, n] = T.rank(m, n)
+    st.rank_min = st.rank_init.copy()
+    st.rank_max = st.rank_init.copy()
+    lock = threading.Lock()
+    ops = []          # (count, i, j)
+
+    def potrf(k):
+        L, iinfo = potrf_tile(T.dense[(k, k)])
+        T.dense[(k, k)] = np.tril(L)
+        if iinfo != 0:
+            with lock:
+                if st.info == 0 or k * nb + iinfo < st.info:
+                    st.info = k * nb + iinfo
+        return [(op_counts("c", nb, 0, 0, 0), k, k)]
+
+    def trsm(m, k):
+        Lkk = T.dense[(k, k)]
+        if m - k < band:
+            T.dense[(m, k)] = sla.solve_triangular(Lkk, T.dense[(m, k)].T, lower=True).T
+            return [(op_counts("t", nb, nb, 1, 0), m, k)]
+        r = T.U[(m, k)].shape[1]
+        if r:
+            T.V[(m, k)] = sla.solve_triangular(Lkk, T.V[(m, k)], lower=True)
+        return [(op_counts("t", nb, r, 1, 0), m, k)]
+
+    def syrk(k, m):
+        if m - k < band:
+            A = T.dense[(m, k)]
+            T.dense[(m, m)] = T.dense[(m, m)] - A @ A.T
+            return [(op_counts("m", nb, nb, nb, 0), m, m)]
+        U, V = T.U[(m, k)], T.V[(m, k)]
+        r = U.shape[1]
+        cnt = op_counts("m", r, r, nb, 0) + op_counts("m", nb, r, r, 0) + op_counts("m", nb, nb, r, 0)
+        if r:
+            T.dense[(m, m)] = T.dense[(m, m)] - U @ ((V.T @ V) @ U.T)
+        return [(cnt, m, m)]
+
+    def gemm(m, n, k):
+        if m - k < band:
+            T.dense[(m, n)] = T.dense[(m, n)] - T.dense[(m, k)] @ T.dense[(n, k)].T
+            return [(op_counts("m", nb, nb, nb, 0), m, n)]
+        if n - k < band and m - n < band:
+            Au, Av = T.U[(m, k)], T.V[(m, k)]
+            T.dense[(m, n)] = T.dense[(m, n)] - Au @ (Av.T @ T.dense[(n, k)].T)
+            return [(op_counts("m", nb, nb, Au.shape[1], 0) * 2, m, n)]
+        if m - n < band:
+            Au, Av = T.U[(m, k)], T.V[(m, k)]
+            Bu, Bv = T.U[(n, k)], T.V[(n, k)]
+            ra, rb = Au.shape[1], Bu.shape[1]
+            rr = Av.T @ Bv
+            if ra > rb:
+                T.dense[(m, n)] = T.dense[(m, n)] - (Au @ rr) @ Bu.T
+            else:
+                T.dense[(m, n)] = T.dense[(m, n)] - Au @ (rr @ Bu.T)
+            return [(op_counts("m", nb, nb, min(ra, rb), 0) + op_counts("m", nb, ra, rb, 0) * 2, m, n)]
+        Au, Av = T.U[(m, k)], T.V[(m, k)]
+        ra = Au.shape[1]
+        rc_old = T.U[(m, n)].shape[1]
+        if n - k < band:
+            Y = T.dense[(n, k)] @ Av
+            rb, bdense = 0, True
+        else:
+            Bu, Bv = T.U[(n, k)], T.V[(n, k)]
+            rb, bdense = Bu.shape[1], False
+            if ra == 0 or rb == 0:
+                return []
+            Y = Bu @ (Bv.T @ Av)
+        U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank)
+        T.U[(m, n)], T.V[(m, n)] = U, V
+        with lock:
+            st.overflow += int(ov)
+            st.rank_min[m, n] = min(st.rank_min[m, n], r)
+            st.rank_max[m, n] = max(st.rank_max[m, n], r)
+        return [(gemm_lr_opcount(nb, ra, rb, rc_old, r, bdense), m, n)]
+
+    # task graph: key -> (priority, body, successors), with in-degrees
+    body, succ, indeg = {}, {}, {}
+
+    def add(key, fn, deps):
+        body[key] = fn
+        succ.setdefault(key, [])
+        indeg[key] = 0
+        for d in deps:
+            if d is not None:
+                succ.setdefault(d, []).append(key)
+                indeg[key] += 1
+
+    last = {}     # tile -> last task that wrote it
+    for k in range(nt):
+        add(("P", k), (lambda k=k: potrf(k)), [last.get((k, k))])
+        last[(k, k)] = ("P", k)
+        for m in range(k + 1, nt):
+            add(("T", m, k), (lambda m=m, k=k: trsm(m, k)), [("P", k), last.get((m, k))])
+            last[(m, k)] = ("T", m, k)
+        for m in range(k + 1, nt):
+            add(("S", k, m), (lambda k=k, m=m: syrk(k, m)), [("T", m, k), last.get((m, m))])
+            last[(m, m)] = ("S", k, m)
+        for m in range(k + 2, nt):
+            for n in range(k + 1, m):
+                add(("G", m, n, k), (lambda m=m, n=n, k=k: gemm(m, n, k)),
+                    [("T", m, k), ("T", n, k), last.get((m, n))])
+                last[(m, n)] = ("G", m, n, k)
+    order = {"P": 0, "T": 1, "S": 2, "G": 3}
+
+    def prio(key):
+        return (key[-1], order[key[0]], key)
+
+    ready = [prio(k) for k, d in indeg.items() if d == 0]
+    heapq.heapify(ready)
+    cv = threading.Condition(lock)
+    state = {"left": len(body), "error": None}
+
+    def worker():
+        while True:
+            with cv:
+                while not ready and state["left"] > 0 and state["error"] is None:
+                    cv.wait()
+                if state["left"] == 0 or state["error"] is not None:
+                    cv.notify_all()
+                    return
+                key = heapq.heappop(ready)[2]
+            try:
+                with threadpool_limits(limits=1):
+                    res = body[key]()
+            except BaseException as e:   # noqa: BLE001 - surfaced to the caller below
+                with cv:
+                    state["error"] = e
+                    cv.notify_all()
+                return
+            with cv:
+                ops.extend(res)
+                state["left"] -= 1
+                for s2 in succ[key]:
+                    indeg[s2] -= 1
+                    if indeg[s2] == 0:
+                        heapq.heappush(ready, prio(s2))
+                cv.notify_all()
+
+    ths = [threading.Thread(target=worker, daemon=True) for _ in range(max(1, threads))]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    if state["error"] is not None:
+        raise state["error"]
+    for cnt, i, j in ops:
+        st.tileopcounters[i, j] += np.uint64(cnt & _U64)
+    return st
+
+
 # --------------------------------------------------------------------------
 # Checks, log-determinant, solve, likelihood
 # --------------------------------------------------------------------------

@@ -3,7 +3,10 @@ hicma_parsec/op_counts.h and hicma_parsec/flops.h: builds
 oracle/_ref/op_counts_golden with oracle/Makefile (the reference tree must be
 present) and stores its output.
 
-    python tests/golden/make_op_counts.py [reference root]
+    python tests/golden/make_op_counts.py <reference root>
+
+The reference root may also come from the HICMA_REFERENCE_ROOT environment
+variable; there is no default.
 """
 import json
 import os
@@ -31,4 +34,7 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HICMA_REFERENCE_ROOT", "")
+    if not ref:
+        sys.exit("usage: make_op_counts.py <reference root> (or set HICMA_REFERENCE_ROOT)")
+    main(ref)

@@ -178,3 +178,24 @@ def test_scholqr3_v_side_keeps_ranks_and_accuracy():
     R = O.r_factor_scholqr3(V)
     assert np.allclose(np.tril(R, -1), 0.0)
     assert np.linalg.norm(R.T @ R - V.T @ V) <= 1e-12 * np.linalg.norm(V.T @ V)
+
+
+@pytest.mark.parametrize("band", [1, 2])
+def test_dag_oracle_matches_sequential_oracle(band):
+    """The task-graph run on host threads (the timed CPU baseline) computes the
+    same factorization as the sequential oracle: same ranks, same op counts,
+    factors equal up to BLAS rounding."""
+    prob = O.Problem(kind=2, noise=1e-4)
+    n, nb = 2700, 270
+    pts = O.gen_points(n, 2)
+    T, info = O.generate(prob, n, nb, 1e-8, 130, band, pts)
+    assert info == 0
+    T2 = T.copy()
+    st1 = O.tlr_potrf(T, 1e-8)
+    st2 = O.tlr_potrf_dag(T2, 1e-8, threads=4)
+    assert st1.info == 0 and st2.info == 0
+    assert np.array_equal(T.rank_array(), T2.rank_array())
+    assert np.array_equal(st1.tileopcounters, st2.tileopcounters)
+    assert np.array_equal(st1.rank_min, st2.rank_min) and np.array_equal(st1.rank_max, st2.rank_max)
+    L1, L2 = O.uncompress(T), O.uncompress(T2)
+    assert np.linalg.norm(L1 - L2) <= 1e-10 * np.linalg.norm(L1)
