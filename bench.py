@@ -407,7 +407,8 @@ def run_ours(args, cfg):
     kernels = {"k_gemm_batched": (agg([n for n in prof if n.startswith("gemm")]), "tensor"),
                "k_qr": (prof["qr"], "fp64"), "k_qapply": (prof["qapply"], "fp64"),
                "k_core_svd": (prof["core_svd"], "fp64"), "k_bcgs2": (prof["proj"], "tensor"),
-               "k_copy_batched": (prof["copy"], "hbm"), "k_gram_batched": (prof["gram"], "tensor")}
+               "k_copy_batched": (prof["copy"], "hbm"), "k_gram_batched": (prof["gram"], "tensor"),
+               "k_vside_r": (prof["vside_r"], "tensor")}
     dom = max(kernels, key=lambda k: kernels[k][0]["seconds"])
     pd, kind = kernels[dom]
     launches = int(st[3])  # kernel launches of one factorization (engine counter)
@@ -528,7 +529,9 @@ def run_ours(args, cfg):
                 "tlr_tflops": total_ops / s_per_factor / world / 1e12 if world else None,
                 "op_counts_flops": total_ops,
                 "dense_equiv_gflops": (n ** 3 / 3.0) / s_per_factor / 1e9,
-                "phase_s": {"potrf": st[4], "trsm": st[5], "syrk": st[6], "gemm_recompress": st[7]},
+                "phase_s": {"potrf": st[4], "trsm": st[5], "syrk": st[6], "gemm_recompress": st[7],
+                            "device_idle_between_panels": st[12]},
+                "vside_cholqr_breakdowns": int(st[11]),
                 "jacobi_sweeps_total": st[8],
                 "kernel_classes": prof, "gpu_launches": launches * args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "accuracy": accuracy}

@@ -135,11 +135,15 @@ struct hicma_tlr_ctx_s {
     Arena *ar = nullptr;                // arena of `cur`
     char *h_stage = nullptr, *d_stage = nullptr;
     size_t stage_bytes = 0, stage_off = 0;
-    int *d_flags = nullptr;     // [0] info, [1] overflow, [2] Jacobi sweeps, [3] wait timed out, [4] FP32 updates
+    int *d_flags = nullptr;     // [0] info, [1] overflow, [2] Jacobi sweeps, [3] wait timed out, [4] FP32 updates,
+                                // [5] V-side CholeskyQR breakdowns
     int nsm = 148;              // SM count of the device
     // choices the autotuner measures (defaults: the hand-picked values)
     int gemm_narrow_n = GEMM_NARROW_N;   // rank-wide outputs up to this width use 128 x 32 tiles
     int potrf_grid = 0;                  // CTAs of the persistent tile POTRF (0: one per SM)
+    // V-side R factor of the recompressions: shifted CholeskyQR3 for stacked
+    // ranks up to vside_r_kmax() (1), Householder QR for all (0; HICMA_TLR_VSIDE=qr)
+    int vside_cholqr = 1;
     double *d_scal = nullptr;   // device scalars
     int precision = HICMA_TLR_PREC_FP64;
     long long launches = 0;
@@ -153,7 +157,7 @@ struct hicma_tlr_ctx_s {
     struct ProfRec { int cls; cudaEvent_t a, b; double flops, bytes; };
     std::vector<ProfRec> prof_recs;
     std::vector<cudaEvent_t> ev_pool;
-    double prof_acc[15][4] = {};
+    double prof_acc[32][4] = {};   // per profiling class (P_* below)
 };
 
 struct hicma_tlr_desc_s {
@@ -172,7 +176,7 @@ struct hicma_tlr_desc_s {
     std::vector<int> rk_init, rk_min, rk_max;
     double *d_linv = nullptr;
     bool factored = false;
-    double stats[12] = {0};
+    double stats[16] = {0};
     double async_acc = 0;
     int async_fixed = 0, async_maxrank = 0;
 
@@ -255,6 +259,7 @@ enum {
     // batched DMMA GEMMs by call site (P_GEMM: recompression outputs and the rest)
     P_GEMM_Y, P_GEMM_TRSM, P_GEMM_SYRK, P_GEMM_DENSE, P_GEMM_GEN,
     P_GRAM,   // split-K inner products B_V^T A_V of the recompressions
+    P_VR,     // V-side R factors by shifted CholeskyQR3
     P_NCLASS
 };
 
@@ -493,6 +498,32 @@ int run_qr(hicma_tlr_ctx *c, std::vector<QRTask> &v, int m_max) {
     return check_launch(c);
 }
 
+int run_vside_r(hicma_tlr_ctx *c, std::vector<VRTask> &v, int kmax) {
+    if (v.empty()) return 0;
+#ifdef TLR_BOUNDS_CHECK
+    for (size_t i = 0; i < v.size(); ++i) {
+        const VRTask &t = v[i];
+        BC(t.X, bc_span(t.nb, t.K, t.ldx), "cholqr X", i);
+        BC(t.Z, bc_span(t.nb, t.K, t.nb), "cholqr scratch", i);
+        BC(t.R, bc_span(t.K, t.K, t.K), "cholqr R", i);
+    }
+#endif
+    VRTask *d = stage(c, v.data(), v.size());
+    if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+    double fl = 0, by = 0;
+    for (auto &t : v) {
+        // three Gram products (K^2 nb each, symmetric) and two row substitutions (K^2 nb / 2 FMAs)
+        fl += 3.0 * t.nb * (double)t.K * t.K + 2.0 * t.nb * (double)t.K * t.K;
+        by += 8.0 * t.nb * (double)t.K * 4.0;   // X read twice, scratch written once and read once
+    }
+    {
+        Prof pf(c, P_VR, fl, by);
+        launch_vside_r_batched(d, (int)v.size(), kmax, c->d_flags + 5, c->cur);
+    }
+    v.clear();
+    return check_launch(c);
+}
+
 int run_qapply(hicma_tlr_ctx *c, std::vector<QApplyTask> &v, int m_max) {
     if (v.empty()) return 0;
     TRY(bc_qapply(v, m_max));
@@ -703,7 +734,7 @@ size_t recomp_ws_bytes(int nb, const RecompTask &t) {
     b += A((size_t)nb * K) * 3;                          // Us = [Cu | Wu], Vs = [Cv | -Y], Vk
     b += A(ra) + A(K) + A(npa * pb * pb) + A(npk * pb * pb);  // tau, T factors of Wu and Vs
     b += A((size_t)rc * ra) * 2;                         // Pu, Pu2
-    b += A((size_t)K * K) * 3;                           // RU, SU, T1
+    b += A((size_t)K * K) * 4;                           // RU, SU, T1, RV
     if (K > core_smem_kmax()) b += A(core_work_doubles(K));
     if (t.Bv) b += A((size_t)t.rb * t.ra);
     return b + 1024;
@@ -751,6 +782,8 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
         std::vector<GramTask> grams;
         int *sel = thr2 > 0.0 ? ws_alloc<int>(c, 2 * (tasks.size() - i0) + 2) : nullptr;
         std::vector<QRTask> qrs;
+        std::vector<VRTask> vrs;
+        int vr_kmax = 0;
         std::vector<AssembleTask> asm_;
         std::vector<CoreTask> cores;
         std::vector<QApplyTask> apps;
@@ -810,10 +843,23 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                 if (rc > 0) projs.push_back(ProjTask{Us, Wu, Pu, Pu2, nb, rc, ra});
                 qrs.push_back(QRTask{Wu, tauU, TU, nb, ra, nb});
             }
-            keeps.push_back(make_copy(Vs, nb, Vk, nb, nb, K));
-            qrs.push_back(QRTask{Vs, tauV, TV, nb, K, nb});
+            // V side: R only.  Shifted CholeskyQR3 leaves [Cv, -Y] intact (Vk is
+            // its scratch); the Householder QR overwrites it (Vk keeps a copy).
+            const bool vr = c->vside_cholqr && K <= vside_r_kmax();
+            double *Vsrc = Vs;
+            if (vr) {
+                double *RV = ws_alloc<double>(c, (size_t)K * K);
+                vrs.push_back(VRTask{Vs, Vk, RV, nb, K, nb});
+                vr_kmax = std::max(vr_kmax, K);
+                ct.RV = RV; ct.ldrv = K;
+            } else {
+                keeps.push_back(make_copy(Vs, nb, Vk, nb, nb, K));
+                qrs.push_back(QRTask{Vs, tauV, TV, nb, K, nb});
+                ct.RV = Vs; ct.ldrv = nb;
+                Vsrc = Vk;
+            }
             asm_.push_back(AssembleTask{Pu, Wu, RU, rc, ra, nb});
-            ct.RU = RU; ct.RV = Vs; ct.ldru = K; ct.ldrv = nb;
+            ct.RU = RU; ct.ldru = K;
             ct.SU = SU; ct.RUc = nullptr; ct.work = work;
             cores.push_back(ct);
             // new U = Q(Wu) [U_bot; 0] + Cu U_top
@@ -833,7 +879,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             GemmTask a = make_gemm(1, 0, K, K, K, 1.0, RU, K, SU, K, 0.0, T1, K);
             a.n_dev = ct.rank_task;
             g3.push_back(a);
-            GemmTask b = make_gemm(0, 0, nb, maxrank, K, 1.0, Vk, nb, T1, K, 0.0, t.outV, nb);
+            GemmTask b = make_gemm(0, 0, nb, maxrank, K, 1.0, Vsrc, nb, T1, K, 0.0, t.outV, nb);
             b.n_dev = ct.rank_task;
             g4.push_back(b);
         }
@@ -875,6 +921,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             TRY(check_launch(c));
         }
         TRY(run_qr(c, qrs, nb));
+        TRY(run_vside_r(c, vrs, vr_kmax));
         if (!asm_.empty()) {
             AssembleTask *d = stage(c, asm_.data(), asm_.size());
             if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
@@ -1054,6 +1101,7 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->stream_hi, cudaStreamNonBlocking, prio_hi);
     if (e != cudaSuccess) return fail(e, "priority stream");
     c->cur = c->stream;
+    if (const char *vs = std::getenv("HICMA_TLR_VSIDE")) c->vside_cholqr = std::strcmp(vs, "qr") != 0;
     size_t free_b = 0, total_b = 0;
     e = cudaMemGetInfo(&free_b, &total_b);
     if (e != cudaSuccess) return fail(e, "memory info");
@@ -1928,7 +1976,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         for (int m = n + band; m < NT; ++m) A->rk_init[(size_t)n * NT + m] = A->rank(m, n);
     A->rk_min = A->rk_init;
     A->rk_max = A->rk_init;
-    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 5 * sizeof(int), c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 6 * sizeof(int), c->stream));
     TRY(ctx_sync(c));
     int *d_info = c->d_flags;
     int *rtask = ws_alloc<int>(c, (size_t)NT * NT + 16);
@@ -1944,7 +1992,10 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     std::vector<unsigned long> tops((size_t)NT * NT, 0);
     unsigned long op_total = 0;
     enum { P0, P1, T0, T1, S0, S1, G0, G1, NEV };
-    cudaEvent_t ev[NEV], evP, evT;
+    cudaEvent_t ev[NEV], evP, evT, evEnd;
+    CUDA_TRY(cudaEventCreate(&evEnd));
+    double t_gap = 0.0;      // device idle between a panel's last kernel and the next panel's first
+    bool have_end = false;
     for (auto &e : ev) CUDA_TRY(cudaEventCreate(&e));
     CUDA_TRY(cudaEventCreateWithFlags(&evP, cudaEventDisableTiming));
     CUDA_TRY(cudaEventCreateWithFlags(&evT, cudaEventDisableTiming));
@@ -1955,6 +2006,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     // ops of the critical path POTRF(k) -> TRSM(k+1,k) -> SYRK(k,k+1) (the
     // reference's op_path, HiCMA_dpotrf_L_2flow.jdf:201,303-313,443-462)
     unsigned long op_path = 0;
+    double jac_fl = 0.0, jac_n = 0.0;   // Jacobi flops per sweep summed over the cores, and their number
     double t_last = 0.0;   // wall time of the previous panel's end (verbose > 1)
     auto log_op = [&](unsigned long cnt, int i, int j, bool path = false) {
         tops[(size_t)i * NT + j] += cnt;
@@ -1984,6 +2036,12 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         CUDA_TRY(cudaStreamWaitEvent(c->stream, evP, 0));
         // ---- TRSM(m, k): dense C <- C L^-T ; low rank V <- L^-1 V (:366-401)
         CUDA_TRY(cudaEventRecord(ev[T0], c->stream));
+        if (have_end) {
+            // the previous panel ended (both streams) before the host returned from
+            // its synchronisation, so this gap is the device idle time between panels
+            CUDA_TRY(cudaEventSynchronize(ev[T0]));
+            t_gap += elapsed(evEnd, ev[T0]);
+        }
         {
             NvtxRange nv("TRSM");
             c->ar->off = base_mark;
@@ -2131,6 +2189,9 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             CUDA_TRY(cudaEventRecord(ev[G1], c->stream));
         }
         // ---- panel end: info, ranks, timings
+        CUDA_TRY(cudaStreamWaitEvent(c->stream, evP, 0));
+        CUDA_TRY(cudaEventRecord(evEnd, c->stream));
+        have_end = true;
         TRY(ctx_sync(c));
         int hinfo = 0;
         CUDA_TRY(cudaMemcpy(&hinfo, d_info, sizeof(int), cudaMemcpyDeviceToHost));
@@ -2146,7 +2207,19 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         }
         for (size_t i = 0; i < rec.size(); ++i) {
             const auto &mt = rec_meta[i];
-            log_op(gemm_lr_ops(NB, mt[2], mt[3], mt[4], A->rank(mt[0], mt[1]), rec_case[i] == 1), mt[0], mt[1]);
+            const int rn = A->rank(mt[0], mt[1]);
+            log_op(gemm_lr_ops(NB, mt[2], mt[3], mt[4], rn, rec_case[i] == 1), mt[0], mt[1]);
+            if (c->prof) {
+                // algorithmic flops of the kernels whose work depends on the new
+                // rank (known once the panel is done): the core (M = R_U R_V^T,
+                // pivoted QR stopped at the rank, Jacobi sweeps counted at the end)
+                // and the Q application of the U side (ra reflectors on rn columns)
+                const double K = mt[2] + mt[4], k = rn, ra = mt[2];
+                c->prof_acc[P_CORE][2] += K * K * K / 3.0 + 4.0 * K * K * k - 4.0 * K * k * k + 4.0 / 3.0 * k * k * k;
+                jac_fl += 6.0 * K * k * k;
+                ++jac_n;
+                if (ra > 0) c->prof_acc[P_QAPPLY][2] += 4.0 * NB * ra * k;
+            }
         }
         t_phase[1] += elapsed(ev[T0], ev[T1]);
         if (k + 1 < NT) {
@@ -2171,15 +2244,18 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     for (auto &e : ev) cudaEventDestroy(e);
     cudaEventDestroy(evP);
     cudaEventDestroy(evT);
+    cudaEventDestroy(evEnd);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-    int flags_h[5] = {0, 0, 0, 0, 0};
-    CUDA_TRY(cudaMemcpy(flags_h, c->d_flags, 5 * sizeof(int), cudaMemcpyDeviceToHost));
+    int flags_h[6] = {0, 0, 0, 0, 0, 0};
+    CUDA_TRY(cudaMemcpy(flags_h, c->d_flags, 6 * sizeof(int), cudaMemcpyDeviceToHost));
     if (flags_h[3]) {
         cudaMemset(c->d_flags + 3, 0, sizeof(int));
         set_err("a bounded device wait gave up (tile POTRF task queue)");
         return HICMA_TLR_ERR_TIMEOUT;
     }
     const int overflow = flags_h[1];
+    // Jacobi work: the sweeps counted on the device times the mean work of a sweep
+    if (c->prof && jac_n > 0) c->prof_acc[P_CORE][2] += (double)flags_h[2] * jac_fl / jac_n;
     A->stats[8] = flags_h[2];
     A->stats[9] = flags_h[4];
     if (tileops)
@@ -2195,6 +2271,9 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     A->stats[3] = (double)(c->launches - launches0);
     A->stats[4] = t_phase[0]; A->stats[5] = t_phase[1]; A->stats[6] = t_phase[2]; A->stats[7] = t_phase[3];
     A->stats[10] = (double)op_path;
+    A->stats[11] = flags_h[5];
+    A->stats[12] = t_gap;
+    A->stats[13] = NT;
     A->factored = (info == 0);
     c->main_ar.off = 0;
     c->hi_ar.off = 0;
@@ -2260,7 +2339,7 @@ int hicma_tlr_dpotrf_L_wait(hicma_tlr_ctx *c, hicma_tlr_desc *A, int *Ar) {
 
 int hicma_tlr_last_stats(hicma_tlr_desc *A, double *stats, int nstats) {
     ARG_CHECK(A && stats, "null");
-    for (int i = 0; i < nstats && i < 12; ++i) stats[i] = A->stats[i];
+    for (int i = 0; i < nstats && i < 16; ++i) stats[i] = A->stats[i];
     return 0;
 }
 

@@ -209,6 +209,19 @@ struct QApplyTask {
 };
 void launch_qapply_batched(const QApplyTask *d_tasks, int ntasks, int m_max, cudaStream_t st);
 
+// R factor (upper, K x K, ld K) of an nb x K matrix X by shifted CholeskyQR3
+// (one CTA per task; X is read, not changed; Z is nb x K scratch, ld nb).
+// Tasks of one launch have K <= kmax <= vside_r_kmax().  fail counts tasks
+// whose Cholesky broke down under every shift (R left as the identity).
+struct VRTask {
+    const double *X;
+    double *Z;
+    double *R;
+    int nb, K, ldx;
+};
+int vside_r_kmax();
+void launch_vside_r_batched(const VRTask *d_tasks, int ntasks, int kmax, int *fail, cudaStream_t st);
+
 // ------------------------------------------------------------- core SVD -----
 // M = RU RV^T (RU, RV: K x K upper from the QRs; RU == nullptr means I),
 // one-sided Jacobi SVD, truncation and outputs SU = U_r, SV = V_r Sigma_r

@@ -182,7 +182,7 @@ class Context:
         return self.lib.hicma_tlr_stream(self.h) or 0
 
     PROF_CLASSES = ("gemm", "qr", "qapply", "core_svd", "potrf", "cov", "copy", "other", "proj",
-                    "gemm_y", "gemm_trsm", "gemm_syrk", "gemm_dense", "gemm_gen", "gram")
+                    "gemm_y", "gemm_trsm", "gemm_syrk", "gemm_dense", "gemm_gen", "gram", "vside_r")
 
     def prof_enable(self, on: bool = True) -> None:
         _check(self.lib.hicma_tlr_prof_enable(self.h, int(on)), "hicma_tlr_prof_enable")
@@ -338,8 +338,8 @@ class TLRMatrix:
         return info
 
     def stats(self) -> np.ndarray:
-        s = np.zeros(12)
-        _check(self.lib.hicma_tlr_last_stats(self.h, _p(s), 12), "hicma_tlr_last_stats")
+        s = np.zeros(16)
+        _check(self.lib.hicma_tlr_last_stats(self.h, _p(s), 16), "hicma_tlr_last_stats")
         return s
 
     def copy_from(self, other: "TLRMatrix") -> None:

@@ -179,3 +179,33 @@ def test_probe_residual_matches_dense_check(ctx):
     assert est == A.check_probe(prob, 16, 7)
     assert est <= 10 * TOL
     assert 0.5 * exact <= est <= 2.0 * exact, (est, exact)
+
+
+def test_vside_cholqr_matches_householder(monkeypatch):
+    """The V-side R factor by shifted CholeskyQR3 (default for stacked ranks up
+    to 64) against the Householder QR path (HICMA_TLR_VSIDE=qr): same final
+    ranks within 1, both residuals within the bar, log-determinants equal to
+    1e-10, and no CholeskyQR breakdown."""
+    from hicma_parsec_b200 import tlr
+    out = {}
+    for mode in ("qr", "cholqr"):
+        if mode == "qr":
+            monkeypatch.setenv("HICMA_TLR_VSIDE", "qr")
+        else:
+            monkeypatch.delenv("HICMA_TLR_VSIDE", raising=False)
+        with tlr.Context(0, 1 << 30) as c:
+            prob = tlr.Problem(kind=2, noise=1e-4)
+            A = tlr.TLRMatrix(c, N, NB, MAXRANK, 1)
+            assert A.generate(prob, TOL, MAXRANK) == 0
+            assert A.potrf(TOL, MAXRANK) == 0
+            st = A.stats()
+            prof = None
+            out[mode] = (A.rank_map(), A.logdet(), O.check_dpotrf2(A.uncompress(), O.dense_matrix(
+                O.Problem(kind=2, noise=1e-4), O.gen_points(N, 2))), st[11])
+            A.close()
+    (Gq, ldq, rq, _), (Gc, ldc, rc, brk) = out["qr"], out["cholqr"]
+    off = Gq >= 0
+    assert np.max(np.abs(Gq[off] - Gc[off])) <= 1
+    assert rq <= 10 * TOL and rc <= 10 * TOL
+    assert abs(ldq - ldc) <= 1e-10 * abs(ldq)
+    assert brk == 0

@@ -35,14 +35,20 @@ torch = pytest.importorskip("torch")
 
 N, NB = 27000, 2700
 
-# kind 2: 2D sqexp, kind 4: 3D exp, kind 3: 3D sqexp
+# kind 2: 2D sqexp, kind 4: 3D exp, kind 3: 3D sqexp.  logdet_e8: the bound met
+# at e = 1e-8 (measured on a B200: 2D 7.6e-8, the oracle's own error on the same
+# tiles to the digits shown; 3D exp below 1e-15); e_strict: the accuracy at which
+# the 2D twin meets the 1e-8 bar (7.9e-10 measured at e = 1e-9).  The 3D sqexp twin
+# is generated at band 4: at N = 27,000 its tiles are eight times the volume of the
+# N = 216,000 workload's and the ones within distance 3 of the diagonal exceed
+# maxrank 500 (at N = 216,000 every off-band tile compresses at band 1).
 TWINS = {
-    "2D sqexp, maxrank 150": dict(kind=2, maxrank=150, autoband=False, oracle_ranks=True,
-                                  logdet_e8=1e-6, e_strict=1e-10),
-    "3D exp, maxrank 1350, auto band": dict(kind=4, maxrank=1350, autoband=True, oracle_ranks=False,
-                                            logdet_e8=1e-6, e_strict=1e-10),
-    "3D sqexp, maxrank 500, auto band": dict(kind=3, maxrank=500, autoband=True, oracle_ranks=True,
-                                             logdet_e8=1e-6, e_strict=1e-10),
+    "2D sqexp, maxrank 150": dict(kind=2, maxrank=150, band0=1, autoband=False, oracle_ranks=True,
+                                  logdet_e8=1.5e-7, e_strict=1e-9),
+    "3D exp, maxrank 1350, auto band": dict(kind=4, maxrank=1350, band0=1, autoband=True, oracle_ranks=False,
+                                            logdet_e8=1e-8, e_strict=None),
+    "3D sqexp, maxrank 500, auto band": dict(kind=3, maxrank=500, band0=4, autoband=True, oracle_ranks=True,
+                                             logdet_e8=1e-8, e_strict=None),
 }
 
 
@@ -79,11 +85,11 @@ def _snapshot(A, nt, band, maxrank):
 
 
 def _factor(tlr, ctx, prob, cfg, acc, want_snapshot):
-    A = tlr.TLRMatrix(ctx, N, NB, cfg["maxrank"], 1)
+    A = tlr.TLRMatrix(ctx, N, NB, cfg["maxrank"], cfg["band0"])
     assert A.generate(prob, acc, cfg["maxrank"]) == 0
     if cfg["autoband"]:
         b = tlr.parsec_band_size_auto_tuning(A.rank_map(), N // NB, NB)
-        if b > 1:
+        if b > A.band_size:
             A.band_regenerate(prob, b)
     T = _snapshot(A, N // NB, A.band_size, cfg["maxrank"]) if want_snapshot else None
     assert A.potrf(acc, cfg["maxrank"]) == 0
@@ -116,10 +122,11 @@ def test_scaled_twin(name):
             assert np.max(np.abs(G[off] - Gref[off])) <= 2, np.max(np.abs(G[off] - Gref[off]))
         A.close()
         A = None
-        # the accuracy at which the log-determinant meets the 1e-8 bar
-        A, _ = _factor(tlr, ctx, prob, cfg, cfg["e_strict"], False)
-        err = abs(A.logdet() - ld_dense) / abs(ld_dense)
-        assert err <= 1e-8, (err, cfg["e_strict"])
+        if cfg["e_strict"]:
+            # the accuracy at which the log-determinant meets the 1e-8 bar
+            A, _ = _factor(tlr, ctx, prob, cfg, cfg["e_strict"], False)
+            err = abs(A.logdet() - ld_dense) / abs(ld_dense)
+            assert err <= 1e-8, (err, cfg["e_strict"])
     finally:
         if A is not None:
             A.close()
