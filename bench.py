@@ -47,6 +47,10 @@ CONFIGS = {
                workload="2D sqexp N=2700 NB=270 e=1e-8 maxrank=130 band=1 FP64"),
     "c2s": dict(kind=2, n=27000, nb=2700, maxrank=150, acc=1e-8, noise=1e-4, band=1, autoband=False,
                 workload="2D sqexp N=27000 NB=2700 e=1e-8 maxrank=150 band=1 FP64 (scaled twin of N=270000)"),
+    # the leading 10 x 10 tiles of the N=270,000 workload (its first 27,000 Morton-ordered points)
+    "c2t": dict(kind=2, n=27000, n_full=270000, nb=2700, maxrank=150, acc=1e-8, noise=1e-4, band=1,
+                autoband=False,
+                workload="2D sqexp leading 10x10 tiles of the N=270000 matrix, NB=2700 e=1e-8 maxrank=150 band=1 FP64"),
     "c3": dict(kind=4, n=108000, nb=2700, maxrank=1350, acc=1e-8, noise=1e-4, band=1, autoband=True,
                workload="3D exp N=108000 NB=2700 e=1e-8 maxrank=1350 band auto FP64"),
     "c3s": dict(kind=4, n=27000, nb=2700, maxrank=1350, acc=1e-8, noise=1e-4, band=1, autoband=True,
@@ -132,18 +136,27 @@ class ClockSampler:
 TWIN_N = 27000            # full CPU runs: the workload's scaled twin (10 x 10 tiles of 2700)
 
 
+def workload_points(tlr, prob, cfg):
+    """Points of a workload: its own (None: the library generates them), or
+    the first n of the n_full-point set for a leading-tiles twin."""
+    if "n_full" not in cfg:
+        return None
+    return np.ascontiguousarray(tlr.points(prob, cfg["n_full"])[:, :cfg["n"]])
+
+
 def cpu_twin_matrix(cfg, threads: int):
-    """The scaled twin of a workload (same kernel, tile size, accuracy,
-    maxrank and nugget at N = 27,000, or the workload itself when smaller),
-    generated on the host cores by the oracle's randomized compression (one
-    BLAS thread per tile, tiles in parallel).  Returns (matrix, seconds)."""
+    """The twin of a workload: its leading 10 x 10 tiles (the first 27,000 of
+    its Morton-ordered points, so the tiles are the workload's own; the
+    workload itself when smaller), generated on the host cores by the oracle's
+    randomized compression (one BLAS thread per tile, tiles in parallel).
+    Returns (matrix, seconds)."""
     from concurrent.futures import ThreadPoolExecutor
     from threadpoolctl import threadpool_limits
     from oracle import tlr_oracle as O
     nb, mr, acc = cfg["nb"], cfg["maxrank"], cfg["acc"]
     n = min(cfg["n"], TWIN_N)
     prob = O.Problem(kind=cfg["kind"], noise=cfg["noise"])
-    pts = O.problem_points(prob, n, nb)
+    pts = np.ascontiguousarray(O.problem_points(prob, cfg.get("n_full", cfg["n"]), nb)[:n])
     nt = n // nb
     T = O.TLRMatrix(n, nb, 1, mr)
 
@@ -300,7 +313,7 @@ def run_profile(args, cfg):
     n, nb, mr, acc = cfg["n"], cfg["nb"], cfg["maxrank"], cfg["acc"]
     A = tlr.TLRMatrix(ctx, n, nb, mr, cfg["band"])
     ctx.prof_enable(True)
-    if A.generate(prob, acc, mr) != 0:
+    if A.generate(prob, acc, mr, pts=workload_points(tlr, prob, cfg)) != 0:
         raise SystemExit("generation rejected a tile")
     if cfg["autoband"]:
         band = tlr.parsec_band_size_auto_tuning(A.rank_map(), n // nb, nb)
@@ -342,7 +355,8 @@ def run_ours(args, cfg):
     tuned = ctx.autotune(nb, mr) if getattr(args, "autotune", False) else None
     A0 = tlr.TLRMatrix(ctx, n, nb, mr, cfg["band"])
     t0 = time.perf_counter()
-    info = A0.generate(prob, acc, mr)
+    pts_w = workload_points(tlr, prob, cfg)
+    info = A0.generate(prob, acc, mr, pts=pts_w)
     t_gen = time.perf_counter() - t0
     if info != 0:
         raise SystemExit(f"generation rejected a tile (info={info})")
@@ -361,7 +375,7 @@ def run_ours(args, cfg):
     # the working copy gets A0's layout: created at the generation band, then widened
     W = tlr.TLRMatrix(ctx, n, nb, mr, cfg["band"])
     if A0.band_size != cfg["band"]:
-        W.generate(prob, acc, mr)
+        W.generate(prob, acc, mr, pts=pts_w)
         W.band_regenerate(prob, A0.band_size)
     stream = torch.cuda.ExternalStream(ctx.stream)
 
@@ -450,7 +464,7 @@ def run_ours(args, cfg):
     t_loglik = time.perf_counter() - t0
     if args.accuracy:
         R = tlr.TLRMatrix(ctx, n, nb, mr, cfg["band"])
-        if R.generate(prob, acc / 100, mr) != 0:
+        if R.generate(prob, acc / 100, mr, pts=pts_w) != 0:
             accuracy["logdet_ref"] = None
         else:
             if A0.band_size != cfg["band"]:
@@ -492,6 +506,32 @@ def run_ours(args, cfg):
                "path": "hicma_tlr_store_set (pinned host -> HBM) + hicma_tlr_dpotrf_L + hicma_tlr_store_get"}
         del host, out
 
+    # the mixed-precision form on the same matrix (FP32 products of small-norm
+    # updates, everything else FP64): s/factor, probe residual and log det
+    fin_stats = list(tlr.HICMA_get_stat2(W.rank_map(), n // nb, W.band_size))
+    mixed = None
+    if args.precision == "fp64" and not args.no_mixed:
+        ctx.set_precision(tlr.PREC_MIXED)
+        step()
+        m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        for _ in range(2):
+            step()
+        m1.record(stream)
+        m1.synchronize()
+        ms = m0.elapsed_time(m1) * 1e-3 / 2
+        mst = W.stats()
+        mld = W.logdet()
+        mixed = {"value": ms, "unit": UNIT, "steps": 2, "speedup_vs_fp64": s_per_factor / ms,
+                 "updates_fp32": int(mst[9]), "residual_probe": W.check_probe(prob, 16, 0), "logdet": mld,
+                 "logdet_rel_diff_vs_fp64": abs(mld - ld) / abs(ld)}
+        ctx.set_precision(tlr.PREC_FP64)
+
+    serving_line = None
+    if rank == 0 and world == 1 and args.serving_requests > 0:
+        serving_line = serving_stream(args.serving_requests, args.serving_nmax_default, args.slots, args.rate,
+                                      min(args.workspace_gb, 8.0))
+
     if rank == 0 and world == 1 and not args.no_cpu and cpu_twin_supported(cfg):
         # whole factorizations on the host cores: the N=27000 twin (scaled to this
         # run's op count) and the reference's own 2700 case
@@ -506,7 +546,8 @@ def run_ours(args, cfg):
         T_n = min(n, TWIN_N)
         cpu = {"value": csecs * total_ops / cops if T_n < n else csecs, "unit": UNIT, "cores": threads,
                "kind": "port",
-               "sample": (f"whole TLR factorization of the N={T_n} twin on the host cores (oracle task graph, "
+               "sample": (f"whole TLR factorization of the N={T_n} twin (leading tiles of the workload) on the "
+                          f"host cores (oracle task graph, "
                           f"one BLAS thread per task): {csecs:.2f} s for {cops:.3e} op_counts flops"
                           + (f", scaled to this run's {total_ops:.3e} op_counts flops" if T_n < n else "")),
                "full_run_s": csecs, "full_run_ops": cops, "full_run_n": T_n,
@@ -525,7 +566,7 @@ def run_ours(args, cfg):
                            "kernel_choices": {"gemm_narrow_n": ctx.tuning()[0], "potrf_grid": ctx.tuning()[1],
                                               "autotuned": tuned is not None},
                            "rank_min_max_avg": [rmin, rmax, ravg],
-                           "final_rank_min_max_avg": list(tlr.HICMA_get_stat2(W.rank_map(), n // nb, W.band_size))},
+                           "final_rank_min_max_avg": fin_stats},
                 "tlr_tflops": total_ops / s_per_factor / world / 1e12 if world else None,
                 "op_counts_flops": total_ops,
                 "dense_equiv_gflops": (n ** 3 / 3.0) / s_per_factor / 1e9,
@@ -534,7 +575,8 @@ def run_ours(args, cfg):
                 "vside_cholqr_breakdowns": int(st[11]),
                 "jacobi_sweeps_total": st[8],
                 "kernel_classes": prof, "gpu_launches": launches * args.steps,
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "accuracy": accuracy}
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "accuracy": accuracy,
+                "mixed_precision": mixed, "serving": serving_line}
         print(json.dumps(line), flush=True)
     W.close()
     A0.close()
@@ -542,6 +584,35 @@ def run_ours(args, cfg):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def serving_stream(requests: int, nmax: int, slots: int, rate: float, workspace_gb: float) -> dict:
+    """The same seeded ML requests served sequentially on one slot and by the
+    continuous-batching loop (all at t=0): solves/s, p50/p99 latency, and the
+    largest relative log-likelihood difference between the two runs."""
+    import torch
+    from hicma_parsec_b200 import serving
+    reqs = serving.sample_requests(requests, seed=0, rate=rate, n_max=nmax)
+    out = {}
+    ref = None
+    for mode, sl in (("sequential", 1), ("continuous", slots)):
+        srv = serving.MLEServer(0, slots=sl, workspace_bytes=int(workspace_gb * (1 << 30) / max(sl, 1)))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = srv.run(reqs, realtime=False)
+        mk = time.perf_counter() - t0
+        srv.close()
+        out[mode] = serving.summarize(res, mk)
+        out[mode]["slots"] = sl
+        if ref is None:
+            ref = res
+        else:
+            d = [abs(a.loglik - b.loglik) / abs(a.loglik) for a, b in zip(ref, res) if a.status == 0 and b.status == 0]
+            out[mode]["max_rel_diff_vs_sequential"] = max(d) if d else None
+    seq, con = out["sequential"]["solves_per_s"], out["continuous"]["solves_per_s"]
+    out["speedup_vs_sequential"] = con / seq if seq and con else None
+    out["workload"] = f"{requests} ML requests (seed 0), N log-U[1e4,{nmax}], tile 1000-2700, 2D/3D sqexp or 3D exp"
+    return out
 
 
 def run_serving(args):
@@ -586,6 +657,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
+    ap.add_argument("--serving-requests", type=int, default=8,
+                    help="requests of the short serving stream in the default run (0: skip)")
+    ap.add_argument("--serving-nmax-default", type=int, default=60000,
+                    help="largest N of the short serving stream in the default run")
     ap.add_argument("--autotune", action="store_true",
                     help="measure the kernel choices (hicma_tlr_autotune) before generation and use them")
     ap.add_argument("--serving", action="store_true", help="run the MLE serving benchmark instead")

@@ -18,21 +18,27 @@
 // backward-stable triangular solve the method's error bounds assume; an
 // explicit inverse of R1 would add an error of order u cond(R1) ||X||).
 //
-// Layout: 256 threads, one row per thread in chunks of 256 rows; a thread
-// keeps its row in registers for the substitution, then the chunk is staged
-// column-major in shared memory (leading dimension 260: conflict-free both
-// for the row-per-thread stores and for the DMMA fragment loads) and each
-// warp accumulates its own 8 x 8 tiles of the lower triangle of G with
-// mma.sync m8n8k4 f64 over the chunk.  Tiles are owned, so no cross-warp
-// reduction is needed.  The K x K Cholesky runs in shared memory on one warp.
+// Layout: 8 warps, each working on its own 32-row chunks (rows warp*32 +
+// 256 i + lane) with no CTA barrier inside a pass.  A lane keeps its row in
+// registers for the substitution (R read as broadcasts from shared memory),
+// stages the row into its warp's slice of shared memory (column-major, pitch
+// 36: conflict-free for the row stores and for the DMMA fragment loads), and
+// the warp accumulates the whole lower triangle of the chunk's Gram product
+// with mma.sync m8n8k4 f64 (one fragment load per 8-column block and row
+// quad, reused by every tile of that block).  The eight per-warp Gram
+// partials are added in warp order at the end of a pass (deterministic), and
+// one warp factors G in shared memory.  Kernels are instantiated per width
+// bucket (KM = 16, 32, 48 columns) so that unrolled loops do not run far past
+// the actual K; the row and the Gram accumulators of the widest bucket fill
+// the register file, so wider stacks take the Householder path.
 #include "tlr_internal.h"
 
 namespace tlr {
 namespace {
 
-constexpr int VR_THREADS = 256;
-constexpr int VR_CH = 256;              // rows per chunk (one per thread)
-constexpr int VR_LDZ = VR_CH + 4;       // staged chunk leading dimension (== 4 mod 16)
+constexpr int VR_WARPS = 8;
+constexpr int VR_THREADS = VR_WARPS * 32;
+constexpr int VR_PITCH = 36;            // per-warp staged chunk pitch (== 4 mod 16)
 
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -44,10 +50,30 @@ template <int KM>
 struct VRSmem {
     static constexpr int NT8 = KM / 8;
     static constexpr int NTILE = NT8 * (NT8 + 1) / 2;
-    static constexpr int TPW = (NTILE + 7) / 8;     // tiles per warp (at most)
-    static constexpr size_t Z = (size_t)KM * VR_LDZ; // staged chunk; also G and scratch between passes
-    static constexpr size_t bytes() { return sizeof(double) * (Z + 2 * (size_t)KM * KM + 2 * KM); }
+    static constexpr size_t W = (size_t)KM * VR_PITCH;    // one warp's staged chunk
+    static constexpr size_t KK = (size_t)KM * KM;
+    // staged chunks | G | G copy / product scratch | Rr (row-major R of the pass) | Rt | d | 1/diag
+    static constexpr size_t bytes() { return sizeof(double) * (VR_WARPS * W + 4 * KK + 2 * KM); }
 };
+
+// x <- x R^-1 for one row x (registers): right-looking substitution with the
+// row-major upper R in shared memory.  Written as compile-time recursion so
+// that every index into x is static and x stays in registers at any width.
+template <int KM, int J, int C>
+__device__ __forceinline__ void subst_cols(double (&x)[KM], double xj, const double *rj) {
+    if constexpr (C < KM) {
+        x[C] -= xj * rj[C];
+        subst_cols<KM, J, C + 1>(x, xj, rj);
+    }
+}
+template <int KM, int J>
+__device__ __forceinline__ void subst_rows(double (&x)[KM], const double *Rr, const double *rdg) {
+    if constexpr (J < KM) {
+        x[J] *= rdg[J];
+        subst_cols<KM, J, J + 1>(x, x[J], Rr + J * KM);
+        subst_rows<KM, J + 1>(x, Rr, rdg);
+    }
+}
 
 // In-place lower Cholesky of the K x K matrix G (column-major, ld KM) by one
 // warp (lanes own rows); returns false on a non-positive pivot.
@@ -75,64 +101,45 @@ __device__ bool warp_cholesky(double *G, int K, int lane) {
 template <int KM>
 __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const VRTask *__restrict__ tasks, int *fail) {
     using S = VRSmem<KM>;
+    constexpr int NT8 = S::NT8, NTILE = S::NTILE;
     extern __shared__ double sm[];
-    double *Zs = sm;                          // KM x VR_LDZ staged chunk (column j at j * VR_LDZ)
-    double *Rp = Zs + S::Z;                   // this pass's R (upper, column-major, ld KM)
-    double *Rt = Rp + (size_t)KM * KM;        // accumulated R
-    double *dsc = Rt + (size_t)KM * KM;       // column norms d_j
-    double *rdg = dsc + KM;                   // 1 / diag(Rp)
     __shared__ int ok_sh;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, tig = lane & 3;
+    double *Zw = sm + warp * S::W;                 // this warp's staged chunk
+    double *G = sm + VR_WARPS * S::W;              // K x K Gram (column-major, ld KM)
+    double *Gc = G + S::KK;                        // copy for a retry; product scratch
+    double *Rr = Gc + S::KK;                       // R of the pass, row-major: Rr[j * KM + k] = R(j, k)
+    double *Rt = Rr + S::KK;                       // accumulated R (column-major)
+    double *dsc = Rt + S::KK;                      // column norms d_j (1 / d_j from pass 1 on)
+    double *rdg = dsc + KM;                        // 1 / diag(R)
 
     const VRTask t = tasks[blockIdx.x];
     const int K = t.K, nb = t.nb, ldx = t.ldx;
     if (K <= 0) return;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, tig = lane & 3;
-    const int nt8 = (K + 7) / 8;
     const double u = 1.1102230246251565e-16;
 
-    // this warp's tiles of the lower triangle of G (8 x 8 blocks (mi, ni), mi >= ni)
-    int tmi[S::TPW], tni[S::TPW];
-#pragma unroll
-    for (int q = 0; q < S::TPW; ++q) {
-        const int tile = warp + 8 * q;
-        int mi = 0;
-        while ((mi + 1) * (mi + 2) / 2 <= tile) ++mi;
-        tmi[q] = (tile < S::NTILE && mi < nt8) ? mi : -1;
-        tni[q] = tile - mi * (mi + 1) / 2;
-    }
-
     for (int pass = 0; pass < 3; ++pass) {
-        // two accumulators per tile (even and odd row quads): independent DMMA chains
-        double acc[S::TPW][2][2];
+        double acc[NTILE][2];
 #pragma unroll
-        for (int q = 0; q < S::TPW; ++q) acc[q][0][0] = acc[q][0][1] = acc[q][1][0] = acc[q][1][1] = 0.0;
+        for (int q = 0; q < NTILE; ++q) acc[q][0] = acc[q][1] = 0.0;
+        const double *src = pass == 2 ? t.Z : t.X;
+        const int lds = pass == 2 ? nb : ldx;
 
-        for (int c0 = 0; c0 < nb; c0 += VR_CH) {
-            const int row = c0 + tid;
+        for (int r0 = warp * 32; r0 < nb; r0 += VR_THREADS) {
+            const int row = r0 + lane;
             const bool valid = row < nb;
             double x[KM];
-            const double *src = pass == 2 ? t.Z : t.X;
-            const int lds = pass == 2 ? nb : ldx;
 #pragma unroll
             for (int j = 0; j < KM; ++j) x[j] = (valid && j < K) ? src[(size_t)row + (size_t)j * lds] : 0.0;
             if (pass > 0) {
                 if (pass == 1) {
 #pragma unroll
-                    for (int j = 0; j < KM; ++j)
-                        if (j < K) x[j] /= dsc[j];
+                    for (int j = 0; j < KM; ++j) x[j] *= dsc[j];
                 }
-                // x <- x Rp^-1 (right-looking row substitution)
-#pragma unroll
-                for (int j = 0; j < KM; ++j) {
-                    if (j < K) {
-                        x[j] *= rdg[j];
-                        const double xj = x[j];
-#pragma unroll
-                        for (int k = j + 1; k < KM; ++k)
-                            if (k < K) x[k] -= xj * Rp[j + k * KM];
-                    }
-                }
+                // x <- x R^-1 (right-looking row substitution; R and 1/diag are
+                // zero past K, so the padding columns stay zero)
+                subst_rows<KM, 0>(x, Rr, rdg);
                 if (pass == 1 && valid) {
 #pragma unroll
                     for (int j = 0; j < KM; ++j)
@@ -140,40 +147,44 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
                 }
             }
 #pragma unroll
-            for (int j = 0; j < KM; ++j) Zs[j * VR_LDZ + tid] = x[j];
-            __syncthreads();
-            // G += Zc^T Zc over this chunk, all of this warp's tiles per row quad
-#pragma unroll 2
-            for (int r = 0; r < VR_CH; r += 8) {
+            for (int j = 0; j < KM; ++j) Zw[j * VR_PITCH + lane] = x[j];
+            __syncwarp();
+            // Gram of the chunk: row quads s, one fragment per 8-column block
+#pragma unroll 1
+            for (int s = 0; s < 32; s += 4) {
+                double a[NT8];
 #pragma unroll
-                for (int q = 0; q < S::TPW; ++q) {
-                    if (tmi[q] < 0) continue;
-                    const double *za = Zs + (8 * tmi[q] + g) * VR_LDZ + tig + r;
-                    const double *zb = Zs + (8 * tni[q] + g) * VR_LDZ + tig + r;
-                    dmma884(acc[q][0], za[0], zb[0]);
-                    dmma884(acc[q][1], za[4], zb[4]);
-                }
+                for (int mi = 0; mi < NT8; ++mi) a[mi] = Zw[(8 * mi + g) * VR_PITCH + s + tig];
+                int q = 0;
+#pragma unroll
+                for (int mi = 0; mi < NT8; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni <= mi; ++ni, ++q) dmma884(acc[q], a[mi], a[ni]);
             }
-            __syncthreads();
+            __syncwarp();
         }
-        // accumulators -> G (column-major KM x KM in the chunk buffer), both triangles
-        double *G = Zs;
-        double *Gc = Zs + (size_t)KM * KM;    // copy for a retry
-#pragma unroll
-        for (int q = 0; q < S::TPW; ++q) {
-            if (tmi[q] < 0) continue;
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-                const int i = 8 * tmi[q] + g, j = 8 * tni[q] + 2 * tig + e;
-                const double v = acc[q][0][e] + acc[q][1][e];
-                G[i + j * KM] = v;
-                G[j + i * KM] = v;
-            }
-        }
+        // per-warp partials -> G in warp order (both triangles)
+        for (int idx = tid; idx < KM * KM; idx += VR_THREADS) G[idx] = 0.0;
         __syncthreads();
+        for (int w = 0; w < VR_WARPS; ++w) {
+            if (warp == w) {
+                int q = 0;
+#pragma unroll
+                for (int mi = 0; mi < NT8; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni <= mi; ++ni, ++q)
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const int i = 8 * mi + g, j = 8 * ni + 2 * tig + e;
+                            G[i + j * KM] += acc[q][e];
+                            if (mi != ni) G[j + i * KM] += acc[q][e];
+                        }
+            }
+            __syncthreads();
+        }
         if (pass == 0) {
-            for (int j = tid; j < K; j += VR_THREADS) {
-                const double d = sqrt(G[j + j * KM]);
+            for (int j = tid; j < KM; j += VR_THREADS) {
+                const double d = j < K ? sqrt(G[j + j * KM]) : 1.0;
                 dsc[j] = d > 0.0 ? d : 1.0;
             }
             __syncthreads();
@@ -183,7 +194,7 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
             }
             __syncthreads();
         }
-        // shift from the trace of G
+        // shift from the trace of G; Cholesky on warp 0
         if (warp == 0) {
             double tr = 0.0;
             for (int j = lane; j < K; j += 32) tr += G[j + j * KM];
@@ -222,38 +233,45 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
             }
         }
         __syncthreads();
-        // Rp = L^T (upper), 1 / diag
+        // R of the pass, row-major (upper): Rr[j][k] = L(k, j); zero outside K
         for (int idx = tid; idx < KM * KM; idx += VR_THREADS) {
-            const int i = idx % KM, j = idx / KM;
+            const int j = idx / KM, k = idx % KM;
             double v = 0.0;
-            if (i <= j && j < K) v = ok_sh ? G[j + i * KM] : (i == j ? 1.0 : 0.0);
-            Rp[i + j * KM] = v;
+            if (j <= k && k < K) v = ok_sh ? G[k + j * KM] : (j == k ? 1.0 : 0.0);
+            Rr[j * KM + k] = v;
         }
         __syncthreads();
-        for (int j = tid; j < K; j += VR_THREADS) rdg[j] = 1.0 / Rp[j + j * KM];
-        // Rt <- Rp Rt (pass 0: Rt = Rp); upper times upper, via the G buffer
+        for (int j = tid; j < KM; j += VR_THREADS) rdg[j] = j < K ? 1.0 / Rr[j * KM + j] : 0.0;
         if (pass == 0) {
-            for (int idx = tid; idx < KM * KM; idx += VR_THREADS) Rt[idx] = Rp[idx];
+            for (int idx = tid; idx < KM * KM; idx += VR_THREADS) {
+                const int i = idx % KM, j = idx / KM;
+                Rt[idx] = Rr[i * KM + j];
+            }
         } else {
-            double *T = Zs + 2 * (size_t)KM * KM;
+            // Rt <- R Rt (upper times upper) through the scratch
             for (int idx = tid; idx < K * K; idx += VR_THREADS) {
                 const int i = idx % K, j = idx / K;
                 double s = 0.0;
-                for (int k = i; k <= j; ++k) s += Rp[i + k * KM] * Rt[k + j * KM];
-                T[i + j * KM] = i <= j ? s : 0.0;
+                for (int k = i; k <= j; ++k) s += Rr[i * KM + k] * Rt[k + j * KM];
+                Gc[i + j * KM] = i <= j ? s : 0.0;
             }
             __syncthreads();
             for (int idx = tid; idx < K * K; idx += VR_THREADS) {
                 const int i = idx % K, j = idx / K;
-                Rt[i + j * KM] = T[i + j * KM];
+                Rt[i + j * KM] = Gc[i + j * KM];
             }
         }
         __syncthreads();
+        if (pass == 0) {
+            // the substitution of pass 1 scales by 1/d first
+            for (int j = tid; j < KM; j += VR_THREADS) dsc[j] = 1.0 / dsc[j];
+            __syncthreads();
+        }
     }
-    // R = Rt D
+    // R = Rt D (dsc holds 1/d)
     for (int idx = tid; idx < K * K; idx += VR_THREADS) {
         const int i = idx % K, j = idx / K;
-        t.R[i + (size_t)j * K] = i <= j ? Rt[i + j * KM] * dsc[j] : 0.0;
+        t.R[i + (size_t)j * K] = i <= j ? Rt[i + j * KM] / dsc[j] : 0.0;
     }
 }
 
@@ -267,12 +285,17 @@ void launch_vr(const VRTask *d_tasks, int ntasks, int *fail, cudaStream_t st) {
 
 }  // namespace
 
-int vside_r_kmax() { return 64; }
+int vside_r_kmax() { return 48; }
+
+int vside_r_bucket(int K) { return K <= 16 ? 16 : K <= 32 ? 32 : 48; }
 
 void launch_vside_r_batched(const VRTask *d_tasks, int ntasks, int kmax, int *fail, cudaStream_t st) {
     if (ntasks <= 0) return;
-    if (kmax <= 32) launch_vr<32>(d_tasks, ntasks, fail, st);
-    else launch_vr<64>(d_tasks, ntasks, fail, st);
+    switch (vside_r_bucket(kmax)) {
+        case 16: launch_vr<16>(d_tasks, ntasks, fail, st); break;
+        case 32: launch_vr<32>(d_tasks, ntasks, fail, st); break;
+        default: launch_vr<48>(d_tasks, ntasks, fail, st); break;
+    }
 }
 
 }  // namespace tlr

@@ -508,20 +508,33 @@ int run_vside_r(hicma_tlr_ctx *c, std::vector<VRTask> &v, int kmax) {
         BC(t.R, bc_span(t.K, t.K, t.K), "cholqr R", i);
     }
 #endif
-    VRTask *d = stage(c, v.data(), v.size());
-    if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
-    double fl = 0, by = 0;
-    for (auto &t : v) {
-        // three Gram products (K^2 nb each, symmetric) and two row substitutions (K^2 nb / 2 FMAs)
-        fl += 3.0 * t.nb * (double)t.K * t.K + 2.0 * t.nb * (double)t.K * t.K;
-        by += 8.0 * t.nb * (double)t.K * 4.0;   // X read twice, scratch written once and read once
-    }
-    {
-        Prof pf(c, P_VR, fl, by);
-        launch_vside_r_batched(d, (int)v.size(), kmax, c->d_flags + 5, c->cur);
+    (void)kmax;
+    // one launch per width bucket (the kernel is instantiated per bucket)
+    std::vector<VRTask> b;
+    int lo = 0;
+    while (lo < vside_r_kmax()) {
+        const int hi = vside_r_bucket(lo + 1);
+        b.clear();
+        for (auto &t : v)
+            if (t.K > lo && t.K <= hi) b.push_back(t);
+        lo = hi;
+        if (b.empty()) continue;
+        VRTask *d = stage(c, b.data(), b.size());
+        if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+        double fl = 0, by = 0;
+        for (auto &t : b) {
+            // three Gram products (K^2 nb each, symmetric) and two row substitutions (K^2 nb / 2 FMAs)
+            fl += 3.0 * t.nb * (double)t.K * t.K + 2.0 * t.nb * (double)t.K * t.K;
+            by += 8.0 * t.nb * (double)t.K * 4.0;   // X read twice, scratch written once and read once
+        }
+        {
+            Prof pf(c, P_VR, fl, by);
+            launch_vside_r_batched(d, (int)b.size(), hi, c->d_flags + 5, c->cur);
+        }
+        TRY(check_launch(c));
     }
     v.clear();
-    return check_launch(c);
+    return 0;
 }
 
 int run_qapply(hicma_tlr_ctx *c, std::vector<QApplyTask> &v, int m_max) {

@@ -220,6 +220,7 @@ struct VRTask {
     int nb, K, ldx;
 };
 int vside_r_kmax();
+int vside_r_bucket(int K);   // width of the kernel instance that takes K
 void launch_vside_r_batched(const VRTask *d_tasks, int ntasks, int kmax, int *fail, cudaStream_t st);
 
 // ------------------------------------------------------------- core SVD -----

@@ -1,8 +1,11 @@
-"""Scaled twins of the full-size workloads, fully checked at N = 27,000
-(10 x 10 tiles of 2700), where an N x N matrix fits on the device and the CPU
-oracle can replay the factorization: the same kernel, tile size, accuracy and
-maxrank as the N = 270,000 2D squared-exponential, the N = 108,000 3D
-exponential and the N = 216,000 3D squared-exponential workloads.
+"""Twins of the full-size workloads, fully checked at N = 27,000 (10 x 10
+tiles of 2700), where an N x N matrix fits on the device and the CPU oracle
+can replay the factorization: the leading 10 x 10 tiles of the N = 270,000 2D
+squared-exponential, the N = 108,000 3D exponential and the N = 216,000 3D
+squared-exponential matrices (the first 27,000 of their Morton-ordered
+points), so every tile is one of the full-size matrix's own tiles, with its
+kernel, tile size, accuracy and maxrank; the twin's Cholesky factor is the
+leading block of the full factor.
 
 Bars, per twin:
 - ||A - L L^T||_F / ||A||_F <= 10 e against the exact covariance (the
@@ -35,28 +38,31 @@ torch = pytest.importorskip("torch")
 
 N, NB = 27000, 2700
 
-# kind 2: 2D sqexp, kind 4: 3D exp, kind 3: 3D sqexp.  logdet_e8: the bound met
-# at e = 1e-8 (measured on a B200: 2D 7.6e-8, the oracle's own error on the same
-# tiles to the digits shown; 3D exp below 1e-15); e_strict: the accuracy at which
-# the 2D twin meets the 1e-8 bar (7.9e-10 measured at e = 1e-9).  The 3D sqexp twin
-# is generated at band 4: at N = 27,000 its tiles are eight times the volume of the
-# N = 216,000 workload's and the ones within distance 3 of the diagonal exceed
-# maxrank 500 (at N = 216,000 every off-band tile compresses at band 1).
+# kind 2: 2D sqexp, kind 4: 3D exp, kind 3: 3D sqexp; n_full: the workload
+# whose leading tiles the twin takes.  logdet_e8: the log-determinant bound met
+# at e = 1e-8, and e_strict (when set): the accuracy at which the twin meets the
+# 1e-8 bar (both measured on a B200 and recorded beside the full-size results).
 TWINS = {
-    "2D sqexp, maxrank 150": dict(kind=2, maxrank=150, band0=1, autoband=False, oracle_ranks=True,
+    "2D sqexp, maxrank 150": dict(kind=2, n_full=270000, maxrank=150, autoband=False, oracle_ranks=True,
                                   logdet_e8=1.5e-7, e_strict=1e-9),
-    "3D exp, maxrank 1350, auto band": dict(kind=4, maxrank=1350, band0=1, autoband=True, oracle_ranks=False,
-                                            logdet_e8=1e-8, e_strict=None),
-    "3D sqexp, maxrank 500, auto band": dict(kind=3, maxrank=500, band0=4, autoband=True, oracle_ranks=True,
-                                             logdet_e8=1e-8, e_strict=None),
+    "3D exp, maxrank 1350, auto band": dict(kind=4, n_full=108000, maxrank=1350, autoband=True,
+                                            oracle_ranks=False, logdet_e8=1e-8, e_strict=None),
+    "3D sqexp, maxrank 500, auto band": dict(kind=3, n_full=216000, maxrank=500, autoband=True,
+                                             oracle_ranks=True, logdet_e8=1e-8, e_strict=None),
 }
 
 
-def _dense_logdet(tlr, prob, n):
-    """2 sum log diag chol(A) of the exact covariance, built on the device
-    by the library's covariance kernel and factored by cuSOLVER."""
+def twin_points(tlr, prob, cfg):
+    """The first N Morton-ordered points of the full-size workload."""
+    return np.ascontiguousarray(tlr.points(prob, cfg["n_full"])[:, :N])
+
+
+def _dense_logdet(tlr, prob, n, points):
+    """2 sum log diag chol(A) of the exact covariance at the given points,
+    built on the device by the library's covariance kernel and factored by
+    cuSOLVER."""
     lib = tlr.load_library()
-    pts = torch.from_numpy(np.ascontiguousarray(tlr.points(prob, n))).cuda()
+    pts = torch.from_numpy(np.ascontiguousarray(points)).cuda()
     A = torch.empty((n, n), dtype=torch.float64, device="cuda")   # row-major view = column-major A^T = A
     cp = prob.c()
     torch.cuda.synchronize()
@@ -84,12 +90,12 @@ def _snapshot(A, nt, band, maxrank):
     return T
 
 
-def _factor(tlr, ctx, prob, cfg, acc, want_snapshot):
-    A = tlr.TLRMatrix(ctx, N, NB, cfg["maxrank"], cfg["band0"])
-    assert A.generate(prob, acc, cfg["maxrank"]) == 0
+def _factor(tlr, ctx, prob, cfg, acc, want_snapshot, pts):
+    A = tlr.TLRMatrix(ctx, N, NB, cfg["maxrank"], 1)
+    assert A.generate(prob, acc, cfg["maxrank"], pts=pts) == 0
     if cfg["autoband"]:
         b = tlr.parsec_band_size_auto_tuning(A.rank_map(), N // NB, NB)
-        if b > A.band_size:
+        if b > 1:
             A.band_regenerate(prob, b)
     T = _snapshot(A, N // NB, A.band_size, cfg["maxrank"]) if want_snapshot else None
     assert A.potrf(acc, cfg["maxrank"]) == 0
@@ -102,11 +108,12 @@ def test_scaled_twin(name):
     cfg = TWINS[name]
     acc = 1e-8
     prob = tlr.Problem(kind=cfg["kind"], noise=1e-4, beta=0.1, sigma=1.0, seed=0)
-    ld_dense = _dense_logdet(tlr, prob, N)
+    pts = twin_points(tlr, prob, cfg)
+    ld_dense = _dense_logdet(tlr, prob, N, pts)
     ctx = tlr.Context(0, 16 << 30)
     A = None
     try:
-        A, T = _factor(tlr, ctx, prob, cfg, acc, cfg["oracle_ranks"])
+        A, T = _factor(tlr, ctx, prob, cfg, acc, cfg["oracle_ranks"], pts)
         res, _ = A.check(prob)
         assert res <= 10 * acc, res
         est = A.check_probe(prob, 16, 0)
@@ -124,7 +131,7 @@ def test_scaled_twin(name):
         A = None
         if cfg["e_strict"]:
             # the accuracy at which the log-determinant meets the 1e-8 bar
-            A, _ = _factor(tlr, ctx, prob, cfg, cfg["e_strict"], False)
+            A, _ = _factor(tlr, ctx, prob, cfg, cfg["e_strict"], False, pts)
             err = abs(A.logdet() - ld_dense) / abs(ld_dense)
             assert err <= 1e-8, (err, cfg["e_strict"])
     finally:
