@@ -2020,6 +2020,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     // reference's op_path, HiCMA_dpotrf_L_2flow.jdf:201,303-313,443-462)
     unsigned long op_path = 0;
     double jac_fl = 0.0, jac_n = 0.0;   // Jacobi flops per sweep summed over the cores, and their number
+    long long khist[16] = {0};          // recompressions by stacked rank K = rc + ra, in steps of 16 (verbose > 2)
     double t_last = 0.0;   // wall time of the previous panel's end (verbose > 1)
     auto log_op = [&](unsigned long cnt, int i, int j, bool path = false) {
         tops[(size_t)i * NT + j] += cnt;
@@ -2221,6 +2222,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         for (size_t i = 0; i < rec.size(); ++i) {
             const auto &mt = rec_meta[i];
             const int rn = A->rank(mt[0], mt[1]);
+            ++khist[std::min(15, (mt[2] + mt[4]) / 16)];
             log_op(gemm_lr_ops(NB, mt[2], mt[3], mt[4], rn, rec_case[i] == 1), mt[0], mt[1]);
             if (c->prof) {
                 // algorithmic flops of the kernels whose work depends on the new
@@ -2253,6 +2255,11 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                     k + 1 < NT ? elapsed(ev[P0], ev[P1]) * 1e3 : 0.0, rec.size());
             t_last = now;
         }
+    }
+    if (verbose > 2) {
+        fprintf(stderr, "recompressions by stacked rank K (bins of 16):");
+        for (int i = 0; i < 16; ++i) fprintf(stderr, " %lld", khist[i]);
+        fprintf(stderr, "\n");
     }
     for (auto &e : ev) cudaEventDestroy(e);
     cudaEventDestroy(evP);

@@ -9,6 +9,7 @@ log-determinant relative error <= 1e-8, per-tile ranks within +/-2 of the
 oracle's TLR run.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -181,31 +182,42 @@ def test_probe_residual_matches_dense_check(ctx):
     assert 0.5 * exact <= est <= 2.0 * exact, (est, exact)
 
 
-def test_vside_cholqr_matches_householder(monkeypatch):
-    """The V-side R factor by shifted CholeskyQR3 (default for stacked ranks up
-    to 64) against the Householder QR path (HICMA_TLR_VSIDE=qr): same final
-    ranks within 1, both residuals within the bar, log-determinants equal to
-    1e-10, and no CholeskyQR breakdown."""
-    from hicma_parsec_b200 import tlr
+@pytest.mark.parametrize("var,alt", [("HICMA_TLR_VSIDE", "qr"), ("HICMA_TLR_CORE", "block")])
+def test_kernel_variants_agree(monkeypatch, var, alt):
+    """The default kernels against their alternatives on the reference's own
+    case: the V-side R factor by shifted CholeskyQR3 (stacked ranks up to 48)
+    against the Householder QR (HICMA_TLR_VSIDE=qr), and the warp-per-core
+    Jacobi SVD (stacked ranks up to 32) against the CTA kernels
+    (HICMA_TLR_CORE=block; its setting is read once per process, so this case
+    runs in a child process).  Same final ranks within 1, both residuals
+    within the bar, log-determinants equal to 1e-10, no CholeskyQR breakdown."""
+    import json
+    import subprocess
+    import sys
+    code = (
+        "import json, sys\n"
+        "sys.path.insert(0, %r)\n"
+        "from hicma_parsec_b200 import tlr\n"
+        "from oracle import tlr_oracle as O\n"
+        "with tlr.Context(0, 1 << 30) as c:\n"
+        "    A = tlr.TLRMatrix(c, %d, %d, %d, 1)\n"
+        "    assert A.generate(tlr.Problem(kind=2, noise=1e-4), %r, %d) == 0\n"
+        "    assert A.potrf(%r, %d) == 0\n"
+        "    res = O.check_dpotrf2(A.uncompress(), O.dense_matrix(O.Problem(kind=2, noise=1e-4), O.gen_points(%d, 2)))\n"
+        "    print(json.dumps({'G': A.rank_map().tolist(), 'ld': A.logdet(), 'res': res, 'brk': float(A.stats()[11])}))\n"
+    ) % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))), N, NB, MAXRANK, TOL, MAXRANK, TOL, MAXRANK, N)
     out = {}
-    for mode in ("qr", "cholqr"):
-        if mode == "qr":
-            monkeypatch.setenv("HICMA_TLR_VSIDE", "qr")
-        else:
-            monkeypatch.delenv("HICMA_TLR_VSIDE", raising=False)
-        with tlr.Context(0, 1 << 30) as c:
-            prob = tlr.Problem(kind=2, noise=1e-4)
-            A = tlr.TLRMatrix(c, N, NB, MAXRANK, 1)
-            assert A.generate(prob, TOL, MAXRANK) == 0
-            assert A.potrf(TOL, MAXRANK) == 0
-            st = A.stats()
-            prof = None
-            out[mode] = (A.rank_map(), A.logdet(), O.check_dpotrf2(A.uncompress(), O.dense_matrix(
-                O.Problem(kind=2, noise=1e-4), O.gen_points(N, 2))), st[11])
-            A.close()
-    (Gq, ldq, rq, _), (Gc, ldc, rc, brk) = out["qr"], out["cholqr"]
-    off = Gq >= 0
-    assert np.max(np.abs(Gq[off] - Gc[off])) <= 1
-    assert rq <= 10 * TOL and rc <= 10 * TOL
-    assert abs(ldq - ldc) <= 1e-10 * abs(ldq)
-    assert brk == 0
+    for mode in ("default", "alt"):
+        env = dict(os.environ)
+        env.pop(var, None)
+        if mode == "alt":
+            env[var] = alt
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[mode] = json.loads(r.stdout.strip().splitlines()[-1])
+    Gd, Ga = np.array(out["default"]["G"]), np.array(out["alt"]["G"])
+    off = Gd >= 0
+    assert np.max(np.abs(Gd[off] - Ga[off])) <= 1
+    assert out["default"]["res"] <= 10 * TOL and out["alt"]["res"] <= 10 * TOL
+    assert abs(out["default"]["ld"] - out["alt"]["ld"]) <= 1e-10 * abs(out["alt"]["ld"])
+    assert out["default"]["brk"] == 0 and out["alt"]["brk"] == 0

@@ -41,14 +41,17 @@ N, NB = 27000, 2700
 # kind 2: 2D sqexp, kind 4: 3D exp, kind 3: 3D sqexp; n_full: the workload
 # whose leading tiles the twin takes.  logdet_e8: the log-determinant bound met
 # at e = 1e-8, and e_strict (when set): the accuracy at which the twin meets the
-# 1e-8 bar (both measured on a B200 and recorded beside the full-size results).
+# 1e-8 bar.  Measured on a B200: 2D 1.15e-6 at e = 1e-8, 1.1e-8 at 1e-9, 1.0e-10
+# at 1e-10; 3D exponential below 1e-15 at every e; 3D squared exponential
+# 1.55e-7 at 1e-8, 1.0e-9 at 1e-9.  The oracle replaying the same tiles has the
+# same error to the digits shown: it is the truncation error of the algorithm.
 TWINS = {
     "2D sqexp, maxrank 150": dict(kind=2, n_full=270000, maxrank=150, autoband=False, oracle_ranks=True,
-                                  logdet_e8=1.5e-7, e_strict=1e-9),
+                                  logdet_e8=1.5e-6, e_strict=1e-10),
     "3D exp, maxrank 1350, auto band": dict(kind=4, n_full=108000, maxrank=1350, autoband=True,
                                             oracle_ranks=False, logdet_e8=1e-8, e_strict=None),
     "3D sqexp, maxrank 500, auto band": dict(kind=3, n_full=216000, maxrank=500, autoband=True,
-                                             oracle_ranks=True, logdet_e8=1e-8, e_strict=None),
+                                             oracle_ranks=True, logdet_e8=2e-7, e_strict=1e-9),
 }
 
 
@@ -118,7 +121,8 @@ def test_scaled_twin(name):
         assert res <= 10 * acc, res
         est = A.check_probe(prob, 16, 0)
         assert 0.5 * res <= est <= 2.0 * res, (res, est)
-        err = abs(A.logdet() - ld_dense) / abs(ld_dense)
+        ld = A.logdet()
+        err = abs(ld - ld_dense) / abs(ld_dense)
         assert err <= cfg["logdet_e8"], (err, cfg["logdet_e8"])
         if T is not None:
             G = A.rank_map()
@@ -127,6 +131,8 @@ def test_scaled_twin(name):
             off = Gref >= 0
             assert np.array_equal(G >= 0, off)
             assert np.max(np.abs(G[off] - Gref[off])) <= 2, np.max(np.abs(G[off] - Gref[off]))
+            # the device factor's log-determinant is the oracle's on the same tiles
+            assert abs(ld - O.logdet(T)) <= 1e-9 * abs(ld_dense)
         A.close()
         A = None
         if cfg["e_strict"]:
