@@ -1,17 +1,21 @@
-// R factor of a tall-skinny matrix by shifted CholeskyQR3, one CTA per
-// matrix, FP64 (Gram products on the FP64 tensor cores).
+// QR factorization of a tall-skinny matrix by shifted CholeskyQR3, one CTA
+// per matrix, FP64 (Gram products on the FP64 tensor cores).
 //
-// Replaces the V-side QR of HCORE_dgemm_qr_svd (call sites
-// hicma_parsec/HiCMA_dpotrf_L_2flow.jdf:830-903,985-1058): only R_V of
-// [Cv, -Y] = Q_V R_V is needed there (the new V is formed as
-// [Cv, -Y] R_U^T U_r), so no Q is kept.
+// Replaces both QRs of HCORE_dgemm_qr_svd (call sites
+// hicma_parsec/HiCMA_dpotrf_L_2flow.jdf:830-903,985-1058): the U side
+// [Cu, Au] = Q_U R_U with Q_U formed (the new U is Q_U U_r, which replaces
+// the Householder Q application of HCORE_dgemm_ormqr), and the V side
+// [Cv, -Y] = Q_V R_V with R only (the new V is [Cv, -Y] R_U^T U_r).  The
+// matrix is given as two column blocks read where they lie, so [Cu, Au] is
+// never copied.
 //
 // Algorithm (Fukaya, Kannan, Nakatsukasa, Yamamoto, Yanagisawa, "Shifted
 // Cholesky QR for computing the QR factorization of ill-conditioned
 // matrices", SIAM J. Sci. Comput. 42(1), 2020): with D the column norms,
 //   pass 0: G = D^-1 X^T X D^-1 + s I,  R1 = chol(G)
 //   pass 1: X1 = X D^-1 R1^-1 (written to scratch), G = X1^T X1, R2 = chol(G)
-//   pass 2: X2 = X1 R2^-1 (not stored),             G = X2^T X2, R3 = chol(G)
+//   pass 2: X2 = X1 R2^-1 (stored when Q is wanted), G = X2^T X2, R3 = chol(G)
+//   pass 3: Q = X2 R3^-1 (only when Q is wanted)
 //   R = R3 R2 R1 D,
 // s = 11 (m K + K (K + 1)) u tr(G); passes 1 and 2 add the same shift only if
 // the plain Cholesky breaks down.  X R^-1 is a row-wise substitution (the
@@ -115,23 +119,31 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
     double *rdg = dsc + KM;                        // 1 / diag(R)
 
     const VRTask t = tasks[blockIdx.x];
-    const int K = t.K, nb = t.nb, ldx = t.ldx;
+    const int k1 = t.k1, K = t.k1 + t.k2, nb = t.nb;
     if (K <= 0) return;
     const double u = 1.1102230246251565e-16;
+    const int npass = t.Q ? 4 : 3;
 
-    for (int pass = 0; pass < 3; ++pass) {
+    for (int pass = 0; pass < npass; ++pass) {
         double acc[NTILE][2];
 #pragma unroll
         for (int q = 0; q < NTILE; ++q) acc[q][0] = acc[q][1] = 0.0;
-        const double *src = pass == 2 ? t.Z : t.X;
-        const int lds = pass == 2 ? nb : ldx;
+        const bool gram = pass < 3;
 
         for (int r0 = warp * 32; r0 < nb; r0 += VR_THREADS) {
             const int row = r0 + lane;
             const bool valid = row < nb;
             double x[KM];
+            if (pass < 2) {
 #pragma unroll
-            for (int j = 0; j < KM; ++j) x[j] = (valid && j < K) ? src[(size_t)row + (size_t)j * lds] : 0.0;
+                for (int j = 0; j < KM; ++j) {
+                    const double *p = j < k1 ? t.X1 + (size_t)j * t.ld1 : t.X2 + (size_t)(j - k1) * t.ld2;
+                    x[j] = (valid && j < K) ? p[row] : 0.0;
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < KM; ++j) x[j] = (valid && j < K) ? t.Z[(size_t)row + (size_t)j * nb] : 0.0;
+            }
             if (pass > 0) {
                 if (pass == 1) {
 #pragma unroll
@@ -140,12 +152,16 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
                 // x <- x R^-1 (right-looking row substitution; R and 1/diag are
                 // zero past K, so the padding columns stay zero)
                 subst_rows<KM, 0>(x, Rr, rdg);
-                if (pass == 1 && valid) {
+                // pass 1 stores X1, pass 2 X2 (when Q is wanted), pass 3 Q: each
+                // lane rewrites only the row it read
+                double *dst = pass == 3 ? t.Q : t.Z;
+                if (valid && (pass == 1 || pass == 3 || (pass == 2 && t.Q))) {
 #pragma unroll
                     for (int j = 0; j < KM; ++j)
-                        if (j < K) t.Z[(size_t)row + (size_t)j * nb] = x[j];
+                        if (j < K) dst[(size_t)row + (size_t)j * nb] = x[j];
                 }
             }
+            if (!gram) continue;
 #pragma unroll
             for (int j = 0; j < KM; ++j) Zw[j * VR_PITCH + lane] = x[j];
             __syncwarp();
@@ -163,6 +179,7 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
             }
             __syncwarp();
         }
+        if (!gram) break;
         // per-warp partials -> G in warp order (both triangles)
         for (int idx = tid; idx < KM * KM; idx += VR_THREADS) G[idx] = 0.0;
         __syncthreads();

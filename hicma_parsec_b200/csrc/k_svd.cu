@@ -29,8 +29,6 @@
 #include "tlr_internal.h"
 
 #include <cooperative_groups.h>
-#include <cstdlib>
-#include <cstring>
 
 namespace tlr {
 namespace {
@@ -628,164 +626,6 @@ __global__ void __launch_bounds__(CL_CT) k_core_svd_cl(const CoreTask *__restric
     }
 }
 
-// Small cores (K <= 32, absolute truncation): one warp per core, eight cores
-// per CTA, no CTA barrier.  Lane c holds column c of T = M^T (M = R_U R_V^T)
-// and column c of the accumulated rotation J, both in registers; one-sided
-// Jacobi with the round-robin tournament ordering rotates all K/2 pairs of a
-// round at once, each lane fetching its partner's columns with shuffles (both
-// lanes of a pair compute the same sums in the same order, hence the same
-// rotation).  At convergence T J = V Sigma, so J holds the left singular
-// vectors of M exactly (no division by small singular values), sorted by
-// decreasing sigma on the way out.
-constexpr int CW = 32;              // columns per warp core
-
-// HICMA_TLR_CORE=block sends every core to the CTA kernels (for comparisons).
-bool core_warp_enabled() {
-    static const bool on = [] {
-        const char *v = std::getenv("HICMA_TLR_CORE");
-        return !(v && std::strcmp(v, "block") == 0);
-    }();
-    return on;
-}
-constexpr int CW_WARPS = 8;
-constexpr int CW_PITCH = CW + 1;
-
-__device__ __forceinline__ int tourney_partner(int c, int round, int Kp) {
-    // slot of c in this round, then the slot paired with it
-    if (c >= Kp) return c;
-    int slot;
-    if (c == 0) slot = 0;
-    else slot = 1 + ((c - 1 - round) % (Kp - 1) + (Kp - 1)) % (Kp - 1);
-    const int ps = Kp - 1 - slot;
-    return ps == 0 ? 0 : 1 + ((ps - 1 + round) % (Kp - 1));
-}
-
-__global__ void __launch_bounds__(CW_WARPS * 32) k_core_warp(const CoreTask *__restrict__ tasks, int ntasks,
-                                                              CoreParams p) {
-    extern __shared__ double rvs_dyn[];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ti = blockIdx.x * CW_WARPS + warp;
-    if (ti >= ntasks) return;
-    const CoreTask t = tasks[ti];
-    const int K = t.K;
-    if (K <= 0) {
-        if (lane == 0) {
-            if (t.rank_out) *t.rank_out = 0;
-            if (t.rank_task) *t.rank_task = 0;
-        }
-        return;
-    }
-    const int c = lane;
-    double *R = rvs_dyn + (size_t)warp * CW * CW_PITCH;
-    // R_V (upper, zero below the diagonal and past K) into shared memory: R[i * pitch + l] = RV(i, l)
-    for (int idx = lane; idx < CW * CW; idx += 32) {
-        const int i = idx % CW, l = idx / CW;
-        R[i * CW_PITCH + l] = (i <= l && l < K) ? t.RV[(size_t)i + (size_t)l * t.ldrv] : 0.0;
-    }
-    __syncwarp();
-    // column c of T = M^T: T(i, c) = M(c, i) = sum_l RU(c, l) RV(i, l)  (RU null: T = R_V)
-    double x[CW], jv[CW];
-    if (t.RU) {
-        double ru[CW];
-#pragma unroll
-        for (int l = 0; l < CW; ++l) ru[l] = (c < K && l >= c && l < K) ? t.RU[(size_t)c + (size_t)l * t.ldru] : 0.0;
-#pragma unroll
-        for (int i = 0; i < CW; ++i) {
-            double s = 0.0;
-#pragma unroll
-            for (int l = 0; l < CW; ++l) s += ru[l] * R[i * CW_PITCH + l];
-            x[i] = s;
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < CW; ++i) x[i] = c < K ? R[i * CW_PITCH + c] : 0.0;
-    }
-#pragma unroll
-    for (int i = 0; i < CW; ++i) jv[i] = (i == c && c < K) ? 1.0 : 0.0;
-
-    const double tau = (p.fixed_rank <= 0) ? 1e-3 * p.tol : 0.0;
-    const double tau2 = tau * tau;
-    const double tolj = 4.4e-16 * (double)(K > 16 ? K : 16);
-    const int Kp = K + (K & 1);
-    int sweeps = 0;
-    if (K > 1) {
-        for (int sweep = 0; sweep < MAX_SWEEPS; ++sweep) {
-            ++sweeps;
-            bool rot = false;
-            for (int round = 0; round < Kp - 1; ++round) {
-                const int pc = tourney_partner(c, round, Kp);
-                double xp[CW];
-                double aa = 0.0, bb = 0.0, cc = 0.0;
-#pragma unroll
-                for (int i = 0; i < CW; ++i) {
-                    xp[i] = __shfl_sync(0xffffffffu, x[i], pc);
-                    aa += x[i] * x[i];
-                    bb += xp[i] * xp[i];
-                    cc += x[i] * xp[i];
-                }
-                const bool lo = c < pc;
-                const double na = lo ? aa : bb, nbv = lo ? bb : aa;
-                bool doit = pc != c && c < K && pc < K && cc != 0.0 && na > tau2 && nbv > tau2 && na >= 1e-290 &&
-                            nbv >= 1e-290 && fabs(cc) > tolj * sqrt(na) * sqrt(nbv);
-                double cs = 1.0, sn = 0.0;
-                if (doit) {
-                    const double zeta = (nbv - na) / (2.0 * cc);
-                    double tt;
-                    if (fabs(zeta) > 1e150) tt = 0.5 / zeta;
-                    else tt = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                    cs = 1.0 / sqrt(1.0 + tt * tt);
-                    sn = cs * tt;
-                    rot = true;
-                }
-                // both lanes of a pair: (a, b) <- (cs a - sn b, sn a + cs b), a the lower column
-#pragma unroll
-                for (int i = 0; i < CW; ++i) {
-                    const double jp = __shfl_sync(0xffffffffu, jv[i], pc);
-                    if (doit) {
-                        if (lo) {
-                            x[i] = cs * x[i] - sn * xp[i];
-                            jv[i] = cs * jv[i] - sn * jp;
-                        } else {
-                            x[i] = sn * xp[i] + cs * x[i];
-                            jv[i] = sn * jp + cs * jv[i];
-                        }
-                    }
-                }
-            }
-            if (!__any_sync(0xffffffffu, rot)) break;
-        }
-    }
-    // singular values, descending order, rank
-    double sg = 0.0;
-#pragma unroll
-    for (int i = 0; i < CW; ++i) sg += x[i] * x[i];
-    sg = c < K ? sqrt(sg) : -1.0;
-    int pos = 0, nge = 0;
-    for (int l = 0; l < K; ++l) {
-        const double sl = __shfl_sync(0xffffffffu, sg, l);
-        pos += (sl > sg) || (sl == sg && l < c);
-        nge += sl >= p.tol;
-    }
-    int r;
-    if (p.fixed_rank > 0) r = p.fixed_rank < K ? p.fixed_rank : K;
-    else r = nge;
-    if (r > p.maxrank) {
-        r = p.maxrank;
-        if (lane == 0 && p.overflow) atomicAdd(p.overflow, 1);
-    }
-    if (lane == 0) {
-        if (t.rank_out) *t.rank_out = r;
-        if (t.rank_task) *t.rank_task = r;
-        if (p.sweeps) atomicAdd(p.sweeps, sweeps);
-    }
-    if (c < K) {
-        double *dst = t.SU + (size_t)pos * K;
-#pragma unroll
-        for (int i = 0; i < CW; ++i)
-            if (i < K) dst[i] = jv[i];
-    }
-}
-
 template <int LP, int CT>
 void launch_lp(const CoreTask *d, int n, size_t smem, const CoreParams &p, cudaStream_t st) {
     cudaFuncSetAttribute(k_core_svd<LP, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -802,13 +642,6 @@ void launch_core_svd_batched(const CoreTask *d_tasks, int ntasks, int kmax, cons
                              cudaStream_t st) {
     if (ntasks <= 0) return;
     if (kmax < 1) kmax = 1;
-    if (kmax <= CW && p.mode == 0 && core_warp_enabled()) {
-        const int smw = (int)(sizeof(double) * CW_WARPS * CW * CW_PITCH);
-        // per device and thread-safe: set on every launch (a host-side call, no synchronisation)
-        cudaFuncSetAttribute(k_core_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, smw);
-        k_core_warp<<<(ntasks + CW_WARPS - 1) / CW_WARPS, CW_WARPS * 32, smw, st>>>(d_tasks, ntasks, p);
-        return;
-    }
     size_t smem;
     // W (K x K, on chip when small), partial norms / sigma, Householder vector,
     // order and pivot

@@ -141,8 +141,8 @@ struct hicma_tlr_ctx_s {
     // choices the autotuner measures (defaults: the hand-picked values)
     int gemm_narrow_n = GEMM_NARROW_N;   // rank-wide outputs up to this width use 128 x 32 tiles
     int potrf_grid = 0;                  // CTAs of the persistent tile POTRF (0: one per SM)
-    // V-side R factor of the recompressions: shifted CholeskyQR3 for stacked
-    // ranks up to vside_r_kmax() (1), Householder QR for all (0; HICMA_TLR_VSIDE=qr)
+    // QRs of the recompressions: shifted CholeskyQR3 on both sides for stacked
+    // ranks up to vside_r_kmax() (1), the Householder pipeline for all (0; HICMA_TLR_VSIDE=qr)
     int vside_cholqr = 1;
     double *d_scal = nullptr;   // device scalars
     int precision = HICMA_TLR_PREC_FP64;
@@ -503,9 +503,12 @@ int run_vside_r(hicma_tlr_ctx *c, std::vector<VRTask> &v, int kmax) {
 #ifdef TLR_BOUNDS_CHECK
     for (size_t i = 0; i < v.size(); ++i) {
         const VRTask &t = v[i];
-        BC(t.X, bc_span(t.nb, t.K, t.ldx), "cholqr X", i);
-        BC(t.Z, bc_span(t.nb, t.K, t.nb), "cholqr scratch", i);
-        BC(t.R, bc_span(t.K, t.K, t.K), "cholqr R", i);
+        const int K = t.k1 + t.k2;
+        if (t.k1) BC(t.X1, bc_span(t.nb, t.k1, t.ld1), "cholqr X1", i);
+        if (t.k2) BC(t.X2, bc_span(t.nb, t.k2, t.ld2), "cholqr X2", i);
+        BC(t.Z, bc_span(t.nb, K, t.nb), "cholqr scratch", i);
+        BC(t.R, bc_span(K, K, K), "cholqr R", i);
+        if (t.Q) BC(t.Q, bc_span(t.nb, K, t.nb), "cholqr Q", i);
     }
 #endif
     (void)kmax;
@@ -516,16 +519,19 @@ int run_vside_r(hicma_tlr_ctx *c, std::vector<VRTask> &v, int kmax) {
         const int hi = vside_r_bucket(lo + 1);
         b.clear();
         for (auto &t : v)
-            if (t.K > lo && t.K <= hi) b.push_back(t);
+            if (t.k1 + t.k2 > lo && t.k1 + t.k2 <= hi) b.push_back(t);
         lo = hi;
         if (b.empty()) continue;
         VRTask *d = stage(c, b.data(), b.size());
         if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
         double fl = 0, by = 0;
         for (auto &t : b) {
-            // three Gram products (K^2 nb each, symmetric) and two row substitutions (K^2 nb / 2 FMAs)
-            fl += 3.0 * t.nb * (double)t.K * t.K + 2.0 * t.nb * (double)t.K * t.K;
-            by += 8.0 * t.nb * (double)t.K * 4.0;   // X read twice, scratch written once and read once
+            // three Gram products (K^2 nb each, symmetric) and two row substitutions (K^2 nb / 2
+            // FMAs each), a third substitution when Q is formed
+            const double K = t.k1 + t.k2;
+            fl += 3.0 * t.nb * K * K + (t.Q ? 3.0 : 2.0) * t.nb * K * K;
+            // X read twice, scratch written and read once (Q: X2 and Q written, X2 read)
+            by += 8.0 * t.nb * K * (t.Q ? 7.0 : 4.0);
         }
         {
             Prof pf(c, P_VR, fl, by);
@@ -796,7 +802,6 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
         int *sel = thr2 > 0.0 ? ws_alloc<int>(c, 2 * (tasks.size() - i0) + 2) : nullptr;
         std::vector<QRTask> qrs;
         std::vector<VRTask> vrs;
-        int vr_kmax = 0;
         std::vector<AssembleTask> asm_;
         std::vector<CoreTask> cores;
         std::vector<QApplyTask> apps;
@@ -814,25 +819,20 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             ct.rank_task = rank_task + (i - i0);
             ct.K = K;
             if (K == 0) { cores.push_back(ct); continue; }
-            const int pbw = qr_panel_width(nb);
-            const size_t npk = (size_t)(K + pbw - 1) / pbw + 1, npa = (size_t)(ra + pbw - 1) / pbw + 1;
-            double *Us = ws_alloc<double>(c, (size_t)nb * K);
+            // Stacks up to vside_r_kmax() columns: both QRs by shifted CholeskyQR3
+            // (U side [Cu, Au] read in place with Q_U formed, V side R only);
+            // wider stacks: block Gram-Schmidt + Householder on the U side and a
+            // Householder QR on the V side.
+            const bool cq = c->vside_cholqr && K <= vside_r_kmax();
             double *Vs = ws_alloc<double>(c, (size_t)nb * K);
             double *Vk = ws_alloc<double>(c, (size_t)nb * K);
-            double *tauU = ws_alloc<double>(c, ra), *tauV = ws_alloc<double>(c, K);
-            double *TU = ws_alloc<double>(c, npa * pbw * pbw), *TV = ws_alloc<double>(c, npk * pbw * pbw);
-            double *Pu = ws_alloc<double>(c, (size_t)rc * ra), *Pu2 = ws_alloc<double>(c, (size_t)rc * ra);
+            double *Us = ws_alloc<double>(c, (size_t)nb * K);    // CholeskyQR path: scratch and Q_U
             double *RU = ws_alloc<double>(c, (size_t)K * K);
             double *SU = ws_alloc<double>(c, (size_t)K * K), *T1 = ws_alloc<double>(c, (size_t)K * K);
             double *work = K > core_smem_kmax() ? ws_alloc<double>(c, core_work_doubles(K)) : nullptr;
-            double *Wu = Us + (size_t)nb * rc;
             double *Yb = Vs + (size_t)nb * rc;
-            if (rc > 0) {
-                copies.push_back(make_copy(t.Cu, nb, Us, nb, nb, rc));
-                copies.push_back(make_copy(t.Cv, nb, Vs, nb, nb, rc));
-            }
+            if (rc > 0) copies.push_back(make_copy(t.Cv, nb, Vs, nb, nb, rc));
             if (ra > 0) {
-                copies.push_back(make_copy(t.Au, nb, Wu, nb, nb, ra));
                 if (t.Bv) {
                     double *P = ws_alloc<double>(c, (size_t)t.rb * ra);
                     GemmTask a1 = make_gemm(1, 0, t.rb, ra, nb, 1.0, t.Bv, nb, t.Av, nb, 0.0, P, t.rb);
@@ -852,39 +852,45 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                 } else {
                     g1.push_back(make_gemm(0, 0, nb, ra, nb, -1.0, t.Bu, nb, t.Av, nb, 0.0, Yb, nb));
                 }
-                // two rounds of projection of Au against the old orthonormal U
-                if (rc > 0) projs.push_back(ProjTask{Us, Wu, Pu, Pu2, nb, rc, ra});
-                qrs.push_back(QRTask{Wu, tauU, TU, nb, ra, nb});
             }
-            // V side: R only.  Shifted CholeskyQR3 leaves [Cv, -Y] intact (Vk is
-            // its scratch); the Householder QR overwrites it (Vk keeps a copy).
-            const bool vr = c->vside_cholqr && K <= vside_r_kmax();
             double *Vsrc = Vs;
-            if (vr) {
+            if (cq) {
                 double *RV = ws_alloc<double>(c, (size_t)K * K);
-                vrs.push_back(VRTask{Vs, Vk, RV, nb, K, nb});
-                vr_kmax = std::max(vr_kmax, K);
+                vrs.push_back(VRTask{t.Cu, t.Au, Us, RU, Us, nb, rc, ra, nb, nb});
+                vrs.push_back(VRTask{Vs, nullptr, Vk, RV, nullptr, nb, K, 0, nb, nb});
                 ct.RV = RV; ct.ldrv = K;
             } else {
+                const int pbw = qr_panel_width(nb);
+                const size_t npk = (size_t)(K + pbw - 1) / pbw + 1, npa = (size_t)(ra + pbw - 1) / pbw + 1;
+                double *tauU = ws_alloc<double>(c, ra), *tauV = ws_alloc<double>(c, K);
+                double *TU = ws_alloc<double>(c, npa * pbw * pbw), *TV = ws_alloc<double>(c, npk * pbw * pbw);
+                double *Pu = ws_alloc<double>(c, (size_t)rc * ra), *Pu2 = ws_alloc<double>(c, (size_t)rc * ra);
+                double *Wu = Us + (size_t)nb * rc;
+                if (rc > 0) copies.push_back(make_copy(t.Cu, nb, Us, nb, nb, rc));
+                if (ra > 0) {
+                    copies.push_back(make_copy(t.Au, nb, Wu, nb, nb, ra));
+                    // two rounds of projection of Au against the old orthonormal U
+                    if (rc > 0) projs.push_back(ProjTask{Us, Wu, Pu, Pu2, nb, rc, ra});
+                    qrs.push_back(QRTask{Wu, tauU, TU, nb, ra, nb});
+                    apps.push_back(QApplyTask{Wu, TU, SU + rc, t.outU, ct.rank_task, nb, ra, nb, K, nb, maxrank});
+                }
                 keeps.push_back(make_copy(Vs, nb, Vk, nb, nb, K));
                 qrs.push_back(QRTask{Vs, tauV, TV, nb, K, nb});
+                asm_.push_back(AssembleTask{Pu, Wu, RU, rc, ra, nb});
                 ct.RV = Vs; ct.ldrv = nb;
                 Vsrc = Vk;
             }
-            asm_.push_back(AssembleTask{Pu, Wu, RU, rc, ra, nb});
             ct.RU = RU; ct.ldru = K;
             ct.SU = SU; ct.RUc = nullptr; ct.work = work;
             cores.push_back(ct);
-            // new U = Q(Wu) [U_bot; 0] + Cu U_top
-            if (ra > 0) {
-                apps.push_back(QApplyTask{Wu, TU, SU + rc, t.outU, ct.rank_task, nb, ra, nb, K, nb, maxrank});
-                if (rc > 0) {
-                    GemmTask u = make_gemm(0, 0, nb, maxrank, rc, 1.0, Us, nb, SU, K, 1.0, t.outU, nb);
-                    u.n_dev = ct.rank_task;
-                    gU.push_back(u);
-                }
-            } else {
-                GemmTask u = make_gemm(0, 0, nb, maxrank, rc, 1.0, Us, nb, SU, K, 0.0, t.outU, nb);
+            if (cq) {
+                // new U = Q_U U_r
+                GemmTask u = make_gemm(0, 0, nb, maxrank, K, 1.0, Us, nb, SU, K, 0.0, t.outU, nb);
+                u.n_dev = ct.rank_task;
+                gU.push_back(u);
+            } else if (rc > 0) {
+                // new U = Q(Wu) [U_bot; 0] + Cu U_top (beta 1 after the Q application when ra > 0)
+                GemmTask u = make_gemm(0, 0, nb, maxrank, rc, 1.0, Us, nb, SU, K, ra > 0 ? 1.0 : 0.0, t.outU, nb);
                 u.n_dev = ct.rank_task;
                 gU.push_back(u);
             }
@@ -934,7 +940,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             TRY(check_launch(c));
         }
         TRY(run_qr(c, qrs, nb));
-        TRY(run_vside_r(c, vrs, vr_kmax));
+        TRY(run_vside_r(c, vrs, 0));
         if (!asm_.empty()) {
             AssembleTask *d = stage(c, asm_.data(), asm_.size());
             if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }

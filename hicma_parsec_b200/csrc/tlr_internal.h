@@ -209,15 +209,17 @@ struct QApplyTask {
 };
 void launch_qapply_batched(const QApplyTask *d_tasks, int ntasks, int m_max, cudaStream_t st);
 
-// R factor (upper, K x K, ld K) of an nb x K matrix X by shifted CholeskyQR3
-// (one CTA per task; X is read, not changed; Z is nb x K scratch, ld nb).
-// Tasks of one launch have K <= kmax <= vside_r_kmax().  fail counts tasks
+// QR of an nb x K matrix X = [X1 (nb x k1, ld1), X2 (nb x k2, ld2)] by
+// shifted CholeskyQR3 (one CTA per task; X is read, not changed): R (upper,
+// K x K, ld K) and, if Q is set, Q (nb x K, ld nb; may equal Z).  Z is
+// nb x K scratch (ld nb).  K = k1 + k2 <= vside_r_kmax(); fail counts tasks
 // whose Cholesky broke down under every shift (R left as the identity).
 struct VRTask {
-    const double *X;
+    const double *X1, *X2;
     double *Z;
     double *R;
-    int nb, K, ldx;
+    double *Q;
+    int nb, k1, k2, ld1, ld2;
 };
 int vside_r_kmax();
 int vside_r_bucket(int K);   // width of the kernel instance that takes K

@@ -515,6 +515,28 @@ def band_autotune(G: np.ndarray, nt: int, nb: int, verbose: bool = False) -> int
 # --------------------------------------------------------------------------
 # Tile kernels (HCORE / CORE_d* restated)
 # --------------------------------------------------------------------------
+def qr_scholqr3(V: np.ndarray):
+    """(Q, R) of V = Q R by shifted CholeskyQR3 as in :func:`r_factor_scholqr3`,
+    with Q = V D^-1 R_1^-1 R_2^-1 R_3^-1 formed by three row-wise triangular
+    solves.  The device's U side of a recompression: [Cu, Au] = Q_U R_U."""
+    m, K = V.shape
+    d = np.linalg.norm(V, axis=0)
+    d[d == 0.0] = 1.0
+    X = V / d
+    R = np.eye(K)
+    u = np.finfo(np.float64).eps / 2
+    for p in range(3):
+        G = X.T @ X
+        shift = 11.0 * (m * K + K * (K + 1)) * u * float(np.trace(G))
+        try:
+            Rp = np.linalg.cholesky(G + (shift if p == 0 else 0.0) * np.eye(K)).T
+        except np.linalg.LinAlgError:
+            Rp = np.linalg.cholesky(G + shift * np.eye(K)).T
+        X = sla.solve_triangular(Rp, X.T, trans="T", lower=False).T
+        R = Rp @ R
+    return X, R * d
+
+
 def r_factor_scholqr3(V: np.ndarray) -> np.ndarray:
     """R of V = Q R (Q not formed) by shifted CholeskyQR3 (Fukaya, Kannan,
     Nakatsukasa, Yamamoto and Yanagisawa, SIAM J. Sci. Comput. 42(1), 2020):
@@ -542,19 +564,20 @@ def r_factor_scholqr3(V: np.ndarray) -> np.ndarray:
     return R * d
 
 
-def recompress(Cu, Cv, Au, Y, acc, maxrank, fixed_rank=0, v_side="householder"):
+def recompress(Cu, Cv, Au, Y, acc, maxrank, fixed_rank=0, v_side="householder", u_side="householder"):
     """C_new = [Cu, Au] [Cv, -Y]^T recompressed (restated
     ``HCORE_dgemm_qr_svd`` + ``HCORE_dgemm_ormqr``, call sites
     ``HiCMA_dpotrf_L_2flow.jdf:830-903,985-1058``).  Returns
     (U, V, rank, overflow).  ``v_side="scholqr3"`` takes R_V from
     :func:`r_factor_scholqr3` and forms the new V as [Cv, -Y] R_U^T U_r (no
-    Q_V needed), the form the device uses."""
+    Q_V needed), and ``u_side="scholqr3"`` takes Q_U, R_U from
+    :func:`qr_scholqr3`: the form the device uses for stacked ranks up to 48."""
     Us = np.hstack([Cu, Au])
     Vs = np.hstack([Cv, -Y])
     nb, K = Us.shape
     if K == 0:
         return np.zeros((nb, 0)), np.zeros((nb, 0)), 0, False
-    Qu, Ru = np.linalg.qr(Us)
+    Qu, Ru = qr_scholqr3(Us) if u_side == "scholqr3" else np.linalg.qr(Us)
     if v_side == "scholqr3":
         Rv = r_factor_scholqr3(Vs)
     else:
@@ -611,7 +634,7 @@ def potrf_tile(A: np.ndarray):
 
 
 def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool = True,
-              v_side: str = "householder") -> FactorStats:
+              v_side: str = "householder", u_side: str = "householder") -> FactorStats:
     """In-place 2-flow TLR Cholesky (``HiCMA_dpotrf_L_2flow.jdf:175-1113``)
     run in a sequential order compatible with its data flow."""
     nt, nb, band = T.nt, T.nb, T.band
@@ -702,7 +725,7 @@ def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool
                     ra = Au.shape[1]
                     rc_old = T.U[(m, n)].shape[1]
                     Y = T.dense[(n, k)] @ Av
-                    U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank, v_side)
+                    U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank, v_side, u_side)
                     st.overflow += int(ov)
                     T.U[(m, n)], T.V[(m, n)] = U, V
                     track(m, n, r)
@@ -715,7 +738,7 @@ def tlr_potrf(T: TLRMatrix, acc: float, fixed_rank: int = 0, stop_on_error: bool
                         continue
                     rc_old = T.U[(m, n)].shape[1]
                     Y = Bu @ (Bv.T @ Av)
-                    U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank, v_side)
+                    U, V, r, ov = recompress(T.U[(m, n)], T.V[(m, n)], Au, Y, acc, T.maxrank, fixed_rank, v_side, u_side)
                     st.overflow += int(ov)
                     T.U[(m, n)], T.V[(m, n)] = U, V
                     track(m, n, r)

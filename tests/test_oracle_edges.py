@@ -180,6 +180,36 @@ def test_scholqr3_v_side_keeps_ranks_and_accuracy():
     assert np.linalg.norm(R.T @ R - V.T @ V) <= 1e-12 * np.linalg.norm(V.T @ V)
 
 
+def test_scholqr3_both_sides_keeps_ranks_and_accuracy():
+    """The device's form for stacked ranks up to 48: shifted CholeskyQR3 on both
+    sides of every recompression ([Cu, Au] = Q_U R_U with Q_U formed, no
+    Gram-Schmidt projection; R_V only on the V side) gives the Householder
+    oracle's final ranks, residual and log det on the reference's case, and
+    Q_U is orthonormal to working precision even with dependent columns."""
+    prob = O.Problem(kind=2, noise=1e-4)
+    pts = O.gen_points(2700, 2)
+    T0, info = O.generate(prob, 2700, 270, 1e-8, 130, 1, pts)
+    assert info == 0
+    Th, Tc = T0.copy(), T0.copy()
+    assert O.tlr_potrf(Th, 1e-8).info == 0
+    assert O.tlr_potrf(Tc, 1e-8, v_side="scholqr3", u_side="scholqr3").info == 0
+    assert np.array_equal(Th.rank_array(), Tc.rank_array())
+    A = O.dense_matrix(prob, pts)
+    rh, rc = O.check_dpotrf2(O.uncompress(Th), A), O.check_dpotrf2(O.uncompress(Tc), A)
+    assert rc <= 10 * 1e-8 and abs(rc - rh) <= 0.01 * rh
+    assert abs(O.logdet(Tc) - O.logdet(Th)) <= 1e-12 * abs(O.logdet(Th))
+    for (m, n), U in Tc.U.items():
+        r = U.shape[1]
+        if r:
+            assert np.linalg.norm(U.T @ U - np.eye(r)) <= 1e-12
+    rng = np.random.default_rng(3)
+    Q0, _ = np.linalg.qr(rng.standard_normal((500, 20)))
+    V = np.hstack([Q0, Q0[:, :5] @ rng.standard_normal((5, 8)) + 1e-13 * rng.standard_normal((500, 8))])
+    Q, R = O.qr_scholqr3(V)
+    assert np.allclose(np.tril(R, -1), 0.0)
+    assert np.linalg.norm(Q @ R - V) <= 1e-13 * np.linalg.norm(V)
+
+
 @pytest.mark.parametrize("band", [1, 2])
 def test_dag_oracle_matches_sequential_oracle(band):
     """The task-graph run on host threads (the timed CPU baseline) computes the
