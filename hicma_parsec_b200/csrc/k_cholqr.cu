@@ -32,9 +32,9 @@
 // quad, reused by every tile of that block).  The eight per-warp Gram
 // partials are added in warp order at the end of a pass (deterministic), and
 // one warp factors G in shared memory.  Kernels are instantiated per width
-// bucket (KM = 16, 32, 48 columns) so that unrolled loops do not run far past
-// the actual K; the row and the Gram accumulators of the widest bucket fill
-// the register file, so wider stacks take the Householder path.
+// bucket (KM = 16, 32, 48, 64 columns) so that unrolled loops do not run far
+// past the actual K; at width 64 the CTA stages 256-row chunks instead (see
+// VRSmem).  Wider stacks take the Householder path.
 #include "tlr_internal.h"
 
 namespace tlr {
@@ -50,14 +50,25 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
+constexpr int VR_CH = VR_THREADS;       // rows of a CTA-staged chunk (one per thread)
+constexpr int VR_LDZ = VR_CH + 4;       // its pitch (== 4 mod 16)
+
+// Widths up to 48: every warp stages and reduces its own 32-row chunks.
+// Width 64 (CTA-staged): the row and the accumulators of all 36 tiles would
+// not fit a thread's registers, so the CTA stages 256-row chunks and each
+// warp accumulates the tiles it owns (no reduction); G and the scratch then
+// live in the chunk buffer between passes.
 template <int KM>
 struct VRSmem {
+    static constexpr bool STAGED = KM > 48;
     static constexpr int NT8 = KM / 8;
     static constexpr int NTILE = NT8 * (NT8 + 1) / 2;
+    static constexpr int TPW = (NTILE + VR_WARPS - 1) / VR_WARPS;   // owned tiles per warp (staged)
     static constexpr size_t W = (size_t)KM * VR_PITCH;    // one warp's staged chunk
     static constexpr size_t KK = (size_t)KM * KM;
-    // staged chunks | G | G copy / product scratch | Rr (row-major R of the pass) | Rt | d | 1/diag
-    static constexpr size_t bytes() { return sizeof(double) * (VR_WARPS * W + 4 * KK + 2 * KM); }
+    static constexpr size_t CHUNK = STAGED ? (size_t)KM * VR_LDZ : VR_WARPS * W;
+    // chunk buffer(s) | [G | G copy / product scratch, unless in the chunk buffer] | Rr | Rt | d | 1/diag
+    static constexpr size_t bytes() { return sizeof(double) * (CHUNK + (STAGED ? 2 : 4) * KK + 2 * KM); }
 };
 
 // x <- x R^-1 for one row x (registers): right-looking substitution with the
@@ -110,10 +121,11 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
     __shared__ int ok_sh;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, tig = lane & 3;
-    double *Zw = sm + warp * S::W;                 // this warp's staged chunk
-    double *G = sm + VR_WARPS * S::W;              // K x K Gram (column-major, ld KM)
+    constexpr bool STAGED = S::STAGED;
+    double *Zw = sm + warp * S::W;                 // this warp's staged chunk (widths up to 48)
+    double *G = STAGED ? sm : sm + S::CHUNK;       // K x K Gram (column-major, ld KM)
     double *Gc = G + S::KK;                        // copy for a retry; product scratch
-    double *Rr = Gc + S::KK;                       // R of the pass, row-major: Rr[j * KM + k] = R(j, k)
+    double *Rr = STAGED ? sm + S::CHUNK : Gc + S::KK;   // R of the pass, row-major: Rr[j * KM + k] = R(j, k)
     double *Rt = Rr + S::KK;                       // accumulated R (column-major)
     double *dsc = Rt + S::KK;                      // column norms d_j (1 / d_j from pass 1 on)
     double *rdg = dsc + KM;                        // 1 / diag(R)
@@ -124,21 +136,42 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
     const double u = 1.1102230246251565e-16;
     const int npass = t.Q ? 4 : 3;
 
-    for (int pass = 0; pass < npass; ++pass) {
-        double acc[NTILE][2];
+    // tiles owned by this warp in the CTA-staged form
+    int tmi[S::TPW], tni[S::TPW];
 #pragma unroll
-        for (int q = 0; q < NTILE; ++q) acc[q][0] = acc[q][1] = 0.0;
+    for (int q = 0; q < S::TPW; ++q) {
+        const int tile = warp + VR_WARPS * q;
+        int mi = 0;
+        while ((mi + 1) * (mi + 2) / 2 <= tile) ++mi;
+        tmi[q] = (tile < NTILE && 8 * mi < K) ? mi : -1;
+        tni[q] = tile - mi * (mi + 1) / 2;
+    }
+
+    for (int pass = 0; pass < npass; ++pass) {
+        constexpr int NACC = STAGED ? 2 * S::TPW : NTILE;
+        double acc[NACC][2];
+#pragma unroll
+        for (int q = 0; q < NACC; ++q) acc[q][0] = acc[q][1] = 0.0;
         const bool gram = pass < 3;
 
-        for (int r0 = warp * 32; r0 < nb; r0 += VR_THREADS) {
-            const int row = r0 + lane;
+        for (int r0 = STAGED ? 0 : warp * 32; r0 < nb; r0 += VR_THREADS) {
+            const int row = r0 + (STAGED ? tid : lane);
             const bool valid = row < nb;
             double x[KM];
             if (pass < 2) {
+                // two column blocks, walked with one running pointer each
+                const double *p1 = t.X1 + row, *p2 = t.X2 + row;
 #pragma unroll
                 for (int j = 0; j < KM; ++j) {
-                    const double *p = j < k1 ? t.X1 + (size_t)j * t.ld1 : t.X2 + (size_t)(j - k1) * t.ld2;
-                    x[j] = (valid && j < K) ? p[row] : 0.0;
+                    double v = 0.0;
+                    if (j < k1) {
+                        if (valid) v = *p1;
+                        p1 += t.ld1;
+                    } else if (j < K) {
+                        if (valid) v = *p2;
+                        p2 += t.ld2;
+                    }
+                    x[j] = v;
                 }
             } else {
 #pragma unroll
@@ -162,42 +195,80 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
                 }
             }
             if (!gram) continue;
+            if constexpr (STAGED) {
+#pragma unroll
+                for (int j = 0; j < KM; ++j) sm[j * VR_LDZ + tid] = x[j];
+                __syncthreads();
+                // owned tiles over the 256 rows, two chains per tile (even / odd row quads)
+#pragma unroll 2
+                for (int s = 0; s < VR_CH; s += 8) {
+#pragma unroll
+                    for (int q = 0; q < S::TPW; ++q) {
+                        if (tmi[q] < 0) continue;
+                        const double *za = sm + (8 * tmi[q] + g) * VR_LDZ + tig + s;
+                        const double *zb = sm + (8 * tni[q] + g) * VR_LDZ + tig + s;
+                        dmma884(acc[2 * q], za[0], zb[0]);
+                        dmma884(acc[2 * q + 1], za[4], zb[4]);
+                    }
+                }
+                __syncthreads();
+                continue;
+            }
 #pragma unroll
             for (int j = 0; j < KM; ++j) Zw[j * VR_PITCH + lane] = x[j];
             __syncwarp();
             // Gram of the chunk: row quads s, one fragment per 8-column block
+            if constexpr (!STAGED) {
 #pragma unroll 1
-            for (int s = 0; s < 32; s += 4) {
-                double a[NT8];
+                for (int s = 0; s < 32; s += 4) {
+                    double a[NT8];
 #pragma unroll
-                for (int mi = 0; mi < NT8; ++mi) a[mi] = Zw[(8 * mi + g) * VR_PITCH + s + tig];
-                int q = 0;
+                    for (int mi = 0; mi < NT8; ++mi) a[mi] = Zw[(8 * mi + g) * VR_PITCH + s + tig];
+                    int q = 0;
 #pragma unroll
-                for (int mi = 0; mi < NT8; ++mi)
+                    for (int mi = 0; mi < NT8; ++mi)
 #pragma unroll
-                    for (int ni = 0; ni <= mi; ++ni, ++q) dmma884(acc[q], a[mi], a[ni]);
+                        for (int ni = 0; ni <= mi; ++ni, ++q) dmma884(acc[q], a[mi], a[ni]);
+                }
             }
             __syncwarp();
         }
         if (!gram) break;
-        // per-warp partials -> G in warp order (both triangles)
-        for (int idx = tid; idx < KM * KM; idx += VR_THREADS) G[idx] = 0.0;
-        __syncthreads();
-        for (int w = 0; w < VR_WARPS; ++w) {
-            if (warp == w) {
-                int q = 0;
+        if constexpr (STAGED) {
+            // owned tiles -> G (both triangles; the chunk buffer is free after the last barrier)
 #pragma unroll
-                for (int mi = 0; mi < NT8; ++mi)
+            for (int q = 0; q < S::TPW; ++q) {
+                if (tmi[q] < 0) continue;
 #pragma unroll
-                    for (int ni = 0; ni <= mi; ++ni, ++q)
-#pragma unroll
-                        for (int e = 0; e < 2; ++e) {
-                            const int i = 8 * mi + g, j = 8 * ni + 2 * tig + e;
-                            G[i + j * KM] += acc[q][e];
-                            if (mi != ni) G[j + i * KM] += acc[q][e];
-                        }
+                for (int e = 0; e < 2; ++e) {
+                    const int i = 8 * tmi[q] + g, j = 8 * tni[q] + 2 * tig + e;
+                    const double v = acc[2 * q][e] + acc[2 * q + 1][e];
+                    G[i + j * KM] = v;
+                    G[j + i * KM] = v;
+                }
             }
+            // tiles past K (not computed) stay out of the factorization, which reads [0, K)
             __syncthreads();
+        } else {
+            // per-warp partials -> G in warp order (both triangles)
+            for (int idx = tid; idx < KM * KM; idx += VR_THREADS) G[idx] = 0.0;
+            __syncthreads();
+            for (int w = 0; w < VR_WARPS; ++w) {
+                if (warp == w) {
+                    int q = 0;
+#pragma unroll
+                    for (int mi = 0; mi < NT8; ++mi)
+#pragma unroll
+                        for (int ni = 0; ni <= mi; ++ni, ++q)
+#pragma unroll
+                            for (int e = 0; e < 2; ++e) {
+                                const int i = 8 * mi + g, j = 8 * ni + 2 * tig + e;
+                                G[i + j * KM] += acc[q][e];
+                                if (mi != ni) G[j + i * KM] += acc[q][e];
+                            }
+                }
+                __syncthreads();
+            }
         }
         if (pass == 0) {
             for (int j = tid; j < KM; j += VR_THREADS) {
@@ -302,16 +373,17 @@ void launch_vr(const VRTask *d_tasks, int ntasks, int *fail, cudaStream_t st) {
 
 }  // namespace
 
-int vside_r_kmax() { return 48; }
+int vside_r_kmax() { return 64; }
 
-int vside_r_bucket(int K) { return K <= 16 ? 16 : K <= 32 ? 32 : 48; }
+int vside_r_bucket(int K) { return K <= 16 ? 16 : K <= 32 ? 32 : K <= 48 ? 48 : 64; }
 
 void launch_vside_r_batched(const VRTask *d_tasks, int ntasks, int kmax, int *fail, cudaStream_t st) {
     if (ntasks <= 0) return;
     switch (vside_r_bucket(kmax)) {
         case 16: launch_vr<16>(d_tasks, ntasks, fail, st); break;
         case 32: launch_vr<32>(d_tasks, ntasks, fail, st); break;
-        default: launch_vr<48>(d_tasks, ntasks, fail, st); break;
+        case 48: launch_vr<48>(d_tasks, ntasks, fail, st); break;
+        default: launch_vr<64>(d_tasks, ntasks, fail, st); break;
     }
 }
 

@@ -2068,6 +2068,13 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             std::vector<GemmTask> g;
             std::vector<CopyTask> cp;
             for (int m = k + 1; m < NT; ++m) {
+                if (m == k + 2) {
+                    // TRSM(k+1, k) is all the critical chain SYRK(k, k+1) -> POTRF(k+1)
+                    // needs: it goes first, on its own, and releases the chain
+                    TRY(run_gemms(c, g, false, P_GEMM_TRSM)); TRY(run_copies(c, cp));
+                    CUDA_TRY(cudaEventRecord(evT, c->stream));
+                    c->ar->off = base_mark;
+                }
                 const bool dense = A->is_dense(m, k);
                 const int r = dense ? NB : A->rank(m, k);
                 log_op(op_counts('t', NB, r, 1, 0), m, k, m == k + 1);
@@ -2103,7 +2110,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             }
         }
         CUDA_TRY(cudaEventRecord(ev[T1], c->stream));
-        CUDA_TRY(cudaEventRecord(evT, c->stream));
+        if (k + 2 >= NT) CUDA_TRY(cudaEventRecord(evT, c->stream));
         std::vector<RecompTask> rec;
         std::vector<int> rec_case;
         std::vector<std::array<int, 5>> rec_meta;
