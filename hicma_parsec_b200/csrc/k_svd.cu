@@ -650,12 +650,8 @@ void launch_core_svd_batched(const CoreTask *d_tasks, int ntasks, int kmax, cons
     else
         smem = 2 * sizeof(double) * (size_t)kmax + 2 * sizeof(int) * kmax;
     smem = (smem + 15) / 16 * 16;
-    // lanes per pair ~ K/8 elements each; more pair groups per CTA for large K.
-    // Small cores run on one or two warps per CTA: their steps are separated by
-    // CTA barriers, which are cheap on a single warp, and many such CTAs share
-    // an SM.
-    if (kmax <= 32) launch_lp<8, 32>(d_tasks, ntasks, smem, p, st);
-    else if (kmax <= 64) launch_lp<8, 64>(d_tasks, ntasks, smem, p, st);
+    // lanes per pair ~ K/8 elements each; more pair groups per CTA for large K
+    if (kmax <= 64) launch_lp<8, 256>(d_tasks, ntasks, smem, p, st);
     else if (kmax <= 96) launch_lp<16, 256>(d_tasks, ntasks, smem, p, st);
     else if (kmax <= KMAX_SMEM) launch_lp<16, 512>(d_tasks, ntasks, smem, p, st);
     else {

@@ -128,6 +128,8 @@ struct hicma_tlr_ctx_s {
     int device = 0;
     cudaStream_t stream = nullptr;      // bulk work
     cudaStream_t stream_hi = nullptr;   // critical path (high priority): SYRK(k,k+1) + POTRF(k+1)
+    cudaStream_t stream_side = nullptr; // wide recompressions (Householder chain) beside the CholeskyQR chain
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaStream_t cur = nullptr;         // stream the helpers launch on
     char *d_ws = nullptr;
     size_t ws_bytes = 0;
@@ -200,6 +202,7 @@ size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
 int ctx_sync(hicma_tlr_ctx *c) {
     CUDA_TRY(cudaStreamSynchronize(c->stream_hi));
+    CUDA_TRY(cudaStreamSynchronize(c->stream_side));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->stage_off = 0;
     return 0;
@@ -242,6 +245,7 @@ T *stage(hicma_tlr_ctx *c, const T *src, size_t n) {
     if (bytes > c->stage_bytes) return nullptr;
     if (c->stage_off + bytes > c->stage_bytes) {
         if (cudaStreamSynchronize(c->stream_hi) != cudaSuccess) return nullptr;
+        if (cudaStreamSynchronize(c->stream_side) != cudaSuccess) return nullptr;
         if (cudaStreamSynchronize(c->stream) != cudaSuccess) return nullptr;
         c->stage_off = 0;
     }
@@ -794,8 +798,12 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
     size_t i0 = 0;
     while (i0 < tasks.size()) {
         c->ar->off = mark;
-        std::vector<CopyTask> copies, keeps;
-        std::vector<GemmTask> g1, g2, g1s, g2s, gU, g3, g4;
+        // common prefix (Y products, V-side stacks) on the bulk stream; then the
+        // CholeskyQR chain (F) there and the Householder chain of the wide
+        // updates (S) on the side stream, joined at the end of the chunk
+        std::vector<CopyTask> copies, copiesS, keeps;
+        std::vector<GemmTask> g1, g2, g1s, g2s, gU, g3, g4, gUS, g3S, g4S;
+        std::vector<CoreTask> coresS;
         std::vector<ProjTask> projs;
         std::vector<SelTask> sels;
         std::vector<GramTask> grams;
@@ -866,9 +874,9 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                 double *TU = ws_alloc<double>(c, npa * pbw * pbw), *TV = ws_alloc<double>(c, npk * pbw * pbw);
                 double *Pu = ws_alloc<double>(c, (size_t)rc * ra), *Pu2 = ws_alloc<double>(c, (size_t)rc * ra);
                 double *Wu = Us + (size_t)nb * rc;
-                if (rc > 0) copies.push_back(make_copy(t.Cu, nb, Us, nb, nb, rc));
+                if (rc > 0) copiesS.push_back(make_copy(t.Cu, nb, Us, nb, nb, rc));
                 if (ra > 0) {
-                    copies.push_back(make_copy(t.Au, nb, Wu, nb, nb, ra));
+                    copiesS.push_back(make_copy(t.Au, nb, Wu, nb, nb, ra));
                     // two rounds of projection of Au against the old orthonormal U
                     if (rc > 0) projs.push_back(ProjTask{Us, Wu, Pu, Pu2, nb, rc, ra});
                     qrs.push_back(QRTask{Wu, tauU, TU, nb, ra, nb});
@@ -882,7 +890,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             }
             ct.RU = RU; ct.ldru = K;
             ct.SU = SU; ct.RUc = nullptr; ct.work = work;
-            cores.push_back(ct);
+            (cq ? cores : coresS).push_back(ct);
             if (cq) {
                 // new U = Q_U U_r
                 GemmTask u = make_gemm(0, 0, nb, maxrank, K, 1.0, Us, nb, SU, K, 0.0, t.outU, nb);
@@ -892,15 +900,15 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                 // new U = Q(Wu) [U_bot; 0] + Cu U_top (beta 1 after the Q application when ra > 0)
                 GemmTask u = make_gemm(0, 0, nb, maxrank, rc, 1.0, Us, nb, SU, K, ra > 0 ? 1.0 : 0.0, t.outU, nb);
                 u.n_dev = ct.rank_task;
-                gU.push_back(u);
+                gUS.push_back(u);
             }
             // V Sigma = M^T U = R_V (R_U^T U): new V = [Cv, -Y] (R_U^T U_r)
             GemmTask a = make_gemm(1, 0, K, K, K, 1.0, RU, K, SU, K, 0.0, T1, K);
             a.n_dev = ct.rank_task;
-            g3.push_back(a);
+            (cq ? g3 : g3S).push_back(a);
             GemmTask b = make_gemm(0, 0, nb, maxrank, K, 1.0, Vsrc, nb, T1, K, 0.0, t.outV, nb);
             b.n_dev = ct.rank_task;
-            g4.push_back(b);
+            (cq ? g4 : g4S).push_back(b);
         }
         TRY(bc_recompress_parts(sels, grams, projs, asm_));
         TRY(run_copies(c, copies));
@@ -926,6 +934,14 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
         TRY(run_gemms(c, g1s, true, P_GEMM_Y));
         TRY(run_gemms(c, g2, false, P_GEMM_Y));
         TRY(run_gemms(c, g2s, true, P_GEMM_Y));
+        const bool side = !coresS.empty();
+        cudaStream_t bulk = c->cur;
+        if (side) {
+            CUDA_TRY(cudaEventRecord(c->ev_fork, bulk));
+            CUDA_TRY(cudaStreamWaitEvent(c->stream_side, c->ev_fork, 0));
+            c->cur = c->stream_side;
+        }
+        TRY(run_copies(c, copiesS));
         TRY(run_copies(c, keeps));
         if (!projs.empty()) {
             double fl = 0.0, by = 0.0;
@@ -940,7 +956,6 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             TRY(check_launch(c));
         }
         TRY(run_qr(c, qrs, nb));
-        TRY(run_vside_r(c, vrs, 0));
         if (!asm_.empty()) {
             AssembleTask *d = stage(c, asm_.data(), asm_.size());
             if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
@@ -948,11 +963,22 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             TRY(check_launch(c));
         }
         CoreParams cp{0, acc, maxrank, fixed_rank, nb, c->d_flags + 1, c->d_flags + 2};
-        TRY(run_core_buckets(c, cores, cp));
+        TRY(run_core_buckets(c, coresS, cp));
         TRY(run_qapply(c, apps, nb));
+        TRY(run_gemms(c, gUS));
+        TRY(run_gemms(c, g3S));
+        TRY(run_gemms(c, g4S));
+        if (side) {
+            CUDA_TRY(cudaEventRecord(c->ev_join, c->stream_side));
+            c->cur = bulk;
+        }
+        TRY(run_vside_r(c, vrs, 0));
+        TRY(run_core_buckets(c, cores, cp));
         TRY(run_gemms(c, gU));
         TRY(run_gemms(c, g3));
         TRY(run_gemms(c, g4));
+        // the next chunk reuses the workspace: it starts after both chains
+        if (side) CUDA_TRY(cudaStreamWaitEvent(bulk, c->ev_join, 0));
         i0 = i;
     }
     c->ar->off = mark;
@@ -1096,6 +1122,9 @@ static void ctx_release(hicma_tlr_ctx *c) {
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->d_flags) cudaFree(c->d_flags);
     if (c->d_scal) cudaFree(c->d_scal);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->stream_side) cudaStreamDestroy(c->stream_side);
     if (c->stream_hi) cudaStreamDestroy(c->stream_hi);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1119,6 +1148,10 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     e = cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->stream_hi, cudaStreamNonBlocking, prio_hi);
     if (e != cudaSuccess) return fail(e, "priority stream");
+    e = cudaStreamCreateWithFlags(&c->stream_side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return fail(e, "side stream");
     c->cur = c->stream;
     if (const char *vs = std::getenv("HICMA_TLR_VSIDE")) c->vside_cholqr = std::strcmp(vs, "qr") != 0;
     size_t free_b = 0, total_b = 0;
@@ -1594,7 +1627,7 @@ static size_t compress_ws_bytes(int nb, int s) {
     b += align_up(sizeof(double) * (size_t)nb * s + 1) * 4;   // Y, Q, W, Wkeep
     b += align_up(sizeof(double) * (size_t)s + 1) * 2;
     b += align_up(sizeof(double) * npan * pb * pb + 1) * 2;
-    b += align_up(sizeof(double) * (size_t)s * s + 1);
+    b += align_up(sizeof(double) * (size_t)s * s + 1) * 3;    // SU (+ R_Y, R_W of the CholeskyQR path)
     if (s > core_smem_kmax()) b += align_up(sizeof(double) * core_work_doubles(s) + 1);
     return b + 1024;
 }
@@ -1612,6 +1645,11 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
         std::vector<QRTask> qy, qw;
         std::vector<QApplyTask> aq, au;
         std::vector<CoreTask> cores;
+        std::vector<VRTask> cqy, cqw;
+        std::vector<GemmTask> gu;
+        // up to vside_r_kmax() samples: both QRs by shifted CholeskyQR3 (Q of Y
+        // formed directly, R of W only), U = Q_Y U_r as a GEMM
+        const bool cq = c->vside_cholqr && s <= vside_r_kmax();
         size_t i = i0;
         for (; i < tasks.size(); ++i) {
             if (compress_ws_bytes(nb, s) > ws_free(c)) {
@@ -1619,6 +1657,32 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
                 break;
             }
             const CompressTask &t = tasks[i];
+            if (cq) {
+                double *Y = ws_alloc<double>(c, (size_t)nb * s);
+                double *Q = ws_alloc<double>(c, (size_t)nb * s);
+                double *W = ws_alloc<double>(c, (size_t)nb * s);
+                double *Z = ws_alloc<double>(c, (size_t)nb * s);
+                double *RY = ws_alloc<double>(c, (size_t)s * s), *RW = ws_alloc<double>(c, (size_t)s * s);
+                double *SU = ws_alloc<double>(c, (size_t)s * s);
+                int *rt = d_rank_task_base + (i - i0);
+                gy.push_back(make_gemm(0, 0, nb, s, nb, 1.0, t.A, nb, Omega, nb, 0.0, Y, nb));
+                cqy.push_back(VRTask{Y, nullptr, Q, RY, Q, nb, s, 0, nb, nb});
+                gw.push_back(make_gemm(1, 0, nb, s, nb, 1.0, t.A, nb, Q, nb, 0.0, W, nb));
+                cqw.push_back(VRTask{W, nullptr, Z, RW, nullptr, nb, s, 0, nb, nb});
+                CoreTask ct{};
+                ct.RU = nullptr; ct.RV = RW; ct.ldru = s; ct.ldrv = s;
+                ct.SU = SU; ct.RUc = nullptr; ct.work = nullptr;
+                ct.rank_out = t.rank_dst; ct.rank_task = rt; ct.K = s;
+                cores.push_back(ct);
+                GemmTask gU = make_gemm(0, 0, nb, maxrank, s, 1.0, Q, nb, SU, s, 0.0, t.outU, nb);
+                gU.n_dev = rt;
+                gu.push_back(gU);
+                // V Sigma = (A^T Q) U_r  (R_U = I)
+                GemmTask g = make_gemm(0, 0, nb, maxrank, s, 1.0, W, nb, SU, s, 0.0, t.outV, nb);
+                g.n_dev = rt;
+                gv.push_back(g);
+                continue;
+            }
             double *Y = ws_alloc<double>(c, (size_t)nb * s);
             double *Q = ws_alloc<double>(c, (size_t)nb * s);
             double *W = ws_alloc<double>(c, (size_t)nb * s);
@@ -1647,13 +1711,16 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
         }
         TRY(run_gemms(c, gy, false, P_GEMM_GEN));
         TRY(run_qr(c, qy, nb));
+        TRY(run_vside_r(c, cqy, 0));
         TRY(run_qapply(c, aq, nb));
         TRY(run_gemms(c, gw, false, P_GEMM_GEN));
         TRY(run_copies(c, keeps));
         TRY(run_qr(c, qw, nb));
+        TRY(run_vside_r(c, cqw, 0));
         CoreParams cp{1, tol, maxrank, 0, nb, nullptr, nullptr};
         TRY(run_core_buckets(c, cores, cp));
         TRY(run_qapply(c, au, nb));
+        TRY(run_gemms(c, gu, false, P_GEMM_GEN));
         TRY(run_gemms(c, gv, false, P_GEMM_GEN));
         i0 = i;
     }
@@ -1685,10 +1752,11 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
     // off-band tiles: generate dense into the workspace, compress into slots.
     // The reference samples min(maxrank + 10, NB) columns for every tile
     // (STARSH_gen.jdf:262-266); the sampled singular values only matter up to
-    // the rank, so tiles start with s = min(160, s_full) samples (the on-chip
-    // core) and a tile whose rank comes within max(32, s/4) of s is generated
-    // again with twice the samples, up to s_full.  Rejected tiles (2r >= NB)
-    // stay rejected: more samples can only raise the rank.
+    // the rank, so tiles start with s = min(64, s_full) samples (the CholeskyQR
+    // path; 160 with the Householder path) and a tile whose rank comes within
+    // max(32, s/4) of s is generated again with twice the samples, up to
+    // s_full.  Rejected tiles (2r >= NB) stay rejected: more samples can only
+    // raise the rank.
     const int s_full = std::min(maxrank + 10, NB);
     double *Omega = ws_alloc<double>(c, (size_t)NB * s_full);
     double *Ident = ws_alloc<double>(c, (size_t)s_full * s_full);
@@ -1700,7 +1768,7 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
     for (int m = A->band; m < NT; ++m)
         for (int n = 0; n <= m - A->band; ++n) pending.push_back({m, n});
     const CovParams cp = cov_params(A, prob);
-    int s = std::min(160, s_full);
+    int s = std::min(c->vside_cholqr ? vside_r_kmax() : 160, s_full);
     while (!pending.empty()) {
         launch_set_identity(Ident, s, s, c->stream);
         TRY(check_launch(c));
