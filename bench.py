@@ -51,6 +51,10 @@ CONFIGS = {
     "c2t": dict(kind=2, n=27000, n_full=270000, nb=2700, maxrank=150, acc=1e-8, noise=1e-4, band=1,
                 autoband=False,
                 workload="2D sqexp leading 10x10 tiles of the N=270000 matrix, NB=2700 e=1e-8 maxrank=150 band=1 FP64"),
+    # the leading 30 x 30 tiles: launches of hundreds of tasks with the full size's ranks (for profiles)
+    "c2m": dict(kind=2, n=81000, n_full=270000, nb=2700, maxrank=150, acc=1e-8, noise=1e-4, band=1,
+                autoband=False,
+                workload="2D sqexp leading 30x30 tiles of the N=270000 matrix, NB=2700 e=1e-8 maxrank=150 band=1 FP64"),
     "c3": dict(kind=4, n=108000, nb=2700, maxrank=1350, acc=1e-8, noise=1e-4, band=1, autoband=True,
                workload="3D exp N=108000 NB=2700 e=1e-8 maxrank=1350 band auto FP64"),
     "c3s": dict(kind=4, n=27000, nb=2700, maxrank=1350, acc=1e-8, noise=1e-4, band=1, autoband=True,
@@ -422,7 +426,7 @@ def run_ours(args, cfg):
                "k_qr": (prof["qr"], "fp64"), "k_qapply": (prof["qapply"], "fp64"),
                "k_core_svd": (prof["core_svd"], "fp64"), "k_bcgs2": (prof["proj"], "tensor"),
                "k_copy_batched": (prof["copy"], "hbm"), "k_gram_batched": (prof["gram"], "tensor"),
-               "k_vside_r": (prof["vside_r"], "tensor")}
+               "k_cholqr3": (prof["cholqr3"], "tensor")}
     dom = max(kernels, key=lambda k: kernels[k][0]["seconds"])
     pd, kind = kernels[dom]
     launches = int(st[3])  # kernel launches of one factorization (engine counter)
@@ -572,7 +576,7 @@ def run_ours(args, cfg):
                 "dense_equiv_gflops": (n ** 3 / 3.0) / s_per_factor / 1e9,
                 "phase_s": {"potrf": st[4], "trsm": st[5], "syrk": st[6], "gemm_recompress": st[7],
                             "device_idle_between_panels": st[12]},
-                "vside_cholqr_breakdowns": int(st[11]),
+                "cholqr3_breakdowns": int(st[11]),
                 "jacobi_sweeps_total": st[8],
                 "kernel_classes": prof, "gpu_launches": launches * args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "accuracy": accuracy,

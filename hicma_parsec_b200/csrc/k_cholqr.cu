@@ -34,15 +34,15 @@
 // one warp factors G in shared memory.  Kernels are instantiated per width
 // bucket (KM = 16, 32, 48, 64 columns) so that unrolled loops do not run far
 // past the actual K; at width 64 the CTA stages 256-row chunks instead (see
-// VRSmem).  Wider stacks take the Householder path.
+// CQSmem).  Wider stacks take the Householder path.
 #include "tlr_internal.h"
 
 namespace tlr {
 namespace {
 
-constexpr int VR_WARPS = 8;
-constexpr int VR_THREADS = VR_WARPS * 32;
-constexpr int VR_PITCH = 36;            // per-warp staged chunk pitch (== 4 mod 16)
+constexpr int CQ_WARPS = 8;
+constexpr int CQ_THREADS = CQ_WARPS * 32;
+constexpr int CQ_PITCH = 36;            // per-warp staged chunk pitch (== 4 mod 16)
 
 __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -50,8 +50,8 @@ __device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-constexpr int VR_CH = VR_THREADS;       // rows of a CTA-staged chunk (one per thread)
-constexpr int VR_LDZ = VR_CH + 4;       // its pitch (== 4 mod 16)
+constexpr int CQ_CH = CQ_THREADS;       // rows of a CTA-staged chunk (one per thread)
+constexpr int CQ_LDZ = CQ_CH + 4;       // its pitch (== 4 mod 16)
 
 // Widths up to 48: every warp stages and reduces its own 32-row chunks.
 // Width 64 (CTA-staged): the row and the accumulators of all 36 tiles would
@@ -59,14 +59,14 @@ constexpr int VR_LDZ = VR_CH + 4;       // its pitch (== 4 mod 16)
 // warp accumulates the tiles it owns (no reduction); G and the scratch then
 // live in the chunk buffer between passes.
 template <int KM>
-struct VRSmem {
+struct CQSmem {
     static constexpr bool STAGED = KM > 48;
     static constexpr int NT8 = KM / 8;
     static constexpr int NTILE = NT8 * (NT8 + 1) / 2;
-    static constexpr int TPW = (NTILE + VR_WARPS - 1) / VR_WARPS;   // owned tiles per warp (staged)
-    static constexpr size_t W = (size_t)KM * VR_PITCH;    // one warp's staged chunk
+    static constexpr int TPW = (NTILE + CQ_WARPS - 1) / CQ_WARPS;   // owned tiles per warp (staged)
+    static constexpr size_t W = (size_t)KM * CQ_PITCH;    // one warp's staged chunk
     static constexpr size_t KK = (size_t)KM * KM;
-    static constexpr size_t CHUNK = STAGED ? (size_t)KM * VR_LDZ : VR_WARPS * W;
+    static constexpr size_t CHUNK = STAGED ? (size_t)KM * CQ_LDZ : CQ_WARPS * W;
     // chunk buffer(s) | [G | G copy / product scratch, unless in the chunk buffer] | Rr | Rt | d | 1/diag
     static constexpr size_t bytes() { return sizeof(double) * (CHUNK + (STAGED ? 2 : 4) * KK + 2 * KM); }
 };
@@ -114,8 +114,8 @@ __device__ bool warp_cholesky(double *G, int K, int lane) {
 }
 
 template <int KM>
-__global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const VRTask *__restrict__ tasks, int *fail) {
-    using S = VRSmem<KM>;
+__global__ void __launch_bounds__(CQ_THREADS, KM <= 32 ? 2 : 1) k_cholqr3(const CQTask *__restrict__ tasks, int *fail) {
+    using S = CQSmem<KM>;
     constexpr int NT8 = S::NT8, NTILE = S::NTILE;
     extern __shared__ double sm[];
     __shared__ int ok_sh;
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
     double *dsc = Rt + S::KK;                      // column norms d_j (1 / d_j from pass 1 on)
     double *rdg = dsc + KM;                        // 1 / diag(R)
 
-    const VRTask t = tasks[blockIdx.x];
+    const CQTask t = tasks[blockIdx.x];
     const int k1 = t.k1, K = t.k1 + t.k2, nb = t.nb;
     if (K <= 0) return;
     const double u = 1.1102230246251565e-16;
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
     int tmi[S::TPW], tni[S::TPW];
 #pragma unroll
     for (int q = 0; q < S::TPW; ++q) {
-        const int tile = warp + VR_WARPS * q;
+        const int tile = warp + CQ_WARPS * q;
         int mi = 0;
         while ((mi + 1) * (mi + 2) / 2 <= tile) ++mi;
         tmi[q] = (tile < NTILE && 8 * mi < K) ? mi : -1;
@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
         for (int q = 0; q < NACC; ++q) acc[q][0] = acc[q][1] = 0.0;
         const bool gram = pass < 3;
 
-        for (int r0 = STAGED ? 0 : warp * 32; r0 < nb; r0 += VR_THREADS) {
+        for (int r0 = STAGED ? 0 : warp * 32; r0 < nb; r0 += CQ_THREADS) {
             const int row = r0 + (STAGED ? tid : lane);
             const bool valid = row < nb;
             double x[KM];
@@ -197,16 +197,16 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
             if (!gram) continue;
             if constexpr (STAGED) {
 #pragma unroll
-                for (int j = 0; j < KM; ++j) sm[j * VR_LDZ + tid] = x[j];
+                for (int j = 0; j < KM; ++j) sm[j * CQ_LDZ + tid] = x[j];
                 __syncthreads();
                 // owned tiles over the 256 rows, two chains per tile (even / odd row quads)
 #pragma unroll 2
-                for (int s = 0; s < VR_CH; s += 8) {
+                for (int s = 0; s < CQ_CH; s += 8) {
 #pragma unroll
                     for (int q = 0; q < S::TPW; ++q) {
                         if (tmi[q] < 0) continue;
-                        const double *za = sm + (8 * tmi[q] + g) * VR_LDZ + tig + s;
-                        const double *zb = sm + (8 * tni[q] + g) * VR_LDZ + tig + s;
+                        const double *za = sm + (8 * tmi[q] + g) * CQ_LDZ + tig + s;
+                        const double *zb = sm + (8 * tni[q] + g) * CQ_LDZ + tig + s;
                         dmma884(acc[2 * q], za[0], zb[0]);
                         dmma884(acc[2 * q + 1], za[4], zb[4]);
                     }
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
                 continue;
             }
 #pragma unroll
-            for (int j = 0; j < KM; ++j) Zw[j * VR_PITCH + lane] = x[j];
+            for (int j = 0; j < KM; ++j) Zw[j * CQ_PITCH + lane] = x[j];
             __syncwarp();
             // Gram of the chunk: row quads s, one fragment per 8-column block
             if constexpr (!STAGED) {
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
                 for (int s = 0; s < 32; s += 4) {
                     double a[NT8];
 #pragma unroll
-                    for (int mi = 0; mi < NT8; ++mi) a[mi] = Zw[(8 * mi + g) * VR_PITCH + s + tig];
+                    for (int mi = 0; mi < NT8; ++mi) a[mi] = Zw[(8 * mi + g) * CQ_PITCH + s + tig];
                     int q = 0;
 #pragma unroll
                     for (int mi = 0; mi < NT8; ++mi)
@@ -251,9 +251,9 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
             __syncthreads();
         } else {
             // per-warp partials -> G in warp order (both triangles)
-            for (int idx = tid; idx < KM * KM; idx += VR_THREADS) G[idx] = 0.0;
+            for (int idx = tid; idx < KM * KM; idx += CQ_THREADS) G[idx] = 0.0;
             __syncthreads();
-            for (int w = 0; w < VR_WARPS; ++w) {
+            for (int w = 0; w < CQ_WARPS; ++w) {
                 if (warp == w) {
                     int q = 0;
 #pragma unroll
@@ -271,12 +271,12 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
             }
         }
         if (pass == 0) {
-            for (int j = tid; j < KM; j += VR_THREADS) {
+            for (int j = tid; j < KM; j += CQ_THREADS) {
                 const double d = j < K ? sqrt(G[j + j * KM]) : 1.0;
                 dsc[j] = d > 0.0 ? d : 1.0;
             }
             __syncthreads();
-            for (int idx = tid; idx < K * K; idx += VR_THREADS) {
+            for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
                 const int i = idx % K, j = idx / K;
                 G[i + j * KM] /= dsc[i] * dsc[j];
             }
@@ -322,29 +322,29 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
         }
         __syncthreads();
         // R of the pass, row-major (upper): Rr[j][k] = L(k, j); zero outside K
-        for (int idx = tid; idx < KM * KM; idx += VR_THREADS) {
+        for (int idx = tid; idx < KM * KM; idx += CQ_THREADS) {
             const int j = idx / KM, k = idx % KM;
             double v = 0.0;
             if (j <= k && k < K) v = ok_sh ? G[k + j * KM] : (j == k ? 1.0 : 0.0);
             Rr[j * KM + k] = v;
         }
         __syncthreads();
-        for (int j = tid; j < KM; j += VR_THREADS) rdg[j] = j < K ? 1.0 / Rr[j * KM + j] : 0.0;
+        for (int j = tid; j < KM; j += CQ_THREADS) rdg[j] = j < K ? 1.0 / Rr[j * KM + j] : 0.0;
         if (pass == 0) {
-            for (int idx = tid; idx < KM * KM; idx += VR_THREADS) {
+            for (int idx = tid; idx < KM * KM; idx += CQ_THREADS) {
                 const int i = idx % KM, j = idx / KM;
                 Rt[idx] = Rr[i * KM + j];
             }
         } else {
             // Rt <- R Rt (upper times upper) through the scratch
-            for (int idx = tid; idx < K * K; idx += VR_THREADS) {
+            for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
                 const int i = idx % K, j = idx / K;
                 double s = 0.0;
                 for (int k = i; k <= j; ++k) s += Rr[i * KM + k] * Rt[k + j * KM];
                 Gc[i + j * KM] = i <= j ? s : 0.0;
             }
             __syncthreads();
-            for (int idx = tid; idx < K * K; idx += VR_THREADS) {
+            for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
                 const int i = idx % K, j = idx / K;
                 Rt[i + j * KM] = Gc[i + j * KM];
             }
@@ -352,38 +352,38 @@ __global__ void __launch_bounds__(VR_THREADS, KM <= 32 ? 2 : 1) k_vside_r(const 
         __syncthreads();
         if (pass == 0) {
             // the substitution of pass 1 scales by 1/d first
-            for (int j = tid; j < KM; j += VR_THREADS) dsc[j] = 1.0 / dsc[j];
+            for (int j = tid; j < KM; j += CQ_THREADS) dsc[j] = 1.0 / dsc[j];
             __syncthreads();
         }
     }
     // R = Rt D (dsc holds 1/d)
-    for (int idx = tid; idx < K * K; idx += VR_THREADS) {
+    for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
         const int i = idx % K, j = idx / K;
         t.R[i + (size_t)j * K] = i <= j ? Rt[i + j * KM] / dsc[j] : 0.0;
     }
 }
 
 template <int KM>
-void launch_vr(const VRTask *d_tasks, int ntasks, int *fail, cudaStream_t st) {
-    const size_t smem = VRSmem<KM>::bytes();
+void launch_cq(const CQTask *d_tasks, int ntasks, int *fail, cudaStream_t st) {
+    const size_t smem = CQSmem<KM>::bytes();
     // per device and thread-safe: set on every launch (a host-side call, no synchronisation)
-    cudaFuncSetAttribute(k_vside_r<KM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_vside_r<KM><<<ntasks, VR_THREADS, smem, st>>>(d_tasks, fail);
+    cudaFuncSetAttribute(k_cholqr3<KM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_cholqr3<KM><<<ntasks, CQ_THREADS, smem, st>>>(d_tasks, fail);
 }
 
 }  // namespace
 
-int vside_r_kmax() { return 64; }
+int cholqr3_kmax() { return 64; }
 
-int vside_r_bucket(int K) { return K <= 16 ? 16 : K <= 32 ? 32 : K <= 48 ? 48 : 64; }
+int cholqr3_bucket(int K) { return K <= 16 ? 16 : K <= 32 ? 32 : K <= 48 ? 48 : 64; }
 
-void launch_vside_r_batched(const VRTask *d_tasks, int ntasks, int kmax, int *fail, cudaStream_t st) {
+void launch_cholqr3_batched(const CQTask *d_tasks, int ntasks, int kmax, int *fail, cudaStream_t st) {
     if (ntasks <= 0) return;
-    switch (vside_r_bucket(kmax)) {
-        case 16: launch_vr<16>(d_tasks, ntasks, fail, st); break;
-        case 32: launch_vr<32>(d_tasks, ntasks, fail, st); break;
-        case 48: launch_vr<48>(d_tasks, ntasks, fail, st); break;
-        default: launch_vr<64>(d_tasks, ntasks, fail, st); break;
+    switch (cholqr3_bucket(kmax)) {
+        case 16: launch_cq<16>(d_tasks, ntasks, fail, st); break;
+        case 32: launch_cq<32>(d_tasks, ntasks, fail, st); break;
+        case 48: launch_cq<48>(d_tasks, ntasks, fail, st); break;
+        default: launch_cq<64>(d_tasks, ntasks, fail, st); break;
     }
 }
 

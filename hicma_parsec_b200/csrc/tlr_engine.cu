@@ -144,8 +144,9 @@ struct hicma_tlr_ctx_s {
     int gemm_narrow_n = GEMM_NARROW_N;   // rank-wide outputs up to this width use 128 x 32 tiles
     int potrf_grid = 0;                  // CTAs of the persistent tile POTRF (0: one per SM)
     // QRs of the recompressions: shifted CholeskyQR3 on both sides for stacked
-    // ranks up to vside_r_kmax() (1), the Householder pipeline for all (0; HICMA_TLR_VSIDE=qr)
-    int vside_cholqr = 1;
+    // ranks up to cholqr3_kmax() and the generation range finder up to that many samples
+    // (1), the Householder pipeline for all (0; HICMA_TLR_QR=householder)
+    int cholqr = 1;
     double *d_scal = nullptr;   // device scalars
     int precision = HICMA_TLR_PREC_FP64;
     long long launches = 0;
@@ -263,7 +264,7 @@ enum {
     // batched DMMA GEMMs by call site (P_GEMM: recompression outputs and the rest)
     P_GEMM_Y, P_GEMM_TRSM, P_GEMM_SYRK, P_GEMM_DENSE, P_GEMM_GEN,
     P_GRAM,   // split-K inner products B_V^T A_V of the recompressions
-    P_VR,     // V-side R factors by shifted CholeskyQR3
+    P_CHOLQR,     // V-side R factors by shifted CholeskyQR3
     P_NCLASS
 };
 
@@ -502,11 +503,11 @@ int run_qr(hicma_tlr_ctx *c, std::vector<QRTask> &v, int m_max) {
     return check_launch(c);
 }
 
-int run_vside_r(hicma_tlr_ctx *c, std::vector<VRTask> &v, int kmax) {
+int run_cholqr3(hicma_tlr_ctx *c, std::vector<CQTask> &v, int kmax) {
     if (v.empty()) return 0;
 #ifdef TLR_BOUNDS_CHECK
     for (size_t i = 0; i < v.size(); ++i) {
-        const VRTask &t = v[i];
+        const CQTask &t = v[i];
         const int K = t.k1 + t.k2;
         if (t.k1) BC(t.X1, bc_span(t.nb, t.k1, t.ld1), "cholqr X1", i);
         if (t.k2) BC(t.X2, bc_span(t.nb, t.k2, t.ld2), "cholqr X2", i);
@@ -517,16 +518,16 @@ int run_vside_r(hicma_tlr_ctx *c, std::vector<VRTask> &v, int kmax) {
 #endif
     (void)kmax;
     // one launch per width bucket (the kernel is instantiated per bucket)
-    std::vector<VRTask> b;
+    std::vector<CQTask> b;
     int lo = 0;
-    while (lo < vside_r_kmax()) {
-        const int hi = vside_r_bucket(lo + 1);
+    while (lo < cholqr3_kmax()) {
+        const int hi = cholqr3_bucket(lo + 1);
         b.clear();
         for (auto &t : v)
             if (t.k1 + t.k2 > lo && t.k1 + t.k2 <= hi) b.push_back(t);
         lo = hi;
         if (b.empty()) continue;
-        VRTask *d = stage(c, b.data(), b.size());
+        CQTask *d = stage(c, b.data(), b.size());
         if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
         double fl = 0, by = 0;
         for (auto &t : b) {
@@ -538,8 +539,8 @@ int run_vside_r(hicma_tlr_ctx *c, std::vector<VRTask> &v, int kmax) {
             by += 8.0 * t.nb * K * (t.Q ? 7.0 : 4.0);
         }
         {
-            Prof pf(c, P_VR, fl, by);
-            launch_vside_r_batched(d, (int)b.size(), hi, c->d_flags + 5, c->cur);
+            Prof pf(c, P_CHOLQR, fl, by);
+            launch_cholqr3_batched(d, (int)b.size(), hi, c->d_flags + 5, c->cur);
         }
         TRY(check_launch(c));
     }
@@ -809,7 +810,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
         std::vector<GramTask> grams;
         int *sel = thr2 > 0.0 ? ws_alloc<int>(c, 2 * (tasks.size() - i0) + 2) : nullptr;
         std::vector<QRTask> qrs;
-        std::vector<VRTask> vrs;
+        std::vector<CQTask> vrs;
         std::vector<AssembleTask> asm_;
         std::vector<CoreTask> cores;
         std::vector<QApplyTask> apps;
@@ -827,11 +828,11 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             ct.rank_task = rank_task + (i - i0);
             ct.K = K;
             if (K == 0) { cores.push_back(ct); continue; }
-            // Stacks up to vside_r_kmax() columns: both QRs by shifted CholeskyQR3
+            // Stacks up to cholqr3_kmax() columns: both QRs by shifted CholeskyQR3
             // (U side [Cu, Au] read in place with Q_U formed, V side R only);
             // wider stacks: block Gram-Schmidt + Householder on the U side and a
             // Householder QR on the V side.
-            const bool cq = c->vside_cholqr && K <= vside_r_kmax();
+            const bool cq = c->cholqr && K <= cholqr3_kmax();
             double *Vs = ws_alloc<double>(c, (size_t)nb * K);
             double *Vk = ws_alloc<double>(c, (size_t)nb * K);
             double *Us = ws_alloc<double>(c, (size_t)nb * K);    // CholeskyQR path: scratch and Q_U
@@ -864,8 +865,8 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             double *Vsrc = Vs;
             if (cq) {
                 double *RV = ws_alloc<double>(c, (size_t)K * K);
-                vrs.push_back(VRTask{t.Cu, t.Au, Us, RU, Us, nb, rc, ra, nb, nb});
-                vrs.push_back(VRTask{Vs, nullptr, Vk, RV, nullptr, nb, K, 0, nb, nb});
+                vrs.push_back(CQTask{t.Cu, t.Au, Us, RU, Us, nb, rc, ra, nb, nb});
+                vrs.push_back(CQTask{Vs, nullptr, Vk, RV, nullptr, nb, K, 0, nb, nb});
                 ct.RV = RV; ct.ldrv = K;
             } else {
                 const int pbw = qr_panel_width(nb);
@@ -972,7 +973,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             CUDA_TRY(cudaEventRecord(c->ev_join, c->stream_side));
             c->cur = bulk;
         }
-        TRY(run_vside_r(c, vrs, 0));
+        TRY(run_cholqr3(c, vrs, 0));
         TRY(run_core_buckets(c, cores, cp));
         TRY(run_gemms(c, gU));
         TRY(run_gemms(c, g3));
@@ -1153,7 +1154,7 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) return fail(e, "side stream");
     c->cur = c->stream;
-    if (const char *vs = std::getenv("HICMA_TLR_VSIDE")) c->vside_cholqr = std::strcmp(vs, "qr") != 0;
+    if (const char *q = std::getenv("HICMA_TLR_QR")) c->cholqr = std::strcmp(q, "householder") != 0;
     size_t free_b = 0, total_b = 0;
     e = cudaMemGetInfo(&free_b, &total_b);
     if (e != cudaSuccess) return fail(e, "memory info");
@@ -1645,11 +1646,11 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
         std::vector<QRTask> qy, qw;
         std::vector<QApplyTask> aq, au;
         std::vector<CoreTask> cores;
-        std::vector<VRTask> cqy, cqw;
+        std::vector<CQTask> cqy, cqw;
         std::vector<GemmTask> gu;
-        // up to vside_r_kmax() samples: both QRs by shifted CholeskyQR3 (Q of Y
+        // up to cholqr3_kmax() samples: both QRs by shifted CholeskyQR3 (Q of Y
         // formed directly, R of W only), U = Q_Y U_r as a GEMM
-        const bool cq = c->vside_cholqr && s <= vside_r_kmax();
+        const bool cq = c->cholqr && s <= cholqr3_kmax();
         size_t i = i0;
         for (; i < tasks.size(); ++i) {
             if (compress_ws_bytes(nb, s) > ws_free(c)) {
@@ -1666,9 +1667,9 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
                 double *SU = ws_alloc<double>(c, (size_t)s * s);
                 int *rt = d_rank_task_base + (i - i0);
                 gy.push_back(make_gemm(0, 0, nb, s, nb, 1.0, t.A, nb, Omega, nb, 0.0, Y, nb));
-                cqy.push_back(VRTask{Y, nullptr, Q, RY, Q, nb, s, 0, nb, nb});
+                cqy.push_back(CQTask{Y, nullptr, Q, RY, Q, nb, s, 0, nb, nb});
                 gw.push_back(make_gemm(1, 0, nb, s, nb, 1.0, t.A, nb, Q, nb, 0.0, W, nb));
-                cqw.push_back(VRTask{W, nullptr, Z, RW, nullptr, nb, s, 0, nb, nb});
+                cqw.push_back(CQTask{W, nullptr, Z, RW, nullptr, nb, s, 0, nb, nb});
                 CoreTask ct{};
                 ct.RU = nullptr; ct.RV = RW; ct.ldru = s; ct.ldrv = s;
                 ct.SU = SU; ct.RUc = nullptr; ct.work = nullptr;
@@ -1711,12 +1712,12 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
         }
         TRY(run_gemms(c, gy, false, P_GEMM_GEN));
         TRY(run_qr(c, qy, nb));
-        TRY(run_vside_r(c, cqy, 0));
+        TRY(run_cholqr3(c, cqy, 0));
         TRY(run_qapply(c, aq, nb));
         TRY(run_gemms(c, gw, false, P_GEMM_GEN));
         TRY(run_copies(c, keeps));
         TRY(run_qr(c, qw, nb));
-        TRY(run_vside_r(c, cqw, 0));
+        TRY(run_cholqr3(c, cqw, 0));
         CoreParams cp{1, tol, maxrank, 0, nb, nullptr, nullptr};
         TRY(run_core_buckets(c, cores, cp));
         TRY(run_qapply(c, au, nb));
@@ -1768,7 +1769,7 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
     for (int m = A->band; m < NT; ++m)
         for (int n = 0; n <= m - A->band; ++n) pending.push_back({m, n});
     const CovParams cp = cov_params(A, prob);
-    int s = std::min(c->vside_cholqr ? vside_r_kmax() : 160, s_full);
+    int s = std::min(c->cholqr ? cholqr3_kmax() : 160, s_full);
     while (!pending.empty()) {
         launch_set_identity(Ident, s, s, c->stream);
         TRY(check_launch(c));

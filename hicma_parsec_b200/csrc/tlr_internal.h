@@ -212,18 +212,18 @@ void launch_qapply_batched(const QApplyTask *d_tasks, int ntasks, int m_max, cud
 // QR of an nb x K matrix X = [X1 (nb x k1, ld1), X2 (nb x k2, ld2)] by
 // shifted CholeskyQR3 (one CTA per task; X is read, not changed): R (upper,
 // K x K, ld K) and, if Q is set, Q (nb x K, ld nb; may equal Z).  Z is
-// nb x K scratch (ld nb).  K = k1 + k2 <= vside_r_kmax(); fail counts tasks
+// nb x K scratch (ld nb).  K = k1 + k2 <= cholqr3_kmax(); fail counts tasks
 // whose Cholesky broke down under every shift (R left as the identity).
-struct VRTask {
+struct CQTask {
     const double *X1, *X2;
     double *Z;
     double *R;
     double *Q;
     int nb, k1, k2, ld1, ld2;
 };
-int vside_r_kmax();
-int vside_r_bucket(int K);   // width of the kernel instance that takes K
-void launch_vside_r_batched(const VRTask *d_tasks, int ntasks, int kmax, int *fail, cudaStream_t st);
+int cholqr3_kmax();
+int cholqr3_bucket(int K);   // width of the kernel instance that takes K
+void launch_cholqr3_batched(const CQTask *d_tasks, int ntasks, int kmax, int *fail, cudaStream_t st);
 
 // ------------------------------------------------------------- core SVD -----
 // M = RU RV^T (RU, RV: K x K upper from the QRs; RU == nullptr means I),

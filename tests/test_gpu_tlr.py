@@ -182,12 +182,12 @@ def test_probe_residual_matches_dense_check(ctx):
     assert 0.5 * exact <= est <= 2.0 * exact, (est, exact)
 
 
-@pytest.mark.parametrize("var,alt", [("HICMA_TLR_VSIDE", "qr")])
+@pytest.mark.parametrize("var,alt", [("HICMA_TLR_QR", "householder")])
 def test_kernel_variants_agree(monkeypatch, var, alt):
     """The default recompression against its alternative on the reference's
     own case: both QRs by shifted CholeskyQR3 for stacked ranks up to 48 (the
     default) against the block Gram-Schmidt + Householder pipeline for every
-    update (HICMA_TLR_VSIDE=qr, read when a context is created; each run is a
+    update (HICMA_TLR_QR=householder, read when a context is created; each run is a
     child process).  Same final ranks within 1, both residuals within the bar,
     log-determinants equal to 1e-10, no CholeskyQR breakdown."""
     import json
