@@ -362,7 +362,7 @@ struct ItemList {
 std::mutex g_items_mu;
 std::map<std::pair<int, long long>, ItemList> g_items;   // (device, nblk*2 + inv)
 
-const ItemList *get_items(int nblk, bool inv) {
+const ItemList *get_items(int nblk, bool inv, cudaStream_t st) {
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lk(g_items_mu);
@@ -372,7 +372,10 @@ const ItemList *get_items(int nblk, bool inv) {
     std::vector<PItem> h = build_items(nblk, inv);
     ItemList L;
     if (cudaMalloc(&L.d, h.size() * sizeof(PItem)) != cudaSuccess) { cudaGetLastError(); return nullptr; }
-    if (cudaMemcpy(L.d, h.data(), h.size() * sizeof(PItem), cudaMemcpyHostToDevice) != cudaSuccess) {
+    // ordered on the launch stream and complete before the list is used (a
+    // legacy-stream copy from pageable memory may land after the kernel reads it)
+    if (cudaMemcpyAsync(L.d, h.data(), h.size() * sizeof(PItem), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
         cudaFree(L.d);
         return nullptr;
     }
@@ -404,7 +407,7 @@ size_t potrf_tile_scratch_ints(int n) {
 int launch_potrf_tile(double *A, int lda, int n, double *X, int ldx, double *D, int *cnt, int *info,
                       int info_base, int *timeout, int grid, cudaStream_t st) {
     const int nblk = (n + TB - 1) / TB;
-    const ItemList *L = get_items(nblk, X != nullptr);
+    const ItemList *L = get_items(nblk, X != nullptr, st);
     if (!L) return -1;
     if (cudaMemsetAsync(cnt, 0, potrf_tile_scratch_ints(n) * sizeof(int), st) != cudaSuccess) return -1;
     const int smem = (int)sizeof(double) * (2 * TB * TPITCH > 2 * TB * LDS + 32 * 32 + TB ? 2 * TB * TPITCH

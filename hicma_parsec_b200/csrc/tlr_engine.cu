@@ -211,12 +211,27 @@ int ctx_sync(hicma_tlr_ctx *c) {
 
 void ws_reset(hicma_tlr_ctx *c) { c->ar->off = 0; }
 
+// Host <-> device transfers and clears, ordered on the context stream and
+// complete on return.  (cudaMemcpy and cudaMemset run on the legacy default
+// stream, which the context's non-blocking streams do not wait for, and a
+// cudaMemcpy from pageable host memory may return before its data has
+// landed: a kernel launched next on the context stream could then read the
+// old contents, or have its results overwritten by the late copy.)
+cudaError_t xfer(hicma_tlr_ctx *c, void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, c->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(c->stream) : e;
+}
+cudaError_t xclear(hicma_tlr_ctx *c, void *dst, size_t bytes) {
+    cudaError_t e = cudaMemsetAsync(dst, 0, bytes, c->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(c->stream) : e;
+}
+
 // After a synchronisation: report (and clear) a bounded device wait that gave up.
 int check_timeout(hicma_tlr_ctx *c) {
     int f = 0;
-    CUDA_TRY(cudaMemcpy(&f, c->d_flags + 3, sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(xfer(c, &f, c->d_flags + 3, sizeof(int), cudaMemcpyDeviceToHost));
     if (f) {
-        CUDA_TRY(cudaMemset(c->d_flags + 3, 0, sizeof(int)));
+        CUDA_TRY(xclear(c, c->d_flags + 3, sizeof(int)));
         set_err("a bounded device wait gave up (tile POTRF task queue)");
         return HICMA_TLR_ERR_TIMEOUT;
     }
@@ -1187,7 +1202,7 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     bc_add(c->d_stage, c->stage_bytes);
     bc_add(c->d_flags, 64 * sizeof(int));
     bc_add(c->d_scal, 64 * sizeof(double));
-    if ((e = cudaMemset(c->d_flags, 0, 64 * sizeof(int))) != cudaSuccess) return fail(e, "flags reset");
+    if ((e = xclear(c, c->d_flags, 64 * sizeof(int))) != cudaSuccess) return fail(e, "flags reset");
     if ((e = cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
         return fail(e, "SM count");
     *out = c;
@@ -1319,7 +1334,7 @@ int hicma_tlr_autotune(hicma_tlr_ctx *c, int NB, int maxrank, int reps, int *tun
         if (ms < best_t) { best_t = ms; best_g = grids[gi]; }
     }
     int hinfo = 0;
-    CUDA_TRY(cudaMemcpy(&hinfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(xfer(c, &hinfo, dinfo, sizeof(int), cudaMemcpyDeviceToHost));
     if (hinfo != 0) { restore(); set_err("autotune: test tile not positive definite (info %d)", hinfo); return HICMA_TLR_ERR_STATE; }
     TRY(check_timeout(c));
 
@@ -1419,7 +1434,7 @@ int hicma_tlr_desc_create(hicma_tlr_ctx *c, int N, int NB, int maxrank, int band
     A->h_rank.assign((size_t)NT * NT, -1);
     for (int m = 0; m < NT; ++m)
         for (int n = 0; n <= m - A->band; ++n) A->h_rank[(size_t)n * NT + m] = 0;
-    const cudaError_t e = cudaMemcpy(A->d_rank, A->h_rank.data(), (size_t)NT * NT * sizeof(int), cudaMemcpyHostToDevice);
+    const cudaError_t e = xfer(c, A->d_rank, A->h_rank.data(), (size_t)NT * NT * sizeof(int), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         set_err("rank map upload: %s", cudaGetErrorString(e));
         dev_free(c, A->d_band); dev_free(c, A->d_lr); dev_free(c, A->d_rank);
@@ -1799,7 +1814,7 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
         }
         if (s >= s_full) break;
         TRY(ctx_sync(c));
-        CUDA_TRY(cudaMemcpy(A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
+        CUDA_TRY(xfer(c, A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
         std::vector<std::pair<int, int>> more;
         const int margin = std::max(32, s / 4);
         for (auto &t : pending) {
@@ -1810,7 +1825,7 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
         s = std::min(2 * s, s_full);
     }
     TRY(ctx_sync(c));
-    CUDA_TRY(cudaMemcpy(A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(xfer(c, A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
     int bad = 0;
     for (int m = A->band; m < NT; ++m)
         for (int n = 0; n <= m - A->band; ++n)
@@ -1826,7 +1841,7 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
         for (int m = A->band; m < NT; ++m)
             for (int n = 0; n <= m - A->band; ++n)
                 if (A->h_rank[(size_t)n * NT + m] < 0) A->h_rank[(size_t)n * NT + m] = 0;
-        CUDA_TRY(cudaMemcpy(A->d_rank, A->h_rank.data(), (size_t)NT * NT * sizeof(int), cudaMemcpyHostToDevice));
+        CUDA_TRY(xfer(c, A->d_rank, A->h_rank.data(), (size_t)NT * NT * sizeof(int), cudaMemcpyHostToDevice));
         if (info) *info = -1;
     }
     A->factored = false;
@@ -2290,9 +2305,9 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         have_end = true;
         TRY(ctx_sync(c));
         int hinfo = 0;
-        CUDA_TRY(cudaMemcpy(&hinfo, d_info, sizeof(int), cudaMemcpyDeviceToHost));
+        CUDA_TRY(xfer(c, &hinfo, d_info, sizeof(int), cudaMemcpyDeviceToHost));
         if (!rec.empty()) {
-            CUDA_TRY(cudaMemcpy(A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
+            CUDA_TRY(xfer(c, A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
             // each tile takes at most one update per panel, so per-panel minima
             // and maxima are the per-update ones of the reference
             for (const auto &mt : rec_meta) {
@@ -2349,9 +2364,9 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     cudaEventDestroy(evEnd);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     int flags_h[6] = {0, 0, 0, 0, 0, 0};
-    CUDA_TRY(cudaMemcpy(flags_h, c->d_flags, 6 * sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(xfer(c, flags_h, c->d_flags, 6 * sizeof(int), cudaMemcpyDeviceToHost));
     if (flags_h[3]) {
-        cudaMemset(c->d_flags + 3, 0, sizeof(int));
+        xclear(c, c->d_flags + 3, sizeof(int));
         set_err("a bounded device wait gave up (tile POTRF task queue)");
         return HICMA_TLR_ERR_TIMEOUT;
     }
@@ -2454,14 +2469,14 @@ int hicma_tlr_tile_get(hicma_tlr_ctx *c, hicma_tlr_desc *A, int m, int n, double
     TRY(ctx_sync(c));
     if (A->is_dense(m, n)) {
         if (rank) *rank = -1;
-        if (buf) CUDA_TRY(cudaMemcpy(buf, A->dense(m, n), NB * NB * sizeof(double), cudaMemcpyDeviceToHost));
+        if (buf) CUDA_TRY(xfer(c, buf, A->dense(m, n), NB * NB * sizeof(double), cudaMemcpyDeviceToHost));
         return 0;
     }
     const int r = A->rank(m, n);
     if (rank) *rank = r;
     if (buf && r > 0) {
-        CUDA_TRY(cudaMemcpy(buf, A->U(m, n), NB * r * sizeof(double), cudaMemcpyDeviceToHost));
-        CUDA_TRY(cudaMemcpy(buf + NB * r, A->V(m, n), NB * r * sizeof(double), cudaMemcpyDeviceToHost));
+        CUDA_TRY(xfer(c, buf, A->U(m, n), NB * r * sizeof(double), cudaMemcpyDeviceToHost));
+        CUDA_TRY(xfer(c, buf + NB * r, A->V(m, n), NB * r * sizeof(double), cudaMemcpyDeviceToHost));
     }
     return 0;
 }
@@ -2473,17 +2488,17 @@ int hicma_tlr_tile_set(hicma_tlr_ctx *c, hicma_tlr_desc *A, int m, int n, const 
     const size_t NB = A->NB, NT = A->NT;
     TRY(ctx_sync(c));
     if (A->is_dense(m, n)) {
-        CUDA_TRY(cudaMemcpy(A->dense(m, n), buf, NB * NB * sizeof(double), cudaMemcpyHostToDevice));
+        CUDA_TRY(xfer(c, A->dense(m, n), buf, NB * NB * sizeof(double), cudaMemcpyHostToDevice));
         A->factored = false;   // the held factor no longer belongs to this matrix
         return 0;
     }
     ARG_CHECK(rank >= 0 && rank <= A->maxrank, "rank in [0, maxrank]");
     if (rank > 0) {
-        CUDA_TRY(cudaMemcpy(A->U(m, n), buf, NB * rank * sizeof(double), cudaMemcpyHostToDevice));
-        CUDA_TRY(cudaMemcpy(A->V(m, n), buf + NB * rank, NB * rank * sizeof(double), cudaMemcpyHostToDevice));
+        CUDA_TRY(xfer(c, A->U(m, n), buf, NB * rank * sizeof(double), cudaMemcpyHostToDevice));
+        CUDA_TRY(xfer(c, A->V(m, n), buf + NB * rank, NB * rank * sizeof(double), cudaMemcpyHostToDevice));
     }
     A->h_rank[(size_t)n * NT + m] = rank;
-    CUDA_TRY(cudaMemcpy(A->d_rank + (size_t)n * NT + m, &rank, sizeof(int), cudaMemcpyHostToDevice));
+    CUDA_TRY(xfer(c, A->d_rank + (size_t)n * NT + m, &rank, sizeof(int), cudaMemcpyHostToDevice));
     A->factored = false;
     return 0;
 }
@@ -3025,7 +3040,8 @@ int hicma_tlr_k_wait_probe(long long polls0, long long polls1, int nblocks, doub
     if (e == cudaSuccess) e = cudaEventRecord(e1, st);
     if (e == cudaSuccess) e = cudaEventSynchronize(e1);
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-    if (e == cudaSuccess) e = cudaMemcpy(flags, buf, 3 * sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(flags, buf, 3 * sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaFree(buf);
