@@ -15,7 +15,7 @@
 //   pass 0: G = D^-1 X^T X D^-1 + s I,  R1 = chol(G)
 //   pass 1: X1 = X D^-1 R1^-1 (written to scratch), G = X1^T X1, R2 = chol(G)
 //   pass 2: X2 = X1 R2^-1 (stored when Q is wanted), G = X2^T X2, R3 = chol(G)
-//   pass 3: Q = X2 R3^-1 (only when Q is wanted)
+//   pass 3: Q = X2 R3^-1 (only when Q is wanted; or X2 kept with R3^-1 out)
 //   R = R3 R2 R1 D,
 // s = 11 (m K + K (K + 1)) u tr(G); passes 1 and 2 add the same shift only if
 // the plain Cholesky breaks down.  X R^-1 is a row-wise substitution (the
@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(CQ_THREADS, KM <= 32 ? 2 : 1) k_cholqr3(const 
                 // pass 1 stores X1, pass 2 X2 (when Q is wanted), pass 3 Q: each
                 // lane rewrites only the row it read
                 double *dst = pass == 3 ? t.Q : t.Z;
-                if (valid && (pass == 1 || pass == 3 || (pass == 2 && t.Q))) {
+                if (valid && (pass == 1 || pass == 3 || (pass == 2 && (t.Q || t.Rinv)))) {
 #pragma unroll
                     for (int j = 0; j < KM; ++j)
                         if (j < K) dst[(size_t)row + (size_t)j * nb] = x[j];
@@ -331,22 +331,20 @@ __global__ void __launch_bounds__(CQ_THREADS, KM <= 32 ? 2 : 1) k_cholqr3(const 
         __syncthreads();
         for (int j = tid; j < KM; j += CQ_THREADS) rdg[j] = j < K ? 1.0 / Rr[j * KM + j] : 0.0;
         if (pass == 0) {
-            for (int idx = tid; idx < KM * KM; idx += CQ_THREADS) {
-                const int i = idx % KM, j = idx / KM;
-                Rt[idx] = Rr[i * KM + j];
-            }
+            for (int idx = tid; idx < KM * KM; idx += CQ_THREADS) Rt[idx] = Rr[idx];
         } else {
-            // Rt <- R Rt (upper times upper) through the scratch
+            // Rt <- R Rt (upper times upper, both row-major; consecutive threads
+            // take consecutive columns: R read as a broadcast, Rt conflict-free)
             for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
-                const int i = idx % K, j = idx / K;
+                const int i = idx / K, j = idx % K;
                 double s = 0.0;
-                for (int k = i; k <= j; ++k) s += Rr[i * KM + k] * Rt[k + j * KM];
-                Gc[i + j * KM] = i <= j ? s : 0.0;
+                for (int k = i; k <= j; ++k) s += Rr[i * KM + k] * Rt[k * KM + j];
+                Gc[i * KM + j] = i <= j ? s : 0.0;
             }
             __syncthreads();
             for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
-                const int i = idx % K, j = idx / K;
-                Rt[i + j * KM] = Gc[i + j * KM];
+                const int i = idx / K, j = idx % K;
+                Rt[i * KM + j] = Gc[i * KM + j];
             }
         }
         __syncthreads();
@@ -359,7 +357,35 @@ __global__ void __launch_bounds__(CQ_THREADS, KM <= 32 ? 2 : 1) k_cholqr3(const 
     // R = Rt D (dsc holds 1/d)
     for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
         const int i = idx % K, j = idx / K;
-        t.R[i + (size_t)j * K] = i <= j ? Rt[i + j * KM] / dsc[j] : 0.0;
+        t.R[i + (size_t)j * K] = i <= j ? Rt[i * KM + j] / dsc[j] : 0.0;
+    }
+    // Q deferred: X2 stays in Z and R3^-1 (R3 is the last pass's factor, still
+    // in Rr, close to the identity) goes out, so the caller forms Q times a
+    // small matrix as X2 (R3^-1 S) instead of a fourth pass over the rows.
+    // One warp, rows of the inverse from the bottom up (lanes over columns),
+    // built row-major in the scratch and written out column-major.
+    if (t.Rinv && !t.Q) {
+        if (warp == 0) {
+            for (int i = K - 1; i >= 0; --i) {
+                for (int c = lane; c < K; c += 32) {
+                    double v = 0.0;
+                    if (c == i) {
+                        v = rdg[i];
+                    } else if (c > i) {
+                        double acc = 0.0;
+                        for (int l = i + 1; l <= c; ++l) acc += Rr[i * KM + l] * Gc[l * KM + c];
+                        v = -acc * rdg[i];
+                    }
+                    Gc[i * KM + c] = v;
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
+            const int i = idx % K, c = idx / K;
+            t.Rinv[i + (size_t)c * K] = Gc[i * KM + c];
+        }
     }
 }
 

@@ -529,6 +529,7 @@ int run_cholqr3(hicma_tlr_ctx *c, std::vector<CQTask> &v, int kmax) {
         BC(t.Z, bc_span(t.nb, K, t.nb), "cholqr scratch", i);
         BC(t.R, bc_span(K, K, K), "cholqr R", i);
         if (t.Q) BC(t.Q, bc_span(t.nb, K, t.nb), "cholqr Q", i);
+        if (t.Rinv) BC(t.Rinv, bc_span(K, K, K), "cholqr R3 inverse", i);
     }
 #endif
     (void)kmax;
@@ -550,8 +551,9 @@ int run_cholqr3(hicma_tlr_ctx *c, std::vector<CQTask> &v, int kmax) {
             // FMAs each), a third substitution when Q is formed
             const double K = t.k1 + t.k2;
             fl += 3.0 * t.nb * K * K + (t.Q ? 3.0 : 2.0) * t.nb * K * K;
-            // X read twice, scratch written and read once (Q: X2 and Q written, X2 read)
-            by += 8.0 * t.nb * K * (t.Q ? 7.0 : 4.0);
+            // X read twice, scratch written and read once (Q: X2 and Q written, X2 read;
+            // deferred Q: X2 written)
+            by += 8.0 * t.nb * K * (t.Q ? 7.0 : (t.Rinv ? 5.0 : 4.0));
         }
         {
             Prof pf(c, P_CHOLQR, fl, by);
@@ -773,7 +775,7 @@ size_t recomp_ws_bytes(int nb, const RecompTask &t) {
     b += A((size_t)nb * K) * 3;                          // Us = [Cu | Wu], Vs = [Cv | -Y], Vk
     b += A(ra) + A(K) + A(npa * pb * pb) + A(npk * pb * pb);  // tau, T factors of Wu and Vs
     b += A((size_t)rc * ra) * 2;                         // Pu, Pu2
-    b += A((size_t)K * K) * 4;                           // RU, SU, T1, RV
+    b += A((size_t)K * K) * 6;                           // RU, SU, T1, RV, R3^-1 and R3^-1 U_r
     if (K > core_smem_kmax()) b += A(core_work_doubles(K));
     if (t.Bv) b += A((size_t)t.rb * t.ra);
     return b + 1024;
@@ -818,7 +820,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
         // CholeskyQR chain (F) there and the Householder chain of the wide
         // updates (S) on the side stream, joined at the end of the chunk
         std::vector<CopyTask> copies, copiesS, keeps;
-        std::vector<GemmTask> g1, g2, g1s, g2s, gU, g3, g4, gUS, g3S, g4S;
+        std::vector<GemmTask> g1, g2, g1s, g2s, gTU, gU, g3, g4, gUS, g3S, g4S;
         std::vector<CoreTask> coresS;
         std::vector<ProjTask> projs;
         std::vector<SelTask> sels;
@@ -878,9 +880,14 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                 }
             }
             double *Vsrc = Vs;
+            double *RinvU = nullptr, *TU = nullptr;
             if (cq) {
                 double *RV = ws_alloc<double>(c, (size_t)K * K);
-                vrs.push_back(CQTask{t.Cu, t.Au, Us, RU, Us, nb, rc, ra, nb, nb});
+                RinvU = ws_alloc<double>(c, (size_t)K * K);
+                TU = ws_alloc<double>(c, (size_t)K * K);
+                CQTask u{t.Cu, t.Au, Us, RU, nullptr, nb, rc, ra, nb, nb};
+                u.Rinv = RinvU;          // Q_U = X2 R3^-1 formed inside the output product
+                vrs.push_back(u);
                 vrs.push_back(CQTask{Vs, nullptr, Vk, RV, nullptr, nb, K, 0, nb, nb});
                 ct.RV = RV; ct.ldrv = K;
             } else {
@@ -908,8 +915,11 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             ct.SU = SU; ct.RUc = nullptr; ct.work = work;
             (cq ? cores : coresS).push_back(ct);
             if (cq) {
-                // new U = Q_U U_r
-                GemmTask u = make_gemm(0, 0, nb, maxrank, K, 1.0, Us, nb, SU, K, 0.0, t.outU, nb);
+                // new U = Q_U U_r = X2 (R3^-1 U_r)
+                GemmTask tu = make_gemm(0, 0, K, maxrank, K, 1.0, RinvU, K, SU, K, 0.0, TU, K);
+                tu.n_dev = ct.rank_task;
+                gTU.push_back(tu);
+                GemmTask u = make_gemm(0, 0, nb, maxrank, K, 1.0, Us, nb, TU, K, 0.0, t.outU, nb);
                 u.n_dev = ct.rank_task;
                 gU.push_back(u);
             } else if (rc > 0) {
@@ -990,6 +1000,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
         }
         TRY(run_cholqr3(c, vrs, 0));
         TRY(run_core_buckets(c, cores, cp));
+        TRY(run_gemms(c, gTU));
         TRY(run_gemms(c, gU));
         TRY(run_gemms(c, g3));
         TRY(run_gemms(c, g4));

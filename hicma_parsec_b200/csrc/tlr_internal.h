@@ -211,15 +211,18 @@ void launch_qapply_batched(const QApplyTask *d_tasks, int ntasks, int m_max, cud
 
 // QR of an nb x K matrix X = [X1 (nb x k1, ld1), X2 (nb x k2, ld2)] by
 // shifted CholeskyQR3 (one CTA per task; X is read, not changed): R (upper,
-// K x K, ld K) and, if Q is set, Q (nb x K, ld nb; may equal Z).  Z is
-// nb x K scratch (ld nb).  K = k1 + k2 <= cholqr3_kmax(); fail counts tasks
-// whose Cholesky broke down under every shift (R left as the identity).
+// K x K, ld K) and, if Q is set, Q (nb x K, ld nb; may equal Z).  With Rinv
+// set instead (and Q null) the last pass is not run: Z keeps X2 and Rinv
+// (K x K, ld K) receives R3^-1, so that Q = Z Rinv.  Z is nb x K scratch
+// (ld nb).  K = k1 + k2 <= cholqr3_kmax(); fail counts tasks whose Cholesky
+// broke down under every shift (R left as the identity).
 struct CQTask {
     const double *X1, *X2;
     double *Z;
     double *R;
     double *Q;
     int nb, k1, k2, ld1, ld2;
+    double *Rinv = nullptr;
 };
 int cholqr3_kmax();
 int cholqr3_bucket(int K);   // width of the kernel instance that takes K
