@@ -426,7 +426,7 @@ def run_ours(args, cfg):
                "k_qr": (prof["qr"], "fp64"), "k_qapply": (prof["qapply"], "fp64"),
                "k_core_svd": (prof["core_svd"], "fp64"), "k_bcgs2": (prof["proj"], "tensor"),
                "k_copy_batched": (prof["copy"], "hbm"), "k_gram_batched": (prof["gram"], "tensor"),
-               "k_cholqr3": (prof["cholqr3"], "tensor")}
+               "k_rcholqr": (prof["rcholqr"], "tensor")}
     dom = max(kernels, key=lambda k: kernels[k][0]["seconds"])
     pd, kind = kernels[dom]
     launches = int(st[3])  # kernel launches of one factorization (engine counter)
@@ -576,7 +576,7 @@ def run_ours(args, cfg):
                 "dense_equiv_gflops": (n ** 3 / 3.0) / s_per_factor / 1e9,
                 "phase_s": {"potrf": st[4], "trsm": st[5], "syrk": st[6], "gemm_recompress": st[7],
                             "device_idle_between_panels": st[12]},
-                "cholqr3_breakdowns": int(st[11]),
+                "cholqr_null_pivots": int(st[11]), "cholqr_repeated_passes": int(st[14]),
                 "jacobi_sweeps_total": st[8],
                 "kernel_classes": prof, "gpu_launches": launches * args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "accuracy": accuracy,

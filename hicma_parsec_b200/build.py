@@ -26,7 +26,7 @@ OBJ_CHECKED = os.path.join(OBJ, "checked")
 CHECKED_SOURCES = ["tlr_engine.cu", "serve.cu", "k_potrf.cu"]
 CLI_SRC = os.path.join(HERE, "cli", "testing_dpotrf_tlr.c")
 CLI = os.path.join(LIBDIR, "testing_dpotrf_tlr")
-SOURCES = ["k_gemm.cu", "k_tile.cu", "k_potrf.cu", "k_potrf_tile.cu", "k_qr.cu", "k_cholqr.cu", "k_proj.cu", "k_svd.cu",
+SOURCES = ["k_gemm.cu", "k_tile.cu", "k_potrf.cu", "k_potrf_tile.cu", "k_qr.cu", "k_rcholqr.cu", "k_proj.cu", "k_svd.cu",
            "tlr_engine.cu", "serve.cu"]
 HEADERS = ["tlr_internal.h"]
 

@@ -138,13 +138,13 @@ struct hicma_tlr_ctx_s {
     char *h_stage = nullptr, *d_stage = nullptr;
     size_t stage_bytes = 0, stage_off = 0;
     int *d_flags = nullptr;     // [0] info, [1] overflow, [2] Jacobi sweeps, [3] wait timed out, [4] FP32 updates,
-                                // [5] V-side CholeskyQR breakdowns
+                                // [5] CholeskyQR null pivots, [6] CholeskyQR passes repeated
     int nsm = 148;              // SM count of the device
     // choices the autotuner measures (defaults: the hand-picked values)
     int gemm_narrow_n = GEMM_NARROW_N;   // rank-wide outputs up to this width use 128 x 32 tiles
     int potrf_grid = 0;                  // CTAs of the persistent tile POTRF (0: one per SM)
-    // QRs of the recompressions: shifted CholeskyQR3 on both sides for stacked
-    // ranks up to cholqr3_kmax() and the generation range finder up to that many samples
+    // QRs of the recompressions: randomized CholeskyQR on both sides for stacked
+    // ranks up to rcholqr_kmax() and the generation range finder up to that many samples
     // (1), the Householder pipeline for all (0; HICMA_TLR_QR=householder)
     int cholqr = 1;
     double *d_scal = nullptr;   // device scalars
@@ -279,7 +279,7 @@ enum {
     // batched DMMA GEMMs by call site (P_GEMM: recompression outputs and the rest)
     P_GEMM_Y, P_GEMM_TRSM, P_GEMM_SYRK, P_GEMM_DENSE, P_GEMM_GEN,
     P_GRAM,   // split-K inner products B_V^T A_V of the recompressions
-    P_CHOLQR,     // V-side R factors by shifted CholeskyQR3
+    P_CHOLQR,     // QR factors by randomized CholeskyQR
     P_NCLASS
 };
 
@@ -518,7 +518,7 @@ int run_qr(hicma_tlr_ctx *c, std::vector<QRTask> &v, int m_max) {
     return check_launch(c);
 }
 
-int run_cholqr3(hicma_tlr_ctx *c, std::vector<CQTask> &v, int kmax) {
+int run_rcholqr(hicma_tlr_ctx *c, std::vector<CQTask> &v, int kmax) {
     if (v.empty()) return 0;
 #ifdef TLR_BOUNDS_CHECK
     for (size_t i = 0; i < v.size(); ++i) {
@@ -526,18 +526,25 @@ int run_cholqr3(hicma_tlr_ctx *c, std::vector<CQTask> &v, int kmax) {
         const int K = t.k1 + t.k2;
         if (t.k1) BC(t.X1, bc_span(t.nb, t.k1, t.ld1), "cholqr X1", i);
         if (t.k2) BC(t.X2, bc_span(t.nb, t.k2, t.ld2), "cholqr X2", i);
-        BC(t.Z, bc_span(t.nb, K, t.nb), "cholqr scratch", i);
+        if (t.Q || t.Rinv) BC(t.Z, bc_span(t.nb, K, t.nb), "cholqr Y", i);
         BC(t.R, bc_span(K, K, K), "cholqr R", i);
         if (t.Q) BC(t.Q, bc_span(t.nb, K, t.nb), "cholqr Q", i);
         if (t.Rinv) BC(t.Rinv, bc_span(K, K, K), "cholqr R3 inverse", i);
     }
 #endif
     (void)kmax;
+    // all tasks form Q or none does (the kernel is instantiated both ways)
+    const bool form_q = v[0].Q != nullptr;
+    for (auto &t : v)
+        if ((t.Q != nullptr) != form_q || (form_q && t.Rinv)) {
+            set_err("CholeskyQR batch mixes tasks that form Q with tasks that do not");
+            return HICMA_TLR_ERR_ARG;
+        }
     // one launch per width bucket (the kernel is instantiated per bucket)
     std::vector<CQTask> b;
     int lo = 0;
-    while (lo < cholqr3_kmax()) {
-        const int hi = cholqr3_bucket(lo + 1);
+    while (lo < rcholqr_kmax()) {
+        const int hi = rcholqr_bucket(lo + 1);
         b.clear();
         for (auto &t : v)
             if (t.k1 + t.k2 > lo && t.k1 + t.k2 <= hi) b.push_back(t);
@@ -547,17 +554,18 @@ int run_cholqr3(hicma_tlr_ctx *c, std::vector<CQTask> &v, int kmax) {
         if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
         double fl = 0, by = 0;
         for (auto &t : b) {
-            // three Gram products (K^2 nb each, symmetric) and two row substitutions (K^2 nb / 2
-            // FMAs each), a third substitution when Q is formed
-            const double K = t.k1 + t.k2;
-            fl += 3.0 * t.nb * K * K + (t.Q ? 3.0 : 2.0) * t.nb * K * K;
-            // X read twice, scratch written and read once (Q: X2 and Q written, X2 read;
-            // deferred Q: X2 written)
-            by += 8.0 * t.nb * K * (t.Q ? 7.0 : (t.Rinv ? 5.0 : 4.0));
+            // the sketch (nb K FMAs); shifted CholeskyQR3 of the 256 sketch rows (three Gram
+            // products, K^2 m each, symmetric; two row substitutions, K^2 m / 2 FMAs each); one
+            // pass over the rows (substitution and Gram product), and the Q substitution when Q
+            // is formed
+            const double K = t.k1 + t.k2, m = 256.0;
+            fl += 2.0 * t.nb * K + 5.0 * m * K * K + (t.Q ? 3.0 : 2.0) * t.nb * K * K;
+            // X read twice; Y written when kept; Y read and Q written when Q is formed
+            by += 8.0 * t.nb * K * (2.0 + (t.Q || t.Rinv ? 1.0 : 0.0) + (t.Q ? 2.0 : 0.0));
         }
         {
             Prof pf(c, P_CHOLQR, fl, by);
-            launch_cholqr3_batched(d, (int)b.size(), hi, c->d_flags + 5, c->cur);
+            launch_rcholqr_batched(d, (int)b.size(), hi, form_q, c->d_flags + 5, c->cur);
         }
         TRY(check_launch(c));
     }
@@ -845,14 +853,13 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             ct.rank_task = rank_task + (i - i0);
             ct.K = K;
             if (K == 0) { cores.push_back(ct); continue; }
-            // Stacks up to cholqr3_kmax() columns: both QRs by shifted CholeskyQR3
-            // (U side [Cu, Au] read in place with Q_U formed, V side R only);
-            // wider stacks: block Gram-Schmidt + Householder on the U side and a
-            // Householder QR on the V side.
-            const bool cq = c->cholqr && K <= cholqr3_kmax();
+            // Stacks up to rcholqr_kmax() columns: both QRs by randomized
+            // CholeskyQR (U side [Cu, Au] read in place, Q_U = Y Rc^-1 kept
+            // factored; V side R only); wider stacks: block Gram-Schmidt +
+            // Householder on the U side and a Householder QR on the V side.
+            const bool cq = c->cholqr && K <= rcholqr_kmax();
             double *Vs = ws_alloc<double>(c, (size_t)nb * K);
-            double *Vk = ws_alloc<double>(c, (size_t)nb * K);
-            double *Us = ws_alloc<double>(c, (size_t)nb * K);    // CholeskyQR path: scratch and Q_U
+            double *Us = ws_alloc<double>(c, (size_t)nb * K);    // CholeskyQR path: Y of the U side
             double *RU = ws_alloc<double>(c, (size_t)K * K);
             double *SU = ws_alloc<double>(c, (size_t)K * K), *T1 = ws_alloc<double>(c, (size_t)K * K);
             double *work = K > core_smem_kmax() ? ws_alloc<double>(c, core_work_doubles(K)) : nullptr;
@@ -886,11 +893,12 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                 RinvU = ws_alloc<double>(c, (size_t)K * K);
                 TU = ws_alloc<double>(c, (size_t)K * K);
                 CQTask u{t.Cu, t.Au, Us, RU, nullptr, nb, rc, ra, nb, nb};
-                u.Rinv = RinvU;          // Q_U = X2 R3^-1 formed inside the output product
+                u.Rinv = RinvU;          // Q_U = Y Rc^-1 formed inside the output product
                 vrs.push_back(u);
-                vrs.push_back(CQTask{Vs, nullptr, Vk, RV, nullptr, nb, K, 0, nb, nb});
+                vrs.push_back(CQTask{Vs, nullptr, nullptr, RV, nullptr, nb, K, 0, nb, nb});
                 ct.RV = RV; ct.ldrv = K;
             } else {
+                double *Vk = ws_alloc<double>(c, (size_t)nb * K);
                 const int pbw = qr_panel_width(nb);
                 const size_t npk = (size_t)(K + pbw - 1) / pbw + 1, npa = (size_t)(ra + pbw - 1) / pbw + 1;
                 double *tauU = ws_alloc<double>(c, ra), *tauV = ws_alloc<double>(c, K);
@@ -998,7 +1006,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             CUDA_TRY(cudaEventRecord(c->ev_join, c->stream_side));
             c->cur = bulk;
         }
-        TRY(run_cholqr3(c, vrs, 0));
+        TRY(run_rcholqr(c, vrs, 0));
         TRY(run_core_buckets(c, cores, cp));
         TRY(run_gemms(c, gTU));
         TRY(run_gemms(c, gU));
@@ -1674,9 +1682,9 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
         std::vector<CoreTask> cores;
         std::vector<CQTask> cqy, cqw;
         std::vector<GemmTask> gu;
-        // up to cholqr3_kmax() samples: both QRs by shifted CholeskyQR3 (Q of Y
-        // formed directly, R of W only), U = Q_Y U_r as a GEMM
-        const bool cq = c->cholqr && s <= cholqr3_kmax();
+        // up to rcholqr_kmax() samples: both QRs by randomized CholeskyQR (Q of
+        // Y formed, R of W only), U = Q_Y U_r as a GEMM
+        const bool cq = c->cholqr && s <= rcholqr_kmax();
         size_t i = i0;
         for (; i < tasks.size(); ++i) {
             if (compress_ws_bytes(nb, s) > ws_free(c)) {
@@ -1688,14 +1696,13 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
                 double *Y = ws_alloc<double>(c, (size_t)nb * s);
                 double *Q = ws_alloc<double>(c, (size_t)nb * s);
                 double *W = ws_alloc<double>(c, (size_t)nb * s);
-                double *Z = ws_alloc<double>(c, (size_t)nb * s);
                 double *RY = ws_alloc<double>(c, (size_t)s * s), *RW = ws_alloc<double>(c, (size_t)s * s);
                 double *SU = ws_alloc<double>(c, (size_t)s * s);
                 int *rt = d_rank_task_base + (i - i0);
                 gy.push_back(make_gemm(0, 0, nb, s, nb, 1.0, t.A, nb, Omega, nb, 0.0, Y, nb));
                 cqy.push_back(CQTask{Y, nullptr, Q, RY, Q, nb, s, 0, nb, nb});
                 gw.push_back(make_gemm(1, 0, nb, s, nb, 1.0, t.A, nb, Q, nb, 0.0, W, nb));
-                cqw.push_back(CQTask{W, nullptr, Z, RW, nullptr, nb, s, 0, nb, nb});
+                cqw.push_back(CQTask{W, nullptr, nullptr, RW, nullptr, nb, s, 0, nb, nb});
                 CoreTask ct{};
                 ct.RU = nullptr; ct.RV = RW; ct.ldru = s; ct.ldrv = s;
                 ct.SU = SU; ct.RUc = nullptr; ct.work = nullptr;
@@ -1738,12 +1745,12 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
         }
         TRY(run_gemms(c, gy, false, P_GEMM_GEN));
         TRY(run_qr(c, qy, nb));
-        TRY(run_cholqr3(c, cqy, 0));
+        TRY(run_rcholqr(c, cqy, 0));
         TRY(run_qapply(c, aq, nb));
         TRY(run_gemms(c, gw, false, P_GEMM_GEN));
         TRY(run_copies(c, keeps));
         TRY(run_qr(c, qw, nb));
-        TRY(run_cholqr3(c, cqw, 0));
+        TRY(run_rcholqr(c, cqw, 0));
         CoreParams cp{1, tol, maxrank, 0, nb, nullptr, nullptr};
         TRY(run_core_buckets(c, cores, cp));
         TRY(run_qapply(c, au, nb));
@@ -1795,7 +1802,7 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
     for (int m = A->band; m < NT; ++m)
         for (int n = 0; n <= m - A->band; ++n) pending.push_back({m, n});
     const CovParams cp = cov_params(A, prob);
-    int s = std::min(c->cholqr ? cholqr3_kmax() : 160, s_full);
+    int s = std::min(c->cholqr ? rcholqr_kmax() : 160, s_full);
     while (!pending.empty()) {
         launch_set_identity(Ident, s, s, c->stream);
         TRY(check_launch(c));
@@ -2090,7 +2097,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         for (int m = n + band; m < NT; ++m) A->rk_init[(size_t)n * NT + m] = A->rank(m, n);
     A->rk_min = A->rk_init;
     A->rk_max = A->rk_init;
-    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 6 * sizeof(int), c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->d_flags, 0, 7 * sizeof(int), c->stream));
     TRY(ctx_sync(c));
     int *d_info = c->d_flags;
     int *rtask = ws_alloc<int>(c, (size_t)NT * NT + 16);
@@ -2374,8 +2381,8 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     cudaEventDestroy(evT);
     cudaEventDestroy(evEnd);
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-    int flags_h[6] = {0, 0, 0, 0, 0, 0};
-    CUDA_TRY(xfer(c, flags_h, c->d_flags, 6 * sizeof(int), cudaMemcpyDeviceToHost));
+    int flags_h[7] = {0, 0, 0, 0, 0, 0, 0};
+    CUDA_TRY(xfer(c, flags_h, c->d_flags, 7 * sizeof(int), cudaMemcpyDeviceToHost));
     if (flags_h[3]) {
         xclear(c, c->d_flags + 3, sizeof(int));
         set_err("a bounded device wait gave up (tile POTRF task queue)");
@@ -2402,6 +2409,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     A->stats[11] = flags_h[5];
     A->stats[12] = t_gap;
     A->stats[13] = NT;
+    A->stats[14] = flags_h[6];
     A->factored = (info == 0);
     c->main_ar.off = 0;
     c->hi_ar.off = 0;

@@ -210,12 +210,15 @@ struct QApplyTask {
 void launch_qapply_batched(const QApplyTask *d_tasks, int ntasks, int m_max, cudaStream_t st);
 
 // QR of an nb x K matrix X = [X1 (nb x k1, ld1), X2 (nb x k2, ld2)] by
-// shifted CholeskyQR3 (one CTA per task; X is read, not changed): R (upper,
-// K x K, ld K) and, if Q is set, Q (nb x K, ld nb; may equal Z).  With Rinv
-// set instead (and Q null) the last pass is not run: Z keeps X2 and Rinv
-// (K x K, ld K) receives R3^-1, so that Q = Z Rinv.  Z is nb x K scratch
-// (ld nb).  K = k1 + k2 <= cholqr3_kmax(); fail counts tasks whose Cholesky
-// broke down under every shift (R left as the identity).
+// randomized CholeskyQR (a 256-row CountSketch factored by shifted
+// CholeskyQR3, then one CholeskyQR pass over the rows; one CTA per task; X is
+// read, not changed): R (upper, K x K, ld K) and, if Q is set, Q (nb x K,
+// ld nb; may equal Z).  With Rinv set instead (and Q null), Z keeps
+// Y = X Rs^-1 and Rinv (K x K, ld K) receives Rc^-1, so that Q = Z Rinv.  Z
+// (nb x K, ld nb) is written only when Q or Rinv is set.  K = k1 + k2 <=
+// rcholqr_kmax().  flags[0] counts the null pivots (columns of Y dependent on
+// the ones before them, or zero) met by the passes over the rows, flags[1]
+// the passes repeated because the sketch missed a direction.
 struct CQTask {
     const double *X1, *X2;
     double *Z;
@@ -224,9 +227,11 @@ struct CQTask {
     int nb, k1, k2, ld1, ld2;
     double *Rinv = nullptr;
 };
-int cholqr3_kmax();
-int cholqr3_bucket(int K);   // width of the kernel instance that takes K
-void launch_cholqr3_batched(const CQTask *d_tasks, int ntasks, int kmax, int *fail, cudaStream_t st);
+int rcholqr_kmax();
+int rcholqr_bucket(int K);   // width of the kernel instance that takes K
+// form_q: every task of the launch sets Q (and none sets Rinv); otherwise none sets Q
+void launch_rcholqr_batched(const CQTask *d_tasks, int ntasks, int kmax, bool form_q, int *flags,
+                            cudaStream_t st);
 
 // ------------------------------------------------------------- core SVD -----
 // M = RU RV^T (RU, RV: K x K upper from the QRs; RU == nullptr means I),

@@ -182,7 +182,7 @@ class Context:
         return self.lib.hicma_tlr_stream(self.h) or 0
 
     PROF_CLASSES = ("gemm", "qr", "qapply", "core_svd", "potrf", "cov", "copy", "other", "proj",
-                    "gemm_y", "gemm_trsm", "gemm_syrk", "gemm_dense", "gemm_gen", "gram", "cholqr3")
+                    "gemm_y", "gemm_trsm", "gemm_syrk", "gemm_dense", "gemm_gen", "gram", "rcholqr")
 
     def prof_enable(self, on: bool = True) -> None:
         _check(self.lib.hicma_tlr_prof_enable(self.h, int(on)), "hicma_tlr_prof_enable")

@@ -253,11 +253,12 @@ int hicma_tlr_serve_loglik(hicma_tlr_ctx *ctx, const hicma_tlr_problem *prob, in
  * [7] GEMM/recompression s, [8] Jacobi sweeps summed over all cores, [9] recompressions
  * whose products ran in FP32 under HICMA_TLR_PREC_MIXED, [10] op count of the
  * critical path POTRF(k) -> TRSM(k+1,k) -> SYRK(k,k+1) (the reference's op_path;
- * the rest of [1] is its op_offpath), [11] QR factors of the recompressions whose shifted
- * CholeskyQR broke down under every shift (0 in a sound run), [12] seconds
- * the device sat idle between panels (from the end of a panel's last kernel
- * to the start of the next panel's first, CUDA events), [13] panels.
- * nstats <= 16. */
+ * the rest of [1] is its op_offpath), [11] null pivots met by the passes of
+ * the recompressions' randomized CholeskyQR over the rows (columns dependent on
+ * the ones before them, or zero; 0 in the usual run), [12] seconds the device sat idle between panels (from the end
+ * of a panel's last kernel to the start of the next panel's first, CUDA
+ * events), [13] panels, [14] CholeskyQR passes over a stack's rows repeated
+ * because its sketch missed a direction (0 in the usual run).  nstats <= 16. */
 int hicma_tlr_last_stats(hicma_tlr_desc *A, double *stats, int nstats);
 
 /* --check of the reference driver (check_dpotrf2 and check_diff,
@@ -282,7 +283,7 @@ int hicma_tlr_check_probe(hicma_tlr_ctx *ctx, hicma_tlr_desc *L, const hicma_tlr
  * 5 covariance generation, 6 copies, 7 other, 8 Gram-Schmidt projections, then the batched
  * GEMMs by call site: 0 recompression outputs and the rest, 9 recompression products (Y),
  * 10 TRSM, 11 SYRK, 12 dense band cases, 13 generation; 14 split-K inner products (Gram kernel),
- * 15 QR factors by shifted CholeskyQR3 (both sides of narrow recompressions, the generation
+ * 15 QR factors by randomized CholeskyQR (both sides of narrow recompressions, the generation
  * range finder).  out[4*k + j]: j = 0 launches,
  * 1 seconds, 2 algorithmic flops, 3 algorithmic bytes.  Enabling resets. */
 int hicma_tlr_prof_enable(hicma_tlr_ctx *ctx, int on);

@@ -564,6 +564,95 @@ def r_factor_scholqr3(V: np.ndarray) -> np.ndarray:
     return R * d
 
 
+# randomized CholeskyQR as the device runs it (k_cholqr.cu)
+RCQ_ROWS = 256       # sketch rows (one per thread of the device's CTA)
+RCQ_APPLY = 3        # passes over the rows at most
+RCQ_GMAX = 1e4       # ||Y^T Y||_inf above this: the sketch missed a direction of range(X)
+RCQ_TINY = 1e-200    # pivot floor when the Gram matrix is zero
+RCQ_KMAX = 64        # widest stack the device factors this way
+
+
+def sketch_signs(m: int) -> np.ndarray:
+    """Signs of rows 0..m-1 in the CountSketch of :func:`qr_rcholqr`: the low
+    bit of a 32-bit integer hash of the row index (xor-shift / multiply rounds
+    of the "lowbias32" mixer; arithmetic modulo 2^32)."""
+    x = np.arange(m, dtype=np.uint32)
+    x ^= x >> np.uint32(16)
+    x *= np.uint32(0x7FEB352D)
+    x ^= x >> np.uint32(15)
+    x *= np.uint32(0x846CA68B)
+    x ^= x >> np.uint32(16)
+    return np.where(x & np.uint32(1), -1.0, 1.0)
+
+
+def _chol_local(G: np.ndarray, m: float, shifted: bool):
+    """R = chol(G + shift)^T as the device factors it: right-looking
+    elimination with s = 11 (m K + K (K + 1)) u tr(G) added to the diagonal
+    when ``shifted``; a pivot that is not positive (a column dependent on the
+    ones before it, or zero) becomes s (RCQ_TINY when s = 0) with its column
+    below the diagonal zeroed and no trailing update, so the other columns keep
+    their factor.  Returns (R, number of such null pivots)."""
+    K = G.shape[0]
+    u = np.finfo(np.float64).eps / 2
+    s0 = 11.0 * (m * K + K * (K + 1)) * u * float(np.trace(G))
+    floor = s0 if s0 > 0.0 else RCQ_TINY
+    A = np.array(G, dtype=np.float64)
+    if shifted and s0 > 0.0:
+        A[np.diag_indices(K)] += s0
+    L = np.zeros((K, K))
+    nnull = 0
+    for j in range(K):
+        d = A[j, j]
+        if not d > 0.0:
+            nnull += 1
+            L[j, j] = math.sqrt(floor)
+            continue
+        p = math.sqrt(d)
+        L[j, j] = p
+        L[j + 1:, j] = A[j + 1:, j] / p
+        A[j + 1:, j + 1:] -= np.outer(A[j + 1:, j], A[j + 1:, j] / d)
+    return L.T, nnull
+
+
+def qr_rcholqr(X: np.ndarray):
+    """QR of a tall-skinny X by randomized CholeskyQR, the device's form for
+    stacks up to 64 columns (both sides of a recompression, the generation
+    range finder): a 256-row CountSketch S (row i of X, times
+    :func:`sketch_signs`, added to row i mod 256), Rs = R of S by shifted
+    CholeskyQR3 (column norms D of S, R1 = chol(D^-1 S^T S D^-1 + s I) with
+    m = 256, then two unshifted steps; Rs = R3 R2 R1 D), then
+    Y = X Rs^-1, Rc = chol(Y^T Y), R = Rc Rs, Q = Y Rc^-1; repeated with R
+    in place of Rs while ||Y^T Y||_inf > RCQ_GMAX (at most RCQ_APPLY passes).
+    Every Cholesky factorization treats a non-positive pivot locally
+    (:func:`_chol_local`).
+    Published algorithms: Fan, Guo and Lin (2021) and Balabanov (2022) for the
+    randomized preconditioning, Fukaya et al. (SIAM J. Sci. Comput. 42(1),
+    2020) for shifted CholeskyQR3.  Returns (Y, Rc, R, passes)."""
+    m, K = X.shape
+    S = np.zeros((RCQ_ROWS, K))
+    np.add.at(S, np.arange(m) % RCQ_ROWS, X * sketch_signs(m)[:, None])
+    G = S.T @ S
+    d = np.sqrt(np.diag(G)).copy()
+    d[~(d > 0.0)] = 1.0
+    R1, _ = _chol_local(G / np.outer(d, d), RCQ_ROWS, True)
+    Rt = R1 * d
+    Sk = sla.solve_triangular(R1, (S / d).T, trans="T", lower=False).T
+    for rnd in range(2):
+        Rp, _ = _chol_local(Sk.T @ Sk, RCQ_ROWS, False)
+        Rt = Rp @ Rt
+        if rnd == 0:
+            Sk = sla.solve_triangular(Rp, Sk.T, trans="T", lower=False).T
+    for p in range(RCQ_APPLY):
+        Y = sla.solve_triangular(Rt, X.T, trans="T", lower=False).T
+        G = Y.T @ Y
+        gmax = float(np.abs(G).sum(axis=1).max()) if K else 0.0
+        Rc, _ = _chol_local(G, m, False)
+        Rt = Rc @ Rt
+        if gmax <= RCQ_GMAX:
+            break
+    return Y, Rc, Rt, p + 1
+
+
 def recompress(Cu, Cv, Au, Y, acc, maxrank, fixed_rank=0, v_side="householder", u_side="householder"):
     """C_new = [Cu, Au] [Cv, -Y]^T recompressed (restated
     ``HCORE_dgemm_qr_svd`` + ``HCORE_dgemm_ormqr``, call sites
@@ -571,15 +660,27 @@ def recompress(Cu, Cv, Au, Y, acc, maxrank, fixed_rank=0, v_side="householder", 
     (U, V, rank, overflow).  ``v_side="scholqr3"`` takes R_V from
     :func:`r_factor_scholqr3` and forms the new V as [Cv, -Y] R_U^T U_r (no
     Q_V needed), and ``u_side="scholqr3"`` takes Q_U, R_U from
-    :func:`qr_scholqr3`: the form the device uses for stacked ranks up to 48."""
+    :func:`qr_scholqr3`; ``"rcholqr"`` on either side takes them from
+    :func:`qr_rcholqr` for stacks up to RCQ_KMAX columns (Householder for
+    wider ones), as the device does."""
     Us = np.hstack([Cu, Au])
     Vs = np.hstack([Cv, -Y])
     nb, K = Us.shape
     if K == 0:
         return np.zeros((nb, 0)), np.zeros((nb, 0)), 0, False
-    Qu, Ru = qr_scholqr3(Us) if u_side == "scholqr3" else np.linalg.qr(Us)
+    # the device takes the randomized CholeskyQR for stacks up to RCQ_KMAX columns
+    if K > RCQ_KMAX:
+        u_side = "householder" if u_side == "rcholqr" else u_side
+        v_side = "householder" if v_side == "rcholqr" else v_side
+    if u_side == "rcholqr":
+        Yu, Rcu, Ru, _ = qr_rcholqr(Us)
+        Qu = sla.solve_triangular(Rcu, Yu.T, trans="T", lower=False).T
+    else:
+        Qu, Ru = qr_scholqr3(Us) if u_side == "scholqr3" else np.linalg.qr(Us)
     if v_side == "scholqr3":
         Rv = r_factor_scholqr3(Vs)
+    elif v_side == "rcholqr":
+        Rv = qr_rcholqr(Vs)[2]
     else:
         Qv, Rv = np.linalg.qr(Vs)
     u, s, vt = np.linalg.svd(Ru @ Rv.T)
@@ -589,7 +690,7 @@ def recompress(Cu, Cv, Au, Y, acc, maxrank, fixed_rank=0, v_side="householder", 
         r = int(np.count_nonzero(s >= acc))
     overflow = r > maxrank
     r = min(r, maxrank)
-    if v_side == "scholqr3":
+    if v_side in ("scholqr3", "rcholqr"):
         return (np.ascontiguousarray(Qu @ u[:, :r]), np.ascontiguousarray(Vs @ (Ru.T @ u[:, :r])), r, overflow)
     return (np.ascontiguousarray(Qu @ u[:, :r]),
             np.ascontiguousarray(Qv @ (vt[:r].T * s[:r])), r, overflow)

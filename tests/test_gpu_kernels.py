@@ -174,6 +174,59 @@ def test_lr_update_matches_oracle(ctx, case):
     assert np.linalg.norm(U.T @ U - np.eye(r)) < 1e-12   # U keeps orthonormal columns
 
 
+@pytest.mark.parametrize("case", ["sketch_null", "zero_column", "near_dependent"])
+def test_lr_update_cholqr_adversarial(ctx, case):
+    """Recompressions whose stacks (18 columns: the randomized CholeskyQR path)
+    are built against it: a column of Cu that the sketch cannot see (rows 3 and
+    259 share a bucket and cancel under its signs, so the repeat rule has to
+    fire), a zero column in Cu, and an update lying within 1e-12 of span(Cu).
+    Rank within 1 of the Householder oracle, U V^T within the truncation bound
+    of the exact product, U orthonormal to 1e-12."""
+    from hicma_parsec_b200 import tlr
+    import ctypes as C
+    nb, cap = 270, 64
+    rng = np.random.default_rng(11)
+    Q0, _ = np.linalg.qr(rng.standard_normal((nb, 12)))
+    if case == "sketch_null":
+        s = O.sketch_signs(nb)
+        c = np.zeros(nb)
+        c[3], c[3 + O.RCQ_ROWS] = s[3], -s[3 + O.RCQ_ROWS]
+        c /= np.sqrt(2.0)
+        Q1, _ = np.linalg.qr(Q0[:, :11] - np.outer(c, c @ Q0[:, :11]))
+        Cu = np.hstack([Q1, c[:, None]])
+    elif case == "zero_column":
+        Cu = np.hstack([Q0[:, :11], np.zeros((nb, 1))])
+    else:
+        Cu = Q0
+    Cv = rng.standard_normal((nb, 12)) * 10.0 ** -np.linspace(0, 6, 12)
+    if case == "near_dependent":
+        Au, _ = np.linalg.qr(Q0[:, :4] @ rng.standard_normal((4, 6)) + 1e-12 * rng.standard_normal((nb, 6)))
+    else:
+        Au, _ = np.linalg.qr(rng.standard_normal((nb, 6)))
+    Av = 1e-2 * rng.standard_normal((nb, 6))
+    Bu, _ = np.linalg.qr(rng.standard_normal((nb, 6)))
+    Bv = rng.standard_normal((nb, 6))
+    Y = Bu @ (Bv.T @ Av)
+    _, _, rref, _ = O.recompress(Cu, Cv, Au, Y, 1e-8, cap)
+    dAu, dAv = _slot(Au, Av, cap)
+    dBu, dBv = _slot(Bu, Bv, cap)
+    dCu, dCv = _slot(Cu, Cv, cap)
+    rc = C.c_int(Cu.shape[1])
+    torch.cuda.synchronize()
+    code = tlr.load_library().hicma_tlr_k_lr_update(ctx.h, nb, dAu.data_ptr(), dAv.data_ptr(), 6, dBu.data_ptr(),
+                                                   dBv.data_ptr(), 6, dCu.data_ptr(), dCv.data_ptr(), C.byref(rc),
+                                                   1e-8, cap, 0)
+    assert code == 0, tlr.last_error()
+    r = rc.value
+    assert abs(r - rref) <= 1, (r, rref)
+    U, V = host(dCu)[:, :r], host(dCv)[:, :r]
+    assert np.isfinite(U).all() and np.isfinite(V).all()
+    exact = Cu @ Cv.T - Au @ Y.T
+    # absolute truncation at acc = 1e-8 per singular value: error <= sqrt(K) * acc
+    assert np.linalg.norm(U @ V.T - exact, 2) <= math.sqrt(18) * 1e-8
+    assert np.linalg.norm(U.T @ U - np.eye(r)) < 1e-12
+
+
 def test_compress_matches_oracle(ctx):
     from hicma_parsec_b200 import tlr
     import ctypes as C

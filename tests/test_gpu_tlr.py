@@ -185,11 +185,12 @@ def test_probe_residual_matches_dense_check(ctx):
 @pytest.mark.parametrize("var,alt", [("HICMA_TLR_QR", "householder")])
 def test_kernel_variants_agree(monkeypatch, var, alt):
     """The default recompression against its alternative on the reference's
-    own case: both QRs by shifted CholeskyQR3 for stacked ranks up to 48 (the
+    own case: both QRs by randomized CholeskyQR for stacks up to 64 columns (the
     default) against the block Gram-Schmidt + Householder pipeline for every
     update (HICMA_TLR_QR=householder, read when a context is created; each run is a
     child process).  Same final ranks within 1, both residuals within the bar,
-    log-determinants equal to 1e-10, no CholeskyQR breakdown."""
+    log-determinants equal to 1e-10, no null pivot and no repeated pass in the
+    CholeskyQR."""
     import json
     import subprocess
     import sys
@@ -203,7 +204,9 @@ def test_kernel_variants_agree(monkeypatch, var, alt):
         "    assert A.generate(tlr.Problem(kind=2, noise=1e-4), %r, %d) == 0\n"
         "    assert A.potrf(%r, %d) == 0\n"
         "    res = O.check_dpotrf2(A.uncompress(), O.dense_matrix(O.Problem(kind=2, noise=1e-4), O.gen_points(%d, 2)))\n"
-        "    print(json.dumps({'G': A.rank_map().tolist(), 'ld': A.logdet(), 'res': res, 'brk': float(A.stats()[11])}))\n"
+        "    st = A.stats()\n"
+        "    print(json.dumps({'G': A.rank_map().tolist(), 'ld': A.logdet(), 'res': res, 'brk': float(st[11]),\n"
+        "                      'rep': float(st[14])}))\n"
     ) % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))), N, NB, MAXRANK, TOL, MAXRANK, TOL, MAXRANK, N)
     out = {}
     for mode in ("default", "alt"):
@@ -220,3 +223,4 @@ def test_kernel_variants_agree(monkeypatch, var, alt):
     assert out["default"]["res"] <= 10 * TOL and out["alt"]["res"] <= 10 * TOL
     assert abs(out["default"]["ld"] - out["alt"]["ld"]) <= 1e-10 * abs(out["alt"]["ld"])
     assert out["default"]["brk"] == 0 and out["alt"]["brk"] == 0
+    assert out["default"]["rep"] == 0

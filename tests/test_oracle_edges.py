@@ -210,6 +210,116 @@ def test_scholqr3_both_sides_keeps_ranks_and_accuracy():
     assert np.linalg.norm(Q @ R - V) <= 1e-13 * np.linalg.norm(V)
 
 
+def test_rcholqr_both_sides_keeps_ranks_and_accuracy():
+    """The device's form for stacks up to 64 columns: randomized CholeskyQR on
+    both sides of every recompression gives the Householder oracle's final
+    ranks, residual and log det on the reference's case, with Q_U orthonormal
+    to working precision and one pass over the rows per QR."""
+    import scipy.linalg as sla
+    prob = O.Problem(kind=2, noise=1e-4)
+    pts = O.gen_points(2700, 2)
+    T0, info = O.generate(prob, 2700, 270, 1e-8, 130, 1, pts)
+    assert info == 0
+    Th, Tc = T0.copy(), T0.copy()
+    assert O.tlr_potrf(Th, 1e-8).info == 0
+    passes = []
+    orig = O.qr_rcholqr
+
+    def counted(X):
+        out = orig(X)
+        passes.append(out[3])
+        return out
+
+    O.qr_rcholqr = counted
+    try:
+        assert O.tlr_potrf(Tc, 1e-8, v_side="rcholqr", u_side="rcholqr").info == 0
+    finally:
+        O.qr_rcholqr = orig
+    assert passes and max(passes) == 1
+    assert np.array_equal(Th.rank_array(), Tc.rank_array())
+    A = O.dense_matrix(prob, pts)
+    rh, rc = O.check_dpotrf2(O.uncompress(Th), A), O.check_dpotrf2(O.uncompress(Tc), A)
+    assert rc <= 10 * 1e-8 and abs(rc - rh) <= 0.01 * rh
+    assert abs(O.logdet(Tc) - O.logdet(Th)) <= 1e-12 * abs(O.logdet(Th))
+    for (m, n), U in Tc.U.items():
+        r = U.shape[1]
+        if r:
+            assert np.linalg.norm(U.T @ U - np.eye(r)) <= 1e-12
+    # the factors themselves
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((2700, 60)) @ np.diag(10.0 ** (-0.2 * np.arange(60)))
+    Y, Rc, R, p = O.qr_rcholqr(X)
+    Q = sla.solve_triangular(Rc, Y.T, trans="T", lower=False).T
+    assert p == 1 and np.allclose(np.tril(R, -1), 0.0)
+    assert np.linalg.norm(Q @ R - X) <= 1e-14 * np.linalg.norm(X)
+    assert np.linalg.norm(Q.T @ Q - np.eye(60)) <= 1e-13
+
+
+def _rcholqr_q(X):
+    import scipy.linalg as sla
+    Y, Rc, R, p = O.qr_rcholqr(X)
+    return sla.solve_triangular(Rc, Y.T, trans="T", lower=False).T, R, p
+
+
+def sketch_null_column(m, i):
+    """A unit column whose sketch is exactly zero: rows i and i + 256 share a
+    bucket, with entries that cancel under the sketch's signs."""
+    s = O.sketch_signs(m)
+    c = np.zeros(m)
+    c[i], c[i + O.RCQ_ROWS] = s[i], -s[i + O.RCQ_ROWS]
+    return c / np.sqrt(2.0)
+
+
+@pytest.mark.parametrize("case", ["sketch_null", "zero_and_dependent", "all_zero", "scaled", "short", "near_dependent"])
+def test_rcholqr_adversarial_inputs(case):
+    """Randomized CholeskyQR on inputs built against it: a column the sketch
+    cannot see (the repeat rule must fire and restore orthogonality), zero and
+    exactly dependent columns (no repeat; Q R = X), an all-zero matrix (R = 0,
+    everything finite), column scales 1e-150..1e100, fewer rows than sketch
+    rows, and nearly dependent blocks."""
+    rng = np.random.default_rng(5)
+    m = 100 if case == "short" else 2700
+    Q0, _ = np.linalg.qr(rng.standard_normal((m, 20)))
+    if case == "sketch_null":
+        c = sketch_null_column(m, 5)
+        Q0 = Q0 - np.outer(c, c @ Q0)
+        X = np.hstack([Q0, c[:, None]])
+    elif case == "zero_and_dependent":
+        X = np.hstack([Q0, np.zeros((m, 3)), 2.0 * Q0[:, :4]])
+    elif case == "all_zero":
+        X = np.zeros((m, 12))
+    elif case == "scaled":
+        X = rng.standard_normal((m, 30)) * 10.0 ** np.linspace(-150, 100, 30)
+    elif case == "short":
+        X = rng.standard_normal((m, 40))
+    else:
+        X = np.hstack([Q0, Q0[:, :5] @ rng.standard_normal((5, 8)) + 1e-13 * rng.standard_normal((m, 8))])
+    Q, R, p = _rcholqr_q(X)
+    K = X.shape[1]
+    assert np.isfinite(Q).all() and np.isfinite(R).all()
+    assert np.allclose(np.tril(R, -1), 0.0)
+    assert p == (2 if case == "sketch_null" else 1)
+    if case == "all_zero":
+        assert not R.any()
+        return
+    assert np.linalg.norm(Q @ R - X) <= 1e-14 * np.linalg.norm(X)
+    if case in ("sketch_null", "scaled", "short", "near_dependent"):
+        assert np.linalg.norm(Q.T @ Q - np.eye(K)) <= 1e-13
+    else:
+        # the live columns stay orthonormal; the null directions of X carry R(j, j) ~ 0
+        live = np.abs(np.diag(R)) > 1e-6 * np.abs(np.diag(R)).max()
+        Ql = Q[:, live]
+        assert np.linalg.norm(Ql.T @ Ql - np.eye(Ql.shape[1])) <= 1e-13
+
+
+def test_sketch_signs_pinned():
+    """The sketch's row signs (lowbias32 hash, low bit) for rows 0..15, pinned so
+    that the restatement and the device's hash cannot drift apart unnoticed."""
+    # computed independently by a C program (uint32 arithmetic)
+    assert O.sketch_signs(16).tolist() == [1.0, 1.0, -1.0, -1.0, -1.0, 1.0, -1.0, 1.0,
+                                           1.0, -1.0, -1.0, -1.0, 1.0, -1.0, 1.0, -1.0]
+
+
 @pytest.mark.parametrize("band", [1, 2])
 def test_dag_oracle_matches_sequential_oracle(band):
     """The task-graph run on host threads (the timed CPU baseline) computes the
