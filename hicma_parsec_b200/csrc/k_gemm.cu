@@ -233,7 +233,24 @@ __global__ void __launch_bounds__(256) k_sgemm_batched(const GemmTask *__restric
     }
 }
 
+__global__ void k_gemm_devcount(const GemmTask *__restrict__ tasks, int ntasks, double *acc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ntasks) return;
+    const GemmTask t = tasks[i];
+    if (!t.n_dev) return;
+    const int nd = *t.n_dev;
+    const double n = nd < t.n ? nd : t.n;
+    if (n <= 0) return;
+    atomicAdd(acc, 2.0 * t.m * n * t.k);
+    atomicAdd(acc + 1, 8.0 * ((double)t.m * t.k + (double)t.k * n + (t.beta != 0.0 ? 2.0 : 1.0) * t.m * n));
+}
+
 }  // namespace
+
+void launch_gemm_devcount(const GemmTask *d_tasks, int ntasks, double *acc, cudaStream_t st) {
+    if (ntasks <= 0) return;
+    k_gemm_devcount<<<(ntasks + 255) / 256, 256, 0, st>>>(d_tasks, ntasks, acc);
+}
 
 void launch_gemm_batched(const GemmTask *d_tasks, const int *d_tile_off, int ntasks, int total_tiles,
                          cudaStream_t st, bool fp32) {

@@ -100,73 +100,170 @@ struct CQSmem {
     static constexpr int NACC = STAGED ? 2 * TPW : NTILE;           // accumulators per lane
     static constexpr size_t W = (size_t)KM * CQ_PITCH;    // one warp's staged chunk
     static constexpr size_t KK = (size_t)KM * KM;
+    static constexpr int RLD = KM + 4;                     // row pitch of the K x K factors (== 4 mod 16)
+    static constexpr size_t RR = (size_t)KM * RLD;
     static constexpr size_t CHUNK = STAGED ? (size_t)KM * CQ_LDZ : CQ_WARPS * W;
-    // chunk buffer(s) | [G, unless in the chunk buffer] | Rr | Rt | 1/diag Rr | 1/diag Rt | d
-    static constexpr size_t bytes() { return sizeof(double) * (CHUNK + (STAGED ? 2 : 3) * KK + 3 * KM); }
-    static_assert(!STAGED || CHUNK >= KK, "G lives in the chunk buffer");
+    static constexpr size_t WS = CQ_WARPS * 96;           // per-warp 8 x 8 scratch (pitch 12), end of the chunk buffer
+    // chunk buffer(s) | [G / product scratch, unless in the chunk buffer] | Rr | Rt |
+    // 1/diag Rr | 1/diag Rt | d | 1/pivots
+    static constexpr size_t bytes() { return sizeof(double) * (CHUNK + (STAGED ? 2 : 3) * RR + 4 * KM); }
+    static_assert(CHUNK >= WS && (!STAGED || CHUNK >= RR + WS), "scratch regions fit the chunk buffer");
+    static_assert(RR >= KK, "G fits its region");
+    static_assert(STAGED || W >= (size_t)NTILE * 64, "per-warp Gram partials fit the warp's chunk slice");
 };
 
 // x <- x R^-1 for one row x (registers): right-looking substitution with the
-// row-major upper R in shared memory.  Written as compile-time recursion so
-// that every index into x is static and x stays in registers at any width.
-template <int KM, int J, int C>
+// row-major upper R (pitch RLD) in shared memory, read as broadcasts, two
+// entries per 128-bit load (rows start 16-byte aligned: RLD is even).  Written
+// as compile-time recursion so that every index into x is static and x stays
+// in registers at any width.
+template <int KM, int C>
 __device__ __forceinline__ void subst_cols(double (&x)[KM], double xj, const double *rj) {
     if constexpr (C < KM) {
-        x[C] -= xj * rj[C];
-        subst_cols<KM, J, C + 1>(x, xj, rj);
+        if constexpr ((C & 1) == 0 && C + 1 < KM) {
+            const double2 r = *reinterpret_cast<const double2 *>(rj + C);
+            x[C] -= xj * r.x;
+            x[C + 1] -= xj * r.y;
+            subst_cols<KM, C + 2>(x, xj, rj);
+        } else {
+            x[C] -= xj * rj[C];
+            subst_cols<KM, C + 1>(x, xj, rj);
+        }
     }
 }
 template <int KM, int J>
-__device__ __forceinline__ void subst_rows(double (&x)[KM], const double *Rr, const double *rdg) {
+__device__ __forceinline__ void subst_rows(double (&x)[KM], const double *R, const double *rd) {
     if constexpr (J < KM) {
-        x[J] *= rdg[J];
-        subst_cols<KM, J, J + 1>(x, x[J], Rr + J * KM);
-        subst_rows<KM, J + 1>(x, Rr, rdg);
+        x[J] *= rd[J];
+        subst_cols<KM, J + 1>(x, x[J], R + J * CQSmem<KM>::RLD);
+        subst_rows<KM, J + 1>(x, R, rd);
     }
 }
 
-// Gram product of one chunk of rows (x: this thread's row, zero past K and
-// for rows past the end) added to the lane's accumulators.
+// Gram product of a staged 256-row chunk (CTA-staged form, after a barrier):
+// each warp's owned tiles, two chains per tile (even / odd row quads).
+template <int KM>
+__device__ __forceinline__ void gram_tiles(double (&acc)[CQSmem<KM>::NACC][2], const double *sm, int lane,
+                                           const int (&tmi)[CQSmem<KM>::TPW], const int (&tni)[CQSmem<KM>::TPW]) {
+    using S = CQSmem<KM>;
+    const int g = lane >> 2, tig = lane & 3;
+#pragma unroll 2
+    for (int s = 0; s < CQ_CH; s += 8) {
+#pragma unroll
+        for (int q = 0; q < S::TPW; ++q) {
+            if (tmi[q] < 0) continue;
+            const double *za = sm + (8 * tmi[q] + g) * CQ_LDZ + tig + s;
+            const double *zb = sm + (8 * tni[q] + g) * CQ_LDZ + tig + s;
+            dmma884(acc[2 * q], za[0], zb[0]);
+            dmma884(acc[2 * q + 1], za[4], zb[4]);
+        }
+    }
+}
+
+// Gram product of a warp's staged 32-row chunk (per-warp form): row quads s,
+// one fragment per 8-column block, reused by every tile of that block.
+template <int KM>
+__device__ __forceinline__ void gram_warp(double (&acc)[CQSmem<KM>::NACC][2], const double *Zw, int lane) {
+    using S = CQSmem<KM>;
+    const int g = lane >> 2, tig = lane & 3;
+#pragma unroll 1
+    for (int s = 0; s < 32; s += 4) {
+        double a[S::NT8];
+#pragma unroll
+        for (int mi = 0; mi < S::NT8; ++mi) a[mi] = Zw[(8 * mi + g) * CQ_PITCH + s + tig];
+        int q = 0;
+#pragma unroll
+        for (int mi = 0; mi < S::NT8; ++mi)
+#pragma unroll
+            for (int ni = 0; ni <= mi; ++ni, ++q) dmma884(acc[q], a[mi], a[ni]);
+    }
+}
+
+// Gram product of one chunk of rows held in registers (x: this thread's row,
+// zero past K and for rows past the end), staged first.
 template <int KM>
 __device__ __forceinline__ void gram_chunk(const double (&x)[KM], double (&acc)[CQSmem<KM>::NACC][2], double *sm,
                                            int tid, const int (&tmi)[CQSmem<KM>::TPW],
                                            const int (&tni)[CQSmem<KM>::TPW]) {
     using S = CQSmem<KM>;
-    const int lane = tid & 31, g = lane >> 2, tig = lane & 3;
+    const int lane = tid & 31;
     if constexpr (S::STAGED) {
 #pragma unroll
         for (int j = 0; j < KM; ++j) sm[j * CQ_LDZ + tid] = x[j];
         __syncthreads();
-        // owned tiles over the 256 rows, two chains per tile (even / odd row quads)
-#pragma unroll 2
-        for (int s = 0; s < CQ_CH; s += 8) {
-#pragma unroll
-            for (int q = 0; q < S::TPW; ++q) {
-                if (tmi[q] < 0) continue;
-                const double *za = sm + (8 * tmi[q] + g) * CQ_LDZ + tig + s;
-                const double *zb = sm + (8 * tni[q] + g) * CQ_LDZ + tig + s;
-                dmma884(acc[2 * q], za[0], zb[0]);
-                dmma884(acc[2 * q + 1], za[4], zb[4]);
-            }
-        }
+        gram_tiles<KM>(acc, sm, lane, tmi, tni);
         __syncthreads();
     } else {
         double *Zw = sm + (tid >> 5) * S::W;
 #pragma unroll
         for (int j = 0; j < KM; ++j) Zw[j * CQ_PITCH + lane] = x[j];
         __syncwarp();
-        // row quads s, one fragment per 8-column block
-#pragma unroll 1
-        for (int s = 0; s < 32; s += 4) {
-            double a[S::NT8];
+        gram_warp<KM>(acc, Zw, lane);
+        __syncwarp();
+    }
+}
+
+// Row `row` of X = [X1, X2] into v (zero past K and for rows past the end):
+// every load issued before any use.
+template <int KM>
+__device__ __forceinline__ void load_row(const CQTask &t, int row, int nb, int k1, int K, double (&v)[KM]) {
+    const bool valid = row < nb;
+    const double *p1 = t.X1 + row, *p2 = t.X2 + row;
 #pragma unroll
-            for (int mi = 0; mi < S::NT8; ++mi) a[mi] = Zw[(8 * mi + g) * CQ_PITCH + s + tig];
-            int q = 0;
-#pragma unroll
-            for (int mi = 0; mi < S::NT8; ++mi)
-#pragma unroll
-                for (int ni = 0; ni <= mi; ++ni, ++q) dmma884(acc[q], a[mi], a[ni]);
+    for (int j = 0; j < KM; ++j) {
+        double x = 0.0;
+        if (j < k1) {
+            if (valid) x = *p1;
+            p1 += t.ld1;
+        } else if (j < K) {
+            if (valid) x = *p2;
+            p2 += t.ld2;
         }
+        v[j] = x;
+    }
+}
+
+// Y = X R^-1 in place for a warp's 32 staged rows (column-major, pitch P):
+// 8-column blocks J = 0, 1, ...: C = sum_{I<J} Y_I R_IJ on DMMA (four 8-row
+// tiles, the block of R shared), Z_J -= C, then each lane solves its row's
+// 8 x 8 diagonal block by substitution (R broadcast from shared memory).  R is
+// the row-major upper factor (pitch RLD) with rd = 1/diag, zero past K.
+template <int KM, int P>
+__device__ __forceinline__ void warp_trsm(double *zb, const double *R, const double *rd, int K, int lane) {
+    constexpr int L = CQSmem<KM>::RLD;
+    const int g = lane >> 2, tig = lane & 3;
+    const int NK = (K + 7) >> 3;
+    for (int J = 0; J < NK; ++J) {
+        if (J > 0) {
+            double acc[4][2];
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt) acc[mt][0] = acc[mt][1] = 0.0;
+            for (int I = 0; I < J; ++I) {
+#pragma unroll
+                for (int k4 = 0; k4 < 8; k4 += 4) {
+                    const double b = R[(8 * I + k4 + tig) * L + 8 * J + g];
+                    const double *za = zb + (8 * I + k4 + tig) * P + g;
+#pragma unroll
+                    for (int mt = 0; mt < 4; ++mt) dmma884(acc[mt], za[8 * mt], b);
+                }
+            }
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) zb[(8 * J + 2 * tig + e) * P + 8 * mt + g] -= acc[mt][e];
+            __syncwarp();
+        }
+        double z[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) z[c] = zb[(8 * J + c) * P + lane];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            z[c] *= rd[8 * J + c];
+#pragma unroll
+            for (int c2 = c + 1; c2 < 8; ++c2) z[c2] -= z[c] * R[(8 * J + c) * L + 8 * J + c2];
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) zb[(8 * J + c) * P + lane] = z[c];
         __syncwarp();
     }
 }
@@ -174,7 +271,7 @@ __device__ __forceinline__ void gram_chunk(const double (&x)[KM], double (&acc)[
 // Accumulators -> G (column-major, ld KM, both triangles of [0, K)), visible
 // to the CTA on return.
 template <int KM>
-__device__ __forceinline__ void gram_reduce(const double (&acc)[CQSmem<KM>::NACC][2], double *G, int tid,
+__device__ __forceinline__ void gram_reduce(const double (&acc)[CQSmem<KM>::NACC][2], double *G, double *sm, int tid,
                                             const int (&tmi)[CQSmem<KM>::TPW], const int (&tni)[CQSmem<KM>::TPW]) {
     using S = CQSmem<KM>;
     const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, tig = lane & 3;
@@ -194,141 +291,239 @@ __device__ __forceinline__ void gram_reduce(const double (&acc)[CQSmem<KM>::NACC
         }
         __syncthreads();
     } else {
-        // per-warp partials, added in warp order
-        for (int idx = tid; idx < KM * KM; idx += CQ_THREADS) G[idx] = 0.0;
-        __syncthreads();
-        for (int w = 0; w < CQ_WARPS; ++w) {
-            if (warp == w) {
-                int q = 0;
+        // per-warp partials into the warp's own chunk slice (free after its Gram),
+        // then every entry summed over the eight slices in warp order
+        double *Pw = sm + warp * S::W;
+        {
+            int q = 0;
 #pragma unroll
-                for (int mi = 0; mi < S::NT8; ++mi)
+            for (int mi = 0; mi < S::NT8; ++mi)
 #pragma unroll
-                    for (int ni = 0; ni <= mi; ++ni, ++q)
+                for (int ni = 0; ni <= mi; ++ni, ++q)
 #pragma unroll
-                        for (int e = 0; e < 2; ++e) {
-                            const int i = 8 * mi + g, j = 8 * ni + 2 * tig + e;
-                            G[i + j * KM] += acc[q][e];
-                            if (mi != ni) G[j + i * KM] += acc[q][e];
-                        }
-            }
-            __syncthreads();
+                    for (int e = 0; e < 2; ++e) Pw[q * 64 + g * 8 + 2 * tig + e] = acc[q][e];
         }
+        __syncthreads();
+        for (int idx = tid; idx < S::NTILE * 64; idx += CQ_THREADS) {
+            const int q = idx >> 6, r = idx & 63;
+            int mi = 0;
+            while ((mi + 1) * (mi + 2) / 2 <= q) ++mi;
+            const int ni = q - mi * (mi + 1) / 2;
+            double v = 0.0;
+#pragma unroll
+            for (int w = 0; w < CQ_WARPS; ++w) v += sm[w * S::W + idx];
+            const int i = 8 * mi + (r >> 3), j = 8 * ni + (r & 7);
+            G[i + j * KM] = v;
+            G[j + i * KM] = v;
+        }
+        __syncthreads();
     }
 }
 
 // In-place elimination of the K x K symmetric positive semidefinite matrix G
-// (column-major, ld KM, lower part) by the whole CTA: right-looking, one
-// barrier per column, the trailing update with the unscaled pivot column,
-// G(i,k) -= G(i,j) G(k,j) / G(j,j).  On return G(j,j) is the j-th pivot and
-// G(i,j) = L(i,j) sqrt(G(j,j)), i > j.  A pivot that is not positive (column
-// j depends on the columns before it, or is zero, up to rounding) is set to
-// `floor` with its column below the diagonal zeroed and no trailing update:
-// a perturbation of G confined to row and column j (whose Schur complement
-// entries are at rounding level), which leaves the factor of every other
-// column as it was.  Threads form a 16 x 16 grid: rows i by tx (consecutive
-// addresses), columns k by ty.  Returns the number of such null pivots.
+// (column-major, ld KM, lower part), padded to Kp = 8 ceil(K / 8) with an
+// identity block: right-looking in 8-column panels.  Warp 0 eliminates a
+// panel (lanes own rows, two each; the pivot row's entries by shuffles), then
+// the CTA applies the panel's rank-8 update to the trailing lower triangle,
+// G(i,k) -= sum_c G(i,c) G(k,c) / G(c,c) (threads on a 16 x 16 grid of rows
+// and columns, the row's panel entries in registers).  On return G(j,j) is the
+// j-th pivot and G(i,j) = L(i,j) sqrt(G(j,j)), i > j.  A pivot that is not
+// positive (column j depends on the columns before it, or is zero, up to
+// rounding) is set to `floor` with its column below the diagonal zeroed and
+// no update from it: a perturbation of G confined to row and column j (whose
+// Schur complement entries are at rounding level), which leaves the factor of
+// every other column as it was.  iv receives the inverse pivots.  Returns the
+// number of such null pivots on thread 0.
 template <int KM>
-__device__ int cta_cholesky(double *G, int K, double floor, int tid) {
-    const int tx = tid & 15, ty = tid >> 4;
-    int nnull = 0;
-    for (int j = 0; j < K; ++j) {
-        const double d = G[j + j * KM];
-        if (!(d > 0.0)) {
-            ++nnull;
-            __syncthreads();   // every thread has read the pivot
-            if (tid == 0) G[j + j * KM] = floor;
-            for (int i = j + 1 + tid; i < K; i += CQ_THREADS) G[i + j * KM] = 0.0;
-            __syncthreads();
-            continue;
-        }
-        const double id = 1.0 / d;
-        for (int k = j + 1 + ty; k < K; k += 16) {
-            const double gkj = G[k + j * KM] * id;
-            for (int i = k + ((j + 1 + tx - k) & 15); i < K; i += 16) G[i + k * KM] -= G[i + j * KM] * gkj;
+__device__ int cta_cholesky(double *G, int K, double floor, double *iv, int tid) {
+    const int lane = tid & 31, warp = tid >> 5;
+    const int Kp = (K + 7) & ~7;
+    if (Kp > K) {
+        for (int idx = tid; idx < (Kp - K) * Kp; idx += CQ_THREADS) {
+            const int i = K + idx % (Kp - K), j = idx / (Kp - K);
+            G[i + j * KM] = i == j ? 1.0 : 0.0;
         }
         __syncthreads();
+    }
+    int nnull = 0;
+    for (int j0 = 0; j0 < Kp; j0 += 8) {
+        if (warp == 0) {
+            const int ra = j0 + lane, rb = j0 + 32 + lane;
+            double a[8], b[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                a[c] = ra < Kp ? G[ra + (j0 + c) * KM] : 0.0;
+                b[c] = rb < Kp ? G[rb + (j0 + c) * KM] : 0.0;
+            }
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const double d = __shfl_sync(0xffffffffu, a[c], c);
+                if (!(d > 0.0)) {
+                    if (lane > c) a[c] = 0.0;
+                    if (lane == c) a[c] = floor;
+                    b[c] = 0.0;
+                    ++nnull;
+                    continue;
+                }
+                const double id = 1.0 / d;
+#pragma unroll
+                for (int c2 = c + 1; c2 < 8; ++c2) {
+                    const double lc = __shfl_sync(0xffffffffu, a[c], c2) * id;
+                    if (lane > c) a[c2] -= a[c] * lc;
+                    b[c2] -= b[c] * lc;
+                }
+            }
+            double piv = 1.0;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                if (ra < Kp && lane >= c) G[ra + (j0 + c) * KM] = a[c];
+                if (rb < Kp) G[rb + (j0 + c) * KM] = b[c];
+                if (lane == c) piv = a[c];
+            }
+            if (lane < 8) iv[j0 + lane] = 1.0 / piv;
+        }
+        __syncthreads();
+        const int t0 = j0 + 8;
+        if (t0 < Kp) {
+            const int tx = tid & 15, ty = tid >> 4;
+            double ivc[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) ivc[c] = iv[j0 + c];
+            for (int i = t0 + tx; i < Kp; i += 16) {
+                double pi[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) pi[c] = G[i + (j0 + c) * KM] * ivc[c];
+                for (int k = t0 + ty; k <= i; k += 16) {
+                    double v = G[i + k * KM];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) v -= pi[c] * G[k + (j0 + c) * KM];
+                    G[i + k * KM] = v;
+                }
+            }
+            __syncthreads();
+        }
     }
     return nnull;
 }
 
-// R = chol(G + shift)^T into Rr (upper, row-major, zero outside [0, K)) and
-// rdg = 1/diag(Rr), with s = 11 (m K + K (K + 1)) u tr(G): the shift when
-// `shifted` (none otherwise) and the floor of null pivots (CQ_TINY when
-// s = 0).  G must be complete and visible; it is free on return.  Returns the
-// number of null pivots.
+// R = chol(G + shift)^T into Rr (upper, row-major, pitch RLD, zero outside
+// [0, K)) and rdg = 1/diag(Rr), with s = 11 (m K + K (K + 1)) u tr(G): the
+// shift when `shifted` (none otherwise) and the floor of null pivots (CQ_TINY
+// when s = 0).  G must be complete and visible; it is free on return.
+// Returns the number of null pivots (on thread 0).
 template <int KM>
-__device__ int factor(double *G, double *Rr, double *rdg, int K, double m, bool shifted, int tid) {
+__device__ int factor(double *G, double *Rr, double *rdg, double *iv, int K, double m, bool shifted, int tid) {
+    constexpr int L = CQSmem<KM>::RLD;
+    const int lane = tid & 31;
+    // trace: every warp reduces the diagonal the same way (same value everywhere)
     double tr = 0.0;
-    for (int j = 0; j < K; ++j) tr += G[j + j * KM];
+    for (int j = lane; j < K; j += 32) tr += G[j + j * KM];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tr += __shfl_xor_sync(0xffffffffu, tr, o);
     const double s0 = 11.0 * (m * K + (double)K * (K + 1)) * CQ_U * tr;
+    __syncthreads();   // every thread has read the diagonal
     if (shifted && s0 > 0.0) {
-        __syncthreads();   // every thread has read the diagonal
         for (int j = tid; j < K; j += CQ_THREADS) G[j + j * KM] += s0;
         __syncthreads();
     }
-    const int nnull = cta_cholesky<KM>(G, K, s0 > 0.0 ? s0 : CQ_TINY, tid);
-    for (int idx = tid; idx < KM * KM; idx += CQ_THREADS) {
-        const int j = idx / KM, k = idx % KM;
-        double v = 0.0;
-        if (j <= k && k < K) {
-            const double p = sqrt(G[j + j * KM]);
-            v = j == k ? p : G[k + j * KM] / p;
-        }
-        Rr[j * KM + k] = v;
+    const int nnull = cta_cholesky<KM>(G, K, s0 > 0.0 ? s0 : CQ_TINY, iv, tid);
+    for (int j = tid; j < KM; j += CQ_THREADS) {
+        const double p = j < K ? sqrt(G[j + j * KM]) : 0.0;
+        rdg[j] = j < K ? 1.0 / p : 0.0;
+        Rr[j * L + j] = p;
     }
     __syncthreads();
-    for (int j = tid; j < KM; j += CQ_THREADS) rdg[j] = j < K ? 1.0 / Rr[j * KM + j] : 0.0;
+    for (int idx = tid; idx < KM * KM; idx += CQ_THREADS) {
+        const int j = idx / KM, k = idx % KM;
+        if (j != k) Rr[j * L + k] = (j < k && k < K) ? G[k + j * KM] * rdg[j] : 0.0;
+    }
     __syncthreads();
     return nnull;
 }
 
-// Rt <- Rr Rt (upper times upper, both row-major; consecutive threads take
-// consecutive columns: Rr read as a broadcast, Rt conflict-free) through the
-// scratch P, and rdt = 1/diag(Rt).  Entries outside [0, K) stay zero.
+// Rt <- Rr Rt (upper times upper, row-major, pitch RLD) on DMMA: warp w takes
+// the upper 8 x 8 output tiles q = w, w + 8, ... (NK = ceil(K / 8) tiles a
+// side), each the sum over M = I..J of Rr_IM Rt_MJ (the blocks of the two
+// factors are triangular with exact zeros below the diagonal, and zero past
+// K), into the scratch P, copied back after a barrier; rdt = 1/diag(Rt).
 template <int KM>
 __device__ void accumulate(const double *Rr, double *Rt, double *P, double *rdt, int K, int tid) {
-    for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
-        const int i = idx / K, j = idx % K;
-        double s = 0.0;
-        for (int k = i; k <= j; ++k) s += Rr[i * KM + k] * Rt[k * KM + j];
-        P[i * KM + j] = i <= j ? s : 0.0;
+    constexpr int L = CQSmem<KM>::RLD;
+    const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, tig = lane & 3;
+    const int NK = (K + 7) >> 3, NQ = NK * (NK + 1) / 2;
+    for (int q = warp; q < NQ; q += CQ_WARPS) {
+        int I = 0, rem = q;
+        while (rem >= NK - I) {
+            rem -= NK - I;
+            ++I;
+        }
+        const int J = I + rem;
+        double acc[2] = {0.0, 0.0};
+        for (int M = I; M <= J; ++M) {
+#pragma unroll
+            for (int k4 = 0; k4 < 8; k4 += 4)
+                dmma884(acc, Rr[(8 * I + g) * L + 8 * M + k4 + tig], Rt[(8 * M + k4 + tig) * L + 8 * J + g]);
+        }
+        P[(8 * I + g) * L + 8 * J + 2 * tig] = acc[0];
+        P[(8 * I + g) * L + 8 * J + 2 * tig + 1] = acc[1];
     }
     __syncthreads();
-    for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
-        const int i = idx / K, j = idx % K;
-        Rt[i * KM + j] = P[i * KM + j];
+    const int n8 = 8 * NK;
+    for (int idx = tid; idx < n8 * n8; idx += CQ_THREADS) {
+        const int i = idx / n8, j = idx % n8;
+        if ((i >> 3) <= (j >> 3)) Rt[i * L + j] = P[i * L + j];
     }
-    for (int j = tid; j < KM; j += CQ_THREADS) rdt[j] = j < K ? 1.0 / P[j * KM + j] : 0.0;
+    for (int j = tid; j < KM; j += CQ_THREADS) rdt[j] = j < K ? 1.0 / P[j * L + j] : 0.0;
     __syncthreads();
 }
 
-// P = R^-1 (R upper, row-major Rr with rdg = 1/diag), row-major: thread c
-// solves R p = e_c by back substitution (R read as broadcasts, P
-// conflict-free), four partial sums in flight.
+// P = R^-1 (R upper, row-major Rr with pitch RLD, rdg = 1/diag), row-major
+// pitch RLD, upper tiles only: the 8 x 8 diagonal blocks by back substitution
+// (warp I, lanes over columns), then the blocks at distance dlt = 1, 2, ...
+// from the diagonal, X_IJ = -X_II (sum_{M=I+1..J} R_IM X_MJ) on DMMA, one
+// barrier per distance; the inner sum passes through the warp's 8 x 8 scratch
+// in W to become an operand.
 template <int KM>
-__device__ void tri_inverse(const double *Rr, const double *rdg, double *P, int K, int tid) {
-    const int c = tid;
-    if (c < K) {
-        for (int i = K - 1; i >= 0; --i) {
-            double v = 0.0;
-            if (i == c) {
-                v = rdg[i];
-            } else if (i < c) {
-                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-                int l = i + 1;
-                for (; l + 3 <= c; l += 4) {
-                    a0 += Rr[i * KM + l] * P[l * KM + c];
-                    a1 += Rr[i * KM + l + 1] * P[(l + 1) * KM + c];
-                    a2 += Rr[i * KM + l + 2] * P[(l + 2) * KM + c];
-                    a3 += Rr[i * KM + l + 3] * P[(l + 3) * KM + c];
-                }
-                for (; l <= c; ++l) a0 += Rr[i * KM + l] * P[l * KM + c];
-                v = -((a0 + a1) + (a2 + a3)) * rdg[i];
-            }
-            P[i * KM + c] = v;
+__device__ void tri_inverse(const double *Rr, const double *rdg, double *P, double *W, int K, int tid) {
+    constexpr int L = CQSmem<KM>::RLD;
+    const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, tig = lane & 3;
+    const int NK = (K + 7) >> 3;
+    if (warp < NK && lane < 8) {
+        const int b0 = 8 * warp, c = lane;
+        double x[8];
+#pragma unroll
+        for (int i = 7; i >= 0; --i) {
+            double v = i == c ? 1.0 : 0.0;
+#pragma unroll
+            for (int m = i + 1; m < 8; ++m) v -= Rr[(b0 + i) * L + b0 + m] * x[m];
+            x[i] = i <= c ? v * rdg[b0 + i] : 0.0;
         }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) P[(b0 + i) * L + b0 + c] = x[i];
     }
     __syncthreads();
+    double *w = W + warp * 96;
+    for (int dlt = 1; dlt < NK; ++dlt) {
+        const int I = warp, J = warp + dlt;
+        if (J < NK) {
+            double tacc[2] = {0.0, 0.0};
+            for (int M = I + 1; M <= J; ++M) {
+#pragma unroll
+                for (int k4 = 0; k4 < 8; k4 += 4)
+                    dmma884(tacc, Rr[(8 * I + g) * L + 8 * M + k4 + tig], P[(8 * M + k4 + tig) * L + 8 * J + g]);
+            }
+            w[g * 12 + 2 * tig] = tacc[0];
+            w[g * 12 + 2 * tig + 1] = tacc[1];
+            __syncwarp();
+            double xacc[2] = {0.0, 0.0};
+#pragma unroll
+            for (int k4 = 0; k4 < 8; k4 += 4)
+                dmma884(xacc, -P[(8 * I + g) * L + 8 * I + k4 + tig], w[(k4 + tig) * 12 + g]);
+            P[(8 * I + g) * L + 8 * J + 2 * tig] = xacc[0];
+            P[(8 * I + g) * L + 8 * J + 2 * tig + 1] = xacc[1];
+        }
+        __syncthreads();
+    }
 }
 
 // QF: the tasks form Q (the range finder); instances without it carry no Q
@@ -339,15 +534,18 @@ __global__ void __launch_bounds__(CQ_THREADS, KM <= 32 ? 2 : 1) k_rcholqr(const 
     using S = CQSmem<KM>;
     constexpr bool STAGED = S::STAGED;
     constexpr int NACC = S::NACC;
-    extern __shared__ double sm[];
-    __shared__ double gmax_sh;
+    extern __shared__ __align__(16) double sm[];
+    __shared__ double gmax_sh[CQ_WARPS];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double *G = STAGED ? sm : sm + S::CHUNK;       // K x K Gram (column-major, ld KM)
-    double *Rr = STAGED ? sm + S::CHUNK : G + S::KK;    // factor of the step, row-major: Rr[j * KM + k] = R(j, k)
-    double *Rt = Rr + S::KK;                       // accumulated R, row-major
-    double *rdg = Rt + S::KK;                      // 1 / diag(Rr)
+    constexpr int L = S::RLD;
+    double *G = STAGED ? sm : sm + S::CHUNK;       // K x K Gram (column-major, ld KM); product scratch (pitch L)
+    double *Rr = STAGED ? sm + S::CHUNK : G + S::RR;    // factor of the step, row-major: Rr[j * L + k] = R(j, k)
+    double *Rt = Rr + S::RR;                       // accumulated R, row-major
+    double *rdg = Rt + S::RR;                      // 1 / diag(Rr)
     double *rdt = rdg + KM;                        // 1 / diag(Rt)
     double *dsc = rdt + KM;                        // column norms of the sketch, then their inverses
+    double *ivp = dsc + KM;                        // inverse pivots of the elimination
+    double *Wsc = sm + S::CHUNK - S::WS;           // per-warp 8 x 8 scratch
 
     const CQTask t = tasks[blockIdx.x];
     const int k1 = t.k1, K = t.k1 + t.k2, nb = t.nb;
@@ -407,7 +605,7 @@ __global__ void __launch_bounds__(CQ_THREADS, KM <= 32 ? 2 : 1) k_rcholqr(const 
 #pragma unroll
             for (int q = 0; q < NACC; ++q) acc[q][0] = acc[q][1] = 0.0;
             gram_chunk<KM>(s, acc, sm, tid, tmi, tni);
-            gram_reduce<KM>(acc, G, tid, tmi, tni);
+            gram_reduce<KM>(acc, G, sm, tid, tmi, tni);
             if (round == 0) {
                 for (int j = tid; j < KM; j += CQ_THREADS) {
                     const double d = j < K ? sqrt(G[j + j * KM]) : 1.0;
@@ -420,13 +618,16 @@ __global__ void __launch_bounds__(CQ_THREADS, KM <= 32 ? 2 : 1) k_rcholqr(const 
                 }
                 __syncthreads();
             }
-            factor<KM>(G, Rr, rdg, K, (double)CQ_CH, round == 0, tid);
+            factor<KM>(G, Rr, rdg, ivp, K, (double)CQ_CH, round == 0, tid);
             if (round == 0) {
                 // Rt = R1 D, then the substitution of round 1 scales by 1/d first
-                for (int idx = tid; idx < KM * KM; idx += CQ_THREADS) Rt[idx] = Rr[idx] * dsc[idx % KM];
+                for (int idx = tid; idx < KM * KM; idx += CQ_THREADS) {
+                    const int j = idx / KM, k = idx % KM;
+                    Rt[j * L + k] = Rr[j * L + k] * dsc[k];
+                }
                 __syncthreads();
                 for (int j = tid; j < KM; j += CQ_THREADS) {
-                    rdt[j] = j < K ? 1.0 / Rt[j * KM + j] : 0.0;
+                    rdt[j] = j < K ? 1.0 / Rt[j * L + j] : 0.0;
                     dsc[j] = 1.0 / dsc[j];
                 }
                 __syncthreads();
@@ -441,53 +642,58 @@ __global__ void __launch_bounds__(CQ_THREADS, KM <= 32 ? 2 : 1) k_rcholqr(const 
     for (int pass = 0;; ++pass) {
 #pragma unroll
         for (int q = 0; q < NACC; ++q) acc[q][0] = acc[q][1] = 0.0;
+        // this warp's 32 rows of each chunk, staged column-major; at widths of
+        // 48 and up (one CTA per SM, registers to spare) the next chunk's row is
+        // loaded into registers while this one is solved and multiplied
+        constexpr int P = STAGED ? CQ_LDZ : CQ_PITCH;
+        constexpr bool PREFETCH = KM >= 48;
+        double *zb = STAGED ? sm + warp * 32 : sm + warp * S::W;
+        double v[KM];
+        if (PREFETCH) load_row<KM>(t, STAGED ? tid : warp * 32 + lane, nb, k1, K, v);
 #pragma unroll 1
         for (int r0 = STAGED ? 0 : warp * 32; r0 < nb; r0 += CQ_THREADS) {
             const int row = r0 + (STAGED ? tid : lane);
             const bool valid = row < nb;
-            double x[KM];
-            {
-                // two column blocks, walked with one running pointer each
-                const double *p1 = t.X1 + row, *p2 = t.X2 + row;
+            if (!PREFETCH) load_row<KM>(t, row, nb, k1, K, v);
 #pragma unroll
-                for (int j = 0; j < KM; ++j) {
-                    double v = 0.0;
-                    if (j < k1) {
-                        if (valid) v = *p1;
-                        p1 += t.ld1;
-                    } else if (j < K) {
-                        if (valid) v = *p2;
-                        p2 += t.ld2;
-                    }
-                    x[j] = v;
-                }
-            }
-            // rdt and Rt are zero past K, so the padding columns stay zero
-            subst_rows<KM, 0>(x, Rt, rdt);
+            for (int j = 0; j < KM; ++j) zb[j * P + lane] = v[j];
+            if (PREFETCH && r0 + CQ_THREADS < nb) load_row<KM>(t, row + CQ_THREADS, nb, k1, K, v);
+            __syncwarp();
+            // rd and R are zero past K, so the padding columns stay zero
+            warp_trsm<KM, P>(zb, Rt, rdt, K, lane);
             if (valid && keep_y) {
                 double *pz = t.Z + row;
-#pragma unroll
-                for (int j = 0; j < KM; ++j, pz += nb)
-                    if (j < K) *pz = x[j];
+                for (int j = 0; j < K; ++j, pz += nb) *pz = zb[j * P + lane];
             }
-            gram_chunk<KM>(x, acc, sm, tid, tmi, tni);
+            if constexpr (STAGED) {
+                __syncthreads();
+                gram_tiles<KM>(acc, sm, lane, tmi, tni);
+                __syncthreads();
+            } else {
+                gram_warp<KM>(acc, zb, lane);
+                __syncwarp();
+            }
         }
-        gram_reduce<KM>(acc, G, tid, tmi, tni);
-        if (warp == 0) {
-            // ||G||_inf (rows of the symmetric G), max over lanes
+        gram_reduce<KM>(acc, G, sm, tid, tmi, tni);
+        {
+            // ||G||_inf: warp w sums the rows i = w, w + 8, ... (column i of the
+            // symmetric G, lanes over its entries), then the max over the warps
             double mx = 0.0;
-            for (int i = lane; i < K; i += 32) {
+            for (int i = warp; i < K; i += CQ_WARPS) {
                 double r = 0.0;
-                for (int j = 0; j < K; ++j) r += fabs(G[i + j * KM]);
+                for (int j = lane; j < K; j += 32) r += fabs(G[j + i * KM]);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
                 mx = fmax(mx, r);
             }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            if (lane == 0) gmax_sh = mx;
+            if (lane == 0) gmax_sh[warp] = mx;
         }
-        const int nnull = factor<KM>(G, Rr, rdg, K, (double)nb, false, tid);   // barriers: gmax_sh visible
+        const int nnull = factor<KM>(G, Rr, rdg, ivp, K, (double)nb, false, tid);   // barriers: gmax_sh visible
         if (nnull && tid == 0 && flags) atomicAdd(flags, nnull);
-        const bool again = !(gmax_sh <= CQ_GMAX) && pass + 1 < CQ_APPLY;
+        double gmax = 0.0;
+#pragma unroll
+        for (int w = 0; w < CQ_WARPS; ++w) gmax = fmax(gmax, gmax_sh[w]);
+        const bool again = !(gmax <= CQ_GMAX) && pass + 1 < CQ_APPLY;
         accumulate<KM>(Rr, Rt, G, rdt, K, tid);
         if (!again) break;
         if (tid == 0 && flags) atomicAdd(flags + 1, 1);
@@ -496,13 +702,13 @@ __global__ void __launch_bounds__(CQ_THREADS, KM <= 32 ? 2 : 1) k_rcholqr(const 
     // outputs: R (column-major); Rc^-1 for a deferred Q; or Q = Y Rc^-1
     for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
         const int i = idx % K, j = idx / K;
-        t.R[i + (size_t)j * K] = Rt[i * KM + j];
+        t.R[i + (size_t)j * K] = Rt[i * L + j];
     }
     if (!QF && t.Rinv) {
-        tri_inverse<KM>(Rr, rdg, G, K, tid);
+        tri_inverse<KM>(Rr, rdg, G, Wsc, K, tid);
         for (int idx = tid; idx < K * K; idx += CQ_THREADS) {
             const int i = idx % K, c = idx / K;
-            t.Rinv[i + (size_t)c * K] = i <= c ? G[i * KM + c] : 0.0;
+            t.Rinv[i + (size_t)c * K] = i <= c ? G[i * L + c] : 0.0;
         }
     }
     if constexpr (QF) {

@@ -148,6 +148,7 @@ struct hicma_tlr_ctx_s {
     // (1), the Householder pipeline for all (0; HICMA_TLR_QR=householder)
     int cholqr = 1;
     double *d_scal = nullptr;   // device scalars
+    double *d_profacc = nullptr;   // per profiling class: flops, bytes counted on the device
     int precision = HICMA_TLR_PREC_FP64;
     long long launches = 0;
     std::recursive_mutex mu;
@@ -282,6 +283,7 @@ enum {
     P_CHOLQR,     // QR factors by randomized CholeskyQR
     P_NCLASS
 };
+static_assert(P_NCLASS <= 32, "two device counters per class in d_profacc");
 
 cudaEvent_t pool_event(hicma_tlr_ctx *c) {
     if (!c->ev_pool.empty()) {
@@ -603,6 +605,22 @@ int run_core(hicma_tlr_ctx *c, std::vector<CoreTask> &v, int kmax, const CorePar
 
 int run_gemms_narrow(hicma_tlr_ctx *c, std::vector<GemmTask> &v, int cls);
 
+// Algorithmic flops and bytes of a GEMM batch known on the host; tasks whose n
+// is read on the device (n_dev, a rank decided by an earlier kernel) are left
+// out here and counted on the device when profiling (returns whether any).
+bool gemm_work(const std::vector<GemmTask> &v, double &fl, double &by) {
+    bool ndev = false;
+    for (auto &t : v) {
+        if (t.n_dev) {
+            ndev = true;
+            continue;
+        }
+        fl += 2.0 * t.m * (double)t.n * t.k;
+        by += 8.0 * ((double)t.m * t.k + (double)t.k * t.n + (t.beta != 0.0 ? 2.0 : 1.0) * t.m * (double)t.n);
+    }
+    return ndev;
+}
+
 int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false, int cls = 0) {
     if (v.empty()) return 0;
     TRY(bc_gemms(v));
@@ -624,12 +642,12 @@ int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false, int
     int *doff = stage(c, off.data(), off.size());
     if (!dt || !doff) { set_err("task staging failed"); return HICMA_TLR_ERR_CUDA; }
     double fl = 0, by = 0;
-    for (auto &t : v) {
-        fl += 2.0 * t.m * (double)t.n * t.k;
-        by += 8.0 * ((double)t.m * t.k + (double)t.k * t.n + (t.beta != 0.0 ? 2.0 : 1.0) * t.m * (double)t.n);
+    bool ndev = gemm_work(v, fl, by);
+    {
+        Prof pf(c, cls, fl, by);
+        launch_gemm_batched(dt, doff, (int)v.size(), off.back(), c->cur, fp32);
     }
-    Prof pf(c, cls, fl, by);
-    launch_gemm_batched(dt, doff, (int)v.size(), off.back(), c->cur, fp32);
+    if (ndev && c->prof) launch_gemm_devcount(dt, (int)v.size(), c->d_profacc + 2 * cls, c->cur);
     v.clear();
     return check_launch(c);
 }
@@ -647,12 +665,12 @@ int run_gemms_narrow(hicma_tlr_ctx *c, std::vector<GemmTask> &v, int cls) {
     int *doff = stage(c, off.data(), off.size());
     if (!dt || !doff) { set_err("task staging failed"); return HICMA_TLR_ERR_CUDA; }
     double fl = 0, by = 0;
-    for (auto &t : v) {
-        fl += 2.0 * t.m * (double)t.n * t.k;
-        by += 8.0 * ((double)t.m * t.k + (double)t.k * t.n + (t.beta != 0.0 ? 2.0 : 1.0) * t.m * (double)t.n);
+    bool ndev = gemm_work(v, fl, by);
+    {
+        Prof pf(c, cls, fl, by);
+        launch_gemm_batched_narrow(dt, doff, (int)v.size(), off.back(), c->cur);
     }
-    Prof pf(c, cls, fl, by);
-    launch_gemm_batched_narrow(dt, doff, (int)v.size(), off.back(), c->cur);
+    if (ndev && c->prof) launch_gemm_devcount(dt, (int)v.size(), c->d_profacc + 2 * cls, c->cur);
     v.clear();
     return check_launch(c);
 }
@@ -1157,6 +1175,7 @@ static void ctx_release(hicma_tlr_ctx *c) {
     if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->d_flags) cudaFree(c->d_flags);
     if (c->d_scal) cudaFree(c->d_scal);
+    if (c->d_profacc) cudaFree(c->d_profacc);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->stream_side) cudaStreamDestroy(c->stream_side);
@@ -1217,6 +1236,8 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     if ((e = cudaMalloc(&c->d_stage, c->stage_bytes)) != cudaSuccess) { c->d_stage = nullptr; return fail(e, "device staging"); }
     if ((e = cudaMalloc(&c->d_flags, 64 * sizeof(int))) != cudaSuccess) { c->d_flags = nullptr; return fail(e, "flags"); }
     if ((e = cudaMalloc(&c->d_scal, 64 * sizeof(double))) != cudaSuccess) { c->d_scal = nullptr; return fail(e, "scalars"); }
+    if ((e = cudaMalloc(&c->d_profacc, 64 * sizeof(double))) != cudaSuccess) { c->d_profacc = nullptr; return fail(e, "profiling counters"); }
+    if ((e = xclear(c, c->d_profacc, 64 * sizeof(double))) != cudaSuccess) return fail(e, "profiling counters reset");
     bc_add(c->d_ws, c->ws_bytes);
     bc_add(c->d_stage, c->stage_bytes);
     bc_add(c->d_flags, 64 * sizeof(int));
@@ -2735,6 +2756,8 @@ int hicma_tlr_prof_enable(hicma_tlr_ctx *c, int on) {
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     prof_flush(c);
     std::memset(c->prof_acc, 0, sizeof c->prof_acc);
+    TRY(ctx_sync(c));
+    CUDA_TRY(xclear(c, c->d_profacc, 64 * sizeof(double)));
     c->prof = on != 0;
     return 0;
 }
@@ -2743,8 +2766,12 @@ int hicma_tlr_prof_read(hicma_tlr_ctx *c, double *out, int nclass) {
     ARG_CHECK(c && out, "null");
     std::lock_guard<std::recursive_mutex> lk(c->mu);
     prof_flush(c);
+    // work counted on the device (GEMMs whose n is a rank decided on the device)
+    double dev[64];
+    TRY(ctx_sync(c));
+    CUDA_TRY(xfer(c, dev, c->d_profacc, sizeof dev, cudaMemcpyDeviceToHost));
     for (int k = 0; k < nclass && k < P_NCLASS; ++k)
-        for (int j = 0; j < 4; ++j) out[k * 4 + j] = c->prof_acc[k][j];
+        for (int j = 0; j < 4; ++j) out[k * 4 + j] = c->prof_acc[k][j] + (j >= 2 ? dev[2 * k + j - 2] : 0.0);
     return 0;
 }
 

@@ -57,6 +57,10 @@ void launch_gemm_single(const GemmTask &t, cudaStream_t st);
 constexpr int GEMM_NARROW_M = 128, GEMM_NARROW_N = 32;
 void launch_gemm_batched_narrow(const GemmTask *d_tasks, const int *d_tile_off, int ntasks, int total_tiles,
                                 cudaStream_t st);
+// Algorithmic work of the tasks whose n is read on the device (n_dev): adds
+// 2 m n k flops and 8 (m k + k n + m n (2 with beta)) bytes with the device's
+// n to acc[0], acc[1] (profiling; launched after the GEMMs on the same stream).
+void launch_gemm_devcount(const GemmTask *d_tasks, int ntasks, double *acc, cudaStream_t st);
 
 inline int gemm_tiles_m(int m) { return (m + 63) / 64; }
 inline int gemm_tiles(const GemmTask &t) { return gemm_tiles_m(t.m) * gemm_tiles_m(t.n); }
