@@ -141,16 +141,20 @@ __device__ __forceinline__ void gemm_tile(Smem<BM_, BN_> &sm, GemmTask t, int tm
     }
 }
 
+// Task of output tile `bid`: the group table (after the ntasks + 1 prefix
+// sums) names the task of the group's first tile; step forward from there.
+__device__ __forceinline__ int task_of(const int *__restrict__ tile_off, int ntasks, int bid) {
+    int lo = tile_off[ntasks + 1 + bid / GEMM_GROUP];
+    while (lo + 1 < ntasks && tile_off[lo + 1] <= bid) ++lo;
+    return lo;
+}
+
 template <int BM_, int BN_>
 __global__ void __launch_bounds__(NT, 3) k_gemm_batched(const GemmTask *__restrict__ tasks,
                                                      const int *__restrict__ tile_off, int ntasks) {
     __shared__ __align__(16) Smem<BM_, BN_> sm;
     const int bid = blockIdx.x;
-    int lo = 0, hi = ntasks - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tile_off[mid] <= bid) lo = mid; else hi = mid - 1;
-    }
+    const int lo = task_of(tile_off, ntasks, bid);
     const GemmTask t = tasks[lo];
     const int local = bid - tile_off[lo];
     gemm_tile<BM_, BN_>(sm, t, local % t.tiles_m, local / t.tiles_m);
@@ -171,11 +175,7 @@ __global__ void __launch_bounds__(256) k_sgemm_batched(const GemmTask *__restric
     __shared__ float As[FK][FB + 4];
     __shared__ float Bs[FK][FB + 4];
     const int bid = blockIdx.x;
-    int lo = 0, hi = ntasks - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tile_off[mid] <= bid) lo = mid; else hi = mid - 1;
-    }
+    const int lo = task_of(tile_off, ntasks, bid);
     GemmTask t = tasks[lo];
     const int local = bid - tile_off[lo];
     const int i0 = (local % t.tiles_m) * FB, j0 = (local / t.tiles_m) * FB;

@@ -123,20 +123,38 @@ __global__ void k_randtlr_finish(const double *__restrict__ Xr, const double *__
 }
 
 constexpr int CP_COLS = 4;
+constexpr int CP_ROWS = 4;   // row iterations whose loads are issued together
+// Copies (or scales, or adds into) CP_COLS columns of one task per CTA.  Source
+// and destination never overlap (__restrict__), so every thread issues the
+// loads of CP_COLS x CP_ROWS entries before its first store.
 __global__ void __launch_bounds__(256) k_copy_batched(const CopyTask *__restrict__ tasks) {
     const CopyTask t = tasks[blockIdx.y];
     const int c0 = blockIdx.x * CP_COLS;
     if (c0 >= t.cols) return;
-    const int cend = min(c0 + CP_COLS, t.cols);
-    for (int c = c0; c < cend; ++c) {
-        const double *s = t.src + (size_t)c * t.lds;
-        double *d = t.dst + (size_t)c * t.ldd;
-        if (t.beta != 0.0)
-            for (int r = threadIdx.x; r < t.rows; r += blockDim.x) d[r] = t.alpha * s[r] + t.beta * d[r];
-        else if (t.alpha == 1.0)
-            for (int r = threadIdx.x; r < t.rows; r += blockDim.x) d[r] = s[r];
-        else
-            for (int r = threadIdx.x; r < t.rows; r += blockDim.x) d[r] = t.alpha * s[r];
+    const int nc = min(CP_COLS, t.cols - c0);
+    const double *__restrict__ src = t.src + (size_t)c0 * t.lds;
+    double *__restrict__ dst = t.dst + (size_t)c0 * t.ldd;
+    const double alpha = t.alpha, beta = t.beta;
+    for (int r0 = threadIdx.x; r0 < t.rows; r0 += CP_ROWS * blockDim.x) {
+        double v[CP_COLS][CP_ROWS], w[CP_COLS][CP_ROWS];
+#pragma unroll
+        for (int c = 0; c < CP_COLS; ++c)
+#pragma unroll
+            for (int q = 0; q < CP_ROWS; ++q) {
+                const int r = r0 + q * blockDim.x;
+                const bool in = c < nc && r < t.rows;
+                v[c][q] = in ? src[(size_t)c * t.lds + r] : 0.0;
+                w[c][q] = (in && beta != 0.0) ? dst[(size_t)c * t.ldd + r] : 0.0;
+            }
+#pragma unroll
+        for (int c = 0; c < CP_COLS; ++c)
+#pragma unroll
+            for (int q = 0; q < CP_ROWS; ++q) {
+                const int r = r0 + q * blockDim.x;
+                if (c < nc && r < t.rows)
+                    dst[(size_t)c * t.ldd + r] = beta != 0.0 ? alpha * v[c][q] + beta * w[c][q]
+                                                             : (alpha == 1.0 ? v[c][q] : alpha * v[c][q]);
+            }
     }
 }
 

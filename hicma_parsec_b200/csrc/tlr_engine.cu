@@ -605,6 +605,20 @@ int run_core(hicma_tlr_ctx *c, std::vector<CoreTask> &v, int kmax, const CorePar
 
 int run_gemms_narrow(hicma_tlr_ctx *c, std::vector<GemmTask> &v, int cls);
 
+// Appends the group table to the tile prefix sums `off` (ntasks + 1 entries):
+// entry g names the task that holds tile GEMM_GROUP g.
+void gemm_groups(std::vector<int> &off) {
+    const int ntasks = (int)off.size() - 1, total = off[ntasks];
+    const int ngrp = (total + GEMM_GROUP - 1) / GEMM_GROUP;
+    off.reserve(off.size() + ngrp);
+    int task = 0;
+    for (int g = 0; g < ngrp; ++g) {
+        const int tile = g * GEMM_GROUP;
+        while (task + 1 < ntasks && off[task + 1] <= tile) ++task;
+        off.push_back(task);
+    }
+}
+
 // Algorithmic flops and bytes of a GEMM batch known on the host; tasks whose n
 // is read on the device (n_dev, a rank decided by an earlier kernel) are left
 // out here and counted on the device when profiling (returns whether any).
@@ -638,6 +652,7 @@ int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false, int
     off[0] = 0;
     for (size_t i = 0; i < v.size(); ++i) off[i + 1] = off[i] + gemm_tiles(v[i]);
     if (off.back() == 0) { v.clear(); return 0; }
+    gemm_groups(off);
     GemmTask *dt = stage(c, v.data(), v.size());
     int *doff = stage(c, off.data(), off.size());
     if (!dt || !doff) { set_err("task staging failed"); return HICMA_TLR_ERR_CUDA; }
@@ -645,7 +660,7 @@ int run_gemms(hicma_tlr_ctx *c, std::vector<GemmTask> &v, bool fp32 = false, int
     bool ndev = gemm_work(v, fl, by);
     {
         Prof pf(c, cls, fl, by);
-        launch_gemm_batched(dt, doff, (int)v.size(), off.back(), c->cur, fp32);
+        launch_gemm_batched(dt, doff, (int)v.size(), off[v.size()], c->cur, fp32);
     }
     if (ndev && c->prof) launch_gemm_devcount(dt, (int)v.size(), c->d_profacc + 2 * cls, c->cur);
     v.clear();
@@ -661,6 +676,7 @@ int run_gemms_narrow(hicma_tlr_ctx *c, std::vector<GemmTask> &v, int cls) {
         off[i + 1] = off[i] + t.tiles_m * ((t.n + GEMM_NARROW_N - 1) / GEMM_NARROW_N);
     }
     if (off.back() == 0) { v.clear(); return 0; }
+    gemm_groups(off);
     GemmTask *dt = stage(c, v.data(), v.size());
     int *doff = stage(c, off.data(), off.size());
     if (!dt || !doff) { set_err("task staging failed"); return HICMA_TLR_ERR_CUDA; }
@@ -668,9 +684,36 @@ int run_gemms_narrow(hicma_tlr_ctx *c, std::vector<GemmTask> &v, int cls) {
     bool ndev = gemm_work(v, fl, by);
     {
         Prof pf(c, cls, fl, by);
-        launch_gemm_batched_narrow(dt, doff, (int)v.size(), off.back(), c->cur);
+        launch_gemm_batched_narrow(dt, doff, (int)v.size(), off[v.size()], c->cur);
     }
     if (ndev && c->prof) launch_gemm_devcount(dt, (int)v.size(), c->d_profacc + 2 * cls, c->cur);
+    v.clear();
+    return check_launch(c);
+}
+
+// Batched inner products P = C^T W of nb-long columns (split-K DMMA, one CTA
+// per product; k_gram_batched).
+int run_grams(hicma_tlr_ctx *c, std::vector<GramTask> &v, int cls) {
+    if (v.empty()) return 0;
+#ifdef TLR_BOUNDS_CHECK
+    for (size_t i = 0; i < v.size(); ++i) {
+        const GramTask &t = v[i];
+        BC(t.C, bc_span(t.nb, t.rc, t.nb), "gram C", i);
+        BC(t.W, bc_span(t.nb, t.ra, t.nb), "gram W", i);
+        BC(t.P, bc_span(t.rc, t.ra, t.rc), "gram P", i);
+    }
+#endif
+    double fl = 0.0, by = 0.0;
+    for (auto &g : v) {
+        fl += 2.0 * g.nb * (double)g.rc * g.ra;
+        by += 8.0 * g.nb * (double)(g.rc + g.ra);
+    }
+    GramTask *d = stage(c, v.data(), v.size());
+    if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+    {
+        Prof pf(c, cls, fl, by);
+        launch_gram_batched(d, (int)v.size(), c->cur);
+    }
     v.clear();
     return check_launch(c);
 }
@@ -942,15 +985,17 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             (cq ? cores : coresS).push_back(ct);
             if (cq) {
                 // new U = Q_U U_r = X2 (R3^-1 U_r)
-                GemmTask tu = make_gemm(0, 0, K, maxrank, K, 1.0, RinvU, K, SU, K, 0.0, TU, K);
+                // (the new rank, read on the device, is at most min(K, maxrank): the grid stops there)
+                const int rcap = std::min(K, maxrank);
+                GemmTask tu = make_gemm(0, 0, K, rcap, K, 1.0, RinvU, K, SU, K, 0.0, TU, K);
                 tu.n_dev = ct.rank_task;
                 gTU.push_back(tu);
-                GemmTask u = make_gemm(0, 0, nb, maxrank, K, 1.0, Us, nb, TU, K, 0.0, t.outU, nb);
+                GemmTask u = make_gemm(0, 0, nb, rcap, K, 1.0, Us, nb, TU, K, 0.0, t.outU, nb);
                 u.n_dev = ct.rank_task;
                 gU.push_back(u);
             } else if (rc > 0) {
                 // new U = Q(Wu) [U_bot; 0] + Cu U_top (beta 1 after the Q application when ra > 0)
-                GemmTask u = make_gemm(0, 0, nb, maxrank, rc, 1.0, Us, nb, SU, K, ra > 0 ? 1.0 : 0.0, t.outU, nb);
+                GemmTask u = make_gemm(0, 0, nb, std::min(K, maxrank), rc, 1.0, Us, nb, SU, K, ra > 0 ? 1.0 : 0.0, t.outU, nb);
                 u.n_dev = ct.rank_task;
                 gUS.push_back(u);
             }
@@ -958,7 +1003,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             GemmTask a = make_gemm(1, 0, K, K, K, 1.0, RU, K, SU, K, 0.0, T1, K);
             a.n_dev = ct.rank_task;
             (cq ? g3 : g3S).push_back(a);
-            GemmTask b = make_gemm(0, 0, nb, maxrank, K, 1.0, Vsrc, nb, T1, K, 0.0, t.outV, nb);
+            GemmTask b = make_gemm(0, 0, nb, std::min(K, maxrank), K, 1.0, Vsrc, nb, T1, K, 0.0, t.outV, nb);
             b.n_dev = ct.rank_task;
             (cq ? g4 : g4S).push_back(b);
         }
@@ -970,18 +1015,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             launch_precision_select(d, (int)sels.size(), thr2, c->d_flags + 4, c->cur);
             TRY(check_launch(c));
         }
-        if (!grams.empty()) {
-            double fl = 0.0, by = 0.0;
-            for (auto &g : grams) {
-                fl += 2.0 * g.nb * (double)g.rc * g.ra;
-                by += 8.0 * g.nb * (double)(g.rc + g.ra);
-            }
-            Prof pf(c, P_GRAM, fl, by);
-            GramTask *d = stage(c, grams.data(), grams.size());
-            if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
-            launch_gram_batched(d, (int)grams.size(), c->cur);
-            TRY(check_launch(c));
-        }
+        TRY(run_grams(c, grams, P_GRAM));
         TRY(run_gemms(c, g1, false, P_GEMM_Y));
         TRY(run_gemms(c, g1s, true, P_GEMM_Y));
         TRY(run_gemms(c, g2, false, P_GEMM_Y));
@@ -1729,11 +1763,11 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
                 ct.SU = SU; ct.RUc = nullptr; ct.work = nullptr;
                 ct.rank_out = t.rank_dst; ct.rank_task = rt; ct.K = s;
                 cores.push_back(ct);
-                GemmTask gU = make_gemm(0, 0, nb, maxrank, s, 1.0, Q, nb, SU, s, 0.0, t.outU, nb);
+                GemmTask gU = make_gemm(0, 0, nb, std::min(s, maxrank), s, 1.0, Q, nb, SU, s, 0.0, t.outU, nb);
                 gU.n_dev = rt;
                 gu.push_back(gU);
                 // V Sigma = (A^T Q) U_r  (R_U = I)
-                GemmTask g = make_gemm(0, 0, nb, maxrank, s, 1.0, W, nb, SU, s, 0.0, t.outV, nb);
+                GemmTask g = make_gemm(0, 0, nb, std::min(s, maxrank), s, 1.0, W, nb, SU, s, 0.0, t.outV, nb);
                 g.n_dev = rt;
                 gv.push_back(g);
                 continue;
@@ -1760,7 +1794,7 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
             cores.push_back(ct);
             au.push_back(QApplyTask{Y, TY, SU, t.outU, rt, nb, s, nb, s, nb, maxrank});
             // V Sigma = (A^T Q) U_r  (R_U = I)
-            GemmTask g = make_gemm(0, 0, nb, maxrank, s, 1.0, Wk, nb, SU, s, 0.0, t.outV, nb);
+            GemmTask g = make_gemm(0, 0, nb, std::min(s, maxrank), s, 1.0, Wk, nb, SU, s, 0.0, t.outV, nb);
             g.n_dev = rt;
             gv.push_back(g);
         }
@@ -2007,6 +2041,7 @@ static int run_syrk(hicma_tlr_ctx *c, hicma_tlr_desc *A, int k, const std::vecto
     const int NB = A->NB;
     const size_t mark = c->ar->off;
     std::vector<GemmTask> g1, g2, g3;
+    std::vector<GramTask> gw;
     for (int m : ms) {
         if (A->is_dense(m, k)) {
             g1.push_back(make_gemm(0, 1, NB, NB, NB, -1.0, A->dense(m, k), NB, A->dense(m, k), NB, 1.0,
@@ -2018,17 +2053,20 @@ static int run_syrk(hicma_tlr_ctx *c, hicma_tlr_desc *A, int k, const std::vecto
         double *W = ws_alloc<double>(c, (size_t)r * r);
         double *X = ws_alloc<double>(c, (size_t)NB * r);
         if (!W || !X) {
-            TRY(run_gemms(c, g1, false, P_GEMM_SYRK)); TRY(run_gemms(c, g2, false, P_GEMM_SYRK)); TRY(run_gemms(c, g3, false, P_GEMM_SYRK));
+            TRY(run_gemms(c, g1, false, P_GEMM_SYRK)); TRY(run_grams(c, gw, P_GEMM_SYRK));
+            TRY(run_gemms(c, g2, false, P_GEMM_SYRK)); TRY(run_gemms(c, g3, false, P_GEMM_SYRK));
             c->ar->off = mark;
             W = ws_alloc<double>(c, (size_t)r * r);
             X = ws_alloc<double>(c, (size_t)NB * r);
             if (!W || !X) { set_err("workspace too small (syrk)"); return HICMA_TLR_ERR_OOM; }
         }
-        g1.push_back(make_gemm(1, 0, r, r, NB, 1.0, A->V(m, k), NB, A->V(m, k), NB, 0.0, W, r));
+        // V^T V: an NB-long reduction into r x r (split-K, not one long-K GEMM tile)
+        gw.push_back(GramTask{A->V(m, k), A->V(m, k), W, NB, r, r});
         g2.push_back(make_gemm(0, 0, NB, r, r, 1.0, A->U(m, k), NB, W, r, 0.0, X, NB));
         g3.push_back(make_gemm(0, 1, NB, NB, r, -1.0, X, NB, A->U(m, k), NB, 1.0, A->dense(m, m), NB));
     }
     TRY(run_gemms(c, g1, false, P_GEMM_SYRK));
+    TRY(run_grams(c, gw, P_GEMM_SYRK));
     TRY(run_gemms(c, g2, false, P_GEMM_SYRK));
     TRY(run_gemms(c, g3, false, P_GEMM_SYRK));
     c->ar->off = mark;
@@ -2064,19 +2102,20 @@ static int run_syrk_lazy(hicma_tlr_ctx *c, hicma_tlr_desc *A, int m) {
         double *Yc = ws_alloc<double>(c, (size_t)NB * sumr);
         double *Uc = ws_alloc<double>(c, (size_t)NB * sumr);
         if (!Yc || !Uc) { set_err("workspace too small (syrk, K=%zu)", sumr); return HICMA_TLR_ERR_OOM; }
-        std::vector<GemmTask> g1, g2;
+        std::vector<GramTask> g1;
+        std::vector<GemmTask> g2;
         std::vector<CopyTask> cp;
         size_t off = 0;
         for (size_t t = p; t < q; ++t) {
             const int j = js[t], r = A->rank(m, j);
             double *W = ws_alloc<double>(c, (size_t)r * r);
             if (!W) { set_err("workspace too small (syrk)"); return HICMA_TLR_ERR_OOM; }
-            g1.push_back(make_gemm(1, 0, r, r, NB, 1.0, A->V(m, j), NB, A->V(m, j), NB, 0.0, W, r));
+            g1.push_back(GramTask{A->V(m, j), A->V(m, j), W, NB, r, r});
             g2.push_back(make_gemm(0, 0, NB, r, r, 1.0, A->U(m, j), NB, W, r, 0.0, Yc + off * NB, NB));
             cp.push_back(make_copy(A->U(m, j), NB, Uc + off * NB, NB, NB, r));
             off += r;
         }
-        TRY(run_gemms(c, g1, false, P_GEMM_SYRK));
+        TRY(run_grams(c, g1, P_GEMM_SYRK));
         TRY(run_gemms(c, g2, false, P_GEMM_SYRK));
         TRY(run_copies(c, cp));
         std::vector<GemmTask> g3{make_gemm(0, 1, NB, NB, (int)sumr, -1.0, Yc, NB, Uc, NB, 1.0, A->dense(m, m), NB, 1)};

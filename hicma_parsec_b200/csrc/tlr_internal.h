@@ -49,6 +49,10 @@ struct GemmTask {
 // Single-precision variant used by the mixed-precision policy: operands are
 // FP64 in memory, products are formed in FP32 with FP32 accumulation and the
 // result is written back in FP64.
+// d_tile_off: prefix sums of the tasks' tile counts (ntasks + 1 entries),
+// followed by the group table: entry g is the task that holds tile 32 g
+// (ceil(total_tiles / 32) entries), so a CTA finds its task in a step or two.
+constexpr int GEMM_GROUP = 32;
 void launch_gemm_batched(const GemmTask *d_tasks, const int *d_tile_off, int ntasks,
                          int total_tiles, cudaStream_t st, bool fp32 = false);
 void launch_gemm_single(const GemmTask &t, cudaStream_t st);
