@@ -95,7 +95,11 @@ __device__ __forceinline__ void gemm_tile(Smem<BM_, BN_> &sm, GemmTask t, int tm
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
 
-    const int ktiles = (t.k + BK - 1) / BK;
+    // a triangular operand leaves the rest of the inner dimension zero for this tile
+    int kend = t.k;
+    if (t.tri == 1) kend = min(kend, i0 + BM_);
+    else if (t.tri == 2) kend = min(kend, j0 + BN_);
+    const int ktiles = (kend + BK - 1) / BK;
     if (ktiles > 0) load_stage<BM_, BN_>(sm, 0, t, i0, j0, 0);
     for (int kt = 0; kt < ktiles; ++kt) {
         const int s = kt & 1;
@@ -187,7 +191,10 @@ __global__ void __launch_bounds__(256) k_sgemm_batched(const GemmTask *__restric
     if (j0 >= t.n) return;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     float acc[4][4] = {};
-    for (int k0 = 0; k0 < t.k; k0 += FK) {
+    int kend = t.k;
+    if (t.tri == 1) kend = min(kend, i0 + FB);
+    else if (t.tri == 2) kend = min(kend, j0 + FB);
+    for (int k0 = 0; k0 < kend; k0 += FK) {
         for (int e = tid; e < FB * FK; e += 256) {
             int i, kk;
             if (t.opA == 0) { i = e & (FB - 1); kk = e / FB; } else { kk = e & (FK - 1); i = e / FK; }

@@ -629,7 +629,8 @@ bool gemm_work(const std::vector<GemmTask> &v, double &fl, double &by) {
             ndev = true;
             continue;
         }
-        fl += 2.0 * t.m * (double)t.n * t.k;
+        // a triangular operand (L^-1 of a tile) holds half the products: m n k
+        fl += (t.tri ? 1.0 : 2.0) * t.m * (double)t.n * t.k;
         by += 8.0 * ((double)t.m * t.k + (double)t.k * t.n + (t.beta != 0.0 ? 2.0 : 1.0) * t.m * (double)t.n);
     }
     return ndev;
@@ -2248,11 +2249,15 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                     tmp = ws_alloc<double>(c, (size_t)NB * r);
                     if (!tmp) { set_err("workspace too small (trsm)"); return HICMA_TLR_ERR_OOM; }
                 }
+                // L^-1 is lower triangular with zeros above the diagonal: each output
+                // tile runs its inner dimension only as far as L^-1 has entries
                 if (dense) {
                     g.push_back(make_gemm(0, 1, NB, NB, NB, 1.0, A->dense(m, k), NB, Li, NB, 0.0, tmp, NB));
+                    g.back().tri = 2;
                     cp.push_back(make_copy(tmp, NB, A->dense(m, k), NB, NB, NB));
                 } else {
                     g.push_back(make_gemm(0, 0, NB, r, NB, 1.0, Li, NB, A->V(m, k), NB, 0.0, tmp, NB));
+                    g.back().tri = 1;
                     cp.push_back(make_copy(tmp, NB, A->V(m, k), NB, NB, r));
                 }
             }
@@ -2712,6 +2717,7 @@ static int solve_dev(hicma_tlr_ctx *c, hicma_tlr_desc *A, double *X, int nrhs) {
     for (int k = 0; k < NT; ++k) {
         double *xk = X + (size_t)k * NB;
         g1.push_back(make_gemm(0, 0, NB, nrhs, NB, 1.0, A->linv(k), NB, xk, (int)N, 0.0, tmp, NB));
+        g1.back().tri = 1;   // L^-1 lower triangular
         TRY(run_gemms(c, g1));
         cp.push_back(make_copy(tmp, NB, xk, (int)N, NB, nrhs));
         TRY(run_copies(c, cp));

@@ -44,6 +44,8 @@ struct GemmTask {
     int tiles_m;        // ceil(m / 64)
     double alpha, beta;
     const int *n_dev;   // if set, n = min(n, *n_dev) at run time (rank known on device only)
+    int tri = 0;        // 1: A lower triangular (an output row tile at i0 needs k < i0 + BM);
+                        // 2: op(B) upper triangular (a column tile at j0 needs k < j0 + BN)
 };
 
 // Single-precision variant used by the mixed-precision policy: operands are
