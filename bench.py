@@ -593,7 +593,9 @@ def run_ours(args, cfg):
 def serving_stream(requests: int, nmax: int, slots: int, rate: float, workspace_gb: float) -> dict:
     """The same seeded ML requests served sequentially on one slot and by the
     continuous-batching loop (all at t=0): solves/s, p50/p99 latency, and the
-    largest relative log-likelihood difference between the two runs."""
+    largest relative log-likelihood difference between the two runs.  Each
+    mode serves the stream once untimed on its server (first-use costs: slot
+    workspaces, kernel attributes) and is timed on the second pass."""
     import torch
     from hicma_parsec_b200 import serving
     reqs = serving.sample_requests(requests, seed=0, rate=rate, n_max=nmax)
@@ -601,6 +603,7 @@ def serving_stream(requests: int, nmax: int, slots: int, rate: float, workspace_
     ref = None
     for mode, sl in (("sequential", 1), ("continuous", slots)):
         srv = serving.MLEServer(0, slots=sl, workspace_bytes=int(workspace_gb * (1 << 30) / max(sl, 1)))
+        srv.run(reqs, realtime=False)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         res = srv.run(reqs, realtime=False)
@@ -632,6 +635,7 @@ def run_serving(args):
     for mode, slots, realtime in (("sequential", 1, False), ("continuous", args.slots, False),
                                   ("continuous_poisson", args.slots, True)):
         srv = serving.MLEServer(0, slots=slots, workspace_bytes=int(args.workspace_gb * (1 << 30) / max(slots, 1)))
+        srv.run(reqs[:2], realtime=False)   # first-use costs, untimed
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         res = srv.run(reqs, realtime=realtime)
