@@ -129,6 +129,7 @@ struct hicma_tlr_ctx_s {
     cudaStream_t stream = nullptr;      // bulk work
     cudaStream_t stream_hi = nullptr;   // critical path (high priority): SYRK(k,k+1) + POTRF(k+1)
     cudaStream_t stream_side = nullptr; // wide recompressions (Householder chain) beside the CholeskyQR chain
+    cudaStream_t stream_copy = nullptr; // copy-out of final factor columns during a factorization
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaStream_t cur = nullptr;         // stream the helpers launch on
     char *d_ws = nullptr;
@@ -178,6 +179,10 @@ struct hicma_tlr_desc_s {
     // HiCMA_dpotrf_L_2flow.jdf:353-361,683-691,1101-1106): per off-band tile the
     // rank it entered with and the smallest / largest rank it held; -1 elsewhere
     std::vector<int> rk_init, rk_min, rk_max;
+    // copy-out armed by hicma_tlr_store_stream for the next factorization
+    double *strm_buf = nullptr;
+    size_t strm_cap = 0, strm_off = 0;
+    bool strm_over = false;
     double *d_linv = nullptr;
     bool factored = false;
     double stats[16] = {0};
@@ -205,6 +210,7 @@ size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 int ctx_sync(hicma_tlr_ctx *c) {
     CUDA_TRY(cudaStreamSynchronize(c->stream_hi));
     CUDA_TRY(cudaStreamSynchronize(c->stream_side));
+    CUDA_TRY(cudaStreamSynchronize(c->stream_copy));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->stage_off = 0;
     return 0;
@@ -1214,6 +1220,7 @@ static void ctx_release(hicma_tlr_ctx *c) {
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->stream_side) cudaStreamDestroy(c->stream_side);
+    if (c->stream_copy) cudaStreamDestroy(c->stream_copy);
     if (c->stream_hi) cudaStreamDestroy(c->stream_hi);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -1238,6 +1245,7 @@ int hicma_tlr_init(int device, size_t workspace_bytes, hicma_tlr_ctx **out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->stream_hi, cudaStreamNonBlocking, prio_hi);
     if (e != cudaSuccess) return fail(e, "priority stream");
     e = cudaStreamCreateWithFlags(&c->stream_side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream_copy, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) return fail(e, "side stream");
@@ -2035,6 +2043,44 @@ int hicma_tlr_band_regenerate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, con
 }
 
 // ------------------------------------------------------- factorization -----
+// Copy-out of factor column k (armed by hicma_tlr_store_stream) after `ready`
+// on the copy stream, in the stream layout: the band tiles (m, k),
+// m = k..min(NT-1, k+band-1), then the packed [U, V] of the off-band tiles
+// (m, k), m = k+band..NT-1, with their final ranks.  A column that does not
+// fit the buffer stops the copy-out (stats[15] = -1).
+static int stream_column(hicma_tlr_ctx *c, hicma_tlr_desc *A, int k, cudaEvent_t ready) {
+    if (A->strm_over) return 0;
+    const size_t NB = A->NB;
+    const int NT = A->NT;
+    size_t need = 0;
+    for (int m = k; m < NT; ++m)
+        need += A->is_dense(m, k) ? NB * NB : 2 * NB * (size_t)std::max(A->rank(m, k), 0);
+    if (A->strm_off + need * sizeof(double) > A->strm_cap) {
+        A->strm_over = true;
+        return 0;
+    }
+    CUDA_TRY(cudaStreamWaitEvent(c->stream_copy, ready, 0));
+    double *p = A->strm_buf + A->strm_off / sizeof(double);
+    for (int m = k; m < NT; ++m) {
+        if (A->is_dense(m, k)) {
+            CUDA_TRY(cudaMemcpyAsync(p, A->dense(m, k), NB * NB * sizeof(double), cudaMemcpyDeviceToHost,
+                                     c->stream_copy));
+            p += NB * NB;
+        } else {
+            const int r = A->rank(m, k);
+            if (r > 0) {
+                CUDA_TRY(cudaMemcpyAsync(p, A->U(m, k), NB * r * sizeof(double), cudaMemcpyDeviceToHost,
+                                         c->stream_copy));
+                CUDA_TRY(cudaMemcpyAsync(p + NB * r, A->V(m, k), NB * r * sizeof(double), cudaMemcpyDeviceToHost,
+                                         c->stream_copy));
+                p += 2 * NB * (size_t)r;
+            }
+        }
+    }
+    A->strm_off += need * sizeof(double);
+    return 0;
+}
+
 // SYRK(k, m) for the listed m on the current stream/arena:
 // dense T -= A A^T (CORE_dsyrk), low rank T -= U (V^T V) U^T (HCORE_dsyrk),
 // HiCMA_dpotrf_L_2flow.jdf:503-565; rank 0 skips (:511-513).
@@ -2278,6 +2324,9 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
         }
         CUDA_TRY(cudaEventRecord(ev[T1], c->stream));
         if (k + 2 >= NT) CUDA_TRY(cudaEventRecord(evT, c->stream));
+        // column k of the factor is final (POTRF(k) and its TRSMs are done): copy it
+        // out on the copy stream while the later panels run
+        if (A->strm_buf) TRY(stream_column(c, A, k, ev[T1]));
         std::vector<RecompTask> rec;
         std::vector<int> rec_case;
         std::vector<std::array<int, 5>> rec_meta;
@@ -2475,6 +2524,8 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     A->stats[12] = t_gap;
     A->stats[13] = NT;
     A->stats[14] = flags_h[6];
+    A->stats[15] = A->strm_buf ? (A->strm_over ? -1.0 : (double)A->strm_off) : 0.0;
+    A->strm_buf = nullptr;   // the arming is used by one factorization
     A->factored = (info == 0);
     c->main_ar.off = 0;
     c->hi_ar.off = 0;
@@ -2651,6 +2702,16 @@ int hicma_tlr_store_set(hicma_tlr_ctx *c, hicma_tlr_desc *A, const double *buf, 
     CUDA_TRY(cudaMemcpyAsync(A->d_rank, A->h_rank.data(), NT * NT * sizeof(int), cudaMemcpyHostToDevice, c->stream));
     A->factored = false;
     return ctx_sync(c);
+}
+
+int hicma_tlr_store_stream(hicma_tlr_ctx *c, hicma_tlr_desc *A, double *buf, size_t bytes) {
+    ARG_CHECK(c && A, "null");
+    std::lock_guard<std::recursive_mutex> lk(c->mu);
+    A->strm_buf = buf;
+    A->strm_cap = buf ? bytes : 0;
+    A->strm_off = 0;
+    A->strm_over = false;
+    return 0;
 }
 
 int hicma_tlr_uncompress(hicma_tlr_ctx *c, hicma_tlr_desc *A, double *dense, long ld) {

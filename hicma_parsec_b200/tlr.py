@@ -112,6 +112,7 @@ def load_library(path: str | None = None):
         "hicma_tlr_store_bytes": (i, [vp, vp, C.POINTER(C.c_size_t)]),
         "hicma_tlr_store_get": (i, [vp, vp, vp, vp]),
         "hicma_tlr_store_set": (i, [vp, vp, vp, vp]),
+        "hicma_tlr_store_stream": (i, [vp, vp, vp, C.c_size_t]),
         "hicma_tlr_logdet": (i, [vp, vp, dp]),
         "hicma_tlr_solve": (i, [vp, vp, i, vp, C.c_long]),
         "hicma_tlr_loglik": (i, [vp, vp, vp, dp, dp, vp]),
@@ -382,6 +383,12 @@ class TLRMatrix:
 
     def store_set(self, buf_ptr: int, ranks: np.ndarray) -> None:
         _check(self.lib.hicma_tlr_store_set(self.ctx.h, self.h, C.c_void_p(buf_ptr), _p(ranks)), "hicma_tlr_store_set")
+
+    def store_stream(self, buf_ptr: int | None, nbytes: int = 0) -> None:
+        """Arm the copy-out of the next factorization into host memory at
+        buf_ptr (column layout, hicma_tlr_store_stream); None disarms."""
+        _check(self.lib.hicma_tlr_store_stream(self.ctx.h, self.h, C.c_void_p(buf_ptr or 0), nbytes),
+               "hicma_tlr_store_stream")
 
     def check(self, prob: Problem, approx: "TLRMatrix | None" = None):
         """(||L L^T - A|| / ||A||, ||L - L0|| / ||L||) on the device."""

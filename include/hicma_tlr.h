@@ -224,6 +224,19 @@ int hicma_tlr_store_bytes(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, size_t *bytes_n
 int hicma_tlr_store_get(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, double *buf, int *Ar);
 int hicma_tlr_store_set(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, const double *buf, const int *Ar);
 
+/* Copy-out during the factorization (no reference counterpart): the next
+ * hicma_tlr_dpotrf_L on A copies each tile column of the factor into buf as
+ * soon as the column is final, on a copy stream that overlaps the remaining
+ * panels.  Layout, column n = 0..NT-1 in order: the band tiles (m, n),
+ * m = n..min(NT-1, n+band-1), NB x NB each, then the packed [U, V] of the
+ * off-band tiles (m, n), m = n+band..NT-1, NB x rank each with the final ranks
+ * (hicma_tlr_rank_gather).  buf should be page-locked for the copies to
+ * overlap.  When the call returns, hicma_tlr_last_stats s[15] holds the bytes
+ * written, or -1 if a column did not fit in `bytes` (the factor is complete on
+ * the device either way; hicma_tlr_store_get still works).  One factorization
+ * consumes the arming; buf = NULL disarms. */
+int hicma_tlr_store_stream(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, double *buf, size_t bytes);
+
 /* Additions beyond the reference (no reference counterpart; testing_dpotrf.c stops at
  * the factor).  Require a factored descriptor. */
 int hicma_tlr_logdet(hicma_tlr_ctx *ctx, hicma_tlr_desc *A, double *logdet);
@@ -258,7 +271,9 @@ int hicma_tlr_serve_loglik(hicma_tlr_ctx *ctx, const hicma_tlr_problem *prob, in
  * the ones before them, or zero; 0 in the usual run), [12] seconds the device sat idle between panels (from the end
  * of a panel's last kernel to the start of the next panel's first, CUDA
  * events), [13] panels, [14] CholeskyQR passes over a stack's rows repeated
- * because its sketch missed a direction (0 in the usual run).  nstats <= 16. */
+ * because its sketch missed a direction (0 in the usual run), [15] bytes copied
+ * out by hicma_tlr_store_stream (-1: the buffer was too small; 0: not armed).
+ * nstats <= 16. */
 int hicma_tlr_last_stats(hicma_tlr_desc *A, double *stats, int nstats);
 
 /* --check of the reference driver (check_dpotrf2 and check_diff,

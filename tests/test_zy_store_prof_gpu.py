@@ -92,3 +92,49 @@ def test_copy_adopts_a_widened_band(ctx):
         A.close()
         B.close()
         C.close()
+
+
+def test_store_stream_copies_each_final_column(ctx):
+    """hicma_tlr_store_stream: the factorization copies every tile column into a
+    page-locked host buffer as the column becomes final (column layout: band
+    tiles, then the packed [U, V] of the off-band tiles with their final ranks),
+    checked tile by tile against the factored descriptor; stats[15] is the byte
+    count.  A buffer too small for the factor stops the copy-out (stats[15] = -1)
+    and leaves the factor itself unchanged; the arming lasts one factorization."""
+    from hicma_parsec_b200 import tlr
+    nt = N // NB
+    prob = tlr.Problem(kind=2, noise=0.1)
+    A = tlr.TLRMatrix(ctx, N, NB, MAXRANK, BAND)
+    B = tlr.TLRMatrix(ctx, N, NB, MAXRANK, BAND)
+    try:
+        assert A.generate(prob, TOL, MAXRANK) == 0
+        B.copy_from(A)
+        cap = (nt * BAND * NB * NB + nt * nt * NB * MAXRANK) * 8
+        buf = torch.empty(cap // 8, dtype=torch.float64, pin_memory=True)
+        A.store_stream(buf.data_ptr(), cap)
+        assert A.potrf(TOL) == 0
+        written = int(A.stats()[15])
+        assert written > 0
+        host = buf.numpy()
+        p = 0
+        for n in range(nt):
+            for m in range(n, nt):
+                t = A.tile(m, n)
+                if m - n < BAND:
+                    assert np.array_equal(host[p:p + NB * NB].reshape(NB, NB, order="F"), t), (m, n)
+                    p += NB * NB
+                else:
+                    U, V = t
+                    r = U.shape[1]
+                    assert np.array_equal(host[p:p + NB * r].reshape(NB, r, order="F"), U), (m, n)
+                    assert np.array_equal(host[p + NB * r:p + 2 * NB * r].reshape(NB, r, order="F"), V), (m, n)
+                    p += 2 * NB * r
+        assert p * 8 == written
+        # too small: the copy-out stops, the factor does not change; no arming afterwards
+        B.store_stream(buf.data_ptr(), 8 * NB * NB)
+        assert B.potrf(TOL) == 0
+        assert B.stats()[15] == -1
+        assert abs(A.logdet() - B.logdet()) <= 1e-12 * abs(A.logdet())
+    finally:
+        A.close()
+        B.close()
