@@ -2120,17 +2120,19 @@ static int run_syrk(hicma_tlr_ctx *c, hicma_tlr_desc *A, int k, const std::vecto
     return 0;
 }
 
-// All low-rank SYRK contributions to diagonal tile m at once, right before
-// its POTRF: A_mm -= sum_j U_mj (V_mj^T V_mj) U_mj^T over the off-band tiles
-// (m, j), j < m.  The factors of column j are final once panel j is done, so
+// The low-rank SYRK contributions of columns j in [j0, j1) to diagonal tile m
+// at once: A_mm -= sum_j U_mj (V_mj^T V_mj) U_mj^T over the off-band tiles
+// (m, j).  The factors of column j are final once panel j is done, so
 // deferring is exact; applying them as one K-concatenated DMMA GEMM
 // (K = sum of the ranks) reads and writes the dense tile once instead of once
-// per panel.  Chunked to the free workspace.
-static int run_syrk_lazy(hicma_tlr_ctx *c, hicma_tlr_desc *A, int m) {
+// per panel.  The factorization applies columns 0..m-2 one panel early, off the
+// critical path, and only column m-1 right before POTRF(m).  Chunked to the
+// free workspace.
+static int run_syrk_lazy(hicma_tlr_ctx *c, hicma_tlr_desc *A, int m, int j0, int j1) {
     const int NB = A->NB;
     const size_t mark = c->ar->off;
     std::vector<int> js;
-    for (int j = 0; j < m; ++j)
+    for (int j = j0; j < j1; ++j)
         if (!A->is_dense(m, j) && A->rank(m, j) > 0) js.push_back(j);
     size_t p = 0;
     while (p < js.size()) {
@@ -2200,6 +2202,8 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
     c->main_ar.off = 0;
     c->hi_ar.off = 0;
     A->rk_init.assign((size_t)NT * NT, -1);
+    // per diagonal tile: first column whose low-rank SYRK contribution is not yet applied
+    std::vector<int> syrk_from(NT, 0);
     for (int n = 0; n < NT; ++n)
         for (int m = n + band; m < NT; ++m) A->rk_init[(size_t)n * NT + m] = A->rank(m, n);
     A->rk_min = A->rk_init;
@@ -2341,11 +2345,22 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                 c->ar->off = 0;
                 CUDA_TRY(cudaStreamWaitEvent(c->cur, evT, 0));
                 if (A->is_dense(k + 1, k)) TRY(run_syrk(c, A, k, std::vector<int>{k + 1}));
-                TRY(run_syrk_lazy(c, A, k + 1));
+                TRY(run_syrk_lazy(c, A, k + 1, syrk_from[k + 1], k + 1));
+                syrk_from[k + 1] = k + 1;
                 CUDA_TRY(cudaEventRecord(ev[P0], c->cur));
                 TRY(potrf_tile(c, A->dense(k + 1, k + 1), NB, NB, A->linv(k + 1), NB, d_info, (k + 1) * NB));
                 CUDA_TRY(cudaEventRecord(ev[P1], c->cur));
                 CUDA_TRY(cudaEventRecord(evP, c->cur));
+                // the next diagonal tile's low-rank contributions of columns 0..k (all
+                // final after this panel's TRSM), after POTRF(k+1) and behind the event
+                // the bulk stream waits on: they overlap this panel's updates, and the
+                // next panel's chain adds only column k+1's.  (With a band of 3 or more
+                // the bulk stream's dense SYRK writes the same tile: left to the chain.)
+                if (k + 2 < NT && A->band <= 2) {
+                    c->ar->off = 0;
+                    TRY(run_syrk_lazy(c, A, k + 2, syrk_from[k + 2], k + 1));
+                    syrk_from[k + 2] = k + 1;
+                }
             }
             // ---- SYRK(k, m), m > k+1
             NvtxRange nv_syrk("SYRK");
