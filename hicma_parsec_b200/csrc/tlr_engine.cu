@@ -851,6 +851,7 @@ size_t recomp_ws_bytes(int nb, const RecompTask &t) {
     b += A((size_t)nb * K) * 3;                          // Us = [Cu | Wu], Vs = [Cv | -Y], Vk
     b += A(ra) + A(K) + A(npa * pb * pb) + A(npk * pb * pb);  // tau, T factors of Wu and Vs
     b += A((size_t)rc * ra) * 2;                         // Pu, Pu2
+    b += A((size_t)nb * ra) + A((size_t)ra * ra);        // Q and R of the residual (CholeskyQR form)
     b += A((size_t)K * K) * 6;                           // RU, SU, T1, RV, R3^-1 and R3^-1 U_r
     if (K > core_smem_kmax()) b += A(core_work_doubles(K));
     if (t.Bv) b += A((size_t)t.rb * t.ra);
@@ -896,7 +897,8 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
         // CholeskyQR chain (F) there and the Householder chain of the wide
         // updates (S) on the side stream, joined at the end of the chunk
         std::vector<CopyTask> copies, copiesS, keeps;
-        std::vector<GemmTask> g1, g2, g1s, g2s, gTU, gU, g3, g4, gUS, g3S, g4S;
+        std::vector<GemmTask> g1, g2, g1s, g2s, gTU, gU, g3, g4, gQS, gUS, g3S, g4S;
+        std::vector<CQTask> cqS;   // QRs of the wide updates' projected residuals (Q formed)
         std::vector<CoreTask> coresS;
         std::vector<ProjTask> projs;
         std::vector<SelTask> sels;
@@ -973,17 +975,34 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
                 double *TU = ws_alloc<double>(c, npa * pbw * pbw), *TV = ws_alloc<double>(c, npk * pbw * pbw);
                 double *Pu = ws_alloc<double>(c, (size_t)rc * ra), *Pu2 = ws_alloc<double>(c, (size_t)rc * ra);
                 double *Wu = Us + (size_t)nb * rc;
+                // R of the projected residual Wu, as the assembly reads it (top ra x ra, ld)
+                const double *Rw = Wu;
+                int ldrw = nb;
                 if (rc > 0) copiesS.push_back(make_copy(t.Cu, nb, Us, nb, nb, rc));
                 if (ra > 0) {
                     copiesS.push_back(make_copy(t.Au, nb, Wu, nb, nb, ra));
                     // two rounds of projection of Au against the old orthonormal U
                     if (rc > 0) projs.push_back(ProjTask{Us, Wu, Pu, Pu2, nb, rc, ra});
-                    qrs.push_back(QRTask{Wu, tauU, TU, nb, ra, nb});
-                    apps.push_back(QApplyTask{Wu, TU, SU + rc, t.outU, ct.rank_task, nb, ra, nb, K, nb, maxrank});
+                    if (c->cholqr && ra <= rcholqr_kmax()) {
+                        // residual up to 64 columns: randomized CholeskyQR with Q formed,
+                        // and the new U's Q(Wu) U_bot as one GEMM
+                        double *Qw = ws_alloc<double>(c, (size_t)nb * ra);
+                        double *Rq = ws_alloc<double>(c, (size_t)ra * ra);
+                        cqS.push_back(CQTask{Wu, nullptr, Qw, Rq, Qw, nb, ra, 0, nb, nb});
+                        Rw = Rq;
+                        ldrw = ra;
+                        GemmTask q = make_gemm(0, 0, nb, std::min(K, maxrank), ra, 1.0, Qw, nb, SU + rc, K, 0.0,
+                                               t.outU, nb);
+                        q.n_dev = ct.rank_task;
+                        gQS.push_back(q);
+                    } else {
+                        qrs.push_back(QRTask{Wu, tauU, TU, nb, ra, nb});
+                        apps.push_back(QApplyTask{Wu, TU, SU + rc, t.outU, ct.rank_task, nb, ra, nb, K, nb, maxrank});
+                    }
                 }
                 keeps.push_back(make_copy(Vs, nb, Vk, nb, nb, K));
                 qrs.push_back(QRTask{Vs, tauV, TV, nb, K, nb});
-                asm_.push_back(AssembleTask{Pu, Wu, RU, rc, ra, nb});
+                asm_.push_back(AssembleTask{Pu, Rw, RU, rc, ra, ldrw});
                 ct.RV = Vs; ct.ldrv = nb;
                 Vsrc = Vk;
             }
@@ -1049,6 +1068,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
             TRY(check_launch(c));
         }
         TRY(run_qr(c, qrs, nb));
+        TRY(run_rcholqr(c, cqS, 0));
         if (!asm_.empty()) {
             AssembleTask *d = stage(c, asm_.data(), asm_.size());
             if (!d) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
@@ -1058,6 +1078,7 @@ int run_recompress(hicma_tlr_ctx *c, int nb, std::vector<RecompTask> &tasks, dou
         CoreParams cp{0, acc, maxrank, fixed_rank, nb, c->d_flags + 1, c->d_flags + 2};
         TRY(run_core_buckets(c, coresS, cp));
         TRY(run_qapply(c, apps, nb));
+        TRY(run_gemms(c, gQS));   // Q(Wu) U_bot before gUS adds Cu U_top
         TRY(run_gemms(c, gUS));
         TRY(run_gemms(c, g3S));
         TRY(run_gemms(c, g4S));
