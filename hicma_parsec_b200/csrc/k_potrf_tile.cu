@@ -4,23 +4,28 @@
 // :233-242) together with the inverse L^-1 that the panel solves of this
 // engine apply as a GEMM.  The tile is split into 64 x 64 blocks and the
 // blocked right-looking algorithm becomes a list of block tasks:
-//   DIAG(j)      Cholesky of A_jj and D_j = L_jj^-1 (one CTA, shared memory,
-//                8-column panels factored by one warp)
-//   PANEL(j,i)   L_ij = A_ij D_j^T
-//   UPD(j,i,k)   A_ik -= L_ij L_kj^T                       (j < k <= i)
+//   CHAIN        the critical path, run by one CTA from start to end: for each
+//                block column j, Cholesky of A_jj and D_j = L_jj^-1, then
+//                L_j+1,j = A_j+1,j D_j^T and A_j+1,j+1 -= L_j+1,j L_j+1,j^T,
+//                the next diagonal block staying in shared memory
+//   PANEL(j,i)   L_ij = A_ij D_j^T                        (i >= j + 2)
+//   UPD(j,i,k)   A_ik -= L_ij L_kj^T         (j < k <= i, (i,k) != (j+1,j+1))
 //   XDIAG(j,k)   X_jk = D_j B_jk                           (k < j)
 //   XUPD(j,i,k)  B_ik -= L_ij X_jk                         (k <= j < i)
 // where X = L^-1 is produced by block forward substitution on the identity
-// (B starts as zero off the diagonal).  The list is in a topological order
-// and CTAs take tasks from it with an atomic ticket, so every task waits only
-// on tasks already held by running CTAs: the kernel makes progress with any
-// number of resident CTAs and needs no cooperative launch.  Dependencies are
-// per-block counters released with a fence after the block is written and
-// acquired by one thread before the CTA reads (through L2: ld.global.cg).
-// Every wait is bounded; a wait that gives up sets the timeout flag and the
-// abort flag, and every CTA leaves at its next task.  A non-positive pivot
-// sets the reference's INFO (k*NB + iinfo) and aborts the same way.
-// The 64 x 64 products run on the FP64 tensor cores (mma.sync m8n8k4 f64).
+// (B starts as zero off the diagonal).  The chain is the first task; the rest
+// of the list is in a topological order and CTAs take tasks from it with an
+// atomic ticket, so every task waits only on the chain or on tasks already
+// held by running CTAs, and the chain waits only on tasks of earlier block
+// columns, which the other CTAs take in list order: the kernel makes progress
+// with two or more CTAs, whether or not they are resident together, and needs
+// no cooperative launch.  Dependencies are per-block counters released
+// with a fence after the block is written and acquired by one thread before
+// the CTA reads (through L2: ld.global.cg).  Every wait is bounded; a wait
+// that gives up sets the timeout flag and the abort flag, and every CTA leaves
+// at its next task.  A non-positive pivot sets the reference's INFO
+// (k*NB + iinfo) and aborts the same way.  The block products run on the FP64
+// tensor cores (mma.sync m8n8k4 f64).
 #include "tlr_internal.h"
 
 #include <map>
@@ -32,11 +37,11 @@ namespace {
 
 constexpr int TB = 64;          // block edge
 constexpr int TPITCH = 72;      // shared pitch of DMMA operand tiles
-constexpr int LDS = TB + 1;     // shared pitch of the diagonal block
+constexpr int CP = TB + 4;      // shared pitch of the chain CTA's blocks (conflict-free DMMA fragments)
 constexpr int NTH = 256;
 constexpr long long SPIN_LIMIT = 1LL << 24;
 
-enum { IT_DIAG = 0, IT_PANEL, IT_UPD, IT_XDIAG, IT_XUPD };
+enum { IT_CHAIN = 0, IT_PANEL, IT_UPD, IT_XDIAG, IT_XUPD };
 struct PItem {
     unsigned short type, j, i, k;
 };
@@ -83,30 +88,52 @@ __device__ __forceinline__ int bsz(int b, int n) { return min(TB, n - b * TB); }
 
 // C (m x nn, ldc) = beta C + alpha opA(A) opB(B), inner dimension kk <= 64.
 // Operands are staged in shared memory before C is written, so C may alias
-// A or B when beta = 0.
+// A or B when beta = 0 (with beta != 0, C is read before the products and
+// must not alias them).  The operand loads go out in two rounds of 16 per
+// thread, and C's entries are fetched ahead of the products.
 __device__ void blk_gemm(double *sm, double *C, int ldc, int m, int nn, int kk, double alpha, double beta,
                          const double *A, int lda, int opA, const double *B, int ldb, int opB) {
     double *As = sm;                 // As[k][i]
     double *Bs = sm + TB * TPITCH;   // Bs[k][j]
     const int tid = threadIdx.x;
-#pragma unroll 4
-    for (int q = 0; q < (TB * TB) / NTH; ++q) {
-        const int e = tid + q * NTH;
-        int i, k;
-        if (opA == 0) { i = e & (TB - 1); k = e >> 6; } else { k = e & (TB - 1); i = e >> 6; }
-        double v = 0.0;
-        if (i < m && k < kk) v = __ldcg(opA == 0 ? A + i + (size_t)k * lda : A + k + (size_t)i * lda);
-        As[k * TPITCH + i] = v;
-        int j;
-        if (opB == 0) { k = e & (TB - 1); j = e >> 6; } else { j = e & (TB - 1); k = e >> 6; }
-        double w = 0.0;
-        if (j < nn && k < kk) w = __ldcg(opB == 0 ? B + k + (size_t)j * ldb : B + j + (size_t)k * ldb);
-        Bs[k * TPITCH + j] = w;
-    }
-    __syncthreads();
     const int lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, tig = lane & 3;
     const int wm = warp & 1, wn = warp >> 1;   // 2 x 4 warps, 32 x 16 each
+    constexpr int HALF = (TB * TB) / NTH / 2;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        double va[HALF], vb[HALF];
+#pragma unroll
+        for (int q = 0; q < HALF; ++q) {
+            const int e = tid + (h * HALF + q) * NTH;
+            int i, k;
+            if (opA == 0) { i = e & (TB - 1); k = e >> 6; } else { k = e & (TB - 1); i = e >> 6; }
+            va[q] = (i < m && k < kk) ? __ldcg(opA == 0 ? A + i + (size_t)k * lda : A + k + (size_t)i * lda) : 0.0;
+            int j;
+            if (opB == 0) { k = e & (TB - 1); j = e >> 6; } else { j = e & (TB - 1); k = e >> 6; }
+            vb[q] = (j < nn && k < kk) ? __ldcg(opB == 0 ? B + k + (size_t)j * ldb : B + j + (size_t)k * ldb) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < HALF; ++q) {
+            const int e = tid + (h * HALF + q) * NTH;
+            int i, k, j;
+            if (opA == 0) { i = e & (TB - 1); k = e >> 6; } else { k = e & (TB - 1); i = e >> 6; }
+            As[k * TPITCH + i] = va[q];
+            if (opB == 0) { k = e & (TB - 1); j = e >> 6; } else { j = e & (TB - 1); k = e >> 6; }
+            Bs[k * TPITCH + j] = vb[q];
+        }
+    }
+    double cv[4][2][2];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int row = wm * 32 + mi * 8 + g, col = wn * 16 + ni * 8 + 2 * tig + e;
+                cv[mi][ni][e] = (beta != 0.0 && row < m && col < nn) ? __ldcg(C + row + (size_t)col * ldc) : 0.0;
+            }
+    __syncthreads();
     double acc[4][2][2];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -134,115 +161,270 @@ __device__ void blk_gemm(double *sm, double *C, int ldc, int m, int nn, int kk, 
             for (int e = 0; e < 2; ++e) {
                 const int col = wn * 16 + ni * 8 + 2 * tig + e;
                 if (col >= nn) continue;
-                double *cp = C + row + (size_t)col * ldc;
-                double v = alpha * acc[mi][ni][e];
-                if (beta != 0.0) v += beta * __ldcg(cp);
-                *cp = v;
+                C[row + (size_t)col * ldc] = alpha * acc[mi][ni][e] + beta * cv[mi][ni][e];
             }
     }
 }
 
-// Cholesky of the jb x jb block at Ajj (lda) and its inverse, written to Ajj
-// (lower, zero upper) and Dj (ldd).  Returns false on a non-positive pivot.
-__device__ bool diag_block(double *sm, double *Ajj, int lda, int jb, double *Dj, int ldd, int *info, int info_col0) {
-    double *S = sm;                  // S[c * LDS + r] = L(r, c)
-    double *Xs = sm + TB * LDS;      // inverse
-    double *Ts = sm + 2 * TB * LDS;  // 32 x 32 scratch
-    double *invd = Ts + 32 * 32;
-    __shared__ int fail;
+// ------------------------------------------------------------ the chain ----
+// The chain CTA keeps three 64 x 64 column-major blocks in shared memory
+// (pitch CP): S (the diagonal block being factored), Xs (its inverse) and Pn
+// (the panel block below it, and scratch of the inverse).  Blocks smaller
+// than 64 are padded: with the identity on the diagonal of S, with zeros in
+// Pn, so the padded parts factor to the identity and never reach the tile.
+constexpr int CHAIN_SMEM_DOUBLES = 3 * TB * CP + TB;
+
+// M(r, c) = G(r, c) for r < rows, c < cols, else (r == c && pad_id); all of a
+// thread's loads are issued before its shared stores.
+__device__ __forceinline__ void load_frame(double *M, const double *G, int ld, int rows, int cols, bool pad_id) {
     const int tid = threadIdx.x;
-    if (tid == 0) fail = 0;
-    for (int idx = tid; idx < TB * LDS; idx += NTH) Xs[idx] = 0.0;
-    for (int idx = tid; idx < jb * jb; idx += NTH) {
-        const int c = idx / jb, r = idx - c * jb;
-        S[c * LDS + r] = __ldcg(Ajj + r + (size_t)c * lda);
+    double v[(TB * TB) / NTH];
+#pragma unroll
+    for (int q = 0; q < (TB * TB) / NTH; ++q) {
+        const int e = tid + q * NTH, r = e & (TB - 1), c = e >> 6;
+        v[q] = (r < rows && c < cols) ? __ldcg(G + r + (size_t)c * ld) : ((pad_id && r == c) ? 1.0 : 0.0);
     }
-    __syncthreads();
-    // blocked right-looking Cholesky: warp 0 factors each 8-column panel with
-    // warp-level synchronisation only, then all threads apply the panel's
-    // rank-8 update to the trailing block (two CTA barriers per panel)
-    for (int p0 = 0; p0 < jb; p0 += 8) {
-        const int pe = min(jb, p0 + 8);
-        if (tid < 32) {
-            const int lane = tid;
-            for (int c = p0; c < pe; ++c) {
-                const double d = S[c * LDS + c];
-                if (!(d > 0.0)) {
-                    if (lane == 0) {
-                        fail = 1;
-                        if (info) atomicCAS(info, 0, info_col0 + c + 1);
-                    }
-                    break;
-                }
-                const double piv = sqrt(d), inv = 1.0 / piv;
-                __syncwarp();
-                if (lane == 0) { S[c * LDS + c] = piv; invd[c] = inv; }
-                for (int r = c + 1 + lane; r < jb; r += 32) S[c * LDS + r] *= inv;
-                __syncwarp();
-                for (int cc = c + 1; cc < pe; ++cc) {
-                    const double lc = S[c * LDS + cc];
-                    for (int r = cc + lane; r < jb; r += 32) S[cc * LDS + r] -= S[c * LDS + r] * lc;
-                }
-                __syncwarp();
-            }
+#pragma unroll
+    for (int q = 0; q < (TB * TB) / NTH; ++q) {
+        const int e = tid + q * NTH;
+        M[(e >> 6) * CP + (e & (TB - 1))] = v[q];
+    }
+}
+
+// Warp 0: right-looking Cholesky of the 8-column panel p0..p0+7 of S (rows
+// p0..63; lane l holds rows p0+l and p0+32+l in registers).  Entries above
+// the diagonal are carried along unscaled and never read back as L.  Returns
+// the panel column of a non-positive pivot, or -1.  inv = rsqrt(d) scales the
+// column; the pivot is d * inv.
+__device__ int chain_panel(double *S, double *invd, int p0, int lane) {
+    double a0[8], a1[8];
+    const int r0 = p0 + lane, r1 = p0 + 32 + lane;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        a0[c] = r0 < TB ? S[(p0 + c) * CP + r0] : 0.0;
+        a1[c] = r1 < TB ? S[(p0 + c) * CP + r1] : 0.0;
+    }
+    int bad = -1;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const double d = __shfl_sync(0xffffffffu, a0[c], c);
+        if (!(d > 0.0)) { bad = c; break; }     // d is the same on every lane
+        const double inv = rsqrt(d);
+        if (lane == c) a0[c] = d * inv;
+        else if (lane > c) a0[c] *= inv;
+        a1[c] *= inv;
+        if (lane == 0) invd[p0 + c] = inv;
+#pragma unroll
+        for (int cc = c + 1; cc < 8; ++cc) {
+            const double l = __shfl_sync(0xffffffffu, a0[c], cc);
+            a0[cc] = fma(-a0[c], l, a0[cc]);
+            a1[cc] = fma(-a1[c], l, a1[cc]);
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        if (r0 < TB) S[(p0 + c) * CP + r0] = a0[c];
+        if (r1 < TB) S[(p0 + c) * CP + r1] = a1[c];
+    }
+    return bad;
+}
+
+// Cholesky of S in place and its inverse in Xs (Pn is scratch).  Blocked by
+// 8-column panels: warp 0 factors a panel, then every warp applies its rank-8
+// update to the lower 8 x 8 tiles of the trailing block on the tensor cores.
+// The inverse: 8 x 8 diagonal blocks by forward substitution (one thread per
+// column, with the stored inverse pivots), then pairs of blocks merged as
+// X21 = -X22 (L21 X11) at widths 8, 16, 32.  Returns the column (0..63) of a
+// non-positive pivot, or -1.
+__device__ int chain_diag(double *S, double *Xs, double *Pn, double *invd) {
+    __shared__ int bad_sh;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, tig = lane & 3;
+    for (int e = tid; e < TB * CP; e += NTH) Xs[e] = 0.0;
+    for (int p0 = 0; p0 < TB; p0 += 8) {
+        if (warp == 0) {
+            const int b = chain_panel(S, invd, p0, lane);
+            if (lane == 0) bad_sh = b < 0 ? -1 : p0 + b;
         }
         __syncthreads();
-        if (fail) return false;
-        const int w = jb - pe;
-        for (int idx = tid; idx < w * w; idx += NTH) {
-            const int cc = pe + idx / w, r = pe + idx % w;
-            if (r < cc) continue;
-            double acc = S[cc * LDS + r];
-            for (int l = p0; l < pe; ++l) acc -= S[l * LDS + r] * S[l * LDS + cc];
-            S[cc * LDS + r] = acc;
+        if (bad_sh >= 0) return bad_sh;
+        const int nbt = (TB - p0 - 8) / 8;   // trailing 8 x 8 block rows
+        for (int t = warp; t < nbt * (nbt + 1) / 2; t += NTH / 32) {
+            int bi = 0;
+            while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
+            const int bj = t - bi * (bi + 1) / 2;
+            const int m0 = p0 + 8 + 8 * bi, n0 = p0 + 8 + 8 * bj;
+            double acc[2] = {S[(n0 + 2 * tig) * CP + m0 + g], S[(n0 + 2 * tig + 1) * CP + m0 + g]};
+#pragma unroll
+            for (int k = 0; k < 8; k += 4)
+                dmma884(acc, -S[(p0 + k + tig) * CP + m0 + g], S[(p0 + k + tig) * CP + n0 + g]);
+            S[(n0 + 2 * tig) * CP + m0 + g] = acc[0];
+            S[(n0 + 2 * tig + 1) * CP + m0 + g] = acc[1];
         }
         __syncthreads();
     }
-    // (the last column has nothing below its diagonal)
-    // inverse: 8 x 8 diagonal blocks by forward substitution, then pairs of
-    // blocks merged with X21 = -X22 (L21 X11) at widths 8, 16, 32
-    {
-        const int c = tid;
-        if (c < jb) {
-            const int e = min(jb, (c / 8) * 8 + 8);
-            Xs[c * LDS + c] = invd[c];
-            for (int r = c + 1; r < e; ++r) {
-                double s = 0.0;
-                for (int l = c; l < r; ++l) s += S[l * LDS + r] * Xs[c * LDS + l];
-                Xs[c * LDS + r] = -s * invd[r];
-            }
+    if (tid < TB) {
+        const int b0 = tid & ~7, c = tid & 7;
+        double x[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            double s = 0.0;
+#pragma unroll
+            for (int l = 0; l < r; ++l)
+                if (l >= c) s = fma(S[(b0 + l) * CP + b0 + r], x[l], s);
+            x[r] = r < c ? 0.0 : (r == c ? invd[b0 + r] : -s * invd[b0 + r]);
         }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) Xs[(b0 + c) * CP + b0 + r] = x[r];
     }
     __syncthreads();
     for (int h = 8; h < TB; h *= 2) {
-        const int npair = (jb + 2 * h - 1) / (2 * h);
-        // T = L21 X11 (rows s0+h .. e, cols s0 .. s0+h)
-        for (int idx = tid; idx < npair * h * h; idx += NTH) {
-            const int pr = idx / (h * h), rem = idx % (h * h);
-            const int rr = rem % h, cc = rem / h;
-            const int s0 = pr * 2 * h, r = s0 + h + rr, c = s0 + cc;
-            if (r >= jb) continue;
-            double s = 0.0;
-            for (int l = c; l < s0 + h; ++l) s += S[l * LDS + r] * Xs[c * LDS + l];
-            Ts[pr * h * h + cc * h + rr] = s;
+        const int hb = h / 8, tpp = hb * hb, nt = (TB / (2 * h)) * tpp;
+        // T = L21 X11 into the frame position of X21 in Pn (X11 lower: k >= the column block)
+        for (int t = warp; t < nt; t += NTH / 32) {
+            const int s0 = (t / tpp) * 2 * h, ti = (t % tpp) % hb, tj = (t % tpp) / hb;
+            const int m0 = s0 + h + 8 * ti, n0 = s0 + 8 * tj;
+            double acc[2] = {0.0, 0.0};
+            for (int k = s0 + 8 * tj; k < s0 + h; k += 4)
+                dmma884(acc, S[(k + tig) * CP + m0 + g], Xs[(n0 + g) * CP + k + tig]);
+            Pn[(n0 + 2 * tig) * CP + m0 + g] = acc[0];
+            Pn[(n0 + 2 * tig + 1) * CP + m0 + g] = acc[1];
         }
         __syncthreads();
-        // X21 = -X22 T
-        for (int idx = tid; idx < npair * h * h; idx += NTH) {
-            const int pr = idx / (h * h), rem = idx % (h * h);
-            const int rr = rem % h, cc = rem / h;
-            const int s0 = pr * 2 * h, r = s0 + h + rr, c = s0 + cc;
-            if (r >= jb) continue;
-            double s = 0.0;
-            for (int m = s0 + h; m <= r; ++m) s += Xs[m * LDS + r] * Ts[pr * h * h + cc * h + (m - s0 - h)];
-            Xs[c * LDS + r] = -s;
+        // X21 = -X22 T (X22 lower: k up to the row block)
+        for (int t = warp; t < nt; t += NTH / 32) {
+            const int s0 = (t / tpp) * 2 * h, ti = (t % tpp) % hb, tj = (t % tpp) / hb;
+            const int m0 = s0 + h + 8 * ti, n0 = s0 + 8 * tj;
+            double acc[2] = {0.0, 0.0};
+            for (int k = s0 + h; k < m0 + 8; k += 4)
+                dmma884(acc, -Xs[(k + tig) * CP + m0 + g], Pn[(n0 + g) * CP + k + tig]);
+            Xs[(n0 + 2 * tig) * CP + m0 + g] = acc[0];
+            Xs[(n0 + 2 * tig + 1) * CP + m0 + g] = acc[1];
         }
         __syncthreads();
     }
-    for (int idx = tid; idx < jb * jb; idx += NTH) {
-        const int c = idx / jb, r = idx - c * jb;
-        Ajj[r + (size_t)c * lda] = (r >= c) ? S[c * LDS + r] : 0.0;
-        Dj[r + (size_t)c * ldd] = (r >= c) ? Xs[c * LDS + r] : 0.0;
+    return -1;
+}
+
+// One warp's 32 x 16 tile (rows wm*32.., cols wn*16..) of C = alpha X Y^T
+// over k in [0, kend), X and Y column-major in shared memory; acc holds C on
+// entry (or zero).
+__device__ __forceinline__ void chain_mm_nt(double (&acc)[4][2][2], const double *X, const double *Y, double alpha,
+                                            int kend, int wm, int wn, int g, int tig) {
+    for (int k = 0; k < kend; k += 4) {
+        double a[4], b[2];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi) a[mi] = alpha * X[(k + tig) * CP + wm * 32 + mi * 8 + g];
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni) b[ni] = Y[(k + tig) * CP + wn * 16 + ni * 8 + g];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni) dmma884(acc[mi][ni], a[mi], b[ni]);
+    }
+}
+
+// The critical path of the tile: for j = 0, 1, ...: factor the diagonal block
+// held in S, write L_jj and D_j, release ddone(j); then L_j+1,j = A_j+1,j D_j^T
+// (written, released as pdone(j+1, j)) and S = A_j+1,j+1 - L_j+1,j L_j+1,j^T,
+// each after the block's updates from the earlier columns are in.  Returns
+// false if a wait gave up or a pivot failed (the abort flag is then set).
+__device__ bool run_chain(double *sm, const PotrfParams &P) {
+    __shared__ int ok_c;
+    double *S = sm, *Xs = sm + TB * CP, *Pn = sm + 2 * TB * CP, *invd = sm + 3 * TB * CP;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, tig = lane & 3, wm = warp & 1, wn = warp >> 1;
+    const int nb = P.nblk, n = P.n, lda = P.lda;
+    int *ver = P.cnt + 8, *pdone = ver + nb * nb, *ddone = pdone + 3 * nb * nb;
+    auto Ablk = [&](int r, int c) { return P.A + (size_t)r * TB + (size_t)c * TB * lda; };
+    auto wait_all = [&](const int *p, int v) {
+        if (tid == 0) ok_c = wait_ge(p, v, P);
+        __syncthreads();
+        return ok_c != 0;
+    };
+    load_frame(S, Ablk(0, 0), lda, bsz(0, n), bsz(0, n), true);
+    __syncthreads();
+    for (int j = 0; j < nb; ++j) {
+        const int jb = bsz(j, n);
+        const int bad = chain_diag(S, Xs, Pn, invd);
+        if (bad >= 0) {
+            if (tid == 0) {
+                // a pivot of the padding is 1: bad < jb
+                if (P.info) atomicCAS(P.info, 0, P.info_base + j * TB + bad + 1);
+                atomicExch(P.cnt + 1, 1);
+            }
+            return false;
+        }
+        double *Dj = P.X ? P.X + (size_t)j * TB + (size_t)j * TB * P.ldx : P.D + (size_t)j * TB * TB;
+        const int ldd = P.X ? P.ldx : TB;
+        double *Ajj = Ablk(j, j);
+#pragma unroll 4
+        for (int q = 0; q < (TB * TB) / NTH; ++q) {
+            const int e = tid + q * NTH, r = e & (TB - 1), c = e >> 6;
+            if (r < jb && c < jb) {
+                Ajj[r + (size_t)c * lda] = r >= c ? S[c * CP + r] : 0.0;
+                Dj[r + (size_t)c * ldd] = r >= c ? Xs[c * CP + r] : 0.0;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicExch(ddone + j, 1);
+        }
+        const int i = j + 1;
+        if (i >= nb) break;
+        const int ib = bsz(i, n);
+        // L_ij = A_ij D_j^T (D_j^T upper: k stops at the warp's last column)
+        if (!wait_all(ver + i * nb + j, j)) return false;
+        load_frame(Pn, Ablk(i, j), lda, ib, TB, false);
+        __syncthreads();
+        double acc[4][2][2];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+        chain_mm_nt(acc, Pn, Xs, 1.0, wn * 16 + 16, wm, wn, g, tig);
+        __syncthreads();
+        double *Aij = Ablk(i, j);
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi) {
+            const int row = wm * 32 + mi * 8 + g;
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const int col = wn * 16 + ni * 8 + 2 * tig + e;
+                    Pn[col * CP + row] = acc[mi][ni][e];
+                    if (row < ib) Aij[row + (size_t)col * lda] = acc[mi][ni][e];
+                }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicExch(pdone + i * nb + j, 1);
+        }
+        // S = A_ii - L_ij L_ij^T (lower tiles; the warps above the diagonal skip)
+        if (!wait_all(ver + i * nb + i, j)) return false;
+        load_frame(S, Ablk(i, i), lda, ib, ib, true);
+        __syncthreads();
+        if (wm * 32 + 31 >= wn * 16) {
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+                        acc[mi][ni][e] = S[(wn * 16 + ni * 8 + 2 * tig + e) * CP + wm * 32 + mi * 8 + g];
+            chain_mm_nt(acc, Pn, Pn, -1.0, TB, wm, wn, g, tig);
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+                        S[(wn * 16 + ni * 8 + 2 * tig + e) * CP + wm * 32 + mi * 8 + g] = acc[mi][ni][e];
+        }
+        __syncthreads();
     }
     return true;
 }
@@ -266,11 +448,15 @@ __global__ void __launch_bounds__(NTH, 2) k_potrf_tile(PotrfParams P) {
         const int t = item_sh;
         if (t < 0) break;
         const PItem it = P.items[t];
+        if (it.type == IT_CHAIN) {
+            if (!run_chain(sm, P)) break;
+            __syncthreads();
+            continue;
+        }
         const int j = it.j, i = it.i, k = it.k, n = P.n, nb = P.nblk;
         if (tid == 0) {
             bool ok = true;
             switch (it.type) {
-                case IT_DIAG: ok = wait_ge(ver + j * nb + j, j, P); break;
                 case IT_PANEL: ok = wait_ge(ddone + j, 1, P) && wait_ge(ver + i * nb + j, j, P); break;
                 case IT_UPD:
                     ok = wait_ge(pdone + i * nb + j, 1, P) && wait_ge(pdone + k * nb + j, 1, P) &&
@@ -292,11 +478,7 @@ __global__ void __launch_bounds__(NTH, 2) k_potrf_tile(PotrfParams P) {
         auto Xblk = [&](int r, int c) { return P.X + (size_t)r * TB + (size_t)c * TB * P.ldx; };
         double *Dj = P.X ? Xblk(j, j) : P.D + (size_t)j * TB * TB;
         const int ldd = P.X ? P.ldx : TB;
-        bool good = true;
         switch (it.type) {
-            case IT_DIAG:
-                good = diag_block(sm, Ablk(j, j), lda, bsz(j, n), Dj, ldd, P.info, P.info_base + j * TB);
-                break;
             case IT_PANEL:
                 blk_gemm(sm, Ablk(i, j), lda, bsz(i, n), bsz(j, n), bsz(j, n), 1.0, 0.0, Ablk(i, j), lda, 0, Dj, ldd, 1);
                 break;
@@ -316,36 +498,38 @@ __global__ void __launch_bounds__(NTH, 2) k_potrf_tile(PotrfParams P) {
         __syncthreads();
         if (tid == 0) {
             __threadfence();
-            if (!good) {
-                atomicExch(P.cnt + 1, 1);
-            } else {
-                switch (it.type) {
-                    case IT_DIAG: atomicExch(ddone + j, 1); break;
-                    case IT_PANEL: atomicExch(pdone + i * nb + j, 1); break;
-                    case IT_UPD: atomicExch(ver + i * nb + k, j + 1); break;
-                    case IT_XDIAG: atomicExch(xdone + j * nb + k, 1); break;
-                    default: atomicExch(xver + i * nb + k, j - k + 1); break;
-                }
+            switch (it.type) {
+                case IT_PANEL: atomicExch(pdone + i * nb + j, 1); break;
+                case IT_UPD: atomicExch(ver + i * nb + k, j + 1); break;
+                case IT_XDIAG: atomicExch(xdone + j * nb + k, 1); break;
+                default: atomicExch(xver + i * nb + k, j - k + 1); break;
             }
         }
     }
 }
 
+// The bulk tasks column by column (right-looking order: the updates of one
+// block come from different columns, so they never queue behind each other).
+// Each column starts with the three tasks the chain's step after next waits
+// on: PANEL(j, j+2), UPD(j, j+2, j+1) and UPD(j, j+2, j+2).
 std::vector<PItem> build_items(int nblk, bool inv) {
     std::vector<PItem> v;
     auto add = [&](int t, int j, int i, int k) {
         v.push_back(PItem{(unsigned short)t, (unsigned short)j, (unsigned short)i, (unsigned short)k});
     };
-    add(IT_DIAG, 0, 0, 0);
+    add(IT_CHAIN, 0, 0, 0);
     for (int j = 0; j < nblk; ++j) {
-        for (int i = j + 1; i < nblk; ++i) add(IT_PANEL, j, i, 0);
-        if (j + 1 < nblk) {
-            add(IT_UPD, j, j + 1, j + 1);
-            add(IT_DIAG, j + 1, 0, 0);
-            for (int i = j + 2; i < nblk; ++i) add(IT_UPD, j, i, j + 1);
-            for (int k = j + 2; k < nblk; ++k)
-                for (int i = k; i < nblk; ++i) add(IT_UPD, j, i, k);
+        // the chain does PANEL(j, j+1) and UPD(j, j+1, j+1)
+        if (j + 2 < nblk) {
+            add(IT_PANEL, j, j + 2, 0);
+            add(IT_UPD, j, j + 2, j + 1);
+            add(IT_UPD, j, j + 2, j + 2);
         }
+        for (int i = j + 3; i < nblk; ++i) add(IT_PANEL, j, i, 0);
+        for (int i = j + 3; i < nblk; ++i) add(IT_UPD, j, i, j + 1);
+        for (int k = j + 2; k < nblk; ++k)
+            for (int i = k; i < nblk; ++i)
+                if (i != j + 2 || k != j + 2) add(IT_UPD, j, i, k);
         if (inv) {
             for (int k = 0; k < j; ++k) add(IT_XDIAG, j, 0, k);
             for (int i = j + 1; i < nblk; ++i)
@@ -410,13 +594,15 @@ int launch_potrf_tile(double *A, int lda, int n, double *X, int ldx, double *D, 
     const ItemList *L = get_items(nblk, X != nullptr, st);
     if (!L) return -1;
     if (cudaMemsetAsync(cnt, 0, potrf_tile_scratch_ints(n) * sizeof(int), st) != cudaSuccess) return -1;
-    const int smem = (int)sizeof(double) * (2 * TB * TPITCH > 2 * TB * LDS + 32 * 32 + TB ? 2 * TB * TPITCH
-                                                                                        : 2 * TB * LDS + 32 * 32 + TB);
+    const int smem = (int)sizeof(double) * (2 * TB * TPITCH > CHAIN_SMEM_DOUBLES ? 2 * TB * TPITCH : CHAIN_SMEM_DOUBLES);
     // per device and thread-safe: set on every launch (a host-side call, no synchronisation)
     cudaFuncSetAttribute(k_potrf_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     PotrfParams P{A, lda, n, nblk, X, ldx, D, L->d, L->n, cnt, info, info_base, timeout, SPIN_LIMIT};
+    // the chain waits on bulk tasks of earlier block columns, which only the
+    // other CTAs take: with any bulk task in the list the launch has two CTAs
+    // or more (they need not be resident at the same time)
     if (grid > L->n) grid = L->n;
-    if (grid < 1) grid = 1;
+    if (grid < 2) grid = L->n > 1 ? 2 : 1;
     k_potrf_tile<<<grid, NTH, smem, st>>>(P);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

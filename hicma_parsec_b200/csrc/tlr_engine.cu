@@ -2373,11 +2373,14 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                 CUDA_TRY(cudaEventRecord(ev[P1], c->cur));
                 CUDA_TRY(cudaEventRecord(evP, c->cur));
                 // the next diagonal tile's low-rank contributions of columns 0..k (all
-                // final after this panel's TRSM), after POTRF(k+1) and behind the event
-                // the bulk stream waits on: they overlap this panel's updates, and the
-                // next panel's chain adds only column k+1's.  (With a band of 3 or more
-                // the bulk stream's dense SYRK writes the same tile: left to the chain.)
+                // final once this panel's whole TRSM is done: the chain waited only for
+                // TRSM(k+1,k), so it waits for the rest, T1, here), after POTRF(k+1)
+                // and behind the event the bulk stream waits on: they overlap this
+                // panel's updates, and the next panel's chain adds only column k+1's.
+                // (With a band of 3 or more the bulk stream's dense SYRK writes the
+                // same tile: left to the chain.)
                 if (k + 2 < NT && A->band <= 2) {
+                    CUDA_TRY(cudaStreamWaitEvent(c->cur, ev[T1], 0));
                     c->ar->off = 0;
                     TRY(run_syrk_lazy(c, A, k + 2, syrk_from[k + 2], k + 1));
                     syrk_from[k + 2] = k + 1;

@@ -76,3 +76,26 @@ def test_admission_under_tight_budget():
     order = sorted(res, key=lambda r: r.t_admit)
     for prev, nxt in zip(order, order[1:]):
         assert nxt.t_admit >= prev.t_done - 1e-3
+
+
+def test_alone_equals_mix_large():
+    """Requests of up to N = 60,000 (tiles 1000-2700) on four slots: each one's
+    status and log-likelihood equal its sequential run's.  Large requests keep
+    each context's bulk stream busy, so the critical-path stream of one
+    factorization runs far ahead of its bulk updates; a missing cross-stream
+    dependency shows up here as a changed result."""
+    from hicma_parsec_b200 import serving
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    reqs = serving.sample_requests(8, seed=0, rate=1.0, n_max=60000)
+    seq = serving.MLEServer(0, slots=1, workspace_bytes=8 << 30)
+    alone = seq.run(reqs, realtime=False)
+    seq.close()
+    mix_srv = serving.MLEServer(0, slots=4, workspace_bytes=8 << 30)
+    mix = mix_srv.run(reqs, realtime=False)
+    mix_srv.close()
+    assert sum(1 for a in alone if a.status == 0) >= 6
+    for a, b in zip(alone, mix):
+        assert a.status == b.status, (a.rid, a.error, b.error)
+        if a.status == 0:
+            assert abs(a.loglik - b.loglik) <= 1e-12 * abs(a.loglik)
