@@ -172,7 +172,7 @@ __device__ void blk_gemm(double *sm, double *C, int ldc, int m, int nn, int kk, 
 // (the panel block below it, and scratch of the inverse).  Blocks smaller
 // than 64 are padded: with the identity on the diagonal of S, with zeros in
 // Pn, so the padded parts factor to the identity and never reach the tile.
-constexpr int CHAIN_SMEM_DOUBLES = 3 * TB * CP + TB;
+constexpr int CHAIN_SMEM_DOUBLES = 3 * TB * CP;
 
 // M(r, c) = G(r, c) for r < rows, c < cols, else (r == c && pad_id); all of a
 // thread's loads are issued before its shared stores.
@@ -191,60 +191,90 @@ __device__ __forceinline__ void load_frame(double *M, const double *G, int ld, i
     }
 }
 
-// Warp 0: right-looking Cholesky of the 8-column panel p0..p0+7 of S (rows
-// p0..63; lane l holds rows p0+l and p0+32+l in registers).  Entries above
-// the diagonal are carried along unscaled and never read back as L.  Returns
-// the panel column of a non-positive pivot, or -1.  inv = rsqrt(d) scales the
-// column; the pivot is d * inv.
-__device__ int chain_panel(double *S, double *invd, int p0, int lane) {
-    double a0[8], a1[8];
-    const int r0 = p0 + lane, r1 = p0 + 32 + lane;
+// The 8-column panel p0..p0+7 of S on warps 0-2.  Every lane of the three
+// warps factors the panel's 8 x 8 diagonal block itself, its lower part in
+// registers, so the pivot chain has no shuffles (rsqrt(d) scales the column;
+// the pivot is d * rsqrt(d), and the diagonal register keeps the reciprocal).
+// The three warps meet once all of them have read the block; then lane 0 of
+// warp 0 stores the factored block, warps 0 and 1 solve the rows below it (row p0+8+lane, row p0+40+lane), and lanes
+// 0-7 of warp 2 write column `lane` of the block's inverse into Xs by forward
+// substitution.  Returns the panel column of a non-positive pivot, or -1.
+__device__ int chain_panel(double *S, double *Xs, int p0, int warp, int lane) {
+    double d[8][8];   // d[r][c], c <= r
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c <= r; ++c) d[r][c] = S[(p0 + c) * CP + p0 + r];
+    asm volatile("bar.sync 1, 96;" ::: "memory");   // warps 0-2: the block is read before it is rewritten
+    const bool store = warp == 0 && lane == 0;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
-        a0[c] = r0 < TB ? S[(p0 + c) * CP + r0] : 0.0;
-        a1[c] = r1 < TB ? S[(p0 + c) * CP + r1] : 0.0;
+        const double dc = d[c][c];
+        if (!(dc > 0.0)) return c;          // the same on every lane
+        const double inv = rsqrt(dc);
+        d[c][c] = inv;
+        if (store) S[(p0 + c) * CP + p0 + c] = dc * inv;
+#pragma unroll
+        for (int r = c + 1; r < 8; ++r) d[r][c] *= inv;
+#pragma unroll
+        for (int cc = c + 1; cc < 8; ++cc)
+#pragma unroll
+            for (int r = cc; r < 8; ++r) d[r][cc] = fma(-d[r][c], d[cc][c], d[r][cc]);
     }
-    int bad = -1;
+    if (store) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const double d = __shfl_sync(0xffffffffu, a0[c], c);
-        if (!(d > 0.0)) { bad = c; break; }     // d is the same on every lane
-        const double inv = rsqrt(d);
-        if (lane == c) a0[c] = d * inv;
-        else if (lane > c) a0[c] *= inv;
-        a1[c] *= inv;
-        if (lane == 0) invd[p0 + c] = inv;
+        for (int c = 0; c < 8; ++c)
 #pragma unroll
-        for (int cc = c + 1; cc < 8; ++cc) {
-            const double l = __shfl_sync(0xffffffffu, a0[c], cc);
-            a0[cc] = fma(-a0[c], l, a0[cc]);
-            a1[cc] = fma(-a1[c], l, a1[cc]);
+            for (int r = c + 1; r < 8; ++r) S[(p0 + c) * CP + p0 + r] = d[r][c];
+    }
+    if (warp < 2) {
+        const int row = p0 + 8 + 32 * warp + lane;
+        if (row < TB) {
+            double a[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) a[c] = S[(p0 + c) * CP + row];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                a[c] *= d[c][c];
+#pragma unroll
+                for (int cc = c + 1; cc < 8; ++cc) a[cc] = fma(-a[c], d[cc][c], a[cc]);
+            }
+#pragma unroll
+            for (int c = 0; c < 8; ++c) S[(p0 + c) * CP + row] = a[c];
         }
-    }
+    } else if (lane < 8) {
+        const int c = lane;
+        double x[8];
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        if (r0 < TB) S[(p0 + c) * CP + r0] = a0[c];
-        if (r1 < TB) S[(p0 + c) * CP + r1] = a1[c];
+        for (int r = 0; r < 8; ++r) {
+            double s = 0.0;
+#pragma unroll
+            for (int l = 0; l < r; ++l)
+                if (l >= c) s = fma(d[r][l], x[l], s);
+            x[r] = r < c ? 0.0 : (r == c ? d[r][r] : -s * d[r][r]);
+        }
+#pragma unroll
+        for (int r = 0; r < 8; ++r) Xs[(p0 + c) * CP + p0 + r] = x[r];
     }
-    return bad;
+    return -1;
 }
 
 // Cholesky of S in place and its inverse in Xs (Pn is scratch).  Blocked by
-// 8-column panels: warp 0 factors a panel, then every warp applies its rank-8
-// update to the lower 8 x 8 tiles of the trailing block on the tensor cores.
-// The inverse: 8 x 8 diagonal blocks by forward substitution (one thread per
-// column, with the stored inverse pivots), then pairs of blocks merged as
-// X21 = -X22 (L21 X11) at widths 8, 16, 32.  Returns the column (0..63) of a
-// non-positive pivot, or -1.
-__device__ int chain_diag(double *S, double *Xs, double *Pn, double *invd) {
+// 8-column panels (chain_panel, which also inverts the panel's diagonal
+// block), then every warp applies the panel's rank-8 update to the lower 8 x 8
+// tiles of the trailing block on the tensor cores.  The inverse's diagonal
+// blocks are then merged in pairs as X21 = -X22 (L21 X11) at widths 8, 16, 32.
+// Returns the column (0..63) of a non-positive pivot, or -1.
+__device__ int chain_diag(double *S, double *Xs, double *Pn) {
     __shared__ int bad_sh;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, tig = lane & 3;
     for (int e = tid; e < TB * CP; e += NTH) Xs[e] = 0.0;
+    __syncthreads();
     for (int p0 = 0; p0 < TB; p0 += 8) {
-        if (warp == 0) {
-            const int b = chain_panel(S, invd, p0, lane);
-            if (lane == 0) bad_sh = b < 0 ? -1 : p0 + b;
+        if (warp < 3) {
+            const int b = chain_panel(S, Xs, p0, warp, lane);
+            if (warp == 0 && lane == 0) bad_sh = b < 0 ? -1 : p0 + b;
         }
         __syncthreads();
         if (bad_sh >= 0) return bad_sh;
@@ -263,43 +293,33 @@ __device__ int chain_diag(double *S, double *Xs, double *Pn, double *invd) {
         }
         __syncthreads();
     }
-    if (tid < TB) {
-        const int b0 = tid & ~7, c = tid & 7;
-        double x[8];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            double s = 0.0;
-#pragma unroll
-            for (int l = 0; l < r; ++l)
-                if (l >= c) s = fma(S[(b0 + l) * CP + b0 + r], x[l], s);
-            x[r] = r < c ? 0.0 : (r == c ? invd[b0 + r] : -s * invd[b0 + r]);
-        }
-#pragma unroll
-        for (int r = 0; r < 8; ++r) Xs[(b0 + c) * CP + b0 + r] = x[r];
-    }
-    __syncthreads();
     for (int h = 8; h < TB; h *= 2) {
         const int hb = h / 8, tpp = hb * hb, nt = (TB / (2 * h)) * tpp;
         // T = L21 X11 into the frame position of X21 in Pn (X11 lower: k >= the column block)
         for (int t = warp; t < nt; t += NTH / 32) {
             const int s0 = (t / tpp) * 2 * h, ti = (t % tpp) % hb, tj = (t % tpp) / hb;
             const int m0 = s0 + h + 8 * ti, n0 = s0 + 8 * tj;
-            double acc[2] = {0.0, 0.0};
-            for (int k = s0 + 8 * tj; k < s0 + h; k += 4)
+            // two accumulators: the trip count is even, and the chains interleave
+            double acc[2] = {0.0, 0.0}, acd[2] = {0.0, 0.0};
+            for (int k = s0 + 8 * tj; k < s0 + h; k += 8) {
                 dmma884(acc, S[(k + tig) * CP + m0 + g], Xs[(n0 + g) * CP + k + tig]);
-            Pn[(n0 + 2 * tig) * CP + m0 + g] = acc[0];
-            Pn[(n0 + 2 * tig + 1) * CP + m0 + g] = acc[1];
+                dmma884(acd, S[(k + 4 + tig) * CP + m0 + g], Xs[(n0 + g) * CP + k + 4 + tig]);
+            }
+            Pn[(n0 + 2 * tig) * CP + m0 + g] = acc[0] + acd[0];
+            Pn[(n0 + 2 * tig + 1) * CP + m0 + g] = acc[1] + acd[1];
         }
         __syncthreads();
         // X21 = -X22 T (X22 lower: k up to the row block)
         for (int t = warp; t < nt; t += NTH / 32) {
             const int s0 = (t / tpp) * 2 * h, ti = (t % tpp) % hb, tj = (t % tpp) / hb;
             const int m0 = s0 + h + 8 * ti, n0 = s0 + 8 * tj;
-            double acc[2] = {0.0, 0.0};
-            for (int k = s0 + h; k < m0 + 8; k += 4)
+            double acc[2] = {0.0, 0.0}, acd[2] = {0.0, 0.0};
+            for (int k = s0 + h; k < m0 + 8; k += 8) {
                 dmma884(acc, -Xs[(k + tig) * CP + m0 + g], Pn[(n0 + g) * CP + k + tig]);
-            Xs[(n0 + 2 * tig) * CP + m0 + g] = acc[0];
-            Xs[(n0 + 2 * tig + 1) * CP + m0 + g] = acc[1];
+                dmma884(acd, -Xs[(k + 4 + tig) * CP + m0 + g], Pn[(n0 + g) * CP + k + 4 + tig]);
+            }
+            Xs[(n0 + 2 * tig) * CP + m0 + g] = acc[0] + acd[0];
+            Xs[(n0 + 2 * tig + 1) * CP + m0 + g] = acc[1] + acd[1];
         }
         __syncthreads();
     }
@@ -331,7 +351,7 @@ __device__ __forceinline__ void chain_mm_nt(double (&acc)[4][2][2], const double
 // false if a wait gave up or a pivot failed (the abort flag is then set).
 __device__ bool run_chain(double *sm, const PotrfParams &P) {
     __shared__ int ok_c;
-    double *S = sm, *Xs = sm + TB * CP, *Pn = sm + 2 * TB * CP, *invd = sm + 3 * TB * CP;
+    double *S = sm, *Xs = sm + TB * CP, *Pn = sm + 2 * TB * CP;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, tig = lane & 3, wm = warp & 1, wn = warp >> 1;
     const int nb = P.nblk, n = P.n, lda = P.lda;
@@ -346,7 +366,7 @@ __device__ bool run_chain(double *sm, const PotrfParams &P) {
     __syncthreads();
     for (int j = 0; j < nb; ++j) {
         const int jb = bsz(j, n);
-        const int bad = chain_diag(S, Xs, Pn, invd);
+        const int bad = chain_diag(S, Xs, Pn);
         if (bad >= 0) {
             if (tid == 0) {
                 // a pivot of the padding is 1: bad < jb
