@@ -2301,25 +2301,63 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
             c->ar->off = base_mark;
             std::vector<GemmTask> g;
             std::vector<CopyTask> cp;
+            // low-rank tiles below TRSM(k+1, k): their V factors are gathered side by
+            // side into one NB x sum(r) block, so the solve is one wide product
+            // L^-1 [V_m ...] (the triangle bounds each output tile's inner dimension)
+            // instead of one skinny product per tile, then scattered back
+            std::vector<std::pair<int, int>> lr;
+            size_t sumr = 0;
+            // arena bytes of the gathered block and its product for w columns
+            auto lr_need = [&](size_t w) { return w ? 2 * align_up(sizeof(double) * NB * w + 1) : 0; };
+            auto flush = [&]() -> int {
+                TRY(run_gemms(c, g, false, P_GEMM_TRSM));
+                TRY(run_copies(c, cp));
+                if (!lr.empty()) {
+                    double *Vc = ws_alloc<double>(c, (size_t)NB * sumr), *Tc = ws_alloc<double>(c, (size_t)NB * sumr);
+                    if (!Vc || !Tc) { set_err("workspace too small (trsm, %zu columns)", sumr); return HICMA_TLR_ERR_OOM; }
+                    std::vector<CopyTask> gat, sct;
+                    size_t off = 0;
+                    for (const auto &mr : lr) {
+                        gat.push_back(make_copy(A->V(mr.first, k), NB, Vc + off * NB, NB, NB, mr.second));
+                        sct.push_back(make_copy(Tc + off * NB, NB, A->V(mr.first, k), NB, NB, mr.second));
+                        off += (size_t)mr.second;
+                    }
+                    TRY(run_copies(c, gat));
+                    std::vector<GemmTask> one{make_gemm(0, 0, NB, (int)sumr, NB, 1.0, Li, NB, Vc, NB, 0.0, Tc, NB)};
+                    one.back().tri = 1;
+                    TRY(run_gemms(c, one, false, P_GEMM_TRSM));
+                    TRY(run_copies(c, sct));
+                    lr.clear();
+                    sumr = 0;
+                }
+                c->ar->off = base_mark;
+                return 0;
+            };
             for (int m = k + 1; m < NT; ++m) {
                 if (m == k + 2) {
                     // TRSM(k+1, k) is all the critical chain SYRK(k, k+1) -> POTRF(k+1)
                     // needs: it goes first, on its own, and releases the chain
-                    TRY(run_gemms(c, g, false, P_GEMM_TRSM)); TRY(run_copies(c, cp));
+                    TRY(flush());
                     CUDA_TRY(cudaEventRecord(evT, c->stream));
-                    c->ar->off = base_mark;
                 }
                 const bool dense = A->is_dense(m, k);
                 const int r = dense ? NB : A->rank(m, k);
                 log_op(op_counts('t', NB, r, 1, 0), m, k, m == k + 1);
                 if (r == 0) continue;
-                double *tmp = ws_alloc<double>(c, (size_t)NB * r);
-                if (!tmp) {
-                    TRY(run_gemms(c, g, false, P_GEMM_TRSM)); TRY(run_copies(c, cp));
-                    c->ar->off = base_mark;
-                    tmp = ws_alloc<double>(c, (size_t)NB * r);
-                    if (!tmp) { set_err("workspace too small (trsm)"); return HICMA_TLR_ERR_OOM; }
+                if (!dense && m > k + 1) {
+                    // the pending block grows by r columns: flush first if it would not fit
+                    if (lr_need(sumr + r) > ws_free(c)) {
+                        TRY(flush());
+                        if (lr_need(r) > ws_free(c)) { set_err("workspace too small (trsm)"); return HICMA_TLR_ERR_OOM; }
+                    }
+                    lr.push_back({m, r});
+                    sumr += (size_t)r;
+                    continue;
                 }
+                // a per-tile product: its output and the pending block must both fit
+                if (align_up(sizeof(double) * NB * (size_t)r + 1) + lr_need(sumr) > ws_free(c)) TRY(flush());
+                double *tmp = ws_alloc<double>(c, (size_t)NB * r);
+                if (!tmp) { set_err("workspace too small (trsm)"); return HICMA_TLR_ERR_OOM; }
                 // L^-1 is lower triangular with zeros above the diagonal: each output
                 // tile runs its inner dimension only as far as L^-1 has entries
                 if (dense) {
@@ -2332,8 +2370,7 @@ static int factorize(hicma_tlr_ctx *c, hicma_tlr_desc *A, double acc, int fixed_
                     cp.push_back(make_copy(tmp, NB, A->V(m, k), NB, NB, r));
                 }
             }
-            TRY(run_gemms(c, g, false, P_GEMM_TRSM));
-            TRY(run_copies(c, cp));
+            TRY(flush());
             if (mixed) {
                 std::vector<NormTask> nt;
                 for (int m = k + 1; m < NT; ++m)
