@@ -69,8 +69,13 @@ static void usage(void) {
             " -U --compmaxrank  maxrank of buffers (default maxrank)\n"
             " -f --fixedrank    fixed rank in recompression (0 = accuracy mode)\n"
             " -D --kind_of_problem 0: randtlr 1: ed-2d-sin 2: st-2d-sqexp 3: st-3d-sqexp 4: st-3d-exp 5: ed-3d-sin\n"
+            "                      6: md-3d-virus 7: md-3d-cube\n"
             " -w --wavek        wave number of -D 1, 5 (default 50)\n"
-            " -j --adddiag      diagonal of -D 0, 1, 5 (default N)\n"
+            " -j --adddiag      diagonal of -D 0, 1, 5, 6, 7 (default N)\n"
+            " -M --mesh_file    mesh of -D 6 (x y z per node)   -K --numobj  copies of it (default 1)\n"
+            " -B --rbf_kernel   0 Gaussian 1 Expon 2 InvQUAD 3 InvMQUAD 4 Maternc1 5 Maternc2 6 TPS 7 CTPS 8 Wendland\n"
+            " -R --radius       RBF shape radius (-D 6, 7; required)\n"
+            " -O --order        0 none, 1 Morton (default 1)   -S --density  packing of -D 6's copies (-1 random)\n"
             " -Z --band         band size (default 1)\n"
             " -E --auto-band    auto-tune band size (default 1)\n"
             " -Y --lookahead    lookahead (-1: band size)\n"
@@ -87,6 +92,9 @@ int main(int argc, char **argv) {
     int auto_band = 1, lookahead = -1, send_full_tile = 0, two_flow = 0, HNB = 300, check = 0, verbose = 0;
     int device = 0, precision = HICMA_TLR_PREC_FP64, print_rank = 0;
     double tol = 1e-8, noise = 0.1, beta = 0.1, sigma = 1.0, ws_gib = 0.0, wave_k = 50.0, add_diag = 0.0;
+    int rbf_kernel = 0, numobj = 1, order = 1;
+    double radius = 0.0, density = -1.0;
+    const char *mesh_file = NULL;
     unsigned long long seed = 0;
     static struct option opts[] = {
         {"N", required_argument, 0, 'N'},          {"NB", required_argument, 0, 't'},
@@ -112,7 +120,7 @@ int main(int argc, char **argv) {
         {"wavek", required_argument, 0, 'w'},      {"adddiag", required_argument, 0, 'j'},
         {"add_diag", required_argument, 0, 'j'},   {"j", required_argument, 0, 'j'},
         {"grid-rows", required_argument, 0, 'P'},  {"grid-cols", required_argument, 0, 'Q'},
-        /* RBF mesh problems (-D 6, 7; not built): accepted so reference command lines parse */
+        /* RBF mesh problems (-D 6, 7, hicma_parsec.c:78-83) */
         {"rbf_kernel", required_argument, 0, 'B'}, {"B", required_argument, 0, 'B'},
         {"numobj", required_argument, 0, 'K'},     {"K", required_argument, 0, 'K'},
         {"mesh_file", required_argument, 0, 'M'},  {"M", required_argument, 0, 'M'},
@@ -145,7 +153,12 @@ int main(int argc, char **argv) {
             case 'v': verbose = optarg ? atoi(optarg) : 1; break;
             case 'h': usage(); return 0;
             case 'P': case 'Q': case 'c': case 'g': break;
-            case 'B': case 'K': case 'M': case 'O': case 'R': case 'S': break;
+            case 'B': rbf_kernel = atoi(optarg); break;
+            case 'K': numobj = atoi(optarg); break;
+            case 'M': mesh_file = optarg; break;
+            case 'O': order = atoi(optarg); break;
+            case 'R': radius = atof(optarg); break;
+            case 'S': density = atof(optarg); break;
             case 'w': wave_k = atof(optarg); break;
             case 'j': add_diag = atof(optarg); break;
             case 1001: noise = atof(optarg); break;
@@ -164,7 +177,9 @@ int main(int argc, char **argv) {
     if (genmaxrank <= 0) genmaxrank = maxrank;
     if (compmaxrank <= 0) compmaxrank = maxrank;
     if (add_diag <= 0.0) add_diag = (double)N;   /* hicma_parsec.c:289-291 */
-    if (kind < 0 || kind > 5) { fprintf(stderr, "Wrong value of \"kind_of_problem\" parameter (0 to 5)\n"); return 1; }
+    if (kind < 0 || kind > 7) { fprintf(stderr, "Wrong value of \"kind_of_problem\" parameter\n"); return 1; }
+    if (kind == 6 && !mesh_file) { fprintf(stderr, "-D 6 needs a mesh file (-M)\n"); return 1; }
+    if ((kind == 6 || kind == 7) && !(radius > 0.0)) { fprintf(stderr, "-D 6, 7 need a positive radius (-R)\n"); return 1; }
     if (N % NB != 0) { fprintf(stderr, "N must be a multiple of NB\n"); return 1; }
     const int NT = N / NB;
     const double flops = (N * (((1. / 6.) * N + 0.5) * N + (1. / 3.))) + (N * (((1. / 6.) * N) * N - (1. / 6.)));
@@ -172,6 +187,9 @@ int main(int argc, char **argv) {
         printf("M:%d N:%d NB:%d NB:%d HNB:%d HNB:%d\n", N, N, NB, NB, HNB, HNB);
         printf("kind_of_problem:%d %s\n", kind, str_problem[kind]);
         printf("tol:%.1e add_diag:%g fixed_rk:%d wave_k:%g\n", tol, add_diag, fixedrk, wave_k);
+        if (kind == 6 || kind == 7)   /* testing_dpotrf.c:368 */
+            printf("\nRBF, %s, %d, %d, %d, %d, %f, %f\n", mesh_file ? mesh_file : "(null)", N, rbf_kernel, numobj,
+                   order, radius, density);
         printf("noise:%g beta:%g sigma:%g seed:%llu\n", noise, beta, sigma, seed);
         printf("send_full_tile:%d lookahead: %d band_size:%d max_rank:%d gen:%d comp:%d\n", send_full_tile,
                lookahead, band_size, maxrank, genmaxrank, compmaxrank);
@@ -182,7 +200,14 @@ int main(int argc, char **argv) {
     int rc = hicma_tlr_init(device, (size_t)(ws_gib * (1ull << 30)), &ctx);
     if (rc) { fprintf(stderr, "init failed: %s\n", hicma_tlr_last_error()); return 1; }
     hicma_tlr_set_precision(ctx, precision);
-    hicma_tlr_problem prob = {kind, beta, 0.5, noise, sigma, seed, wave_k, add_diag};
+    hicma_tlr_problem prob = {kind, beta, 0.5, noise, sigma, seed, wave_k, add_diag,
+                              rbf_kernel, radius, numobj, order, density};
+    double *mesh_pts = NULL;   /* -D 6: the population of mesh copies */
+    if (kind == 6) {
+        mesh_pts = malloc(sizeof(double) * 3 * (size_t)N);
+        rc = hicma_tlr_points_mesh(&prob, mesh_file, N, mesh_pts);
+        if (rc) { fprintf(stderr, "mesh: %s\n", hicma_tlr_last_error()); return 1; }
+    }
     hicma_tlr_desc *A = NULL;
     const int band_created = band_size;   /* slots of the off-band tiles are laid out for this band */
     rc = hicma_tlr_desc_create(ctx, N, NB, maxrank > genmaxrank ? maxrank : genmaxrank, band_size, &A);
@@ -191,7 +216,7 @@ int main(int argc, char **argv) {
     int info = 0, ret = 0;
     int *rank_array = malloc(sizeof(int) * NT * NT);
     double t0 = wtime();
-    rc = hicma_tlr_generate(ctx, HICMA_TLR_LOWER, A, rank_array, &prob, NULL, tol, genmaxrank, band_size,
+    rc = hicma_tlr_generate(ctx, HICMA_TLR_LOWER, A, rank_array, &prob, mesh_pts, tol, genmaxrank, band_size,
                             send_full_tile, &info);
     const double time_starsh = wtime() - t0;
     printf("[****] TIME(s) %12.5f : STARSH_gen\tPxQ=   1 1   NB= %4d N= %7d\n", time_starsh, NB, N);
@@ -294,17 +319,23 @@ int main(int argc, char **argv) {
            (double)band_ops / (double)offband_ops, path_ops, offpath_ops, path_ops / offpath_ops);
     printf("R-LO %d %d %d %d   %d %d   %d %d %d %d   %d %s %.1e %g %d %g   %d %d %d %d %d %d %d %d   "
            "%g %d %d   %g %d %d   %g %d %d   %lf %lf   %lf %lf %lf %lf    %lf %lf %lf %lf %lf    "
-           "%le %le %le %le %le %lf %lf %d  GITHASH:N/A    \"",
+           "%le %le %le %le %le %lf %lf %d  ",
            N, N, NB, NB, HNB, HNB, 1, 1, 1, 1, kind, str_problem[kind], tol, add_diag, fixedrk, wave_k, send_full_tile,
            band_size, lookahead, 0, auto_band, maxrank, genmaxrank, compmaxrank, iavg_before, imin_before,
            imax_before, iavgrk, iminrk, imaxrk, favgrk, fminrk, fmaxrk, mem, mem_max, cpt[0] + cpt[1] + cpt[2],
            cpt[0], cpt[1], cpt[2], time_starsh, time_hicma, time_opt_band, time_regenerate, 0.0, (double)total,
            (double)band_ops, (double)offband_ops, path_ops, offpath_ops, (double)band_ops / (double)offband_ops,
            path_ops / offpath_ops, two_flow);
+    if (kind == 6 || kind == 7) {   /* testing_dpotrf.c:1044-1047 */
+        printf("%d %d %d  ", order, numobj, rbf_kernel);
+        printf("%g %g ", radius, density);
+    }
+    printf("GITHASH:N/A    \"");
     for (int i = 0; i < argc; ++i) printf("%s ", argv[i]);
     printf("\"\n");
     free(tileops);
     free(rank_array);
+    free(mesh_pts);
     if (A0) hicma_tlr_desc_destroy(A0);
     hicma_tlr_desc_destroy(A);
     hicma_tlr_fini(ctx);

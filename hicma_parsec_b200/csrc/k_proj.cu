@@ -149,7 +149,34 @@ __global__ void __launch_bounds__(PT, 2) k_gram_batched(const GramTask *__restri
     proj_gram(t.C, t.W, t.P, t.nb, t.rc, t.ra, red);
 }
 
+// Orthogonality check of formed Q factors (the generation range finder):
+// fail[i] = 1 when P = Q^T Q of task i (rc x rc, ld rc) differs from the
+// identity by more than thr in an entry between nonzero columns, else 0.  A
+// column of Q that is exactly zero (the sample had no component there) is
+// harmless and skipped; NaN fails.  One warp per task.
+__global__ void k_orth_check(const GramTask *__restrict__ tasks, int n, double thr, int *__restrict__ fail) {
+    const int w = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (w >= n) return;
+    const GramTask t = tasks[w];
+    const int K = t.rc;
+    int bad = 0;
+    for (int idx = lane; idx < K * K; idx += 32) {
+        const int i = idx % K, j = idx / K;
+        const double gii = t.P[i + (size_t)i * K], gjj = t.P[j + (size_t)j * K];
+        if (gii == 0.0 || gjj == 0.0) continue;
+        const double e = t.P[idx] - (i == j ? 1.0 : 0.0);
+        if (!(fabs(e) <= thr)) bad = 1;
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0) fail[w] = bad;
+}
+
 }  // namespace
+
+void launch_orth_check(const GramTask *d_tasks, int ntasks, double thr, int *fail, cudaStream_t st) {
+    if (ntasks <= 0) return;
+    k_orth_check<<<(ntasks + 7) / 8, 256, 0, st>>>(d_tasks, ntasks, thr, fail);
+}
 
 void launch_gram_batched(const GramTask *d_tasks, int ntasks, cudaStream_t st) {
     if (ntasks <= 0) return;

@@ -10,7 +10,12 @@
 // (hicma_parsec/testing_dpotrf.c:330,361): A_ij = sin(k r) / r, and add_diag
 // where r == 0.  randtlr (hicma_parsec/testing_dpotrf.c:315-321) reads a
 // basis instead of points: pts holds [Q | Q diag(S)] (N x 2K, column-major)
-// and A_ij = sum_k Q[i][k] (Q S)[j][k], plus add_diag where i == j.
+// and A_ij = sum_k Q[i][k] (Q S)[j][k], plus add_diag where i == j.  The
+// mesh-deformation kinds (md-3d-virus, md-3d-cube;
+// hicma_parsec/testing_dpotrf.c:366-381, kernels starsh_generate_3d_virus /
+// starsh_generate_3d_cube of the absent STARS-H) evaluate a radial basis
+// function phi(r / radius) (-B, hicma_parsec/hicma_parsec.c:80) and add
+// add_diag where i == j.
 // Distances are accumulated with explicitly rounded operations
 // (no FMA contraction) so that they match the CPU restatement bit for bit;
 // exp/sin/sqrt are CUDA's.
@@ -28,7 +33,32 @@ constexpr int COV_COLS = 8;     // columns per block
 // electrodynamics sin(k r)/r kernels, and the randtlr basis products.  One
 // instantiation each, so the families that need sin or the K-term loop do not
 // add registers or stack to the others.
-enum CovFamily { COV_STATS = 0, COV_ED = 1, COV_RANDTLR = 2 };
+enum CovFamily { COV_STATS = 0, COV_ED = 1, COV_RANDTLR = 2, COV_RBF = 3 };
+
+// Radial basis functions of s = r / radius (HICMA_TLR_RBF_*), polynomials
+// with explicitly rounded operations (no FMA contraction).
+__device__ __forceinline__ double rbf_phi(int f, double s) {
+    switch (f) {
+        case HICMA_TLR_RBF_GAUSSIAN: return exp(-__dmul_rn(s, s));
+        case HICMA_TLR_RBF_EXPON: return exp(-s);
+        case HICMA_TLR_RBF_INVQUAD: return __ddiv_rn(1.0, __dadd_rn(1.0, __dmul_rn(s, s)));
+        case HICMA_TLR_RBF_INVMQUAD: return __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(s, s))));
+        case HICMA_TLR_RBF_MATERNC1: return __dmul_rn(__dadd_rn(1.0, s), exp(-s));
+        case HICMA_TLR_RBF_MATERNC2:
+            return __dmul_rn(__dadd_rn(__dadd_rn(1.0, s), __ddiv_rn(__dmul_rn(s, s), 3.0)), exp(-s));
+        case HICMA_TLR_RBF_TPS: return s > 0.0 ? __dmul_rn(__dmul_rn(s, s), log(s)) : 0.0;
+        case HICMA_TLR_RBF_CTPS: {
+            if (s >= 1.0) return 0.0;
+            const double t = __dsub_rn(1.0, s), t2 = __dmul_rn(t, t);
+            return __dmul_rn(__dmul_rn(t2, t2), t);
+        }
+        default: {  // Wendland
+            if (s >= 1.0) return 0.0;
+            const double t = __dsub_rn(1.0, s), t2 = __dmul_rn(t, t);
+            return __dmul_rn(__dmul_rn(t2, t2), __dadd_rn(__dmul_rn(4.0, s), 1.0));
+        }
+    }
+}
 
 template <int FAM>
 __global__ void __launch_bounds__(COV_ROWS) k_cov_batched(CovParams p, const CovTask *__restrict__ tasks) {
@@ -65,7 +95,10 @@ __global__ void __launch_bounds__(COV_ROWS) k_cov_batched(CovParams p, const Cov
             }
         }
         double v;
-        if (FAM == COV_ED) {
+        if (FAM == COV_RBF) {
+            v = rbf_phi(p.rbf, __dmul_rn(__dsqrt_rn(r2), p.inv_radius));
+            if (gr == gc) v = __dadd_rn(v, p.add_diag);
+        } else if (FAM == COV_ED) {
             const double rr = __dsqrt_rn(r2);
             v = r2 == 0.0 ? p.add_diag : __ddiv_rn(sin(__dmul_rn(p.wave_k, rr)), rr);
         } else {
@@ -314,6 +347,8 @@ void launch_cov_batched(const CovParams &p, const CovTask *d_tasks, int ntasks, 
         k_cov_batched<COV_RANDTLR><<<grid, COV_ROWS, 0, st>>>(p, d_tasks);
     else if (p.kind == HICMA_TLR_KIND_ED_SIN_2D || p.kind == HICMA_TLR_KIND_ED_SIN_3D)
         k_cov_batched<COV_ED><<<grid, COV_ROWS, 0, st>>>(p, d_tasks);
+    else if (p.kind == HICMA_TLR_KIND_MD_VIRUS || p.kind == HICMA_TLR_KIND_MD_CUBE)
+        k_cov_batched<COV_RBF><<<grid, COV_ROWS, 0, st>>>(p, d_tasks);
     else
         k_cov_batched<COV_STATS><<<grid, COV_ROWS, 0, st>>>(p, d_tasks);
 }

@@ -1158,6 +1158,8 @@ int kind_ndim(int kind) {
         case HICMA_TLR_KIND_SQEXP_3D: return 3;
         case HICMA_TLR_KIND_EXP_3D: return 3;
         case HICMA_TLR_KIND_ED_SIN_3D: return 3;
+        case HICMA_TLR_KIND_MD_VIRUS: return 3;
+        case HICMA_TLR_KIND_MD_CUBE: return 3;
         default: return 0;
     }
 }
@@ -1177,6 +1179,70 @@ int grid_side(long long n, int ndim) {
     return (int)s;
 }
 
+// Arguments of the mesh kinds (6, 7): a known basis function, a positive
+// radius and an ordering this build has (0 none, 1 Morton; the reference
+// names Hilbert ordering, hicma_parsec.c:82, but STARS-H does not provide it).
+int rbf_args(const hicma_tlr_problem *prob) {
+    if (prob->kind != HICMA_TLR_KIND_MD_VIRUS && prob->kind != HICMA_TLR_KIND_MD_CUBE) return 0;
+    ARG_CHECK(prob->rbf_kernel >= HICMA_TLR_RBF_GAUSSIAN && prob->rbf_kernel <= HICMA_TLR_RBF_WENDLAND,
+              "rbf_kernel must be 0 to 8 (-B)");
+    ARG_CHECK(prob->radius > 0.0 && std::isfinite(prob->radius), "radius must be positive (-R)");
+    ARG_CHECK(prob->order == 0 || prob->order == 1, "order must be 0 (none) or 1 (Morton) (-O)");
+    return 0;
+}
+
+// 63-bit Morton code of a point of [0, 1)^3 at 21 bits per axis (x in the
+// lowest bit of each triple).
+uint64_t morton3(const double *x) {
+    uint64_t code = 0;
+    for (int a = 0; a < 3; ++a) {
+        long long q = (long long)std::floor(x[a] * 2097152.0);
+        q = std::min<long long>(std::max<long long>(q, 0), 2097151);
+        for (int b = 0; b < 21; ++b) code |= (((uint64_t)q >> b) & 1ull) << (b * 3 + a);
+    }
+    return code;
+}
+
+// The first N of a point set c (AoS, 3 per point) after a stable Morton sort
+// (order 1) or as given (order 0), written [3][N].  Coordinates are mapped
+// to [0, 1)^3 through the set's bounding box for the code only.
+void order_points(const std::vector<double> &c, int order, int N, double *points) {
+    const size_t total = c.size() / 3;
+    std::vector<size_t> idx(total);
+    for (size_t i = 0; i < total; ++i) idx[i] = i;
+    if (order == 1 && total > 0) {
+        double lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) { lo[a] = c[a]; hi[a] = c[a]; }
+        for (size_t i = 0; i < total; ++i)
+            for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], c[3 * i + a]); hi[a] = std::max(hi[a], c[3 * i + a]); }
+        std::vector<uint64_t> code(total);
+        for (size_t i = 0; i < total; ++i) {
+            double u[3];
+            for (int a = 0; a < 3; ++a) {
+                const double w = hi[a] - lo[a];
+                u[a] = w > 0.0 ? (c[3 * i + a] - lo[a]) / w * (1.0 - 0x1.0p-30) : 0.0;
+            }
+            code[i] = morton3(u);
+        }
+        std::stable_sort(idx.begin(), idx.end(), [&](size_t x, size_t y) { return code[x] < code[y]; });
+    }
+    for (int i = 0; i < N; ++i)
+        for (int a = 0; a < 3; ++a) points[(size_t)a * N + i] = c[3 * idx[(size_t)i] + a];
+}
+
+// md-3d-cube nodes: cell centres of an s^3 grid on the unit cube, s = ceil(cbrt(N)).
+int cube_points(int N, int order, double *points) {
+    const int s = grid_side(N, 3);
+    const size_t total = (size_t)s * s * s;
+    std::vector<double> c(3 * total);
+    for (size_t i = 0; i < total; ++i) {
+        const size_t g[3] = {i % s, (i / s) % s, i / ((size_t)s * s)};
+        for (int a = 0; a < 3; ++a) c[3 * i + a] = ((double)g[a] + 0.5) / (double)s;
+    }
+    order_points(c, order, N, points);
+    return 0;
+}
+
 }  // namespace
 
 // ======================================================================
@@ -1188,6 +1254,11 @@ int hicma_tlr_points(const hicma_tlr_problem *prob, int N, double *points) {
     ARG_CHECK(prob && points && N > 0, "hicma_tlr_points");
     const int ndim = kind_ndim(prob->kind);
     ARG_CHECK(ndim > 0, "unsupported problem kind");
+    ARG_CHECK(prob->kind != HICMA_TLR_KIND_MD_VIRUS, "md-3d-virus points come from a mesh file (hicma_tlr_points_mesh)");
+    if (prob->kind == HICMA_TLR_KIND_MD_CUBE) {
+        TRY(rbf_args(prob));
+        return cube_points(N, prob->order, points);
+    }
     const int side = grid_side(N, ndim);
     long long total = 1;
     for (int a = 0; a < ndim; ++a) total *= side;
@@ -1216,6 +1287,65 @@ int hicma_tlr_points(const hicma_tlr_problem *prob, int N, double *points) {
                      [&](long long x, long long y) { return code[(size_t)x] < code[(size_t)y]; });
     for (int i = 0; i < N; ++i)
         for (int a = 0; a < ndim; ++a) points[(size_t)a * N + i] = c[(size_t)order[i] * ndim + a];
+    return 0;
+}
+
+int hicma_tlr_points_mesh(const hicma_tlr_problem *prob, const char *mesh_file, int N, double *points) {
+    ARG_CHECK(prob && mesh_file && points && N > 0, "hicma_tlr_points_mesh");
+    ARG_CHECK(prob->kind == HICMA_TLR_KIND_MD_VIRUS, "hicma_tlr_points_mesh: kind must be md-3d-virus (6)");
+    TRY(rbf_args(prob));
+    FILE *f = std::fopen(mesh_file, "r");
+    ARG_CHECK(f, "cannot open the mesh file");
+    std::vector<double> mesh;
+    char line[4096];
+    while (std::fgets(line, sizeof line, f)) {
+        if (char *h = std::strchr(line, '#')) *h = '\0';
+        char *q = line;
+        for (;;) {
+            char *e = nullptr;
+            const double v = std::strtod(q, &e);
+            if (e == q) break;
+            mesh.push_back(v);
+            q = e;
+        }
+    }
+    std::fclose(f);
+    ARG_CHECK(!mesh.empty() && mesh.size() % 3 == 0, "mesh file: expected x y z triples");
+    const size_t M = mesh.size() / 3;
+    const int nobj = prob->numobj > 0 ? prob->numobj : 1;
+    ARG_CHECK((long long)N <= (long long)nobj * (long long)M, "N exceeds numobj times the mesh's node count");
+    // Centre the object on its bounding-box centre; d = the box diagonal.
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) { lo[a] = mesh[a]; hi[a] = mesh[a]; }
+    for (size_t i = 0; i < M; ++i)
+        for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], mesh[3 * i + a]); hi[a] = std::max(hi[a], mesh[3 * i + a]); }
+    double d2 = 0.0;
+    for (int a = 0; a < 3; ++a) d2 += (hi[a] - lo[a]) * (hi[a] - lo[a]);
+    const double d = std::sqrt(d2) > 0.0 ? std::sqrt(d2) : 1.0;
+    const int side = grid_side(nobj, 3);
+    std::vector<double> ctr(3 * (size_t)nobj);
+    if (prob->density > 0.0) {
+        const double dens = std::min(prob->density, M_PI / 6.0);
+        const double spacing = d * std::cbrt(M_PI / (6.0 * dens));
+        for (int o = 0; o < nobj; ++o) {
+            const int g[3] = {o % side, (o / side) % side, o / (side * side)};
+            for (int a = 0; a < 3; ++a) ctr[3 * o + a] = spacing * (double)g[a];
+        }
+    } else {
+        const double L = 2.0 * d * std::cbrt((double)nobj);
+        const uint64_t base = mix64h((uint64_t)prob->seed ^ 0x4D45534856495255ull);
+        for (int o = 0; o < nobj; ++o)
+            for (int a = 0; a < 3; ++a) {
+                const uint64_t z = mix64h(base + (uint64_t)(3 * o + a));
+                ctr[3 * o + a] = L * ((double)(z >> 11) * 0x1.0p-53);
+            }
+    }
+    std::vector<double> c(3 * (size_t)nobj * M);
+    for (int o = 0; o < nobj; ++o)
+        for (size_t i = 0; i < M; ++i)
+            for (int a = 0; a < 3; ++a)
+                c[3 * ((size_t)o * M + i) + a] = ctr[3 * o + a] + (mesh[3 * i + a] - 0.5 * (lo[a] + hi[a]));
+    order_points(c, prob->order, N, points);
     return 0;
 }
 
@@ -1669,7 +1799,10 @@ static int build_randtlr_basis(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_
 
 static int set_points(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_problem *prob, const double *points) {
     const int ndim = data_ndim(prob->kind, A->NB);
-    ARG_CHECK(ndim > 0, "unsupported problem kind (-D 0, 1, 2, 3, 4 or 5)");
+    ARG_CHECK(ndim > 0, "unsupported problem kind (-D 0 to 7)");
+    TRY(rbf_args(prob));
+    ARG_CHECK(!(prob->kind == HICMA_TLR_KIND_MD_VIRUS && !points),
+              "md-3d-virus needs the mesh points (hicma_tlr_points_mesh)");
     const bool randtlr = prob->kind == HICMA_TLR_KIND_RANDTLR;
     ARG_CHECK(!(randtlr && points), "randtlr takes no points (its bases are built on the device)");
     std::vector<double> h;
@@ -1696,6 +1829,7 @@ static int set_points(hicma_tlr_ctx *c, hicma_tlr_desc *A, const hicma_tlr_probl
 // regeneration and the checks regenerate tiles from it).
 static int check_problem_data(const hicma_tlr_desc *A, const hicma_tlr_problem *prob) {
     ARG_CHECK(A->d_pts, "no points: generate first");
+    TRY(rbf_args(prob));
     ARG_CHECK(data_ndim(prob->kind, A->NB) == A->ndim && A->ndim > 0,
               "problem kind differs from the one the descriptor was generated with");
     return 0;
@@ -1710,6 +1844,8 @@ static CovParams make_cov_params(const hicma_tlr_problem *prob, const double *d_
     p.beta = prob->beta; p.sigma = prob->sigma; p.noise = prob->noise;
     p.wave_k = prob->wave_k;
     p.add_diag = prob->add_diag > 0.0 ? prob->add_diag : (double)N;
+    p.rbf = prob->rbf_kernel;
+    p.inv_radius = prob->radius > 0.0 ? 1.0 / prob->radius : 0.0;
     return p;
 }
 
@@ -1752,8 +1888,19 @@ static size_t compress_ws_bytes(int nb, int s) {
     return b + 1024;
 }
 
+// Largest entry of |Q^T Q - I| accepted from the randomized CholeskyQR range
+// finder.  Healthy samples give about 1e-14; a sample of exactly lower rank
+// than its width (a sparse tile, e.g. a compactly supported RBF) can leave Q
+// far from orthonormal, and such a tile is compressed again on the Householder
+// path.
+constexpr double GEN_ORTH_THR = 1e-10;
+
+// d_fail (optional, one int per task): the CholeskyQR path writes 1 where the
+// range finder's Q fails the orthogonality check, else 0.  force_hh: take the
+// Householder path whatever s is.
 static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const double *Omega, int s,
-                        std::vector<CompressTask> &tasks, const double *d_identity, int *d_rank_task_base) {
+                        std::vector<CompressTask> &tasks, const double *d_identity, int *d_rank_task_base,
+                        int *d_fail = nullptr, bool force_hh = false) {
     const int pb = qr_panel_width(nb);
     const size_t npan = (size_t)(s + pb - 1) / pb + 1;
     const size_t mark = c->ar->off;
@@ -1767,9 +1914,10 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
         std::vector<CoreTask> cores;
         std::vector<CQTask> cqy, cqw;
         std::vector<GemmTask> gu;
+        std::vector<GramTask> gq;
         // up to rcholqr_kmax() samples: both QRs by randomized CholeskyQR (Q of
         // Y formed, R of W only), U = Q_Y U_r as a GEMM
-        const bool cq = c->cholqr && s <= rcholqr_kmax();
+        const bool cq = c->cholqr && s <= rcholqr_kmax() && !force_hh;
         size_t i = i0;
         for (; i < tasks.size(); ++i) {
             if (compress_ws_bytes(nb, s) > ws_free(c)) {
@@ -1786,6 +1934,7 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
                 int *rt = d_rank_task_base + (i - i0);
                 gy.push_back(make_gemm(0, 0, nb, s, nb, 1.0, t.A, nb, Omega, nb, 0.0, Y, nb));
                 cqy.push_back(CQTask{Y, nullptr, Q, RY, Q, nb, s, 0, nb, nb});
+                if (d_fail) gq.push_back(GramTask{Q, Q, ws_alloc<double>(c, (size_t)s * s), nb, s, s});
                 gw.push_back(make_gemm(1, 0, nb, s, nb, 1.0, t.A, nb, Q, nb, 0.0, W, nb));
                 cqw.push_back(CQTask{W, nullptr, nullptr, RW, nullptr, nb, s, 0, nb, nb});
                 CoreTask ct{};
@@ -1831,6 +1980,18 @@ static int run_compress(hicma_tlr_ctx *c, int nb, int maxrank, double tol, const
         TRY(run_gemms(c, gy, false, P_GEMM_GEN));
         TRY(run_qr(c, qy, nb));
         TRY(run_rcholqr(c, cqy, 0));
+        if (!gq.empty()) {
+            // Q^T Q of every formed Q, then the orthogonality flags of this sub-batch
+            GramTask *dq = stage(c, gq.data(), gq.size());
+            if (!dq) { set_err("staging failed"); return HICMA_TLR_ERR_CUDA; }
+            {
+                Prof pf(c, P_GRAM, 2.0 * nb * (double)s * s * gq.size(), 8.0 * nb * (double)s * gq.size());
+                launch_gram_batched(dq, (int)gq.size(), c->cur);
+            }
+            TRY(check_launch(c));
+            launch_orth_check(dq, (int)gq.size(), GEN_ORTH_THR, d_fail + i0, c->cur);
+            TRY(check_launch(c));
+        }
         TRY(run_qapply(c, aq, nb));
         TRY(run_gemms(c, gw, false, P_GEMM_GEN));
         TRY(run_copies(c, keeps));
@@ -1888,7 +2049,14 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
         for (int n = 0; n <= m - A->band; ++n) pending.push_back({m, n});
     const CovParams cp = cov_params(A, prob);
     int s = std::min(c->cholqr ? rcholqr_kmax() : 160, s_full);
+    // force_hh: the round compresses tiles whose CholeskyQR range finder failed
+    // its orthogonality check, on the Householder path at the same s
+    bool force_hh = false;
     while (!pending.empty()) {
+        const size_t mark_round = c->ar->off;
+        const bool cq_round = c->cholqr && s <= rcholqr_kmax() && !force_hh;
+        int *dfail = cq_round ? ws_alloc<int>(c, pending.size()) : nullptr;
+        if (cq_round && !dfail) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
         launch_set_identity(Ident, s, s, c->stream);
         TRY(check_launch(c));
         const size_t per_tile = align_up(sizeof(double) * (size_t)NB * NB + 1) + compress_ws_bytes(NB, s);
@@ -1912,20 +2080,32 @@ int hicma_tlr_generate(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, c
                 launch_cov_batched(cp, dcov, (int)cov.size(), NB, NB, c->stream);
             }
             TRY(check_launch(c));
-            TRY(run_compress(c, NB, maxrank, tol, Omega, s, comp, Ident, rtask));
+            TRY(run_compress(c, NB, maxrank, tol, Omega, s, comp, Ident, rtask, dfail ? dfail + t0 : nullptr,
+                             force_hh));
             c->ar->off = mark;
         }
-        if (s >= s_full) break;
+        std::vector<int> fails;
+        if (dfail) {
+            fails.resize(pending.size());
+            CUDA_TRY(xfer(c, fails.data(), dfail, fails.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        }
+        c->ar->off = mark_round;
+        const bool any_fail = std::find(fails.begin(), fails.end(), 1) != fails.end();
+        if (s >= s_full && !any_fail) break;
         TRY(ctx_sync(c));
         CUDA_TRY(xfer(c, A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
         std::vector<std::pair<int, int>> more;
         const int margin = std::max(32, s / 4);
-        for (auto &t : pending) {
+        bool grow = false;
+        for (size_t i = 0; i < pending.size(); ++i) {
+            const auto &t = pending[i];
+            if (!fails.empty() && fails[i]) { more.push_back(t); continue; }
             const int r = A->rank(t.first, t.second);
-            if (r >= 0 && r > s - margin) more.push_back(t);
+            if (s < s_full && r >= 0 && r > s - margin) { more.push_back(t); grow = true; }
         }
         pending.swap(more);
-        s = std::min(2 * s, s_full);
+        if (grow) s = std::min(2 * s, s_full);
+        force_hh = any_fail;
     }
     TRY(ctx_sync(c));
     CUDA_TRY(xfer(c, A->h_rank.data(), A->d_rank, (size_t)NT * NT * sizeof(int), cudaMemcpyDeviceToHost));
@@ -3192,6 +3372,7 @@ int hicma_tlr_k_cov(const hicma_tlr_problem *prob, const double *d_points, int N
     ARG_CHECK(r0 >= 0 && c0 >= 0 && r0 + nr <= N && c0 + nc <= N, "k_cov range");
     const int ndim = kind_ndim(prob->kind);
     ARG_CHECK(ndim > 0, "kind (randtlr tiles come from hicma_tlr_generate: no points)");
+    TRY(rbf_args(prob));
     const CovParams p = make_cov_params(prob, d_points, N, ndim);
     CovTask t{d_out, ld, r0, c0, nr, nc};
     CovTask *dt = nullptr;
@@ -3352,7 +3533,17 @@ int hicma_tlr_k_compress(hicma_tlr_ctx *c, int nb, const double *d_A, double *d_
     launch_gaussian(Omega, nb, s, nb, 0x5DEECE66Dull, c->stream);
     launch_set_identity(Ident, s, s, c->stream);
     std::vector<CompressTask> v{CompressTask{d_A, d_U, d_V, d_r}};
-    TRY(run_compress(c, nb, maxrank, tol, Omega, s, v, Ident, d_r + 1));
+    int *d_fail = ws_alloc<int>(c, 1);
+    if (!d_fail) { set_err("workspace too small"); return HICMA_TLR_ERR_OOM; }
+    CUDA_TRY(cudaMemsetAsync(d_fail, 0, sizeof(int), c->stream));
+    TRY(run_compress(c, nb, maxrank, tol, Omega, s, v, Ident, d_r + 1, d_fail));
+    int fail = 0;
+    CUDA_TRY(cudaMemcpyAsync(&fail, d_fail, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    TRY(ctx_sync(c));
+    if (fail) {   // the range finder's Q failed its orthogonality check: Householder path
+        v.assign(1, CompressTask{d_A, d_U, d_V, d_r});
+        TRY(run_compress(c, nb, maxrank, tol, Omega, s, v, Ident, d_r + 1, nullptr, true));
+    }
     int r = 0;
     CUDA_TRY(cudaMemcpyAsync(&r, d_r, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     TRY(ctx_sync(c));

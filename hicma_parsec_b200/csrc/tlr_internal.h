@@ -95,7 +95,9 @@ struct CovParams {
     const double *pts;  // [ndim][N]
     int N, ndim, kind;
     double beta, sigma, noise;
-    double wave_k, add_diag;   // electrodynamics kinds
+    double wave_k, add_diag;   // electrodynamics kinds; add_diag also the mesh kinds' regularisation
+    int rbf;                   // mesh kinds: HICMA_TLR_RBF_* basis function
+    double inv_radius;         // mesh kinds: 1 / radius
 };
 void launch_cov_batched(const CovParams &p, const CovTask *d_tasks, int ntasks, int max_nr,
                         int max_nc, cudaStream_t st);
@@ -152,6 +154,9 @@ struct GramTask {
     int nb, rc, ra;
 };
 void launch_gram_batched(const GramTask *d_tasks, int ntasks, cudaStream_t st);
+// fail[i] = 1 when the P of task i (a Q^T Q, rc == ra) is not the identity to
+// within thr between nonzero columns, else 0 (one warp per task).
+void launch_orth_check(const GramTask *d_tasks, int ntasks, double thr, int *fail, cudaStream_t st);
 
 // ------------------------------------------------------ precision policy ---
 // out = sum of squares of X (rows x cols, ld): one CTA per task.

@@ -28,7 +28,10 @@ LIB_PATH_CHECKED = os.path.join(HERE, "lib", "libhicma_tlr_checked.so")
 LOWER = 122
 UPPER = 121
 KIND_RANDTLR, KIND_ED_SIN_2D, KIND_SQEXP_2D, KIND_SQEXP_3D, KIND_EXP_3D, KIND_ED_SIN_3D = 0, 1, 2, 3, 4, 5
-KIND_NDIM = {1: 2, 2: 2, 3: 3, 4: 3, 5: 3}     # point kinds; randtlr has no points
+KIND_MD_VIRUS, KIND_MD_CUBE = 6, 7
+KIND_NDIM = {1: 2, 2: 2, 3: 3, 4: 3, 5: 3, 6: 3, 7: 3}     # point kinds; randtlr has no points
+(RBF_GAUSSIAN, RBF_EXPON, RBF_INVQUAD, RBF_INVMQUAD, RBF_MATERNC1, RBF_MATERNC2, RBF_TPS, RBF_CTPS,
+ RBF_WENDLAND) = range(9)
 PREC_FP64, PREC_MIXED = 0, 1
 ERR_ARG, ERR_CUDA, ERR_OOM, ERR_RANK_OVERFLOW, ERR_TIMEOUT, ERR_STATE, ERR_NOT_SUPPORTED = -1, -2, -3, -4, -5, -6, -7
 
@@ -44,7 +47,8 @@ class TLRError(RuntimeError):
 class CProblem(C.Structure):
     _fields_ = [("kind", C.c_int), ("beta", C.c_double), ("nu", C.c_double), ("noise", C.c_double),
                 ("sigma", C.c_double), ("seed", C.c_ulonglong), ("wave_k", C.c_double),
-                ("add_diag", C.c_double)]
+                ("add_diag", C.c_double), ("rbf_kernel", C.c_int), ("radius", C.c_double),
+                ("numobj", C.c_int), ("order", C.c_int), ("density", C.c_double)]
 
 
 @dataclass
@@ -53,7 +57,11 @@ class Problem:
     arguments, hicma_parsec/testing_dpotrf.c:300-365; defaults of the reference).
     ``wave_k`` applies to the electrodynamics kinds 1 and 5, ``add_diag`` to them
     and to randtlr (kind 0); ``add_diag <= 0`` means N
-    (hicma_parsec/hicma_parsec.c:289-291)."""
+    (hicma_parsec/hicma_parsec.c:289-291).  The mesh kinds 6 (md-3d-virus) and 7
+    (md-3d-cube) evaluate the radial basis function ``rbf_kernel`` of
+    ``r / radius`` plus ``add_diag`` on the diagonal (testing_dpotrf.c:366-381);
+    ``numobj`` and ``density`` place kind 6's mesh copies, ``order`` 1 Morton
+    orders the points of both."""
     kind: int = KIND_SQEXP_2D
     beta: float = 0.1
     nu: float = 0.5
@@ -62,6 +70,11 @@ class Problem:
     seed: int = 0
     wave_k: float = 50.0
     add_diag: float = 0.0
+    rbf_kernel: int = RBF_GAUSSIAN
+    radius: float = 0.0
+    numobj: int = 1
+    order: int = 1
+    density: float = -1.0
 
     @property
     def ndim(self) -> int:
@@ -69,7 +82,7 @@ class Problem:
 
     def c(self) -> CProblem:
         return CProblem(self.kind, self.beta, self.nu, self.noise, self.sigma, self.seed, self.wave_k,
-                        self.add_diag)
+                        self.add_diag, self.rbf_kernel, self.radius, self.numobj, self.order, self.density)
 
 
 def _p(a):
@@ -97,6 +110,7 @@ def load_library(path: str | None = None):
         "hicma_tlr_desc_info": (i, [vp, ip, ip, ip, ip, ip]),
         "hicma_tlr_desc_copy": (i, [vp, vp, vp]),
         "hicma_tlr_points": (i, [C.POINTER(CProblem), i, vp]),
+        "hicma_tlr_points_mesh": (i, [C.POINTER(CProblem), C.c_char_p, i, vp]),
         "hicma_tlr_generate": (i, [vp, i, vp, vp, C.POINTER(CProblem), vp, d, i, i, i, ip]),
         "hicma_tlr_rank_gather": (i, [vp, vp, vp, i]),
         "hicma_tlr_rank_stat": (i, [vp, i, i, ip, ip, dp]),
@@ -165,6 +179,17 @@ def points(prob: Problem, n: int) -> np.ndarray:
     out = np.empty((prob.ndim, n), dtype=np.float64)
     cp = prob.c()
     _check(lib.hicma_tlr_points(C.byref(cp), n, _p(out)), "hicma_tlr_points")
+    return out
+
+
+def points_mesh(prob: Problem, mesh_file: str, n: int) -> np.ndarray:
+    """Points [3][n] of the md-3d-virus problem: ``prob.numobj`` copies of the
+    mesh read from ``mesh_file`` (x y z triples), placed by ``prob.density``
+    and ordered by ``prob.order`` (``hicma_tlr_points_mesh``)."""
+    lib = load_library()
+    out = np.empty((3, n), dtype=np.float64)
+    cp = prob.c()
+    _check(lib.hicma_tlr_points_mesh(C.byref(cp), os.fsencode(mesh_file), n, _p(out)), "hicma_tlr_points_mesh")
     return out
 
 

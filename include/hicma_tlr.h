@@ -46,14 +46,27 @@ extern "C" {
 #define HICMA_TLR_UPPER 121
 #define HICMA_TLR_LOWER 122
 
-/* -D problem kinds (hicma_parsec/testing_dpotrf.c:12, :315-365).  Kinds 6, 7
- * (RBF meshes) are rejected with HICMA_TLR_ERR_ARG. */
+/* -D problem kinds (hicma_parsec/testing_dpotrf.c:12, :315-381). */
 #define HICMA_TLR_KIND_RANDTLR   0   /* random TLR, equal ranks (testing_dpotrf.c:315-321) */
 #define HICMA_TLR_KIND_ED_SIN_2D 1   /* sin(k r)/r, 2D (testing_dpotrf.c:325-334) */
 #define HICMA_TLR_KIND_SQEXP_2D  2
 #define HICMA_TLR_KIND_SQEXP_3D  3
 #define HICMA_TLR_KIND_EXP_3D    4
 #define HICMA_TLR_KIND_ED_SIN_3D 5   /* sin(k r)/r, 3D (testing_dpotrf.c:359-365) */
+#define HICMA_TLR_KIND_MD_VIRUS  6   /* RBF over mesh points read from a file (testing_dpotrf.c:366-374) */
+#define HICMA_TLR_KIND_MD_CUBE   7   /* RBF over the nodes of a cube (testing_dpotrf.c:375-381) */
+
+/* Radial basis functions of the mesh kinds (-B, hicma_parsec.c:80), of
+ * s = r / radius; the CTPS and Wendland functions vanish for s >= 1. */
+#define HICMA_TLR_RBF_GAUSSIAN  0   /* exp(-s^2)                  */
+#define HICMA_TLR_RBF_EXPON     1   /* exp(-s)                    */
+#define HICMA_TLR_RBF_INVQUAD   2   /* 1 / (1 + s^2)              */
+#define HICMA_TLR_RBF_INVMQUAD  3   /* 1 / sqrt(1 + s^2)          */
+#define HICMA_TLR_RBF_MATERNC1  4   /* (1 + s) exp(-s)            */
+#define HICMA_TLR_RBF_MATERNC2  5   /* (1 + s + s^2 / 3) exp(-s)  */
+#define HICMA_TLR_RBF_TPS       6   /* s^2 log s (0 at s = 0)     */
+#define HICMA_TLR_RBF_CTPS      7   /* (1 - s)^5 for s < 1        */
+#define HICMA_TLR_RBF_WENDLAND  8   /* (1 - s)^4 (4 s + 1) for s < 1 */
 
 /* Precision policy of the factorization (no reference counterpart). */
 #define HICMA_TLR_PREC_FP64   0   /* everything in FP64                              */
@@ -71,7 +84,12 @@ typedef struct hicma_tlr_desc_s hicma_tlr_desc;  /* device tile store of a matri
  * + add_diag * [m == n] I, Q_m a random orthonormal basis of block row m
  * (first min(NB, 64) columns; seeded by seed), S_k = 0.5^k (decay of
  * testing_dpotrf.c:318).  randtlr has no points: hicma_tlr_points rejects it
- * and hicma_tlr_generate builds the bases on the device (points must be NULL). */
+ * and hicma_tlr_generate builds the bases on the device (points must be NULL).
+ * Mesh kinds (6, 7): A_ij = phi(|x_i - x_j| / radius), phi the basis function
+ * rbf_kernel, plus add_diag where i == j (the reference passes add_diag as the
+ * regularisation, testing_dpotrf.c:371,379).  Kind 7's points come from
+ * hicma_tlr_points; kind 6 reads a mesh (hicma_tlr_points_mesh) and the caller
+ * passes the points to hicma_tlr_generate. */
 typedef struct {
     int    kind;      /* HICMA_TLR_KIND_*                                   */
     double beta;      /* length scale (reference default 0.1)               */
@@ -80,7 +98,12 @@ typedef struct {
     double sigma;     /* variance (default 1.0)                             */
     unsigned long long seed;  /* point placement seed (reference srand(0)) */
     double wave_k;    /* wave number of kinds 1, 5 (default 50, hicma_parsec.c:188)        */
-    double add_diag;  /* diagonal of kinds 0, 1, 5; <= 0 means N (hicma_parsec.c:289-291) */
+    double add_diag;  /* diagonal of kinds 0, 1, 5, 6, 7; <= 0 means N (hicma_parsec.c:289-291) */
+    int    rbf_kernel;  /* HICMA_TLR_RBF_* of kinds 6, 7 (-B)                            */
+    double radius;      /* shape radius of kinds 6, 7, > 0 (-R)                          */
+    int    numobj;      /* kind 6: copies of the mesh in the population (-K; <= 0 means 1) */
+    int    order;       /* kinds 6, 7: 0 no reordering, 1 Morton (-O; 2 Hilbert rejected) */
+    double density;     /* kind 6: packing density of the copies, -1 random (-S)        */
 } hicma_tlr_problem;
 
 /* ---------------------------------------------------------------- setup -- */
@@ -109,8 +132,26 @@ int hicma_tlr_desc_copy(hicma_tlr_ctx *ctx, const hicma_tlr_desc *src, hicma_tlr
 /* ----------------------------------------------------------- generation -- */
 
 /* Points of the problem (starsh_ssdata_generate, testing_dpotrf.c:305-312,
- * 336-358): jittered grid, Morton order.  points is [ndim][N] (SoA). */
+ * 336-358): jittered grid, Morton order.  points is [ndim][N] (SoA).
+ * md-3d-cube (kind 7, starsh_generate_3d_rbf_mesh_coordinates_cube,
+ * testing_dpotrf.c:375-381; STARS-H's generator is absent from the reference
+ * tree): the cell centres ((i + 1/2) / s, (j + 1/2) / s, (k + 1/2) / s) of an
+ * s x s x s grid on the unit cube, s = ceil(cbrt(N)), in Morton order when
+ * prob->order == 1 and in x-fastest order when 0; the first N are returned. */
 int hicma_tlr_points(const hicma_tlr_problem *prob, int N, double *points);
+
+/* Points of the md-3d-virus problem (starsh_generate_3d_rbf_mesh_coordinates_virus,
+ * testing_dpotrf.c:366-374; STARS-H's reader is absent from the reference tree):
+ * the mesh file holds one object's nodes as whitespace-separated x y z triples
+ * ('#' starts a comment).  prob->numobj copies of the object (centred on its
+ * bounding-box centre, diameter d = the box diagonal) are placed on a cubic
+ * lattice of side ceil(cbrt(numobj)), spacing d * cbrt(pi / (6 density)) (the
+ * copies' bounding spheres fill the fraction density of space, at most pi/6,
+ * where they touch); density <= 0 places the centres uniformly at random
+ * (seeded by prob->seed) in a cube of side 2 d cbrt(numobj).  The population
+ * is Morton ordered when prob->order == 1, and its first N nodes are returned
+ * as [3][N]; N larger than numobj times the node count is an argument error. */
+int hicma_tlr_points_mesh(const hicma_tlr_problem *prob, const char *mesh_file, int N, double *points);
 
 /* STARSH_gen (hicma_parsec/hicma_parsec.h:187-198; STARSH_gen.jdf:342-369):
  * band tiles dense, off-band tiles compressed to tolerance tol and at most

@@ -60,9 +60,16 @@ KIND_SQEXP_2D = 2
 KIND_SQEXP_3D = 3
 KIND_EXP_3D = 4
 KIND_ED_SIN_3D = 5
+KIND_MD_VIRUS = 6
+KIND_MD_CUBE = 7
 KIND_NAMES = {KIND_RANDTLR: "randtlr", KIND_ED_SIN_2D: "ed-2d-sin", KIND_SQEXP_2D: "st-2d-sqexp", KIND_SQEXP_3D: "st-3d-sqexp",
-              KIND_EXP_3D: "st-3d-exp", KIND_ED_SIN_3D: "ed-3d-sin"}
-KIND_NDIM = {KIND_ED_SIN_2D: 2, KIND_SQEXP_2D: 2, KIND_SQEXP_3D: 3, KIND_EXP_3D: 3, KIND_ED_SIN_3D: 3}
+              KIND_EXP_3D: "st-3d-exp", KIND_ED_SIN_3D: "ed-3d-sin", KIND_MD_VIRUS: "md-3d-virus",
+              KIND_MD_CUBE: "md-3d-cube"}
+KIND_NDIM = {KIND_ED_SIN_2D: 2, KIND_SQEXP_2D: 2, KIND_SQEXP_3D: 3, KIND_EXP_3D: 3, KIND_ED_SIN_3D: 3,
+             KIND_MD_VIRUS: 3, KIND_MD_CUBE: 3}
+# Radial basis functions of the mesh kinds (-B, hicma_parsec.c:80)
+RBF_GAUSSIAN, RBF_EXPON, RBF_INVQUAD, RBF_INVMQUAD, RBF_MATERNC1, RBF_MATERNC2, RBF_TPS, RBF_CTPS, RBF_WENDLAND = range(9)
+MESH_SEED_XOR = 0x4D45534856495255
 
 RANDTLR_DECAY = 0.5               # testing_dpotrf.c:318
 RANDTLR_KMAX = 64                 # singular directions kept: 0.5**64 is below FP64 resolution
@@ -139,6 +146,111 @@ def gen_points(n: int, ndim: int, seed: int = 0) -> np.ndarray:
     return np.ascontiguousarray(pts[order[:n]])
 
 
+def _order_points(c: np.ndarray, order: int, n: int) -> np.ndarray:
+    """First n rows of the (total, 3) point set c after a stable Morton sort
+    (order 1; coordinates mapped to [0, 1) through the set's bounding box for
+    the code only) or as given (order 0)."""
+    if order == 1 and c.shape[0] > 0:
+        lo, hi = c.min(axis=0), c.max(axis=0)
+        w = hi - lo
+        u = np.zeros_like(c)
+        for a in range(3):
+            if w[a] > 0.0:
+                u[:, a] = (c[:, a] - lo[a]) / w[a] * (1.0 - 2.0 ** -30)
+        c = c[np.argsort(morton_codes(u), kind="stable")]
+    return np.ascontiguousarray(c[:n])
+
+
+def cube_points(n: int, order: int = 1) -> np.ndarray:
+    """md-3d-cube nodes (``testing_dpotrf.c:375-381``; STARS-H's
+    ``starsh_generate_3d_rbf_mesh_coordinates_cube`` is absent from the
+    reference tree, so this is the restatement's own rule): the cell centres
+    ((i + 1/2)/s, (j + 1/2)/s, (k + 1/2)/s) of an s^3 grid on the unit cube,
+    s = ceil(cbrt(n)), x fastest, Morton ordered when ``order == 1``; the
+    first n.  Same arithmetic as the library's host generator."""
+    s = grid_side(n, 3)
+    i = np.arange(s ** 3, dtype=np.int64)
+    g = np.stack([i % s, (i // s) % s, i // (s * s)], axis=1).astype(np.float64)
+    return _order_points((g + 0.5) / float(s), order, n)
+
+
+def read_mesh(path: str) -> np.ndarray:
+    """x y z triples of a mesh file (whitespace separated, '#' comments)."""
+    vals = []
+    with open(path) as f:
+        for line in f:
+            line = line.split("#", 1)[0]
+            for tok in line.split():
+                vals.append(float(tok))
+    if not vals or len(vals) % 3:
+        raise ValueError("mesh file: expected x y z triples")
+    return np.array(vals, dtype=np.float64).reshape(-1, 3)
+
+
+def virus_points(mesh: np.ndarray, n: int, prob: "Problem") -> np.ndarray:
+    """md-3d-virus population (``testing_dpotrf.c:366-374``; STARS-H's
+    ``starsh_generate_3d_rbf_mesh_coordinates_virus`` is absent from the
+    reference tree, so the placement is the restatement's own rule):
+    ``numobj`` copies of the mesh, each centred on its bounding-box centre
+    (diameter d = the box diagonal), on a cubic lattice of side
+    ceil(cbrt(numobj)) with spacing d cbrt(pi / (6 density)) (density capped
+    at pi/6, where the bounding spheres touch), or, for density <= 0, at
+    centres uniform in a cube of side 2 d cbrt(numobj) (seeded counter
+    generator); Morton ordered when ``order == 1``; the first n nodes."""
+    nobj = prob.numobj if prob.numobj > 0 else 1
+    M = mesh.shape[0]
+    if n > nobj * M:
+        raise ValueError("N exceeds numobj times the mesh's node count")
+    lo, hi = mesh.min(axis=0), mesh.max(axis=0)
+    d2 = 0.0
+    for a in range(3):
+        d2 += (hi[a] - lo[a]) * (hi[a] - lo[a])
+    d = math.sqrt(d2) if math.sqrt(d2) > 0.0 else 1.0
+    side = grid_side(nobj, 3)
+    o = np.arange(nobj, dtype=np.int64)
+    if prob.density > 0.0:
+        dens = min(prob.density, math.pi / 6.0)
+        spacing = d * math.cbrt(math.pi / (6.0 * dens))
+        ctr = spacing * np.stack([o % side, (o // side) % side, o // (side * side)], axis=1).astype(np.float64)
+    else:
+        L = 2.0 * d * math.cbrt(float(nobj))
+        sd = (prob.seed ^ MESH_SEED_XOR) & 0xFFFFFFFFFFFFFFFF
+        ctr = L * uniform01(sd, np.arange(3 * nobj, dtype=np.uint64)).reshape(nobj, 3)
+    centred = mesh - 0.5 * (lo + hi)
+    c = (ctr[:, None, :] + centred[None, :, :]).reshape(-1, 3)
+    return _order_points(c, prob.order, n)
+
+
+def rbf_phi(f: int, s: np.ndarray) -> np.ndarray:
+    """Radial basis functions of s = r / radius (-B, ``hicma_parsec.c:80``):
+    Gaussian exp(-s^2), exponential exp(-s), inverse quadratic 1/(1+s^2),
+    inverse multiquadric 1/sqrt(1+s^2), Matern C1 (1+s) exp(-s), Matern C2
+    (1 + s + s^2/3) exp(-s), thin-plate spline s^2 log s, compactly supported
+    thin-plate (1-s)^5 and Wendland C2 (1-s)^4 (4s+1) on s < 1."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if f == RBF_GAUSSIAN:
+            return np.exp(-(s * s))
+        if f == RBF_EXPON:
+            return np.exp(-s)
+        if f == RBF_INVQUAD:
+            return 1.0 / (1.0 + s * s)
+        if f == RBF_INVMQUAD:
+            return 1.0 / np.sqrt(1.0 + s * s)
+        if f == RBF_MATERNC1:
+            return (1.0 + s) * np.exp(-s)
+        if f == RBF_MATERNC2:
+            return ((1.0 + s) + (s * s) / 3.0) * np.exp(-s)
+        if f == RBF_TPS:
+            return np.where(s > 0.0, (s * s) * np.log(np.where(s > 0.0, s, 1.0)), 0.0)
+        t = 1.0 - s
+        t2 = t * t
+        if f == RBF_CTPS:
+            return np.where(s < 1.0, (t2 * t2) * t, 0.0)
+        if f == RBF_WENDLAND:
+            return np.where(s < 1.0, (t2 * t2) * (4.0 * s + 1.0), 0.0)
+    raise ValueError(f"rbf_kernel {f}")
+
+
 # --------------------------------------------------------------------------
 # Covariance kernels (STARS-H ssdata block kernels, restated)
 # --------------------------------------------------------------------------
@@ -151,7 +263,12 @@ class Problem:
     sigma: float = 1.0         # testing_dpotrf.c:306
     seed: int = 0
     wave_k: float = 50.0       # electrodynamics wave number (hicma_parsec.c:188, flag -w)
-    add_diag: float = 0.0      # electrodynamics diagonal; <= 0 means N (hicma_parsec.c:289-291, flag -j)
+    add_diag: float = 0.0      # electrodynamics / mesh diagonal; <= 0 means N (hicma_parsec.c:289-291, flag -j)
+    rbf_kernel: int = RBF_GAUSSIAN   # mesh kinds: basis function (flag -B)
+    radius: float = 0.0        # mesh kinds: shape radius (flag -R)
+    numobj: int = 1            # md-3d-virus: copies of the mesh (flag -K)
+    order: int = 1             # mesh kinds: 0 no reordering, 1 Morton (flag -O)
+    density: float = -1.0      # md-3d-virus: packing density, <= 0 random (flag -S)
 
     @property
     def ndim(self) -> int:
@@ -207,6 +324,10 @@ def problem_points(prob: "Problem", n: int, nb: int) -> np.ndarray:
     point kernels, the (n, 2K) basis for randtlr."""
     if prob.kind == KIND_RANDTLR:
         return randtlr_basis(n, nb, prob.seed)
+    if prob.kind == KIND_MD_CUBE:
+        return cube_points(n, prob.order)
+    if prob.kind == KIND_MD_VIRUS:
+        raise ValueError("md-3d-virus points come from a mesh (virus_points)")
     return gen_points(n, prob.ndim, prob.seed)
 
 
@@ -235,6 +356,13 @@ def cov_block(prob: Problem, pts: np.ndarray, r0: int, nr: int, c0: int, nc: int
     for a in range(pts.shape[1]):
         d = X[:, a][:, None] - Y[:, a][None, :]
         r2 = r2 + d * d
+    if prob.kind in (KIND_MD_VIRUS, KIND_MD_CUBE):
+        A = rbf_phi(prob.rbf_kernel, np.sqrt(r2) * (1.0 / prob.radius))
+        lo, hi = max(r0, c0), min(r0 + nr, c0 + nc)
+        if lo < hi:
+            i = np.arange(lo, hi)
+            A[i - r0, i - c0] += prob.add_diag if prob.add_diag > 0.0 else float(pts.shape[0])
+        return A
     if prob.kind in (KIND_ED_SIN_2D, KIND_ED_SIN_3D):
         r = np.sqrt(r2)
         diag = prob.add_diag if prob.add_diag > 0.0 else float(pts.shape[0])

@@ -35,7 +35,7 @@ int main(void) {
     printf("band %d\n", hicma_tlr_band_autotune(G, NT, 270, 0));
     printf("q %lu\n", hicma_tlr_op_counts('q', 2700, 150, 0, 0));
     printf("o %lu\n", hicma_tlr_op_counts('o', 2700, 75, 150, 2));
-    prob.kind = 7;   /* an RBF mesh problem: not built */
+    prob.kind = 9;   /* no such problem kind */
     printf("err %d\n", hicma_tlr_points(&prob, N, pts));
     printf("msg %s\n", hicma_tlr_last_error());
     return 0;

@@ -27,11 +27,19 @@ def test_usage_lists_problem_kinds(cli):
     assert "--wavek" in r.stderr and "--adddiag" in r.stderr
 
 
-@pytest.mark.parametrize("kind", ["6", "7", "-1"])
+@pytest.mark.parametrize("kind", ["8", "-1"])
 def test_unsupported_kind_is_rejected_before_gpu_use(cli, kind):
     r = run(cli, "-N", "2700", "-t", "270", "-D", kind)
     assert r.returncode == 1
     assert "kind_of_problem" in r.stderr
+
+
+@pytest.mark.parametrize("args,msg", [(["-D", "6", "-R", "0.5"], "mesh file"), (["-D", "7"], "radius"),
+                                      (["-D", "6", "-M", "m.xyz"], "radius")])
+def test_mesh_kind_arguments_checked_before_gpu_use(cli, args, msg):
+    r = run(cli, "-N", "2700", "-t", "270", *args)
+    assert r.returncode == 1
+    assert msg in r.stderr
 
 
 def test_sizes_are_required(cli):
@@ -48,10 +56,10 @@ def test_n_must_be_a_multiple_of_nb(cli):
 
 def test_reference_option_spellings_parse(cli):
     """The reference driver's long options (hicma_parsec/hicma_parsec.c:89-161),
-    including the RBF mesh flags of the problems that are not built, parse; the
-    run then stops at the unsupported kind before any GPU use."""
+    including the RBF mesh flags, parse; the run then stops at a kind that does
+    not exist (8) before any GPU use."""
     r = run(cli, "--N", "2700", "--NB", "270", "--fixedacc", "1e-8", "--maxrank", "130", "--wavek", "25",
             "--adddiag", "3000", "--grid-rows", "1", "--grid-cols", "1", "--rbf_kernel", "0", "--numobj", "1",
-            "--mesh_file", "x", "--order", "1", "--radius", "0.5", "--density", "0.1", "--kind_of_problem", "7")
+            "--mesh_file", "x", "--order", "1", "--radius", "0.5", "--density", "0.1", "--kind_of_problem", "8")
     assert r.returncode == 1
     assert "kind_of_problem" in r.stderr and "unrecognized" not in r.stderr

@@ -90,15 +90,17 @@ def test_argument_errors_without_gpu(lib):
     assert lib.hicma_tlr_k_wait_probe(1, 1, 65, None, None) == tlr.ERR_ARG
 
 
-@pytest.mark.parametrize("kind", [0, 6, 7])
-def test_kinds_without_points_are_argument_errors(lib, kind):
+@pytest.mark.parametrize("kind,radius", [(0, 0.0), (6, 0.5), (7, 0.0), (8, 0.5)])
+def test_kinds_without_points_are_argument_errors(lib, kind, radius):
     """randtlr (-D 0) has no points (its bases are built on the device by the
-    generator); the RBF mesh problems (-D 6, 7) are not built.  The C library
-    answers hicma_tlr_points with an argument error for all three."""
+    generator); md-3d-virus (-D 6) takes its points from a mesh file
+    (hicma_tlr_points_mesh); md-3d-cube (-D 7) needs a positive RBF radius;
+    kind 8 does not exist.  The C library answers hicma_tlr_points with an
+    argument error for each."""
     import ctypes as C
     from hicma_parsec_b200 import tlr
     buf = np.zeros(30)
-    prob = tlr.CProblem(kind, 0.1, 0.5, 0.1, 1.0, 0, 50.0, 0.0)
+    prob = tlr.CProblem(kind, 0.1, 0.5, 0.1, 1.0, 0, 50.0, 0.0, 0, radius, 1, 1, -1.0)
     assert lib.hicma_tlr_points(C.byref(prob), 10, buf.ctypes.data_as(C.c_void_p)) == tlr.ERR_ARG
 
 
