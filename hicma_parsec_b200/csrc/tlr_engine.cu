@@ -1294,22 +1294,37 @@ int hicma_tlr_points_mesh(const hicma_tlr_problem *prob, const char *mesh_file, 
     ARG_CHECK(prob && mesh_file && points && N > 0, "hicma_tlr_points_mesh");
     ARG_CHECK(prob->kind == HICMA_TLR_KIND_MD_VIRUS, "hicma_tlr_points_mesh: kind must be md-3d-virus (6)");
     TRY(rbf_args(prob));
-    FILE *f = std::fopen(mesh_file, "r");
+    FILE *f = std::fopen(mesh_file, "rb");
     ARG_CHECK(f, "cannot open the mesh file");
+    std::string text;
+    char buf[1 << 16];
+    for (size_t got; (got = std::fread(buf, 1, sizeof buf, f)) > 0;) text.append(buf, got);
+    std::fclose(f);
+    // whitespace-separated numbers, '#' to the end of its line a comment
     std::vector<double> mesh;
-    char line[4096];
-    while (std::fgets(line, sizeof line, f)) {
-        if (char *h = std::strchr(line, '#')) *h = '\0';
-        char *q = line;
+    bool bad = false;
+    for (size_t pos = 0; pos < text.size() && !bad;) {
+        size_t end = text.find('\n', pos);
+        if (end == std::string::npos) end = text.size();
+        std::string line = text.substr(pos, end - pos);
+        pos = end + 1;
+        const size_t h = line.find('#');
+        if (h != std::string::npos) line.resize(h);
+        const char *q = line.c_str();
         for (;;) {
             char *e = nullptr;
             const double v = std::strtod(q, &e);
-            if (e == q) break;
+            if (e == q) {
+                while (*q == ' ' || *q == '\t' || *q == '\r' || *q == '\v' || *q == '\f') ++q;
+                bad = *q != '\0';   // something that is not a number
+                break;
+            }
+            if (!std::isfinite(v)) { bad = true; break; }
             mesh.push_back(v);
             q = e;
         }
     }
-    std::fclose(f);
+    ARG_CHECK(!bad, "mesh file: a token that is not a finite number");
     ARG_CHECK(!mesh.empty() && mesh.size() % 3 == 0, "mesh file: expected x y z triples");
     const size_t M = mesh.size() / 3;
     const int nobj = prob->numobj > 0 ? prob->numobj : 1;

@@ -181,7 +181,10 @@ def read_mesh(path: str) -> np.ndarray:
         for line in f:
             line = line.split("#", 1)[0]
             for tok in line.split():
-                vals.append(float(tok))
+                v = float(tok)
+                if not math.isfinite(v):
+                    raise ValueError("mesh file: a token that is not a finite number")
+                vals.append(v)
     if not vals or len(vals) % 3:
         raise ValueError("mesh file: expected x y z triples")
     return np.array(vals, dtype=np.float64).reshape(-1, 3)

@@ -89,6 +89,27 @@ def test_mesh_argument_errors(tlr, tmp_path):
     assert tlr.points_mesh(tlr.Problem(**ok), path, 100).shape == (3, 100)
 
 
+def test_mesh_file_format(tlr, tmp_path):
+    """The reader takes x y z triples in any line layout (here every node on
+    one line of about 20 KB, with comments and CRLF endings) and refuses
+    tokens that are not finite numbers."""
+    mesh = fib_sphere(500)
+    one = tmp_path / "one_line.xyz"
+    one.write_text("# header\r\n" + " ".join(repr(float(v)) for v in mesh.ravel()) + "  # tail\r\n")
+    prob = tlr.Problem(kind=tlr.KIND_MD_VIRUS, radius=0.5, numobj=2, density=0.3)
+    P = tlr.points_mesh(prob, str(one), 1000)
+    Q = O.virus_points(O.read_mesh(str(one)), 1000, O.Problem(kind=O.KIND_MD_VIRUS, radius=0.5, numobj=2,
+                                                                density=0.3))
+    assert np.array_equal(P.T, Q)
+    for bad in ("0 0 0\n1 abc 2\n", "0 0 0\n1 nan 2\n", "0 0 0\ninf 1 2\n"):
+        f = tmp_path / "bad.xyz"
+        f.write_text(bad)
+        with pytest.raises(tlr.TLRError):
+            tlr.points_mesh(prob, str(f), 2)
+        with pytest.raises(ValueError):
+            O.read_mesh(str(f))
+
+
 def test_rbf_functions():
     s = np.array([0.0, 0.25, 0.5, 1.0, 2.0])
     e = np.exp(-s)
