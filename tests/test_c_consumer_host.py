@@ -1,6 +1,7 @@
 """The C ABI used from C, the reference's own language: a small program is
 compiled with gcc against include/hicma_tlr.h, linked with the library, and
-calls the entry points that need no GPU (point generation, rank statistics,
+calls the entry points that need no GPU (point generation of a statistics
+problem and of the md-3d-cube mesh problem, rank statistics,
 band auto-tuning, the op-count model, argument errors); its output is compared
 with the CPU oracle.  This is the shape of the binding a maintainer adds to
 the reference's driver."""
@@ -35,6 +36,12 @@ int main(void) {
     printf("band %d\n", hicma_tlr_band_autotune(G, NT, 270, 0));
     printf("q %lu\n", hicma_tlr_op_counts('q', 2700, 150, 0, 0));
     printf("o %lu\n", hicma_tlr_op_counts('o', 2700, 75, 150, 2));
+    /* md-3d-cube nodes (an RBF mesh problem), C99 designated initializers */
+    hicma_tlr_problem cube = {.kind = HICMA_TLR_KIND_MD_CUBE, .rbf_kernel = HICMA_TLR_RBF_WENDLAND,
+                              .radius = 0.3, .numobj = 1, .order = 1};
+    double cpts[3 * 27];
+    if (hicma_tlr_points(&cube, 27, cpts) != 0) return 3;
+    for (int i = 0; i < 3 * 27; ++i) printf("c %.17g\n", cpts[i]);
     prob.kind = 9;   /* no such problem kind */
     printf("err %d\n", hicma_tlr_points(&prob, N, pts));
     printf("msg %s\n", hicma_tlr_last_error());
@@ -60,7 +67,9 @@ def test_c_program_against_oracle(tmp_path):
     for n in range(6):
         for m in range(n + 1, 6):
             G[n * 6 + m] = (7 * m + 3 * n) % 40
-    kv = {l.split()[0]: l.split()[1:] for l in out if not l.startswith("p ")}
+    cube = np.array([float(l.split()[1]) for l in out if l.startswith("c ")]).reshape(3, 27)
+    np.testing.assert_array_equal(cube.T, O.cube_points(27, 1))
+    kv = {l.split()[0]: l.split()[1:] for l in out if not l.startswith(("p ", "c "))}
     mn, mx, av = O.rank_stat(G, 6, 1)
     assert (int(kv["stat"][0]), int(kv["stat"][1])) == (mn, mx) and float(kv["stat"][2]) == pytest.approx(av)
     assert int(kv["band"][0]) == O.band_autotune(G, 6, 270)
