@@ -22,9 +22,12 @@ def run(cli, *args):
 def test_usage_lists_problem_kinds(cli):
     r = run(cli, "-h")
     assert r.returncode == 0
-    for name in ("randtlr", "ed-2d-sin", "st-2d-sqexp", "st-3d-sqexp", "st-3d-exp", "ed-3d-sin"):
+    for name in ("randtlr", "ed-2d-sin", "st-2d-sqexp", "st-3d-sqexp", "st-3d-exp", "ed-3d-sin", "md-3d-virus",
+                 "md-3d-cube"):
         assert name in r.stderr
     assert "--wavek" in r.stderr and "--adddiag" in r.stderr
+    for flag in ("--mesh_file", "--numobj", "--rbf_kernel", "--radius", "--order", "--density"):
+        assert flag in r.stderr
 
 
 @pytest.mark.parametrize("kind", ["8", "-1"])
