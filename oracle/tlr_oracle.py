@@ -31,6 +31,12 @@ and restates from their published mathematics the absent third-party pieces:
   exponential / exponential covariance kernels (call sites
   ``testing_dpotrf.c:336-358``) and the electrodynamics ``sin(k r) / r``
   kernels in 2D and 3D (call sites ``testing_dpotrf.c:325-334,359-365``);
+* the mesh-deformation problems (``-D 6`` md-3d-virus, ``-D 7`` md-3d-cube,
+  ``testing_dpotrf.c:366-381``): the nine radial basis functions of ``-B``
+  (``hicma_parsec.c:80``, :func:`rbf_phi`) of r / radius plus ``add_diag`` on
+  the diagonal; STARS-H's point generators for them are absent, so the node
+  rules (:func:`cube_points`, :func:`virus_points`) are this restatement's own,
+  shared with the library's host code;
 * STARS-H ``starsh_dense_dlrrsdd`` rank rule: the smallest rank whose
   discarded singular values have Frobenius norm <= tol * (Frobenius norm of the
   sampled spectrum); a tile is rejected (rank -1, ``STARSH_gen.jdf:169-171``)
