@@ -218,6 +218,23 @@ def max_over_ranks(x: float, device=None) -> float:
     return float(t.item())
 
 
+def class_rates(prof: dict, fp64_peak: float, hbm_peak: float) -> dict:
+    """Achieved rates of every profiled kernel class: algorithmic TFLOP/s and
+    its fraction of the FP64 peak, algorithmic GB/s and its fraction of the HBM
+    peak (classes with no recorded time are left out; a class whose work is
+    counted on the device reports what was counted)."""
+    out = {}
+    for name, r in prof.items():
+        secs = float(r.get("seconds", 0.0) or 0.0)
+        if secs <= 0.0:
+            continue
+        tf = float(r.get("flops", 0.0) or 0.0) / secs / 1e12
+        gb = float(r.get("bytes", 0.0) or 0.0) / secs / 1e9
+        out[name] = {"tflops": tf, "fp64_frac": tf / fp64_peak if fp64_peak > 0 else None,
+                     "gbs": gb, "hbm_frac": gb / hbm_peak if hbm_peak > 0 else None}
+    return out
+
+
 def load_traffic_ratios() -> dict:
     """Measured DRAM bytes per algorithmic unit (flop, or byte for copy-like
     kernels) of each kernel, from an ncu capture summarised under profiles/:
@@ -584,7 +601,9 @@ def run_ours(args, cfg):
                             "device_idle_between_panels": st[12]},
                 "cholqr_null_pivots": int(st[11]), "cholqr_repeated_passes": int(st[14]),
                 "jacobi_sweeps_total": st[8],
-                "kernel_classes": prof, "gpu_launches": launches * args.steps,
+                "kernel_classes": prof,
+                "kernel_class_rates": class_rates(prof, fp64_peak, meas.get("hbm_gbs", 6650.0)),
+                "gpu_launches": launches * args.steps,
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk, "accuracy": accuracy,
                 "mixed_precision": mixed, "serving": serving_line}
         print(json.dumps(line), flush=True)

@@ -7,6 +7,7 @@ import sys
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
+import pytest  # noqa: E402
 import bench  # noqa: E402
 
 
@@ -30,3 +31,17 @@ def test_clock_summary_reasons_and_missing_fields():
     assert bench.ClockSampler.parse([])["reasons"] == ["no samples"]
     only_na = bench.ClockSampler.parse([row("[N/A]", mx="[N/A]")])
     assert only_na["sm_mhz"] is None and only_na["sm_max_mhz"] is None
+
+
+def test_class_rates():
+    """Per-class achieved rates of the bench line: algorithmic flops and bytes
+    over the class's event time, as fractions of the FP64 and HBM peaks;
+    classes with no recorded time are left out."""
+    prof = {"rcholqr": {"launches": 515, "seconds": 0.5, "flops": 2.0e12, "bytes": 5.0e11},
+            "copy": {"launches": 784, "seconds": 0.1, "flops": 0.0, "bytes": 1.5e11},
+            "cov": {"launches": 0, "seconds": 0.0, "flops": 0.0, "bytes": 0.0}}
+    r = bench.class_rates(prof, 40.0, 6000.0)
+    assert set(r) == {"rcholqr", "copy"}
+    assert r["rcholqr"]["tflops"] == pytest.approx(4.0) and r["rcholqr"]["fp64_frac"] == pytest.approx(0.1)
+    assert r["copy"]["gbs"] == pytest.approx(1500.0) and r["copy"]["hbm_frac"] == pytest.approx(0.25)
+    assert r["copy"]["tflops"] == 0.0
