@@ -75,7 +75,7 @@ static void usage(void) {
             " -M --mesh_file    mesh of -D 6 (x y z per node)   -K --numobj  copies of it (default 1)\n"
             " -B --rbf_kernel   0 Gaussian 1 Expon 2 InvQUAD 3 InvMQUAD 4 Maternc1 5 Maternc2 6 TPS 7 CTPS 8 Wendland\n"
             " -R --radius       RBF shape radius (-D 6, 7; required)\n"
-            " -O --order        0 none, 1 Morton (default 1)   -S --density  packing of -D 6's copies (-1 random)\n"
+            " -O --order        0 none (default), 1 Morton   -S --density  packing of -D 6's copies (-1 random)\n"
             " -Z --band         band size (default 1)\n"
             " -E --auto-band    auto-tune band size (default 1)\n"
             " -Y --lookahead    lookahead (-1: band size)\n"
@@ -92,7 +92,7 @@ int main(int argc, char **argv) {
     int auto_band = 1, lookahead = -1, send_full_tile = 0, two_flow = 0, HNB = 300, check = 0, verbose = 0;
     int device = 0, precision = HICMA_TLR_PREC_FP64, print_rank = 0;
     double tol = 1e-8, noise = 0.1, beta = 0.1, sigma = 1.0, ws_gib = 0.0, wave_k = 50.0, add_diag = 0.0;
-    int rbf_kernel = 0, numobj = 1, order = 1;
+    int rbf_kernel = 0, numobj = 1, order = 0;   /* the reference's zero-initialised iparam (testing_dpotrf.c:265) */
     double radius = 0.0, density = -1.0;
     const char *mesh_file = NULL;
     unsigned long long seed = 0;
