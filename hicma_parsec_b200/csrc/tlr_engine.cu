@@ -2167,6 +2167,23 @@ int hicma_tlr_rank_history(hicma_tlr_desc *A, int *initial, int *minimum, int *m
     return 0;
 }
 
+int hicma_tlr_dpotrf_L_rank(hicma_tlr_ctx *c, int uplo, hicma_tlr_desc *A, int *Ar, int *Rank, double acc,
+                            int fixed_rank, int maxrank, int *lookahead, int band_size, int hmb, int compmaxrank,
+                            int send_full_tile, int *two_flow, unsigned long *tileopcounters,
+                            unsigned long *opcounters, double *critical_path_time, int verbose) {
+    const int info = hicma_tlr_dpotrf_L(c, uplo, A, Ar, acc, fixed_rank, maxrank, lookahead, band_size, hmb,
+                                        compmaxrank, send_full_tile, two_flow, tileopcounters, opcounters,
+                                        critical_path_time, verbose);
+    if (info < 0 || !Rank) return info;
+    // the dcRank record: 4 ints per tile (initial, minimum, maximum, final) at (n*NT + m)*4
+    const size_t n2 = (size_t)A->NT * A->NT;
+    std::vector<int> h(4 * n2);
+    TRY(hicma_tlr_rank_history(A, h.data(), h.data() + n2, h.data() + 2 * n2, h.data() + 3 * n2));
+    for (size_t t = 0; t < n2; ++t)
+        for (int q = 0; q < 4; ++q) Rank[4 * t + q] = h[q * n2 + t];
+    return info;
+}
+
 int hicma_tlr_rank_stat(const int *G, int NT, int band_size, int *minrk, int *maxrk, double *avgrk) {
     ARG_CHECK(G && NT > 0 && band_size >= 1, "rank_stat");
     int mn = 2147483647, mx = 0;

@@ -117,6 +117,7 @@ def load_library(path: str | None = None):
         "hicma_tlr_band_autotune": (i, [vp, i, i, i]),
         "hicma_tlr_band_regenerate": (i, [vp, i, vp, C.POINTER(CProblem), i]),
         "hicma_tlr_dpotrf_L": (i, [vp, i, vp, vp, d, i, i, ip, i, i, i, i, ip, vp, vp, vp, i]),
+        "hicma_tlr_dpotrf_L_rank": (i, [vp, i, vp, vp, vp, d, i, i, ip, i, i, i, i, ip, vp, vp, vp, i]),
         "hicma_tlr_set_precision": (i, [vp, i]),
         "hicma_tlr_dpotrf_L_start": (i, [vp, vp, d, i, i]),
         "hicma_tlr_dpotrf_L_wait": (i, [vp, vp, vp]),

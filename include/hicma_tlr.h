@@ -216,6 +216,20 @@ int hicma_tlr_dpotrf_L(hicma_tlr_ctx *ctx, int uplo, hicma_tlr_desc *A, int *Ar,
                        int *two_flow, unsigned long *tileopcounters,
                        unsigned long *opcounters, double *critical_path_time, int verbose);
 
+/* HiCMA_dpotrf_L with the reference's full parameter list, the Rank
+ * descriptor included (hicma_parsec/hicma_parsec.h:38-56): the same call as
+ * hicma_tlr_dpotrf_L, then, when Rank (host, 4*NT*NT ints) is not NULL and the
+ * factorization ran (a return value >= 0), the dcRank record of every tile
+ * (hicma_parsec/testing_dpotrf.c:619-635, filled at
+ * HiCMA_dpotrf_L_2flow.jdf:353-361,683-691,1101-1106): tile (m, n) at
+ * [(n*NT + m)*4 + q], q = 0 initial, 1 minimum, 2 maximum, 3 final rank; -1 for
+ * band and upper tiles (hicma_tlr_rank_history in one array). */
+int hicma_tlr_dpotrf_L_rank(hicma_tlr_ctx *ctx, int uplo, hicma_tlr_desc *A, int *Ar, int *Rank,
+                            double acc, int fixed_rank, int maxrank, int *lookahead,
+                            int band_size, int hmb, int compmaxrank, int send_full_tile,
+                            int *two_flow, unsigned long *tileopcounters,
+                            unsigned long *opcounters, double *critical_path_time, int verbose);
+
 /* Precision policy for later hicma_tlr_dpotrf_L calls on this context. */
 int hicma_tlr_set_precision(hicma_tlr_ctx *ctx, int precision);
 

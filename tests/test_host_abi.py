@@ -85,6 +85,12 @@ def test_argument_errors_without_gpu(lib):
     assert lib.hicma_tlr_autotune(None, 270, 130, 3, t.ctypes.data_as(ctypes.c_void_p), None) == tlr.ERR_ARG
     assert lib.hicma_tlr_tuning_get(None, t.ctypes.data_as(ctypes.c_void_p)) == tlr.ERR_ARG
     assert lib.hicma_tlr_tuning_set(None, t.ctypes.data_as(ctypes.c_void_p)) == tlr.ERR_ARG
+    # the reference-signature factorization (with the Rank record) refuses a
+    # null context before any device work and leaves Rank untouched
+    rank = np.full(16, 7, np.int32)
+    assert lib.hicma_tlr_dpotrf_L_rank(None, tlr.LOWER, None, None, rank.ctypes.data_as(ctypes.c_void_p), 1e-8, 0,
+                                       130, None, 1, 0, 130, 0, None, None, None, None, 0) == tlr.ERR_ARG
+    assert np.all(rank == 7)
     # the wait probe refuses out-of-range limits before touching the device
     assert lib.hicma_tlr_k_wait_probe(0, 1, 1, None, None) == tlr.ERR_ARG
     assert lib.hicma_tlr_k_wait_probe(1, 1, 65, None, None) == tlr.ERR_ARG

@@ -43,3 +43,34 @@ def test_rank_history_and_path_ops_match_oracle(ctx):
         assert 0 < st[10] < st[1]
     finally:
         A.close()
+
+
+def test_reference_signature_fills_rank_record(ctx):
+    """hicma_tlr_dpotrf_L_rank takes HiCMA_dpotrf_L's full parameter list, the
+    Rank descriptor included (hicma_parsec.h:38-56): its 4-int record per tile
+    (initial, minimum, maximum, final at [(n*NT + m)*4 + q]) equals the rank
+    history of the same factorization, and Ar its final rank map."""
+    import ctypes as C
+    from hicma_parsec_b200 import tlr
+    nt = N // NB
+    A = tlr.TLRMatrix(ctx, N, NB, MAXRANK, 1)
+    try:
+        assert A.generate(tlr.Problem(kind=2, noise=0.1), TOL, MAXRANK) == 0
+        la, two = C.c_int(-1), C.c_int(0)
+        cpt = np.zeros(6, dtype=np.float64)
+        Ar = np.zeros(nt * nt, dtype=np.int32)
+        rank = np.full(4 * nt * nt, -7, dtype=np.int32)
+        info = A.lib.hicma_tlr_dpotrf_L_rank(ctx.h, tlr.LOWER, A.h, Ar.ctypes.data_as(C.c_void_p),
+                                             rank.ctypes.data_as(C.c_void_p), TOL, 0, MAXRANK, C.byref(la), 1,
+                                             NB, MAXRANK, 0, C.byref(two), None, None,
+                                             cpt.ctypes.data_as(C.c_void_p), 0)
+        assert info == 0, tlr.last_error()
+        h = A.rank_history()                     # NT x NT arrays indexed [m, n]
+        R = rank.reshape(nt, nt, 4)              # [n, m, q]
+        for q, key in enumerate(("initial", "minimum", "maximum", "final")):
+            assert np.array_equal(R[:, :, q].T, h[key]), key
+        low = h["initial"] >= 0
+        assert low.any()
+        assert np.array_equal(h["final"][low], Ar.reshape(nt, nt).T[low])
+    finally:
+        A.close()
